@@ -1,0 +1,171 @@
+"""Writes the golden fixtures ``tests/golden/*.npz`` by running blochparty's own core engine in float64.
+
+Run once, in a container where the reference source tree is present:
+
+    PYTHONPATH=/root/reference/src python tests/golden/make_golden.py
+
+Each case's inputs are built here with this package's builders and phantoms (seeded), converted to the
+reference's ``Phantom`` / ``Sequence`` classes, and simulated by ``blochparty.simulate(..., engine="core")``
+(``engines/core.py:487``) in float64. The fixture stores the inputs, the reference's signal and final
+magnetization, and, for the gradient cases, the reference's autograd gradients of a fixed linear loss
+(the loss of blochparty ``tests/helpers.py:77-92``: seeded float64 weights on signal and m) with respect to
+every input tensor. The tests never import the reference: they read these files.
+"""
+
+from __future__ import annotations
+
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+import blochparty as bp  # noqa: E402  (the reference, from PYTHONPATH)
+
+from blochparty_b200 import phantoms, sequences  # noqa: E402
+
+F64 = torch.float64
+
+
+def ref_objects(ph, seq):
+    """The reference's Phantom and Sequence with the same tensors."""
+    rph = bp.Phantom(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, b1=ph.b1)
+    rseq = bp.Sequence(seq.dt, seq.rf, seq.grad, seq.adc_phase, list(seq.is_rf), list(seq.adc), list(seq.spoil),
+                       {}, seq.b0_offset)
+    return rph, rseq
+
+
+def weights_like(sig, m, seed=1):
+    g = torch.Generator().manual_seed(seed)
+    return (torch.randn(sig.shape, generator=g, dtype=F64), torch.randn(sig.shape, generator=g, dtype=F64),
+            torch.randn(m.shape, generator=g, dtype=F64))
+
+
+def pack(name, ph, seq, coils, m_init, sig, m, grads=None, weights=None):
+    out = dict(
+        pos=ph.pos.numpy(), pd=ph.pd.numpy(), t1=ph.t1.numpy(), t2=ph.t2.numpy(), db0=ph.db0.numpy(),
+        b1=(ph.b1.numpy() if ph.b1 is not None else np.zeros(0)),
+        coils_re=coils.real.numpy(), coils_im=coils.imag.numpy(),
+        dt=seq.dt.numpy(), rf=seq.rf.numpy(), grad=seq.grad.numpy(), adc_phase=seq.adc_phase.numpy(),
+        b0_offset=(seq.b0_offset.numpy() if seq.b0_offset is not None else np.zeros(0)),
+        is_rf=np.array(seq.is_rf, bool), adc=np.array(seq.adc, bool), spoil=np.array(seq.spoil, bool),
+        m_init=(m_init.numpy() if m_init is not None else np.zeros(0)),
+        sig_re=sig.real.numpy(), sig_im=sig.imag.numpy(), m=m.numpy(),
+    )
+    if grads is not None:
+        for k, v in grads.items():
+            if v is None:
+                continue
+            if v.is_complex():
+                out[f"grad_{k}_re"], out[f"grad_{k}_im"] = v.real.numpy(), v.imag.numpy()
+            else:
+                out[f"grad_{k}"] = v.numpy()
+        out["w_re"], out["w_im"], out["w_m"] = (w.numpy() for w in weights)
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, {k: v.shape for k, v in out.items() if k.startswith(("sig", "m"))})
+
+
+def run(name, ph, seq, coils, m_init=None, with_grads=False):
+    rph, rseq = ref_objects(ph, seq)
+    r = bp.simulate(rph, rseq, coils, m_init=m_init, engine="core")
+    sig, m = r.signal.detach(), r.m.detach()
+    grads = weights = None
+    if with_grads:
+        weights = weights_like(sig, m)
+        leaves = {}
+
+        def leaf(k, t):
+            t = t.detach().clone().requires_grad_()
+            leaves[k] = t
+            return t
+
+        gph = bp.Phantom(leaf("pos", ph.pos), leaf("pd", ph.pd), leaf("t1", ph.t1), leaf("t2", ph.t2),
+                         leaf("db0", ph.db0), b1=None if ph.b1 is None else leaf("b1", ph.b1))
+        gseq = bp.Sequence(leaf("dt", seq.dt), leaf("rf", seq.rf), leaf("grad", seq.grad),
+                           leaf("adc_phase", seq.adc_phase), list(seq.is_rf), list(seq.adc), list(seq.spoil), {},
+                           None if seq.b0_offset is None else leaf("b0_offset", seq.b0_offset))
+        gc = leaf("coils", coils)
+        gm = None if m_init is None else leaf("m_init", m_init)
+        rr = bp.simulate(gph, gseq, gc, m_init=gm, engine="core")
+        wr, wi, wm = weights
+        loss = (rr.signal.real * wr).sum() + (rr.signal.imag * wi).sum() + (rr.m * wm).sum()
+        gs = torch.autograd.grad(loss, list(leaves.values()), allow_unused=True)
+        grads = dict(zip(leaves, gs))
+    pack(name, ph, seq, coils, m_init, sig, m, grads, weights)
+
+
+def rand_case(seed, n=6, n_coils=3):
+    g = torch.Generator().manual_seed(seed)
+    rnd = lambda *s: torch.rand(*s, generator=g, dtype=F64)
+    ph = bp.Phantom(pos=(rnd(n, 3) - 0.5) * 0.2, pd=0.5 + rnd(n), t1=0.2 + rnd(n), t2=0.02 + 0.1 * rnd(n),
+                    db0=(rnd(n) - 0.5) * 200, b1=0.8 + 0.4 * rnd(n))
+    b = sequences.SequenceBuilder()
+    for _ in range(4):
+        b.rf_waveform(((rnd(40, 2) - 0.5) * 2000).numpy(), 10e-6, grad=((rnd(3) - 0.5) * 2000).numpy())
+        b.delay(float(rnd(())) * 3e-3, grad=((rnd(3) - 0.5) * 4000).numpy())
+        b.rf(100e-6, flip_deg=180 * float(rnd(())), phase=2 * math.pi * float(rnd(())))
+        b.readout(8, 20e-6, grad=((rnd(3) - 0.5) * 3000).numpy(), phase=float(rnd(())) * 6.0)
+        b.delay(float(rnd(())) * 3e-3, grad=((rnd(3) - 0.5) * 4000).numpy())
+    b.spoil()
+    b.rf(200e-6, flip_deg=90.0, n_steps=10)
+    b.readout(16, 10e-6, grad=(800.0, -300.0, 150.0), phase=0.7)
+    seq = b.build()
+    seq.b0_offset = (rnd(len(seq)) - 0.5) * 40
+    coils = torch.complex(rnd(n, n_coils) - 0.5, rnd(n, n_coils) - 0.5)
+    return ph, seq, coils
+
+
+def busy_case(seed=3, n=40, n_coils=4):
+    """RF of varying phase, readouts split across runs, a spoiled run without ADC, an ADC right after RF, m_init."""
+    g = torch.Generator().manual_seed(seed)
+    rnd = lambda *s: torch.rand(*s, generator=g, dtype=F64)
+    ph = bp.Phantom(pos=(rnd(n, 3) - 0.5) * 0.2, pd=0.5 + rnd(n), t1=0.2 + rnd(n), t2=0.02 + 0.1 * rnd(n),
+                    db0=(rnd(n) - 0.5) * 200)
+    b = sequences.SequenceBuilder()
+    for i in range(4):
+        b.rf(100e-6, amplitude=1500.0, phase=1.3 * i)
+        b.delay(0.4e-3, grad=(2000.0, float(rnd(()) - 0.5) * 3000, 0.0))
+        b.readout(8, 20e-6, grad=(-2000.0, 0.0, 400.0), phase=0.2 * i)
+        b.delay(0.2e-3, grad=((rnd(3) - 0.5) * 2000).numpy())
+        b.readout(5, 30e-6, grad=((rnd(3) - 0.5) * 2000).numpy())
+        b.delay(1e-3).spoil()
+    b.rf(50e-6, amplitude=1500.0)
+    b._adc[-1] = True  # a sample at the end of the RF segment itself
+    b.readout(3, 10e-6).delay(2e-3, grad=(1e3, 0.0, 0.0)).spoil()
+    seq = b.build()
+    m_init = torch.stack([(rnd(n) - 0.5) * 0.4, (rnd(n) - 0.5) * 0.4, 0.3 + 0.5 * rnd(n)], -1)
+    coils = torch.complex(rnd(n, n_coils) - 0.5, rnd(n, n_coils) - 0.5)
+    return ph, seq, coils, m_init
+
+
+def main():
+    torch.set_default_dtype(F64)
+    for seed in (0, 1):
+        ph, seq, coils = rand_case(seed)
+        run(f"rand{seed}", ph, seq, coils)
+    ph, seq, coils, m_init = busy_case()
+    run("busy", ph, seq, coils, m_init)
+    # 2D GRE, 16 x 16 ellipses, 4 coils, RF spoiling, 5 dummies, radial B1, a b0_offset ramp
+    p = phantoms.ellipse_phantom_2d(16, 0.25, seed=0)
+    p.b1 = phantoms.radial_b1(p.pos)
+    seq = sequences.gre((16, 16), 0.25, flip_deg=30.0, tr=6e-3, te=3e-3, n_dummy=5, dwell=20e-6)
+    seq.b0_offset = torch.linspace(-5.0, 5.0, len(seq), dtype=F64)
+    run("gre16", p, seq, phantoms.birdcage_sensitivities(p.pos, 4))
+    # 3D GRE, 4^3 ellipsoids x 2 sub-voxel spins, a 20-step sinc slab pulse, 2 echoes
+    p = phantoms.ellipsoid_phantom_3d(4, 0.25, spins_per_voxel=2, b0_max=50.0, sigma_vox=1.0)
+    seq = sequences.gre((4, 4, 8), 0.25, flip_deg=20.0, tr=6e-3, te=2.5e-3, dwell=20e-6, rf="sinc",
+                        rf_duration=1e-3, rf_steps=20, slab_thickness=0.2, n_echoes=2, echo_spacing=0.4e-3)
+    run("sinc3d", p, seq, phantoms.birdcage_sensitivities(p.pos, 3))
+    # gradients: small cases with every input differentiated
+    ph, seq, coils = rand_case(7, n=5, n_coils=2)
+    run("grad_rand", ph, seq, coils, with_grads=True)
+    ph, seq, coils, m_init = busy_case(seed=8, n=6, n_coils=2)
+    run("grad_busy", ph, seq, coils, m_init, with_grads=True)
+
+
+if __name__ == "__main__":
+    main()
