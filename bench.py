@@ -1,0 +1,320 @@
+"""Benchmark: isochromat-steps/s (spins x segments / s, blochparty's spin-segments/s, benchmarks/bench.py:64)
+of the forward simulation on the 3D GRE 64^3 workload (1,048,576 spins x 1,097,728 segments, 8 coils; see
+``blochparty_b200/workloads.py``) on N GPUs of one node, one process per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--readout fp32|bf16x3]
+
+Prints ONE JSON line on rank 0. ``value``: the whole job's isochromat-steps/s with the inputs resident in HBM,
+timed with CUDA events (max over ranks). ``e2e``: the same metric through the public ``simulate`` call with host
+inputs, packing and host<->device copies inside the timed region (wall clock around a synchronising call).
+Multi-GPU: weak scaling; every rank simulates its own 1,048,576-spin phantom (the same workload with its own
+sub-voxel offsets), and the float64 raw signal is summed onto rank 0 with one NCCL reduce per step (the spin
+sum is the path's only exchange). ``--impl reference``: the reference algorithm on the host CPU (the float64
+oracle restating blochparty's core engine), on a bounded sample of the workload; rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "isochromat-steps/s (fwd)"
+UNIT = "isochromat-steps/s"
+WORKLOAD = "gre3d_64: 3D spoiled GRE 64^3, 1,048,576 spins, 8 coils, 200-step sinc slab, TR 8 ms"
+
+# algorithmic FP32 flops per spin and segment of the forward kernel (counted from its formulas in
+# blochparty_b200/csrc/bloch_common.cuh; kept fixed across versions): RF segment, free segment with cached
+# factors, free segment recomputing them, and an ADC sample per coil (complex multiply-add, 8 flops) + 2.
+FLOP_RF, FLOP_FREE, FLOP_FREE_MISS, FLOP_ADC_PER_COIL, FLOP_ADC = 125, 16, 34, 8, 2
+# (the free segment is counted at its plain float32 cost, 16 flops, although the kernel evaluates it in
+# float-float arithmetic; the extra work is precision, not algorithm)
+
+
+def flops_per_spin(flags: np.ndarray, n_coils: int) -> int:
+    rf = (flags & 1) != 0
+    same = (flags & 8) != 0
+    n_rf = int(rf.sum())
+    n_free_cached = int((~rf & same).sum())
+    n_free_miss = int((~rf & ~same).sum())
+    n_adc = int(((flags & 2) != 0).sum())
+    return (FLOP_RF * n_rf + FLOP_FREE * n_free_cached + FLOP_FREE_MISS * n_free_miss
+            + (FLOP_ADC_PER_COIL * n_coils + FLOP_ADC) * n_adc)
+
+
+class Clocks:
+    """nvidia-smi samples (every 200 ms) of the GPU's SM clock and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.rows, self.proc = [], None
+        try:
+            p = torch.cuda.get_device_properties(device)
+            self.sel = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        except Exception:
+            self.sel = str(device)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.sel], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        num = lambda v: float(v) if v.replace(".", "", 1).isdigit() else float("nan")
+        sm = [num(r[0]) for r in self.rows]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[4:8]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": num(self.rows[0][1]), "reasons": reasons,
+                "samples": len(self.rows), "power_w_max": max(num(r[2]) for r in self.rows)}
+
+
+def ffma_peak_tflops(dev) -> float:
+    from blochparty_b200 import _lib
+
+    out = torch.empty(4 * torch.cuda.get_device_properties(dev).multi_processor_count * 256, device=dev)
+    flops = np.zeros(1, dtype=np.int64)
+    lib = _lib.lib()
+    best = 0.0
+    for it in (2000, 2000, 2000):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.check(lib.bp_ffma_peak(out.data_ptr(), it, flops.ctypes.data, _lib.stream_ptr()), "bp_ffma_peak")
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, float(flops[0]) / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def cpu_sample(workload_fn, n_spins=4096, n_tr=32, seed=0):
+    """A bounded sample of the workload for the CPU oracle: ``n_spins`` spins drawn with a seeded generator and
+    the segments of the first ``n_tr`` TRs (TR boundaries at the spoiler-fill segments)."""
+    from oracle import bloch
+
+    ph, seq, coils = workload_fn()
+    g = torch.Generator().manual_seed(seed)
+    idx = torch.randperm(len(ph.pd), generator=g)[:n_spins]
+    end = min(len(seq), n_tr * (len(seq) // seq.meta["n_tr"]))
+    c = bloch.case_from(ph, seq, coils)
+    from dataclasses import replace
+
+    c = replace(c, pos=c.pos[idx], pd=c.pd[idx], t1=c.t1[idx], t2=c.t2[idx], db0=c.db0[idx], coils=c.coils[idx],
+                dt=c.dt[:end], rf=c.rf[:end], grad=c.grad[:end], adc_phase=c.adc_phase[:end],
+                b0_offset=None if c.b0_offset is None else c.b0_offset[:end], is_rf=c.is_rf[:end],
+                adc=c.adc[:end], spoil=c.spoil[:end])
+    return c, f"{n_spins} seeded spins x the first {end} segments ({n_tr} TRs) of {workload_fn.__name__}"
+
+
+def time_cpu(case, reps=1):
+    from oracle import bloch
+
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    best = float("inf")
+    for _ in range(reps):
+        t = time.perf_counter()
+        bloch.simulate(case)
+        best = min(best, time.perf_counter() - t)
+    n, s = case.pd.shape[0], case.dt.shape[0]
+    return n * s / best, threads
+
+
+def run_reference(args, rank):
+    from blochparty_b200 import workloads
+
+    if rank != 0:
+        return
+    case, sample = cpu_sample(workloads.gre3d_64)
+    rates = []
+    for i in range(args.warmup + args.steps):
+        v, cores = time_cpu(case)
+        if i >= args.warmup:
+            rates.append(v)
+    value = statistics.median(rates)
+    n, s = case.pd.shape[0], case.dt.shape[0]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": n * s / value * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": sample, "readout": "float64 CPU"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--readout", default="fp32", choices=("fp32", "bf16x3"))
+    ap.add_argument("--n", type=int, default=64, help="grid size of the 3D GRE (64: the measured workload)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    import blochparty_b200 as bpb
+    from blochparty_b200 import _lib, engine, workloads
+
+    ph, seq, coils = workloads.gre3d_64(args.n) if rank == 0 else _rank_workload(args.n, rank)
+    inp = bpb.api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad,
+                         seq.adc_phase, None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
+    pk = engine.pack(inp, dev)
+    samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
+    windows = engine.plan_windows(pk.flags, samp)
+    wdev = torch.from_numpy(windows).to(dev)
+    state0 = engine.initial_state(inp.pd, None, dev)
+    state = torch.empty_like(state0)
+    raw = torch.zeros(pk.n_adc, 2 * pk.n_coils, dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+    n, S = pk.n, len(seq)
+    kstart = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kend = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+
+    def step(i=None):
+        state.copy_(state0)
+        raw.zero_()
+        if i is not None:
+            kstart[i].record()
+        engine.run_forward(pk, state, wdev, 0, windows.shape[0], raw, status)
+        if i is not None:
+            kend[i].record()
+        sig = engine.finish_signal(pk, raw)
+        if world > 1:
+            dist.reduce(raw, dst=0)
+        return sig
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    _lib.check_status(status, "bp_forward")
+    clocks = Clocks(local)
+    elapsed = 0.0
+    with clocks:
+        for i in range(args.steps):
+            flush.zero_()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record()
+            step(i)
+            t1.record()
+            torch.cuda.synchronize()
+            elapsed += t0.elapsed_time(t1)
+    _lib.check_status(status, "bp_forward")
+    ms = torch.tensor([elapsed / args.steps], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms)
+    kernel_ms = statistics.mean(kstart[i].elapsed_time(kend[i]) for i in range(args.steps))
+    value = world * n * S / (ms * 1e-3)
+
+    # end to end: the public simulate() call with host inputs (packing, copies, kernels, result read-back)
+    e2e_ms = []
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        bpb.simulate(ph, seq, coils)
+        e2e_ms.append((time.perf_counter() - t) * 1e3)
+    e2e = world * n * S / (statistics.median(e2e_ms) * 1e-3) if e2e_ms else None
+    h2d = sum(t.numel() * t.element_size() for t in (pk.spins, pk.sens, pk.segs, pk.seg64, pk.psi, wdev, state0))
+    d2h = pk.n_coils * pk.n_adc * 8 + state.numel() * 4
+
+    if rank != 0:
+        dist.destroy_process_group() if world > 1 else None
+        return
+    peak = ffma_peak_tflops(dev)
+    flops = n * flops_per_spin(pk.flags, pk.n_coils)
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "spins_per_gpu": n, "segments": S, "adc_samples": pk.n_adc,
+                   "coils": pk.n_coils, "readout": args.readout, "l2": "inputs larger than L2 (state, spins, coils, "
+                   "segments ~220 MB per GPU) and a 256 MB L2 flush between timed steps"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU; MEASURED_PEAKS.json has no FP32",
+                     "kernel": "bp_forward_kernel", "kernel_ms": kernel_ms,
+                     "flops_per_launch": flops},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": statistics.median(e2e_ms) if e2e_ms else None},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        case, sample = cpu_sample(workloads.gre3d_64)
+        v, cores = time_cpu(case)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _rank_workload(n, rank):
+    """Rank r's own phantom for weak scaling: the workload with sub-voxel offsets seeded by 1 + r."""
+    from blochparty_b200 import phantoms, workloads
+
+    ph0, seq, coils = workloads.gre3d_64(n)
+    ph = phantoms.ellipsoid_phantom_3d(n, 0.25, n_ellipsoids=10, spins_per_voxel=4, seed=0, subvoxel_seed=1 + rank,
+                                       b0_seed=2, b0_max=100.0, sigma_vox=4.0)
+    return ph, seq, phantoms.birdcage_sensitivities(ph.pos, 8)
+
+
+if __name__ == "__main__":
+    main()

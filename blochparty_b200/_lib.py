@@ -1,0 +1,74 @@
+"""ctypes binding of ``libblochparty_b200.so`` (the C ABI of ``include/blochparty_b200.h``).
+
+The library is built in-tree (``blochparty_b200.build``). There is no fallback: if it cannot be loaded, or no
+CUDA device is present, ``lib()`` raises, and nothing computes the simulation any other way.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_double, c_int, c_int64, c_void_p
+from pathlib import Path
+
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "libblochparty_b200.so"
+
+BP_OK, BP_E_ARG, BP_E_ALIGN, BP_E_LAUNCH, BP_E_SIZE = 0, 1, 2, 3, 4
+BP_MAX_COILS = 32
+BP_SEG_MAX = 512
+ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
+          BP_E_SIZE: "size above the documented maximum"}
+STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",
+               2: "a window record was invalid"}
+
+_P = c_void_p
+# (restype, argtypes) of every exported entry point, as declared in include/blochparty_b200.h
+SIGNATURES = {
+    "bp_plan_windows": (c_int, [_P, c_int64, c_int, c_int, _P, _P, c_int64, _P]),
+    "bp_forward_samp_max": (c_int, [c_int]),
+    "bp_forward": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P]),
+    "bp_signal_finish": (c_int, [_P, _P, c_int, c_int, _P, _P]),
+    "bp_ffma_peak": (c_int, [_P, c_int, _P, _P]),
+}
+
+_lib = None
+
+
+def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
+    """The library with every entry point's signature set (no GPU needed to load it)."""
+    if not path.exists():
+        raise RuntimeError(f"{path.name} is not built: run `python -m blochparty_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(str(path))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    return lib
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = load_library()
+    return _lib
+
+
+def check(code: int, what: str) -> None:
+    if code != BP_OK:
+        raise RuntimeError(f"{what}: {ERRORS.get(code, f'error {code}')}")
+
+
+def check_status(status: torch.Tensor, what: str) -> None:
+    """Raise if a kernel OR-ed an error bit into the status word (call after synchronising)."""
+    v = int(status.item())
+    if v:
+        bits = [msg for bit, msg in STATUS_BITS.items() if v & bit]
+        raise RuntimeError(f"{what}: device status {v:#x}: {'; '.join(bits) or 'unknown'}")
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def stream_ptr() -> int:
+    return torch.cuda.current_stream().cuda_stream

@@ -1,0 +1,131 @@
+"""``simulate``: the drop-in entry point of the b200 engine.
+
+Keeps the signature and semantics of blochparty's ``simulate`` (``engines/__init__.py:60-144``) as its GPU
+engines implement them (``engines/gpu/__init__.py:54-96``, ``engines/gpu/cuda/__init__.py:93-132``):
+
+* inputs of any dtype are cast; the simulation computes in float32 (float64 where stated);
+* the result comes back on the CPU: ``signal`` (C, n_adc) complex64, ``m`` (N, 3) float32;
+* gradients come from the hand-written adjoint whenever ``torch.is_grad_enabled()`` and an input requires grad;
+* unsupported features raise ``NotImplementedError`` (``capabilities``); another engine's options ``TypeError``.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+from dataclasses import dataclass
+
+import torch
+from torch import Tensor
+
+from . import capabilities, engine
+from .types import SimResult
+
+ENGINES = ("b200", "gpu", "cuda")  # "gpu" and "cuda" name this engine too, so a caller's engine= still works
+OPTIONS = ("readout", "pulses", "surrogate", "max_ctas")
+REFERENCE_GPU_OPTIONS = ("chunk", "group", "mma", "readouts", "nufft_width", "nufft_terms")
+READOUTS = ("fp32", "bf16x3")
+
+
+@dataclass
+class Inputs:
+    """One case's tensors as the engine reads them (coils complex (N, C), never None)."""
+
+    pos: Tensor
+    pd: Tensor
+    t1: Tensor
+    t2: Tensor
+    db0: Tensor
+    b1: Tensor | None
+    coils: Tensor
+    dt: Tensor
+    rf: Tensor
+    grad: Tensor
+    adc_phase: Tensor
+    b0_offset: Tensor | None
+    is_rf: list
+    adc: list
+    spoil: list
+    m_init: Tensor | None
+
+
+def requires_grad(*objs) -> bool:
+    """Whether any tensor in ``objs`` (tensors, dataclasses, tuples) requires grad (as blochparty
+    ``engines/gpu/__init__.py:39-51``)."""
+    for o in objs:
+        if isinstance(o, Tensor):
+            if o.requires_grad:
+                return True
+        elif dataclasses.is_dataclass(o) and not isinstance(o, type):
+            if requires_grad(*(getattr(o, f.name) for f in dataclasses.fields(o))):
+                return True
+        elif isinstance(o, tuple) and requires_grad(*o):
+            return True
+    return False
+
+
+def _device(device=None) -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("engine='b200' needs a CUDA device (an NVIDIA B200, sm_100a); none is available")
+    return torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+
+
+def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None = None,
+             checkpoint_every: int | None = None, merge_free_runs: bool = True, scanner=None, seed: int = 0,
+             maps=None, engine: str = "b200", **options) -> SimResult:
+    """Run ``seq`` on ``phantom`` on the GPU (blochparty ``simulate``'s arguments; see the module docstring).
+
+    coils: (N, C) complex receive sensitivities (default: one uniform coil), C <= 32.
+    m_init: (N, 3) starting magnetization (default: equilibrium, Mz = PD).
+    checkpoint_every: with gradients, the adjoint stores the state every this many segments (rounded to window
+        boundaries); default about sqrt(segments).
+    options: ``readout`` "fp32" (default: float32 coil products reduced by warp shuffles) or "bf16x3" (the coil
+        contraction on the tensor cores in split bfloat16 with float32 accumulation); ``pulses`` "step"
+        (default) or "surrogate" (shaped pulses through a trained ``surrogate``); ``max_ctas`` caps the grid.
+    """
+    if engine not in ENGINES:
+        raise ValueError(f"engine must be one of {ENGINES}, not {engine!r}")
+    if unknown := sorted(set(options) - set(OPTIONS)):
+        hint = " (an option of blochparty's GPU engines)" if set(unknown) <= set(REFERENCE_GPU_OPTIONS) else ""
+        raise TypeError(f"simulate(engine={engine!r}) got unexpected keyword argument(s) {', '.join(unknown)}{hint}")
+    if not merge_free_runs:
+        raise ValueError(f"merge_free_runs=False is the core's segment-by-segment stepping, not engine={engine!r}'s")
+    readout = options.get("readout", "fp32")
+    if readout not in READOUTS:
+        raise ValueError(f"readout must be one of {READOUTS}, not {readout!r}")
+    pulses = options.get("pulses", "step")
+    if pulses not in ("step", "surrogate"):
+        raise ValueError(f"pulses must be 'step' or 'surrogate', not {pulses!r}")
+    n = len(phantom.pd)
+    if coils is not None and (coils.dim() != 2 or coils.shape[0] != n):
+        raise ValueError(f"coils must be (N, C) = ({n}, C), got {tuple(coils.shape)}")
+    if m_init is not None and tuple(m_init.shape) != (n, 3):
+        raise ValueError(f"m_init must be (N, 3) = ({n}, 3), got {tuple(m_init.shape)}")
+    if checkpoint_every is not None and checkpoint_every < 1:
+        raise ValueError(f"checkpoint_every must be positive, got {checkpoint_every}")
+    grad = torch.is_grad_enabled() and requires_grad(phantom, seq, coils, m_init)
+    capabilities.check(capabilities.features(phantom, seq, m_init, scanner, maps), grad=grad)
+    dev = _device()
+    if coils is None:
+        coils = torch.ones(n, 1, dtype=torch.complex64)
+    inp = Inputs(phantom.pos, phantom.pd, phantom.t1, phantom.t2, phantom.db0, getattr(phantom, "b1", None), coils,
+                 seq.dt, seq.rf, seq.grad, seq.adc_phase, getattr(seq, "b0_offset", None), list(seq.is_rf),
+                 list(seq.adc), list(seq.spoil), m_init)
+    if grad:
+        from .adjoint import simulate_grad
+
+        return simulate_grad(inp, dev, checkpoint_every, options)
+    with torch.no_grad():
+        sig, m = _forward(inp, dev, options)
+    return SimResult(sig, m)
+
+
+def _forward(inp: Inputs, dev, options):
+    if options.get("pulses", "step") == "surrogate":
+        from .surrogate import forward_with_surrogate
+
+        return forward_with_surrogate(inp, dev, options)
+    if options.get("readout", "fp32") == "bf16x3":
+        from .readout_mma import forward_bf16x3
+
+        return forward_bf16x3(inp, dev, options.get("max_ctas", 0))
+    return engine.forward(inp, dev, options.get("max_ctas", 0))

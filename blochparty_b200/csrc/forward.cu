@@ -1,0 +1,300 @@
+// Forward propagation kernel (plain float32 readout) and its C-ABI launcher.
+//
+// Replaces blochparty's bloch_chunk / bloch_chunk_mma (engines/gpu/cuda/kernels.cu.in:2-185) for static spins
+// with PD, T1, T2, dB0, B1+, receive coils and b0_offset (the V=0 variant), driven by
+// engines/gpu/driver.py:_forward (:197-756).
+//
+// Work decomposition (persistent, window-major):
+//  * The sequence is cut on the host into windows of consecutive segments (at most BP_SEG_MAX segments and
+//    samp_max(NCG) ADC samples each).
+//  * A CTA of 128 threads owns the spin tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (128 spins each, one
+//    spin per thread). For every window it stages the window's segment records into shared memory with one
+//    TMA bulk copy (double-buffered: window w+1 is in flight while window w runs), then runs each of its tiles
+//    through the window: the tile's state is loaded from HBM, propagated in registers, and stored back.
+//  * ADC samples: each warp forms the 2C coil products of its 32 spins and reduces them by warp shuffles
+//    (butterfly reduce-scatter) into its own slice of a per-window accumulator in shared memory, summed over
+//    all of the CTA's tiles. At the window's end the warps' slices are added in fixed order and the CTA's
+//    partial is added to the float64 signal with one float64 atomic per (sample, coil, re/im): the cross-block
+//    sum is float64, and the CTA-level sum covers thousands of spins, so the number of atomics does not grow
+//    with the spin count.
+//  * Demodulation by exp(-i adc_phase) is the same for every spin and is applied after the sum, in float64
+//    (bp_signal_finish).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bloch_common.cuh"
+#include "../../include/blochparty_b200.h"
+
+#define BP_THREADS 128
+#define BP_WARPS (BP_THREADS / 32)
+#define BP_ACC_SAMPLES 64  // accumulator capacity in samples at 8 coils (one coil group)
+
+struct FwdArgs {
+    const float* spins;   // [8][n]: px py pz pd r1 r2 db0 b1
+    const float* sens;    // [16 ncg][n]: coil c real at row 2c, imaginary at 2c + 1, zero rows to pad
+    const SegRec* segs;   // [S]
+    const double4* seg64; // [S]: kx ky kz beta in float64
+    const int4* windows;  // [n_windows]: first segment, end segment, first ADC row, samples
+    int n, n_coils;
+    int w_begin, w_end;
+    float* state;         // [6][n]: mx my mz and their low parts
+    double* raw;          // [n_adc][2C] raw coil sums (float64 atomics), or null: no readout
+    float* wstates;       // null, or [(w_end - w_begin) / stride rounded up][6][n]: state at window starts
+    int wstate_stride;
+    int* status;
+};
+
+template <int NCG>
+__host__ __device__ constexpr int samp_max() {
+    return BP_ACC_SAMPLES / NCG;
+}
+
+template <int NCG>
+__global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    SegRec* segbuf = reinterpret_cast<SegRec*>(smem_raw);                      // [2][BP_SEG_MAX]
+    float* acc = reinterpret_cast<float*>(segbuf + 2 * BP_SEG_MAX);            // [WARPS][samp_max][16 NCG]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(acc + BP_WARPS * samp_max<NCG>() * 16 * NCG);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = a.n;
+    const int n_tiles = (n + BP_THREADS - 1) / BP_THREADS;
+    const int nv = 2 * a.n_coils;
+    constexpr int VG = 16 * NCG;  // accumulator values per sample (coil groups of 8, padded)
+    float* my_acc = acc + warp * samp_max<NCG>() * VG;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    for (int i = tid; i < BP_WARPS * samp_max<NCG>() * VG; i += BP_THREADS) acc[i] = 0.0f;
+    __syncthreads();
+
+    auto issue = [&](int w, int buf) {
+        const int4 win = a.windows[w];
+        const uint32_t bytes = static_cast<uint32_t>(win.y - win.x) * sizeof(SegRec);
+        fence_proxy_async_smem();
+        mbar_expect_tx(&bars[buf], bytes);
+        tma_load_1d(segbuf + buf * BP_SEG_MAX, a.segs + win.x, bytes, &bars[buf]);
+    };
+    if (tid == 0) issue(a.w_begin, 0);
+
+    for (int w = a.w_begin; w < a.w_end; ++w) {
+        const int i = w - a.w_begin, buf = i & 1;
+        const bool ok = mbar_wait_bounded(&bars[buf], (i >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
+            return;
+        }
+        if (tid == 0 && w + 1 < a.w_end) issue(w + 1, buf ^ 1);
+        const int4 win = a.windows[w];
+        const SegRec* q0 = segbuf + buf * BP_SEG_MAX;
+        const int nseg = win.y - win.x;
+        const bool readout = a.raw != nullptr && win.w > 0;
+        const bool save = a.wstates != nullptr && (i % a.wstate_stride) == 0;
+
+        for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+            const int j0 = tile * BP_THREADS + tid;
+            const bool active = j0 < n;
+            const int j = active ? j0 : 0;
+            const Spin p = load_spin(a.spins, n, j, active);
+            float mx = 0.f, my = 0.f, mz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+            if (active) {
+                mx = a.state[j];
+                my = a.state[n + j];
+                mz = a.state[2 * n + j];
+                lx = a.state[3 * n + j];
+                ly = a.state[4 * n + j];
+                lz = a.state[5 * n + j];
+                if (save) {
+                    float* ws = a.wstates + (size_t)(i / a.wstate_stride) * 6 * n;
+                    ws[j] = mx, ws[n + j] = my, ws[2 * n + j] = mz;
+                    ws[3 * n + j] = lx, ws[4 * n + j] = ly, ws[5 * n + j] = lz;
+                }
+            }
+            float sr[8], si[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                sr[c] = (readout && active) ? a.sens[(2 * c) * n + j] : 0.0f;
+                si[c] = (readout && active) ? a.sens[(2 * c + 1) * n + j] : 0.0f;
+            }
+            FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float e1h = 0.f, e2h = 0.f;
+            int row = 0;
+            for (int s = 0; s < nseg; ++s) {
+                const SegRec q = q0[s];
+                const int f = q.flags;
+                if (f & BP_RF) {
+                    if (s == 0 || !(f & BP_SAME_RFDT)) {
+                        e1h = expm1f(-0.5f * q.dt * p.r1);
+                        e2h = expm1f(-0.5f * q.dt * p.r2);
+                    }
+                    rf_step(q, p, e1h, e2h, mx, my, mz, lx, ly, lz);
+                } else {
+                    if (s == 0 || !(f & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
+                    free_step(ff, p, mx, my, mz, lx, ly, lz);
+                }
+                if ((f & BP_ADC) && readout) {
+                    const float ax = mx + lx, ay = my + ly;
+                    float* dst = my_acc + row * VG;
+#pragma unroll
+                    for (int g = 0; g < NCG; ++g) {
+                        float v[16];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            float r_, i_;
+                            if (g == 0) {
+                                r_ = sr[c];
+                                i_ = si[c];
+                            } else {
+                                r_ = active ? a.sens[(16 * g + 2 * c) * n + j] : 0.0f;
+                                i_ = active ? a.sens[(16 * g + 2 * c + 1) * n + j] : 0.0f;
+                            }
+                            v[2 * c] = fmaf(ax, r_, -ay * i_);
+                            v[2 * c + 1] = fmaf(ax, i_, ay * r_);
+                        }
+                        const float t = warp_reduce_scatter16(v, lane);
+                        if (!(lane & 1)) dst[16 * g + ((lane >> 1) & 15)] += t;
+                    }
+                    ++row;
+                }
+                if (f & BP_SPOIL) mx = my = lx = ly = 0.0f;
+            }
+            if (active) {
+                a.state[j] = mx;
+                a.state[n + j] = my;
+                a.state[2 * n + j] = mz;
+                a.state[3 * n + j] = lx;
+                a.state[4 * n + j] = ly;
+                a.state[5 * n + j] = lz;
+            }
+        }
+        __syncthreads();
+        if (readout) {
+            // the warps' slices in fixed order, then one float64 atomic per value; slots are cleared as read
+            for (int k = tid; k < win.w * nv; k += BP_THREADS) {
+                const int r = k / nv, v = k % nv;
+                const int slot = r * VG + v;
+                float t = 0.0f;
+#pragma unroll
+                for (int ww = 0; ww < BP_WARPS; ++ww) {
+                    t += acc[ww * samp_max<NCG>() * VG + slot];
+                    acc[ww * samp_max<NCG>() * VG + slot] = 0.0f;
+                }
+                atomicAdd(a.raw + (size_t)(win.z + r) * nv + v, (double)t);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---- float64 demodulation of the summed signal: out[c][t] = raw[t][c] exp(-i psi[t]) as complex64 ----
+__global__ void bp_signal_finish_kernel(const double* __restrict__ raw, const double* __restrict__ psi, int n_adc,
+                                        int n_coils, float2* __restrict__ out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)n_adc * n_coils) return;
+    const int t = (int)(k % n_adc), c = (int)(k / n_adc);
+    const double re = raw[(size_t)t * 2 * n_coils + 2 * c], im = raw[(size_t)t * 2 * n_coils + 2 * c + 1];
+    double s, co;
+    sincos(psi[t], &s, &co);
+    out[k] = make_float2((float)(re * co + im * s), (float)(im * co - re * s));
+}
+
+// ---- launch helpers ----
+template <int NCG>
+static size_t fwd_smem_bytes() {
+    return 2 * BP_SEG_MAX * sizeof(SegRec) + (size_t)BP_WARPS * samp_max<NCG>() * 16 * NCG * sizeof(float) +
+           2 * sizeof(uint64_t);
+}
+
+static int g_num_sms[64];
+
+static int num_sms(int dev) {
+    if (dev < 0 || dev >= 64) return 148;
+    if (!g_num_sms[dev]) cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    return g_num_sms[dev];
+}
+
+template <int NCG>
+static int launch_forward(const FwdArgs& a, int max_ctas, cudaStream_t stream) {
+    const size_t smem = fwd_smem_bytes<NCG>();
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        if (cudaFuncSetAttribute(bp_forward_kernel<NCG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return BP_E_LAUNCH;
+        configured[dev] = true;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_forward_kernel<NCG>, BP_THREADS, smem) !=
+        cudaSuccess)
+        return BP_E_LAUNCH;
+    if (per_sm < 1) per_sm = 1;
+    const int n_tiles = (a.n + BP_THREADS - 1) / BP_THREADS;
+    int grid = num_sms(dev) * per_sm;
+    if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+    if (grid > n_tiles) grid = n_tiles;
+    if (grid < 1) grid = 1;
+    bp_forward_kernel<NCG><<<grid, BP_THREADS, smem, stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+extern "C" int bp_forward_samp_max(int n_coils) {
+    if (n_coils < 1 || n_coils > BP_MAX_COILS) return 0;
+    const int ncg = (n_coils + 7) / 8;
+    switch (ncg) {
+        case 1: return samp_max<1>();
+        case 2: return samp_max<2>();
+        case 3: return samp_max<3>();
+        default: return samp_max<4>();
+    }
+}
+
+extern "C" int bp_forward(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                          const double* seg64, const int* windows, int w_begin, int w_end, float* state, double* raw,
+                          float* wstates, int wstate_stride, int max_ctas, int* status, void* stream) {
+    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || w_begin < 0 || w_end < w_begin) return BP_E_ARG;
+    if (!spins || !segs || !seg64 || !windows || !state || !status) return BP_E_ARG;
+    if (raw && !sens) return BP_E_ARG;
+    if (wstates && wstate_stride < 1) return BP_E_ARG;
+    if ((reinterpret_cast<uintptr_t>(segs) & 15) != 0) return BP_E_ALIGN;
+    if (w_end == w_begin) return BP_OK;
+    FwdArgs a;
+    a.spins = spins;
+    a.sens = sens;
+    a.segs = static_cast<const SegRec*>(segs);
+    a.seg64 = reinterpret_cast<const double4*>(seg64);
+    a.windows = reinterpret_cast<const int4*>(windows);
+    a.n = n;
+    a.n_coils = n_coils;
+    a.w_begin = w_begin;
+    a.w_end = w_end;
+    a.state = state;
+    a.raw = raw;
+    a.wstates = wstates;
+    a.wstate_stride = wstate_stride > 0 ? wstate_stride : 1;
+    a.status = status;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch ((n_coils + 7) / 8) {
+        case 1: return launch_forward<1>(a, max_ctas, st);
+        case 2: return launch_forward<2>(a, max_ctas, st);
+        case 3: return launch_forward<3>(a, max_ctas, st);
+        default: return launch_forward<4>(a, max_ctas, st);
+    }
+}
+
+extern "C" int bp_signal_finish(const double* raw, const double* psi, int n_adc, int n_coils, void* out,
+                                void* stream) {
+    if (n_adc < 0 || n_coils < 1 || !raw || !psi || !out) return BP_E_ARG;
+    if (n_adc == 0) return BP_OK;
+    const int64_t total = (int64_t)n_adc * n_coils;
+    const int threads = 256;
+    const int64_t blocks = (total + threads - 1) / threads;
+    bp_signal_finish_kernel<<<(unsigned)blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(
+        raw, psi, n_adc, n_coils, static_cast<float2*>(out));
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}

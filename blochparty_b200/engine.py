@@ -1,0 +1,174 @@
+"""Host driver of the b200 engine: inputs into device buffers, the window plan, the launches, the results.
+
+Replaces blochparty's GPU driver for static spins (``engines/gpu/driver.py:_forward``, :197-756): the same
+float64-on-host preparation (positions, rates 1/T1 and 1/T2, per-segment quantities, the state split into a
+float32 high part and its float32 remainder) feeding the C ABI of ``libblochparty_b200.so``.
+
+Device buffers (float32 unless stated; N spins, S segments, C coils, A ADC samples):
+
+* ``spins`` [8][N]: x, y, z, pd, r1, r2, dB0, b1 (structure of arrays: one coalesced row per field);
+* ``sens`` [16 ceil(C/8)][N]: coil c real at row 2c, imaginary at 2c+1, zero padding rows;
+* ``segs`` [S] 32-byte records: dt, -2 pi dt rf_x, -2 pi dt rf_y, g dt (3), b0_offset dt, flags (int32);
+* ``seg64`` [S][4] float64: g dt (3), b0_offset dt: the free segments' phase is evaluated in float64;
+* ``windows`` [W][4] int32: first segment, end segment, first ADC row, samples (``bp_plan_windows``);
+* ``state`` [6][N]: mx, my, mz and their compensation parts;
+* ``raw`` [A][2C] float64: the coil sums before demodulation; ``signal`` (C, A) complex64.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import ptr
+
+TWO_PI = 2.0 * math.pi
+F32, F64 = torch.float32, torch.float64
+
+RF, ADC, SPOIL, SAME_FREE, SAME_RFDT = 1, 2, 4, 8, 16
+
+
+@dataclass
+class Packed:
+    """A case's device buffers (see module docstring) and sizes."""
+
+    n: int
+    n_coils: int
+    n_adc: int
+    spins: torch.Tensor
+    sens: torch.Tensor
+    segs: torch.Tensor  # (S, 8) float32 view of the records (the flags column holds int32 bits)
+    seg64: torch.Tensor
+    psi: torch.Tensor  # (A,) float64 receiver phase of every sample
+    flags: np.ndarray  # (S,) int32 on the host
+    device: torch.device
+
+
+def _np64(t) -> np.ndarray:
+    return t.detach().to(F64).cpu().numpy()
+
+
+def pack_spins(pos, pd, t1, t2, db0, b1, coils, device):
+    n = pd.shape[0]
+    b1 = torch.ones(n, dtype=F64) if b1 is None else b1.detach().to(F64).cpu()
+    rows = [pos[:, 0], pos[:, 1], pos[:, 2], pd, 1.0 / t1, 1.0 / t2, db0, b1]
+    spins = torch.stack([r.detach().to(F64).cpu() for r in rows]).to(F32)
+    n_coils = coils.shape[1]
+    ncg = (n_coils + 7) // 8
+    sens = torch.zeros(16 * ncg, n, dtype=F32)
+    c = coils.detach().to(torch.complex128).cpu()
+    sens[0:2 * n_coils:2] = c.real.T.to(F32)
+    sens[1:2 * n_coils:2] = c.imag.T.to(F32)
+    return spins.to(device).contiguous(), sens.to(device).contiguous()
+
+
+def pack_segments(dt, rf, grad, b0_offset, adc_phase, is_rf, adc, spoil, device):
+    """Segment records (float64 arithmetic, one rounding to float32), the float64 moments, flags and psi."""
+    dt, rf, grad = _np64(dt), _np64(rf), _np64(grad)
+    S = dt.shape[0]
+    b0 = np.zeros(S) if b0_offset is None else _np64(b0_offset)
+    w = -TWO_PI * dt
+    k = grad * dt[:, None]
+    beta = b0 * dt
+    rec = np.empty((S, 8), dtype=np.float32)
+    rec[:, 0] = dt
+    rec[:, 1] = w * rf[:, 0]
+    rec[:, 2] = w * rf[:, 1]
+    rec[:, 3:6] = k
+    rec[:, 6] = beta
+    seg64 = np.empty((S, 4), dtype=np.float64)
+    seg64[:, 0:3] = k
+    seg64[:, 3] = beta
+    is_rf = np.asarray(is_rf, dtype=bool)
+    adc_b = np.asarray(adc, dtype=bool)
+    spoil_b = np.asarray(spoil, dtype=bool)
+    flags = is_rf.astype(np.int32) | (adc_b.astype(np.int32) << 1) | (spoil_b.astype(np.int32) << 2)
+    if S > 1:
+        free = ~is_rf
+        same_dt = rec[1:, 0] == rec[:-1, 0]
+        same_free = free[1:] & free[:-1] & same_dt & (seg64[1:] == seg64[:-1]).all(1)
+        same_rf = is_rf[1:] & is_rf[:-1] & same_dt
+        flags[1:] |= (same_free.astype(np.int32) << 3) | (same_rf.astype(np.int32) << 4)
+    rec.view(np.int32)[:, 7] = flags
+    psi = np.remainder(_np64(adc_phase)[adc_b], TWO_PI)
+    return (torch.from_numpy(rec).to(device).contiguous(), torch.from_numpy(seg64).to(device).contiguous(),
+            torch.from_numpy(psi).to(device).contiguous(), flags, int(adc_b.sum()))
+
+
+def plan_windows(flags: np.ndarray, samp_max: int, seg_max: int = _lib.BP_SEG_MAX, breaks: np.ndarray | None = None):
+    """(W, 4) int32 windows from the native planner (``bp_plan_windows``)."""
+    S = flags.shape[0]
+    n_adc = int(((flags & ADC) != 0).sum())
+    n_breaks = 0 if breaks is None else int(breaks.sum())
+    cap = S // seg_max + n_adc // samp_max + n_breaks + 2
+    out = np.zeros((cap, 4), dtype=np.int32)
+    nw = np.zeros(1, dtype=np.int64)
+    fl = np.ascontiguousarray(flags, dtype=np.int32)
+    br = None if breaks is None else np.ascontiguousarray(breaks, dtype=np.uint8)
+    code = _lib.lib().bp_plan_windows(fl.ctypes.data, S, seg_max, samp_max, None if br is None else br.ctypes.data,
+                                      out.ctypes.data, cap, nw.ctypes.data)
+    _lib.check(code, "bp_plan_windows")
+    return out[: int(nw[0])].copy()
+
+
+def initial_state(pd, m_init, device):
+    """[6][N] float32: m0 split exactly from float64 into a float32 high part and its float32 remainder."""
+    n = pd.shape[0]
+    if m_init is None:
+        m64 = torch.stack([torch.zeros(n, dtype=F64), torch.zeros(n, dtype=F64), pd.detach().to(F64).cpu()])
+    else:
+        m64 = m_init.detach().to(F64).cpu().T
+    hi = m64.to(F32)
+    lo = (m64 - hi.to(F64)).to(F32)
+    return torch.cat([hi, lo]).to(device).contiguous()
+
+
+def final_m(state: torch.Tensor) -> torch.Tensor:
+    s = state.to(F64)
+    return (s[0:3] + s[3:6]).to(F32).T.contiguous().cpu()
+
+
+def pack(case, device) -> Packed:
+    spins, sens = pack_spins(case.pos, case.pd, case.t1, case.t2, case.db0, case.b1, case.coils, device)
+    segs, seg64, psi, flags, n_adc = pack_segments(case.dt, case.rf, case.grad, case.b0_offset, case.adc_phase,
+                                                   case.is_rf, case.adc, case.spoil, device)
+    return Packed(case.pd.shape[0], case.coils.shape[1], n_adc, spins, sens, segs, seg64, psi, flags, device)
+
+
+def run_forward(pk: Packed, state: torch.Tensor, windows_dev: torch.Tensor, w_begin: int, w_end: int,
+                raw: torch.Tensor | None, status: torch.Tensor, wstates: torch.Tensor | None = None,
+                wstate_stride: int = 1, max_ctas: int = 0) -> None:
+    code = _lib.lib().bp_forward(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
+                                 ptr(windows_dev), w_begin, w_end, ptr(state), ptr(raw), ptr(wstates),
+                                 wstate_stride, max_ctas, ptr(status), _lib.stream_ptr())
+    _lib.check(code, "bp_forward")
+
+
+def finish_signal(pk: Packed, raw: torch.Tensor) -> torch.Tensor:
+    """(C, A) complex64 on the device: the float64 sums demodulated by exp(-i psi)."""
+    out = torch.empty(pk.n_coils, max(pk.n_adc, 1), dtype=torch.complex64, device=pk.device)
+    code = _lib.lib().bp_signal_finish(ptr(raw), ptr(pk.psi), pk.n_adc, pk.n_coils, ptr(out), _lib.stream_ptr())
+    _lib.check(code, "bp_signal_finish")
+    return out[:, : pk.n_adc]
+
+
+def forward(case, device, max_ctas: int = 0):
+    """Signal (C, A) complex64 and m (N, 3) float32, both on the CPU, of a case (``oracle.bloch.Case``-like)."""
+    pk = pack(case, device)
+    samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
+    if samp <= 0:
+        raise ValueError(f"at most {_lib.BP_MAX_COILS} coils, got {pk.n_coils}")
+    windows = plan_windows(pk.flags, samp)
+    wdev = torch.from_numpy(windows).to(device).contiguous()
+    state = initial_state(case.pd, case.m_init, device)
+    raw = torch.zeros(max(pk.n_adc, 1), 2 * pk.n_coils, dtype=F64, device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    run_forward(pk, state, wdev, 0, windows.shape[0], raw if pk.n_adc else None, status, max_ctas=max_ctas)
+    sig = finish_signal(pk, raw)
+    torch.cuda.synchronize(device)
+    _lib.check_status(status, "bp_forward")
+    return sig.cpu(), final_m(state)

@@ -1,0 +1,72 @@
+/* C ABI of the B200 Bloch-simulation library (libblochparty_b200.so).
+ *
+ * Every entry point takes plain pointers and sizes: device pointers for all arrays (allocated and owned by the
+ * caller), a CUDA stream as `void*` (NULL: the legacy default stream), and returns an int status (BP_OK = 0).
+ * Kernels are launched asynchronously on the stream; device-side failures (a bounded wait that gave up) are
+ * OR-ed into the caller's `status` word, which the caller reads after synchronising. Nothing here allocates
+ * device memory except where a comment says otherwise.
+ *
+ * These entry points replace the kernel launches of blochparty's GPU driver for static spins:
+ * engines/gpu/cuda/rtc.py:116-126 (_Driver.launch of bloch_chunk / bloch_chunk_mma, bloch_replay,
+ * bloch_adjoint_c*, seg_reduce), driven by engines/gpu/driver.py:_forward (:197-756) and
+ * engines/gpu/adjoint.py:_GPUSimulate (:45-261).
+ */
+#ifndef BLOCHPARTY_B200_H
+#define BLOCHPARTY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BP_OK 0
+#define BP_E_ARG 1      /* invalid argument (size, null pointer, coil count) */
+#define BP_E_ALIGN 2    /* a buffer that is TMA-copied is not 16-byte aligned */
+#define BP_E_LAUNCH 3   /* the CUDA launch failed (cudaGetLastError) */
+#define BP_E_SIZE 4     /* a size above a documented maximum */
+
+#define BP_MAX_COILS 32 /* receive coils of the float32 readout */
+#define BP_SEG_MAX 512  /* segments per window (one TMA-staged block) */
+
+/* Window planner (host code, no GPU): cuts `n_segments` segments with per-segment `flags` (bit 1 RF, 2 ADC,
+ * 4 spoil) into consecutive windows of at most `seg_max` (<= BP_SEG_MAX) segments and `samp_max` ADC samples;
+ * `breaks` (optional, n_segments bytes) forces a window to start at every segment whose byte is nonzero.
+ * Writes 4 ints per window (first segment, end segment, first ADC row, samples) into `windows` (room for
+ * `max_windows`) and the count into `*n_windows`. Replaces the dispatch boundaries of
+ * engines/gpu/driver.py:617-627. Returns BP_E_SIZE when `max_windows` is too small. */
+int bp_plan_windows(const int32_t* flags, int64_t n_segments, int seg_max, int samp_max, const uint8_t* breaks,
+                    int32_t* windows, int64_t max_windows, int64_t* n_windows);
+
+/* ADC samples per window that bp_forward's float32 readout accumulates for `n_coils` coils (0 if unsupported). */
+int bp_forward_samp_max(int n_coils);
+
+/* Forward propagation of windows [w_begin, w_end) (replaces bloch_chunk_mma, engines/gpu/cuda/kernels.cu.in:2-185,
+ * and the dispatch loop engines/gpu/driver.py:658-698).
+ *   spins   [8][n] float32: x y z [m], pd, r1 = 1/T1, r2 = 1/T2 [1/s], dB0 [Hz], B1 scale
+ *   sens    [16 ceil(C/8)][n] float32: coil c real part at row 2c, imaginary at 2c+1, zero padding rows
+ *   segs    [S] 32-byte segment records (dt, -2 pi dt rf_x, -2 pi dt rf_y, g dt (3), b0_offset dt, flags)
+ *   seg64   [S][4] float64: g dt (3), b0_offset dt (the free segments' phase, in float64)
+ *   windows [n_windows][4] int32 from bp_plan_windows
+ *   state   [6][n] float32 in/out: mx my mz and their compensation (low) parts
+ *   raw     [n_adc][2C] float64, accumulated (+=) raw coil sums, not demodulated; NULL: no readout
+ *   wstates NULL or [ceil((w_end - w_begin) / wstate_stride)][6][n]: the state at every stride-th window start
+ *   max_ctas  0: one persistent CTA per resident slot; else at most this many CTAs */
+int bp_forward(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
+               const int32_t* windows, int w_begin, int w_end, float* state, double* raw, float* wstates,
+               int wstate_stride, int max_ctas, int32_t* status, void* stream);
+
+/* signal[c][t] = raw[t][c] exp(-i psi[t]) in float64, written as complex64 (interleaved float pairs), shape
+ * (n_coils, n_adc) (replaces the host-side assembly engines/gpu/driver.py:699-702). */
+int bp_signal_finish(const double* raw, const double* psi, int n_adc, int n_coils, void* out, void* stream);
+
+/* Measurement kernel (the roofline denominator): 4 CTAs x 256 threads per SM, each thread `iters` x 128
+ * independent FFMAs; `*flops` receives the flop count of the launch, which the caller divides by the launch's
+ * CUDA-event duration. `out` needs 4 * SMs * 256 floats (never written in practice). */
+int bp_ffma_peak(float* out, int iters, int64_t* flops, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,123 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports what the header declares, the native
+window planner, the packing of segments and state, the capability refusals and argument errors of ``simulate``."""
+
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import blochparty_b200 as bpb
+from blochparty_b200 import _lib, capabilities, engine, sequences
+
+ROOT = Path(__file__).resolve().parents[1]
+F64 = torch.float64
+
+
+def declared_functions():
+    text = (ROOT / "include" / "blochparty_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|void)\s+(bp_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load_library()
+    names = declared_functions()
+    assert len(names) >= 4
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_planner_windows_cover_the_sequence():
+    g = np.random.default_rng(0)
+    flags = (g.random(5000) < 0.3).astype(np.int32) | ((g.random(5000) < 0.4).astype(np.int32) << 1)
+    for samp in (1, 7, 64):
+        w = engine.plan_windows(flags, samp, seg_max=100)
+        assert w[0, 0] == 0 and w[-1, 1] == 5000
+        assert (w[1:, 0] == w[:-1, 1]).all()
+        assert ((w[:, 1] - w[:, 0]) <= 100).all() and (w[:, 3] <= samp).all()
+        adc = (flags & 2) != 0
+        counts = np.array([adc[a:b].sum() for a, b in w[:, :2]])
+        assert (counts == w[:, 3]).all()
+        assert (w[:, 2] == np.concatenate([[0], np.cumsum(counts)[:-1]])).all()
+
+
+def test_planner_breaks_and_errors():
+    flags = np.zeros(10, np.int32)
+    br = np.zeros(10, np.uint8)
+    br[[3, 7]] = 1
+    w = engine.plan_windows(flags, 4, seg_max=512, breaks=br)
+    assert w[:, 0].tolist() == [0, 3, 7]
+    lib = _lib.lib()
+    out = np.zeros((1, 4), np.int32)
+    nw = np.zeros(1, np.int64)
+    assert lib.bp_plan_windows(flags.ctypes.data, 10, 4, 4, None, out.ctypes.data, 1, nw.ctypes.data) == _lib.BP_E_SIZE
+    assert lib.bp_plan_windows(flags.ctypes.data, 10, 513, 4, None, out.ctypes.data, 9, nw.ctypes.data) == _lib.BP_E_ARG
+    assert lib.bp_forward_samp_max(8) > 0 and lib.bp_forward_samp_max(33) == 0 and lib.bp_forward_samp_max(0) == 0
+
+
+def test_segment_records():
+    b = sequences.SequenceBuilder().rf(1e-4, flip_deg=30.0, phase=0.5, n_steps=2, grad=(0, 0, 100.0))
+    b.readout(4, 1e-5, grad=(1000.0, 0.0, 0.0)).delay(1e-3).spoil()
+    seq = b.build()
+    seq.b0_offset = torch.full((len(seq),), 3.0, dtype=F64)
+    rec, seg64, psi, flags, n_adc = engine.pack_segments(seq.dt, seq.rf, seq.grad, seq.b0_offset, seq.adc_phase,
+                                                         seq.is_rf, seq.adc, seq.spoil, "cpu")
+    assert rec.shape == (len(seq), 8) and rec.dtype == torch.float32 and n_adc == 4
+    assert flags.tolist() == [1, 1 | 16, 2, 2, 2 | 8, 2 | 8, 0, 4]  # first sample half a dwell: not "same"
+    assert abs(float(rec[0, 1]) - (-2 * np.pi * 5e-5 * float(seq.rf[0, 0]))) < 1e-6
+    assert float(seg64[3, 0]) == 1000.0 * 1e-5 and float(seg64[3, 3]) == 3.0 * 1e-5
+    assert rec.view(torch.int32)[:, 7].tolist() == flags.tolist()
+
+
+def test_initial_state_split_is_exact():
+    pd = torch.rand(100, dtype=F64)
+    m = torch.rand(100, 3, dtype=F64)
+    s = engine.initial_state(pd, m, "cpu")
+    assert torch.equal(s[0:3].to(F64) + s[3:6].to(F64), m.T) or (
+        (s[0:3].to(F64) + s[3:6].to(F64) - m.T).abs().max() < 1e-14)
+
+
+def _tiny():
+    ph = bpb.Phantom(torch.zeros(2, 3, dtype=F64), torch.ones(2, dtype=F64), torch.ones(2, dtype=F64),
+                     torch.full((2,), 0.1, dtype=F64), torch.zeros(2, dtype=F64))
+    return ph, sequences.SequenceBuilder().rf(1e-4, flip_deg=10.0).readout(4, 1e-5).build()
+
+
+def test_refusals_use_the_reference_wording():
+    ph, seq = _tiny()
+    ph.diffusion = torch.ones(2, dtype=F64)
+    with pytest.raises(NotImplementedError, match=r"b200 engine: simulating with diffusion \(Phantom.diffusion\) "
+                                                  r"is not implemented; use blochparty.simulate \(the core\)"):
+        bpb.simulate(ph, seq)
+    ph.diffusion = None
+    with pytest.raises(NotImplementedError, match="scanner field model"):
+        bpb.simulate(ph, seq, scanner=object())
+    seq.bound_only = [True] + [False] * (len(seq) - 1)
+    with pytest.raises(NotImplementedError, match="bound-pool-only"):
+        bpb.simulate(ph, seq)
+    used = capabilities.features(ph, seq, torch.zeros(2, 3))
+    assert "m_init" in used and "bound_only" in used
+
+
+def test_argument_errors():
+    ph, seq = _tiny()
+    with pytest.raises(TypeError, match="unexpected keyword argument"):
+        bpb.simulate(ph, seq, chunk=4)
+    with pytest.raises(ValueError, match="merge_free_runs=False"):
+        bpb.simulate(ph, seq, merge_free_runs=False)
+    with pytest.raises(ValueError, match="engine must be one of"):
+        bpb.simulate(ph, seq, engine="metal")
+    with pytest.raises(ValueError, match="readout must be"):
+        bpb.simulate(ph, seq, readout="tf32")
+    with pytest.raises(ValueError, match=r"coils must be \(N, C\)"):
+        bpb.simulate(ph, seq, torch.ones(3, 1, dtype=torch.complex64))
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU error")
+def test_no_gpu_fails_loudly():
+    ph, seq = _tiny()
+    with pytest.raises(RuntimeError, match="needs a CUDA device"):
+        bpb.simulate(ph, seq)
