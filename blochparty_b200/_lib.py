@@ -16,7 +16,8 @@ LIB_PATH = Path(__file__).resolve().parent / "libblochparty_b200.so"
 
 BP_OK, BP_E_ARG, BP_E_ALIGN, BP_E_LAUNCH, BP_E_SIZE = 0, 1, 2, 3, 4
 BP_MAX_COILS = 32
-BP_SEG_MAX = 512
+BP_SEG_MAX = 240
+BP_ADJ_WIN = 32
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",
@@ -30,6 +31,10 @@ SIGNATURES = {
     "bp_forward": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P]),
     "bp_signal_finish": (c_int, [_P, _P, c_int, c_int, _P, _P]),
     "bp_ffma_peak": (c_int, [_P, c_int, _P, _P]),
+    "bp_adjoint_grid": (c_int, [c_int, c_int]),
+    "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P,
+                           c_int, _P]),
+    "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
 }
 
 _lib = None

@@ -1,0 +1,207 @@
+"""Gradients: the forward with checkpoints and the hand-written adjoint behind a ``torch.autograd.Function``.
+
+Replaces blochparty ``engines/gpu/adjoint.py`` (``_GPUSimulate`` :45-261, ``_simulate_grad`` :264-323) for static
+spins. The forward stores the state at the start of every checkpoint interval (``checkpoint_every`` segments, a
+multiple of ``BP_ADJ_WIN`` = 32). The backward walks the intervals in reverse: it replays an interval with the
+forward kernel, storing the state at every 32-segment window start, then runs ``bp_adjoint`` over it (each window
+recomputed into shared memory and swept backward) and ``bp_seg_reduce`` (segment gradients summed over CTAs in
+fixed order, float64). Windows fall on multiples of 32 segments whatever the interval, so the gradients are the
+same bits for every ``checkpoint_every`` and every run.
+
+Chain rules on the host (float64), from the kernels' raw gradients: r1 = 1/T1 -> dL/dT1 = -dL/dr1 / T1^2; the
+segment record (dt, w_x = -2 pi dt rf_x, w_y, k = g dt, beta = b0_offset dt) -> dL/d(dt, rf, grad, b0_offset);
+the receiver phase: signal = raw exp(-i psi), so dL/dpsi = gr Im(signal) - gi Re(signal) (blochparty
+``adjoint.py:241-245``).
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+from torch.autograd.function import once_differentiable
+
+from . import _lib, engine
+from ._lib import ptr
+from .types import SimResult
+
+F32, F64 = torch.float32, torch.float64
+TWO_PI = 2.0 * math.pi
+
+
+def default_checkpoint_every(n_segments: int) -> int:
+    """About sqrt(segments), a multiple of the 32-segment adjoint window."""
+    w = _lib.BP_ADJ_WIN
+    return w * max(1, math.ceil(math.sqrt(max(n_segments, 1)) / w))
+
+
+class Plan:
+    """Windows and intervals of one gradient-carrying simulation."""
+
+    def __init__(self, pk: engine.Packed, every: int, device):
+        S = pk.flags.shape[0]
+        self.every = every
+        self.starts = list(range(0, S, every))
+        breaks = np.zeros(S, dtype=np.uint8)
+        breaks[self.starts] = 1
+        samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
+        self.fwin = engine.plan_windows(pk.flags, samp, breaks=breaks)
+        w = _lib.BP_ADJ_WIN
+        self.awin = engine.plan_windows(pk.flags, w, seg_max=w, breaks=breaks)
+        self.fwin_dev = torch.from_numpy(self.fwin).to(device)
+        self.awin_dev = torch.from_numpy(self.awin).to(device)
+        # window ranges of every interval
+        fstart, astart = self.fwin[:, 0], self.awin[:, 0]
+        self.franges, self.aranges, self.seg_ranges = [], [], []
+        for k, s0 in enumerate(self.starts):
+            s1 = self.starts[k + 1] if k + 1 < len(self.starts) else S
+            fa, fb = np.searchsorted(fstart, s0), np.searchsorted(fstart, s1)
+            aa, ab = np.searchsorted(astart, s0), np.searchsorted(astart, s1)
+            self.franges.append((int(fa), int(fb)))
+            self.aranges.append((int(aa), int(ab)))
+            self.seg_ranges.append((s0, s1))
+        self.max_aw = max(b - a for a, b in self.aranges)
+        self.max_len = max(b - a for a, b in self.seg_ranges)
+
+
+class _Simulate(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0):
+        from .api import Inputs
+
+        dev, every, flags_in = opts["device"], opts["every"], opts["flags"]
+        coils = torch.view_as_complex(coils_ri.detach().contiguous())
+        d = lambda t: None if t is None else t.detach()
+        inp = Inputs(d(pos), d(pd), d(t1), d(t2), d(db0), d(b1), coils, d(dt), d(rf), d(grad), d(adc_phase),
+                     d(b0_offset), *flags_in, d(m0))
+        pk = engine.pack(inp, dev)
+        plan = Plan(pk, every, dev)
+        state = engine.initial_state(inp.pd, inp.m_init, dev)
+        ckpts = torch.empty(len(plan.starts), 6, pk.n, dtype=F32, device=dev)
+        raw = torch.zeros(max(pk.n_adc, 1), 2 * pk.n_coils, dtype=F64, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        for k, (fa, fb) in enumerate(plan.franges):
+            ckpts[k].copy_(state)
+            engine.run_forward(pk, state, plan.fwin_dev, fa, fb, raw if pk.n_adc else None, status)
+        sig = engine.finish_signal(pk, raw)
+        torch.cuda.synchronize(dev)
+        _lib.check_status(status, "bp_forward")
+        ctx.pk, ctx.plan, ctx.ckpts, ctx.dev = pk, plan, ckpts, dev
+        ctx.like = [None if t is None else (t.dtype, t.device) for t in
+                    (pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0)]
+        sig_ri = torch.view_as_real(sig).cpu().contiguous()  # (C, A, 2)
+        ctx.save_for_backward(t1, t2, dt, rf, grad, b0_offset, adc_phase, sig_ri)
+        ctx.set_materialize_grads(False)
+        return sig_ri, engine.final_m(state)
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, g_sig, g_m):
+        t1, t2, dt, rf, grad, b0_offset, adc_phase, sig_ri = ctx.saved_tensors
+        pk, plan, dev = ctx.pk, ctx.plan, ctx.dev
+        # inputs: opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0
+        need = ctx.needs_input_grad
+        if g_sig is None and g_m is None:
+            return (None,) * 14
+        n, C, A, S = pk.n, pk.n_coils, pk.n_adc, len(dt)
+        h = None
+        if g_sig is not None and A:
+            g = torch.complex(g_sig[..., 0].to(F64), g_sig[..., 1].to(F64)).to(dev)  # (C, A)
+            hr = g * torch.exp(1j * pk.psi)[None, :]  # dL/draw = dL/dsignal e^{+i psi}
+            h = torch.view_as_real(hr.T.contiguous()).reshape(A, 2 * C).to(F32).contiguous()
+        lam = torch.zeros(3, n, dtype=F32, device=dev)
+        if g_m is not None:
+            lam.copy_(g_m.T.to(F32))
+        gs = torch.zeros(8, n, dtype=F32, device=dev)
+        gc = torch.zeros(2 * C, n, dtype=F32, device=dev) if (need[7] and h is not None) else None
+        need_seg = any(need[i] for i in (8, 9, 10, 12))
+        grid = _lib.lib().bp_adjoint_grid(n, C)
+        if grid < 1:
+            raise RuntimeError("bp_adjoint_grid failed")
+        gseg = torch.empty(grid, plan.max_len, 8, dtype=F32, device=dev) if need_seg else None
+        seg = torch.zeros(S, 8, dtype=F64, device=dev)
+        wstates = torch.empty(plan.max_aw, 6, n, dtype=F32, device=dev)
+        state = torch.empty(6, n, dtype=F32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        lib, stream = _lib.lib(), _lib.stream_ptr()
+        for k in reversed(range(len(plan.starts))):
+            aa, ab = plan.aranges[k]
+            s0, s1 = plan.seg_ranges[k]
+            state.copy_(ctx.ckpts[k])
+            engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, status, wstates=wstates, wstate_stride=1)
+            code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
+                                  aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
+                                  grid, stream)
+            _lib.check(code, "bp_adjoint")
+            if need_seg:
+                _lib.check(lib.bp_seg_reduce(ptr(gseg), grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
+        torch.cuda.synchronize(dev)
+        _lib.check_status(status, "bp_forward (replay)")
+        gs64, lam64 = gs.to(F64).cpu(), lam.to(F64).cpu()
+        out = [None] * 13
+        if need[1]:
+            out[0] = gs64[0:3].T.contiguous()
+        if need[2]:
+            out[1] = gs64[4]
+        if need[3]:
+            out[2] = -gs64[5] / t1.detach().to(F64).cpu() ** 2
+        if need[4]:
+            out[3] = -gs64[6] / t2.detach().to(F64).cpu() ** 2
+        if need[5]:
+            out[4] = gs64[3]
+        if need[6]:
+            out[5] = gs64[7]
+        if need[7] and gc is not None:
+            g = gc.to(F64).cpu()
+            out[6] = torch.stack([g[0::2].T, g[1::2].T], -1)
+        if need_seg:
+            sg = seg.cpu()
+            dt64, rf64, gr64 = dt.detach().to(F64).cpu(), rf.detach().to(F64).cpu(), grad.detach().to(F64).cpu()
+            b064 = torch.zeros(S, dtype=F64) if b0_offset is None else b0_offset.detach().to(F64).cpu()
+            w = -TWO_PI * dt64
+            if need[8]:
+                out[7] = (sg[:, 0] + sg[:, 1] * (-TWO_PI * rf64[:, 0]) + sg[:, 2] * (-TWO_PI * rf64[:, 1])
+                          + (sg[:, 3:6] * gr64).sum(1) + sg[:, 6] * b064)
+            if need[9]:
+                out[8] = torch.stack([sg[:, 1] * w, sg[:, 2] * w], -1)
+            if need[10]:
+                out[9] = sg[:, 3:6] * dt64[:, None]
+            if need[12]:
+                out[11] = sg[:, 6] * dt64
+        if need[11] and g_sig is not None and A:
+            adc_idx = torch.tensor(np.flatnonzero(pk.flags & engine.ADC))
+            sr, si_ = sig_ri[..., 0].to(F64), sig_ri[..., 1].to(F64)
+            gr, gi = g_sig[..., 0].to(F64), g_sig[..., 1].to(F64)
+            gp = torch.zeros(S, dtype=F64)
+            gp[adc_idx] = (gr * si_ - gi * sr).sum(0)
+            out[10] = gp
+        if need[13]:
+            out[12] = lam64.T.contiguous()
+        return (None, *[None if v is None or not need[i + 1] else v.to(dtype=ctx.like[i][0], device=ctx.like[i][1])
+                        for i, v in enumerate(out)])
+
+
+def simulate_grad(inp, dev, checkpoint_every, options) -> SimResult:
+    """``simulate`` with gradients: the inputs as tensors of ``_Simulate``."""
+    if options.get("readout", "fp32") != "fp32":
+        raise NotImplementedError("b200 engine: gradients through readout='bf16x3' are not implemented; use the "
+                                  "default float32 readout (or torch.no_grad())")
+    if options.get("pulses", "step") != "step":
+        raise NotImplementedError("b200 engine: gradients through pulses='surrogate' are not implemented; use "
+                                  "pulses='step' (or torch.no_grad())")
+    S = len(inp.dt)
+    every = checkpoint_every or default_checkpoint_every(S)
+    if every % _lib.BP_ADJ_WIN:
+        raise ValueError(f"checkpoint_every must be a multiple of {_lib.BP_ADJ_WIN}, got {every}")
+    n = inp.pd.shape[0]
+    m0 = inp.m_init
+    if m0 is None:
+        z = torch.zeros_like(inp.pd)
+        m0 = torch.stack([z, z, inp.pd], -1)
+    coils_ri = torch.view_as_real(inp.coils if inp.coils.is_complex() else inp.coils.to(torch.complex64))
+    opts = {"device": dev, "every": every, "flags": (inp.is_rf, inp.adc, inp.spoil)}
+    sig_ri, m = _Simulate.apply(opts, inp.pos, inp.pd, inp.t1, inp.t2, inp.db0, inp.b1, coils_ri, inp.dt, inp.rf,
+                                inp.grad, inp.adc_phase, inp.b0_offset, m0)
+    signal = torch.view_as_complex(sig_ri.contiguous())
+    return SimResult(signal, m)

@@ -1,0 +1,373 @@
+// Hand-written adjoint (reverse sweep) of the forward kernel, and the fixed-order reduction of its segment
+// gradients. Replaces blochparty's bloch_replay / bloch_adjoint_c<NC> / seg_reduce
+// (engines/gpu/cuda/replay.cu.in:3-33, adjoint.cu.in:5-121, seg_reduce.cu:3-11; the reverse of one segment is
+// shaders/adjoint_common.metal:212-315) for static spins.
+//
+// Checkpointing has three levels. The forward stores the state at the start of every checkpoint interval. The
+// backward replays one interval at a time with the forward kernel (no readout), storing the state at the start
+// of every adjoint window (<= BP_ADJ_WIN segments). This kernel then sweeps the interval's windows in reverse:
+// per window it recomputes the window forward from its start state, keeping the state after every segment in
+// shared memory (one slot per segment and spin), and runs the segments backward from them.
+//
+// Segment s maps the magnetization affinely, m_s = A_s m_{s-1} + b_s. With lambda = dL/dm after segment s
+// (after its spoil), the sweep is lambda_{s-1} = A_s^T (P_s lambda + dL/dm of the sample), P_s the spoil
+// projection; the parameter gradients of segment s follow from lambda and m_{s-1}. Per-spin gradients stay in
+// registers over a window and are added to global memory at its end; per-segment gradients are reduced over the warp by shuffles, over the CTA's
+// warps in fixed order in shared memory, and written as one float32 partial per CTA and segment; bp_seg_reduce
+// adds the CTAs' partials in fixed order in float64. No atomics: every run gives the same bits.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bloch_common.cuh"
+#include "../../include/blochparty_b200.h"
+
+#define ADJ_THREADS 128
+#define ADJ_WARPS (ADJ_THREADS / 32)
+#define ADJ_SLOTS (BP_ADJ_WIN + 1)
+
+// per-spin gradient rows of `gs`
+enum { G_PX, G_PY, G_PZ, G_DB0, G_PD, G_R1, G_R2, G_B1, N_GS };
+// per-segment gradient columns: with respect to the record's dt (its direct uses), -2 pi dt rf_x, -2 pi dt rf_y,
+// the moments g dt, and b0_offset dt
+enum { S_DT, S_WX, S_WY, S_KX, S_KY, S_KZ, S_BETA, N_SG = 8 };
+
+struct AdjArgs {
+    const float* spins;
+    const float* sens;    // [16 ncg][n]
+    const SegRec* segs;
+    const double4* seg64;
+    const int4* windows;  // adjoint windows
+    int n, n_coils;
+    int wa, wb;           // this interval's adjoint windows
+    int seg0, seg_len;    // first segment of the interval, segments in it
+    const float* wstates; // [wb - wa][6][n] state at every window start (replay)
+    const float* h;       // [n_adc][2C] dL/d(raw coil sums), or null
+    float* lam;           // [3][n] in: dL/dm at the interval's end; out: at its start
+    float* gs;            // [N_GS][n] += per-spin gradients
+    float* gc;            // [2C][n] += coil gradients (rows 2c real, 2c+1 imaginary), or null
+    float* gseg;          // [gridDim.x][seg_len][N_SG] per-CTA segment gradients, or null
+};
+
+// Rodrigues rotation factors with the derivative factors f1 = (c - s1)/phi^2, f2 = (s1 - 2 s2)/phi^2 (the
+// derivatives of c, s1, s2 in phi, divided by phi). Below phi^2 = 1 all are Taylor series in phi^2:
+// f1 = sum_{k>=1} (-1)^k 2k phi^(2k-2) / (2k+1)!, f2 = sum_{k>=1} (-1)^k 2k phi^(2k-2) / (2k+2)!.
+__device__ __forceinline__ void rot_factors(float p2, float& c, float& s1, float& s2, float& f1, float& f2) {
+    rodrigues_coeffs(p2, s1, s2);
+    c = fmaf(-s2, p2, 1.0f);
+    if (p2 < 1.0f) {
+        f1 = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -2.5052108385441720e-07f, 2.2045855379188713e-05f),
+                                     -1.1904761904761905e-03f), 3.3333333333333333e-02f), -3.3333333333333333e-01f);
+        f2 = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -2.0876756987868099e-08f, 2.2045855379188713e-06f),
+                                     -1.4880952380952381e-04f), 5.5555555555555556e-03f), -8.3333333333333333e-02f);
+    } else {
+        f1 = (c - s1) / p2;
+        f2 = (s1 - 2.0f * s2) / p2;
+    }
+}
+
+struct SegGrad {
+    float v[N_SG];
+};
+
+// dL/d(offset in cycles) `gc` of a segment: per-spin and per-segment parts (cyc = k.r + dt dB0 + beta)
+__device__ __forceinline__ void offset_grads(float gcyc, const SegRec& q, const Spin& p, float* g, SegGrad& sg) {
+    g[G_PX] = fmaf(gcyc, q.kx, g[G_PX]);
+    g[G_PY] = fmaf(gcyc, q.ky, g[G_PY]);
+    g[G_PZ] = fmaf(gcyc, q.kz, g[G_PZ]);
+    g[G_DB0] = fmaf(gcyc, q.dt, g[G_DB0]);
+    sg.v[S_KX] += gcyc * p.px;
+    sg.v[S_KY] += gcyc * p.py;
+    sg.v[S_KZ] += gcyc * p.pz;
+    sg.v[S_BETA] += gcyc;
+    sg.v[S_DT] += gcyc * p.db0;
+}
+
+// Reverse of an RF segment from its input state (x0, y0, z0): lambda in/out, gradients accumulated.
+__device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, float e1h, float e2h, float x0, float y0,
+                                           float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
+    const float h = 0.5f * q.dt;
+    const float cyc = fmaf(q.kx, p.px, fmaf(q.ky, p.py, fmaf(q.kz, p.pz, fmaf(q.dt, p.db0, q.beta))));
+    const float wz = -BP_TWO_PI_F * cyc, wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
+    const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
+    float c, s1, s2, f1, f2;
+    rot_factors(p2, c, s1, s2, f1, f2);
+    const float a2 = 1.0f + e2h, a1 = 1.0f + e1h;
+    const float m1x = x0 * a2, m1y = y0 * a2, m1z = fmaf(z0 - p.pd, e1h, z0);
+    const float dot = fmaf(wx, m1x, fmaf(wy, m1y, wz * m1z));
+    const float cx = wy * m1z - wz * m1y, cy = wz * m1x - wx * m1z, cz = wx * m1y - wy * m1x;  // w x m1
+    const float nx = fmaf(c, m1x, fmaf(s1, cx, s2 * wx * dot));
+    const float ny = fmaf(c, m1y, fmaf(s1, cy, s2 * wy * dot));
+    const float nz = fmaf(c, m1z, fmaf(s1, cz, s2 * wz * dot));
+    // second half relaxation: m2 = (n a2, n a2, nz + (nz - pd) e1h)
+    float gd2 = fmaf(lx, nx, ly * ny), gd1 = lz * (nz - p.pd), gpd = -lz * e1h;
+    const float ax = lx * a2, ay = ly * a2, az = lz * a1;  // dL/dn
+    // rotation: b = R^T a, gw = dL/dw
+    const float wa = fmaf(wx, ax, fmaf(wy, ay, wz * az));
+    const float bx = fmaf(c, ax, fmaf(-s1, wy * az - wz * ay, s2 * wx * wa));
+    const float by = fmaf(c, ay, fmaf(-s1, wz * ax - wx * az, s2 * wy * wa));
+    const float bz = fmaf(c, az, fmaf(-s1, wx * ay - wy * ax, s2 * wz * wa));
+    const float am = fmaf(ax, m1x, fmaf(ay, m1y, az * m1z));
+    const float awm = fmaf(ax, cx, fmaf(ay, cy, az * cz));
+    const float k = fmaf(-s1, am, fmaf(f1, awm, f2 * wa * dot));
+    const float gwx = fmaf(k, wx, fmaf(s1, m1y * az - m1z * ay, s2 * fmaf(wa, m1x, dot * ax)));
+    const float gwy = fmaf(k, wy, fmaf(s1, m1z * ax - m1x * az, s2 * fmaf(wa, m1y, dot * ay)));
+    const float gwz = fmaf(k, wz, fmaf(s1, m1x * ay - m1y * ax, s2 * fmaf(wa, m1z, dot * az)));
+    // first half relaxation
+    gd2 = fmaf(bx, x0, fmaf(by, y0, gd2));
+    gd1 = fmaf(bz, z0 - p.pd, gd1);
+    gpd = fmaf(-bz, e1h, gpd);
+    lx = bx * a2, ly = by * a2, lz = bz * a1;
+    // e1h = expm1(-h r1): d/dr1 = -h (1 + e1h), d/d(dt) = -(r1 / 2)(1 + e1h)
+    g[G_R1] = fmaf(-gd1 * h, a1, g[G_R1]);
+    g[G_R2] = fmaf(-gd2 * h, a2, g[G_R2]);
+    g[G_PD] += gpd;
+    sg.v[S_DT] -= 0.5f * (gd1 * p.r1 * a1 + gd2 * p.r2 * a2);
+    g[G_B1] = fmaf(gwx, q.wx0, fmaf(gwy, q.wy0, g[G_B1]));
+    sg.v[S_WX] += gwx * p.b1;
+    sg.v[S_WY] += gwy * p.b1;
+    offset_grads(-BP_TWO_PI_F * gwz, q, p, g, sg);
+}
+
+// Reverse of a free segment (rotation about z by phi = -2 pi cyc, then exact relaxation).
+__device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, const FreeFactors& f, float x0, float y0,
+                                             float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
+    const float c = f.ch, s = f.sh, a2 = 1.0f + f.e2, a1 = 1.0f + f.e1;
+    const float ux = fmaf(c, x0, -s * y0), uy = fmaf(s, x0, c * y0);
+    const float gd2 = fmaf(lx, ux, ly * uy);
+    const float gphi = a2 * fmaf(ly, ux, -lx * uy);
+    const float nlx = a2 * fmaf(c, lx, s * ly), nly = a2 * fmaf(-s, lx, c * ly);
+    const float gd1 = lz * (z0 - p.pd);
+    g[G_PD] = fmaf(-lz, f.e1, g[G_PD]);
+    lz = lz * a1;
+    lx = nlx, ly = nly;
+    g[G_R2] = fmaf(-gd2 * q.dt, a2, g[G_R2]);
+    g[G_R1] = fmaf(-gd1 * q.dt, a1, g[G_R1]);
+    sg.v[S_DT] -= gd2 * p.r2 * a2 + gd1 * p.r1 * a1;
+    offset_grads(-BP_TWO_PI_F * gphi, q, p, g, sg);
+}
+
+template <int NCG>
+__global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
+    extern __shared__ __align__(16) float sm[];
+    float* slots = sm;                                     // [ADJ_SLOTS][3][ADJ_THREADS]
+    float* segacc = slots + ADJ_SLOTS * 3 * ADJ_THREADS;  // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
+    const int nv = 2 * a.n_coils;
+    const bool need_seg = a.gseg != nullptr;
+    for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) segacc[i] = 0.0f;
+    if (need_seg)
+        for (int i = tid; i < a.seg_len * N_SG; i += ADJ_THREADS) a.gseg[(size_t)blockIdx.x * a.seg_len * N_SG + i] = 0.0f;
+    __syncthreads();
+
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int j0 = tile * ADJ_THREADS + tid;
+        const bool active = j0 < n;
+        const int j = active ? j0 : 0;
+        const Spin p = load_spin(a.spins, n, j, active);
+        float lx = active ? a.lam[j] : 0.0f, ly = active ? a.lam[n + j] : 0.0f, lz = active ? a.lam[2 * n + j] : 0.0f;
+        float g[N_GS];
+#pragma unroll
+        for (int k = 0; k < N_GS; ++k) g[k] = 0.0f;
+        float gcr[8 * NCG], gci[8 * NCG], sr[8 * NCG], si[8 * NCG];
+#pragma unroll
+        for (int c = 0; c < 8 * NCG; ++c) {
+            gcr[c] = gci[c] = 0.0f;
+            sr[c] = active ? a.sens[(2 * c) * n + j] : 0.0f;
+            si[c] = active ? a.sens[(2 * c + 1) * n + j] : 0.0f;
+        }
+        for (int w = a.wb - 1; w >= a.wa; --w) {
+            const int4 win = a.windows[w];
+            const int nseg = win.y - win.x;
+            // recompute the window: slot k = state after segment k-1 (before its spoil), slot 0 = window start
+            const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
+            float mx = 0.f, my = 0.f, mz = 0.f, llx = 0.f, lly = 0.f, llz = 0.f;
+            if (active) {
+                mx = ws[j], my = ws[n + j], mz = ws[2 * n + j];
+                llx = ws[3 * n + j], lly = ws[4 * n + j], llz = ws[5 * n + j];
+            }
+            slots[tid] = mx + llx, slots[ADJ_THREADS + tid] = my + lly, slots[2 * ADJ_THREADS + tid] = mz + llz;
+            FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+            float e1h = 0.f, e2h = 0.f;
+            for (int s = 0; s < nseg; ++s) {
+                const SegRec q = a.segs[win.x + s];
+                if (q.flags & BP_RF) {
+                    if (s == 0 || !(q.flags & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
+                    rf_step(q, p, rr, mx, my, mz, llx, lly, llz);
+                } else {
+                    if (s == 0 || !(q.flags & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
+                    free_step(ff, p, mx, my, mz, llx, lly, llz);
+                }
+                float* sl = slots + (s + 1) * 3 * ADJ_THREADS;
+                sl[tid] = mx + llx, sl[ADJ_THREADS + tid] = my + lly, sl[2 * ADJ_THREADS + tid] = mz + llz;
+                if (q.flags & BP_SPOIL) mx = my = llx = lly = 0.0f;
+            }
+            // sweep back
+            int row = win.z + win.w;
+            int cached_free = -1, cached_rf = -1;
+            for (int s = nseg - 1; s >= 0; --s) {
+                const SegRec q = a.segs[win.x + s];
+                const int f = q.flags;
+                if (f & BP_SPOIL) lx = ly = 0.0f;
+                if ((f & BP_ADC) && a.h != nullptr) {
+                    --row;
+                    const float* hr = a.h + (size_t)row * nv;
+                    const float* out = slots + (s + 1) * 3 * ADJ_THREADS;
+                    const float ox = out[tid], oy = out[ADJ_THREADS + tid];
+                    float dx = 0.0f, dy = 0.0f;
+#pragma unroll
+                    for (int c = 0; c < 8 * NCG; ++c) {
+                        if (c < a.n_coils) {
+                            const float h0 = hr[2 * c], h1 = hr[2 * c + 1];
+                            dx = fmaf(h0, sr[c], fmaf(h1, si[c], dx));
+                            dy = fmaf(-h0, si[c], fmaf(h1, sr[c], dy));
+                            gcr[c] = fmaf(h0, ox, fmaf(h1, oy, gcr[c]));
+                            gci[c] = fmaf(-h0, oy, fmaf(h1, ox, gci[c]));
+                        }
+                    }
+                    lx += dx, ly += dy;
+                }
+                // the segment's input state: slot s, spoiled by segment s-1 if it spoils
+                const float* in = slots + s * 3 * ADJ_THREADS;
+                float x0 = in[tid], y0 = in[ADJ_THREADS + tid];
+                const float z0 = in[2 * ADJ_THREADS + tid];
+                if (s > 0 && (a.segs[win.x + s - 1].flags & BP_SPOIL)) x0 = y0 = 0.0f;
+                SegGrad sg;
+#pragma unroll
+                for (int k = 0; k < N_SG; ++k) sg.v[k] = 0.0f;
+                if (f & BP_RF) {
+                    if (cached_rf != s + 1 || !(a.segs[win.x + s + 1].flags & BP_SAME_RFDT)) {
+                        e1h = expm1f(-0.5f * q.dt * p.r1);
+                        e2h = expm1f(-0.5f * q.dt * p.r2);
+                    }
+                    cached_rf = s;
+                    rf_reverse(q, p, e1h, e2h, x0, y0, z0, lx, ly, lz, g, sg);
+                } else {
+                    if (cached_free != s + 1 || !(a.segs[win.x + s + 1].flags & BP_SAME_FREE))
+                        ff = free_factors(q, a.seg64[win.x + s], p);
+                    cached_free = s;
+                    free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
+                }
+                if (need_seg) {
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) {
+                        float v = active ? sg.v[k] : 0.0f;
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                        if (lane == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + k] = v;
+                    }
+                }
+            }
+            __syncthreads();  // segacc complete; every thread is done reading this window's slots
+            if (need_seg) {
+                float* dst = a.gseg + ((size_t)blockIdx.x * a.seg_len + (win.x - a.seg0)) * N_SG;
+                for (int i = tid; i < nseg * N_SG; i += ADJ_THREADS) {
+                    float t = 0.0f;
+#pragma unroll
+                    for (int ww = 0; ww < ADJ_WARPS; ++ww) t += segacc[ww * BP_ADJ_WIN * N_SG + i];
+                    dst[i] += t;
+                }
+            }
+            // per-spin gradients flushed at every window end: windows fall on multiples of BP_ADJ_WIN segments
+            // whatever the checkpoint interval, so the sums (and the result) do not depend on it
+            if (active) {
+#pragma unroll
+                for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] += g[k], g[k] = 0.0f;
+                if (a.gc != nullptr) {
+#pragma unroll
+                    for (int c = 0; c < 8 * NCG; ++c) {
+                        if (c < a.n_coils) {
+                            a.gc[(2 * c) * n + j] += gcr[c];
+                            a.gc[(2 * c + 1) * n + j] += gci[c];
+                        }
+                        gcr[c] = gci[c] = 0.0f;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (active) a.lam[j] = lx, a.lam[n + j] = ly, a.lam[2 * n + j] = lz;
+    }
+}
+
+// SEG[seg0 + s][k] += sum over CTAs (in order) of gseg[cta][s][k], in float64
+__global__ void bp_seg_reduce_kernel(const float* __restrict__ gseg, int n_cta, int seg_len, int seg0,
+                                     double* __restrict__ seg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= seg_len * N_SG) return;
+    double t = 0.0;
+    for (int c = 0; c < n_cta; ++c) t += (double)gseg[(size_t)c * seg_len * N_SG + i];
+    seg[(size_t)seg0 * N_SG + i] += t;
+}
+
+template <int NCG>
+static size_t adj_smem() {
+    return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float);
+}
+
+template <int NCG>
+static int adj_grid(int n) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    static bool configured[64] = {false};
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)adj_smem<NCG>()) != cudaSuccess)
+            return -1;
+        configured[dev] = true;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG>, ADJ_THREADS, adj_smem<NCG>()) !=
+        cudaSuccess)
+        return -1;
+    const int n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
+    int grid = sms * (per_sm > 0 ? per_sm : 1);
+    return grid < n_tiles ? grid : n_tiles;
+}
+
+extern "C" int bp_adjoint_grid(int n, int n_coils) {
+    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS) return -BP_E_ARG;
+    switch ((n_coils + 7) / 8) {
+        case 1: return adj_grid<1>(n);
+        case 2: return adj_grid<2>(n);
+        case 3: return adj_grid<3>(n);
+        default: return adj_grid<4>(n);
+    }
+}
+
+template <int NCG>
+static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
+    bp_adjoint_kernel<NCG><<<grid, ADJ_THREADS, adj_smem<NCG>(), st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                          const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                          const float* wstates, const float* h, float* lam, float* gs, float* gc, float* gseg,
+                          int grid, void* stream) {
+    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg_len < 0 || grid < 1)
+        return BP_E_ARG;
+    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs) return BP_E_ARG;
+    if (wb == wa) return BP_OK;
+    AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
+              reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, lam, gs, gc,
+              gseg};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch ((n_coils + 7) / 8) {
+        case 1: return launch_adj<1>(a, grid, st);
+        case 2: return launch_adj<2>(a, grid, st);
+        case 3: return launch_adj<3>(a, grid, st);
+        default: return launch_adj<4>(a, grid, st);
+    }
+}
+
+extern "C" int bp_seg_reduce(const float* gseg, int n_cta, int seg_len, int seg0, double* seg, void* stream) {
+    if (!gseg || !seg || n_cta < 1 || seg_len < 0 || seg0 < 0) return BP_E_ARG;
+    if (seg_len == 0) return BP_OK;
+    const int total = seg_len * N_SG, threads = 256;
+    bp_seg_reduce_kernel<<<(total + threads - 1) / threads, threads, 0, static_cast<cudaStream_t>(stream)>>>(
+        gseg, n_cta, seg_len, seg0, seg);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}

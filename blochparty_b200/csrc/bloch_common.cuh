@@ -95,19 +95,43 @@ __device__ __forceinline__ void rotate_inc(float wx, float wy, float wz, float& 
     two_sum(mz, lz, fmaf(s1, cz, s2 * dz));
 }
 
-// An RF segment with the half-step relaxation increments e1h = expm1(-dt r1 / 2), e2h = expm1(-dt r2 / 2).
-__device__ __forceinline__ void rf_step(const SegRec& q, const Spin& p, float e1h, float e2h, float& mx, float& my,
+// Relaxation factors of an RF segment's two half steps (dt/2 each): e = expm1(-dt r / 2), a = 1 + e, and for the
+// composed segment d = a^2 - 1 = e (2 + e); cz2 = (a1 + 1)(-pd e1h), the recovery term of both halves.
+struct RfRelax {
+    float a1, a2, d1, d2, e1h, cz2;
+};
+
+__device__ __forceinline__ RfRelax rf_relax(float dt, const Spin& p) {
+    RfRelax r;
+    r.e1h = expm1f(-0.5f * dt * p.r1);
+    const float e2h = expm1f(-0.5f * dt * p.r2);
+    r.a1 = 1.0f + r.e1h;
+    r.a2 = 1.0f + e2h;
+    r.d1 = r.e1h * (2.0f + r.e1h);
+    r.d2 = e2h * (2.0f + e2h);
+    r.cz2 = -(r.a1 + 1.0f) * p.pd * r.e1h;
+    return r;
+}
+
+// An RF segment: relax dt/2 (m1 = E m + c, E = diag(a2, a2, a1), c = (0, 0, -pd e1h)), rotate about w (n = R m1),
+// relax dt/2 (E n + c), composed into one increment of m: (E E - I) m + E (R - I) m1 + (E + I) c, with
+// (R - I) m1 = s1 (w x m1) + s2 w x (w x m1). The increment is small next to m and computed from m directly,
+// so one two-sum per component (instead of one per sub-step) keeps the float32 state compensated.
+__device__ __forceinline__ void rf_step(const SegRec& q, const Spin& p, const RfRelax& r, float& mx, float& my,
                                         float& mz, float& lx, float& ly, float& lz) {
     const float cyc = fmaf(q.kx, p.px, fmaf(q.ky, p.py, fmaf(q.kz, p.pz, fmaf(q.dt, p.db0, q.beta))));
     const float wz = -BP_TWO_PI_F * cyc;
     const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
-    two_sum(mx, lx, mx * e2h);
-    two_sum(my, ly, my * e2h);
-    two_sum(mz, lz, (mz - p.pd) * e1h);
-    rotate_inc(wx, wy, wz, mx, my, mz, lx, ly, lz);
-    two_sum(mx, lx, mx * e2h);
-    two_sum(my, ly, my * e2h);
-    two_sum(mz, lz, (mz - p.pd) * e1h);
+    const float m1x = mx * r.a2, m1y = my * r.a2, m1z = fmaf(-p.pd, r.e1h, mz * r.a1);
+    const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
+    float s1, s2;
+    rodrigues_coeffs(p2, s1, s2);
+    const float cx = wy * m1z - wz * m1y, cy = wz * m1x - wx * m1z, cz = wx * m1y - wy * m1x;
+    const float dx = wy * cz - wz * cy, dy = wz * cx - wx * cz, dz = wx * cy - wy * cx;
+    const float qx = fmaf(s1, cx, s2 * dx), qy = fmaf(s1, cy, s2 * dy), qz = fmaf(s1, cz, s2 * dz);
+    two_sum(mx, lx, fmaf(r.d2, mx, r.a2 * qx));
+    two_sum(my, ly, fmaf(r.d2, my, r.a2 * qy));
+    two_sum(mz, lz, fmaf(r.d1, mz, fmaf(r.a1, qz, r.cz2)));
 }
 
 // Free-precession factors of one segment: the rotation (c, s) by -2 pi (k.r + dt dB0 + beta), evaluated in

@@ -11,9 +11,10 @@
 //    spin per thread). For every window it stages the window's segment records into shared memory with one
 //    TMA bulk copy (double-buffered: window w+1 is in flight while window w runs), then runs each of its tiles
 //    through the window: the tile's state is loaded from HBM, propagated in registers, and stored back.
-//  * ADC samples: each warp forms the 2C coil products of its 32 spins and reduces them by warp shuffles
-//    (butterfly reduce-scatter) into its own slice of a per-window accumulator in shared memory, summed over
-//    all of the CTA's tiles. At the window's end the warps' slices are added in fixed order and the CTA's
+//  * ADC samples: each warp stages the (mx, my) of its 32 spins for 16 samples in shared memory, then contracts
+//    them with the spins' coil sensitivities (an FMA chain over the 32 spins per lane: a small matrix product)
+//    into its own slice of a per-window accumulator in shared memory, summed over all of the CTA's tiles. At
+//    the window's end the warps' slices are added in fixed order and the CTA's
 //    partial is added to the float64 signal with one float64 atomic per (sample, coil, re/im): the cross-block
 //    sum is float64, and the CTA-level sum covers thousands of spins, so the number of atomics does not grow
 //    with the spin count.
@@ -29,6 +30,8 @@
 #define BP_THREADS 128
 #define BP_WARPS (BP_THREADS / 32)
 #define BP_ACC_SAMPLES 64  // accumulator capacity in samples at 8 coils (one coil group)
+#define BP_STAGE 16        // samples staged per warp before they are contracted
+#define BP_MB_STRIDE 33    // float2 per staged sample row (32 spins + 1: conflict-free column reads)
 
 struct FwdArgs {
     const float* spins;   // [8][n]: px py pz pd r1 r2 db0 b1
@@ -50,19 +53,68 @@ __host__ __device__ constexpr int samp_max() {
     return BP_ACC_SAMPLES / NCG;
 }
 
+// The warp's staged samples (mb: [BP_STAGE][BP_MB_STRIDE] (mx, my) of its 32 spins) contracted with the coil
+// sensitivities of those spins (st: [32][16 NCG], coil c real at 2c, imaginary at 2c + 1) and added to the warp's
+// accumulator rows acc[row0 + s]. Lane l computes sample l & 15, coils 4 (l >> 4) .. + 3 of every coil group:
+// a chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles).
+template <int NCG>
+__device__ __forceinline__ void warp_contract(const float2* mb, const float* st, int nslot, float* acc, int row0,
+                                              int lane) {
+    constexpr int VG = 16 * NCG;
+    const int smp = lane & 15, half = lane >> 4;
+    if (smp >= nslot) return;
+    const float2* row = mb + smp * BP_MB_STRIDE;
+#pragma unroll
+    for (int g = 0; g < NCG; ++g) {
+        float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 8
+        for (int j = 0; j < 32; ++j) {
+            const float2 m = row[j];
+            const float4* sj = reinterpret_cast<const float4*>(st + j * VG + 16 * g + 8 * half);
+            const float4 a = sj[0], b = sj[1];  // (r0 i0 r1 i1), (r2 i2 r3 i3)
+            re[0] = fmaf(m.x, a.x, fmaf(-m.y, a.y, re[0]));
+            im[0] = fmaf(m.x, a.y, fmaf(m.y, a.x, im[0]));
+            re[1] = fmaf(m.x, a.z, fmaf(-m.y, a.w, re[1]));
+            im[1] = fmaf(m.x, a.w, fmaf(m.y, a.z, im[1]));
+            re[2] = fmaf(m.x, b.x, fmaf(-m.y, b.y, re[2]));
+            im[2] = fmaf(m.x, b.y, fmaf(m.y, b.x, im[2]));
+            re[3] = fmaf(m.x, b.z, fmaf(-m.y, b.w, re[3]));
+            im[3] = fmaf(m.x, b.w, fmaf(m.y, b.z, im[3]));
+        }
+        float4* dst = reinterpret_cast<float4*>(acc + (row0 + smp) * VG + 16 * g + 8 * half);
+        float4 d0 = dst[0], d1 = dst[1];
+        d0.x += re[0], d0.y += im[0], d0.z += re[1], d0.w += im[1];
+        d1.x += re[2], d1.y += im[2], d1.z += re[3], d1.w += im[3];
+        dst[0] = d0, dst[1] = d1;
+    }
+}
+
+template <int NCG>
+__host__ __device__ constexpr size_t fwd_smem_bytes_t() {
+    return 2 * BP_SEG_MAX * sizeof(SegRec)                                   // segment blocks
+           + (size_t)BP_WARPS * samp_max<NCG>() * 16 * NCG * sizeof(float)   // window accumulators
+           + (size_t)BP_WARPS * BP_STAGE * BP_MB_STRIDE * sizeof(float2)     // staged samples
+           + (size_t)BP_WARPS * 32 * 16 * NCG * sizeof(float)                // coil sensitivities of the tile
+           + 2 * sizeof(uint64_t);
+}
+
 template <int NCG>
 __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    SegRec* segbuf = reinterpret_cast<SegRec*>(smem_raw);                      // [2][BP_SEG_MAX]
-    float* acc = reinterpret_cast<float*>(segbuf + 2 * BP_SEG_MAX);            // [WARPS][samp_max][16 NCG]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(acc + BP_WARPS * samp_max<NCG>() * 16 * NCG);
+    constexpr int VG = 16 * NCG;  // accumulator values per sample (coil groups of 8, padded)
+    SegRec* segbuf = reinterpret_cast<SegRec*>(smem_raw);                                   // [2][BP_SEG_MAX]
+    float* acc = reinterpret_cast<float*>(segbuf + 2 * BP_SEG_MAX);                         // [W][samp][VG]
+    float2* mball = reinterpret_cast<float2*>(acc + BP_WARPS * samp_max<NCG>() * VG);       // [W][16][33]
+    float* stall = reinterpret_cast<float*>(mball + BP_WARPS * BP_STAGE * BP_MB_STRIDE);    // [W][32][VG]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stall + BP_WARPS * 32 * VG);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n;
     const int n_tiles = (n + BP_THREADS - 1) / BP_THREADS;
     const int nv = 2 * a.n_coils;
-    constexpr int VG = 16 * NCG;  // accumulator values per sample (coil groups of 8, padded)
     float* my_acc = acc + warp * samp_max<NCG>() * VG;
+    float2* mb = mball + warp * BP_STAGE * BP_MB_STRIDE;
+    float* st = stall + warp * 32 * VG;
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -114,53 +166,45 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
                     ws[3 * n + j] = lx, ws[4 * n + j] = ly, ws[5 * n + j] = lz;
                 }
             }
-            float sr[8], si[8];
+            if (readout) {  // this spin's coil sensitivities into the warp's tile (inactive lanes: zeros)
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                sr[c] = (readout && active) ? a.sens[(2 * c) * n + j] : 0.0f;
-                si[c] = (readout && active) ? a.sens[(2 * c + 1) * n + j] : 0.0f;
+                for (int k = 0; k < VG; k += 4) {
+                    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (active) v = make_float4(a.sens[k * n + j], a.sens[(k + 1) * n + j], a.sens[(k + 2) * n + j],
+                                                a.sens[(k + 3) * n + j]);
+                    *reinterpret_cast<float4*>(st + lane * VG + k) = v;
+                }
+                __syncwarp();
             }
             FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            float e1h = 0.f, e2h = 0.f;
-            int row = 0;
+            RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+            int slot = 0, row0 = 0;
             for (int s = 0; s < nseg; ++s) {
                 const SegRec q = q0[s];
                 const int f = q.flags;
                 if (f & BP_RF) {
-                    if (s == 0 || !(f & BP_SAME_RFDT)) {
-                        e1h = expm1f(-0.5f * q.dt * p.r1);
-                        e2h = expm1f(-0.5f * q.dt * p.r2);
-                    }
-                    rf_step(q, p, e1h, e2h, mx, my, mz, lx, ly, lz);
+                    if (s == 0 || !(f & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
+                    rf_step(q, p, rr, mx, my, mz, lx, ly, lz);
                 } else {
                     if (s == 0 || !(f & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
                     free_step(ff, p, mx, my, mz, lx, ly, lz);
                 }
                 if ((f & BP_ADC) && readout) {
-                    const float ax = mx + lx, ay = my + ly;
-                    float* dst = my_acc + row * VG;
-#pragma unroll
-                    for (int g = 0; g < NCG; ++g) {
-                        float v[16];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {
-                            float r_, i_;
-                            if (g == 0) {
-                                r_ = sr[c];
-                                i_ = si[c];
-                            } else {
-                                r_ = active ? a.sens[(16 * g + 2 * c) * n + j] : 0.0f;
-                                i_ = active ? a.sens[(16 * g + 2 * c + 1) * n + j] : 0.0f;
-                            }
-                            v[2 * c] = fmaf(ax, r_, -ay * i_);
-                            v[2 * c + 1] = fmaf(ax, i_, ay * r_);
-                        }
-                        const float t = warp_reduce_scatter16(v, lane);
-                        if (!(lane & 1)) dst[16 * g + ((lane >> 1) & 15)] += t;
+                    mb[slot * BP_MB_STRIDE + lane] = make_float2(mx + lx, my + ly);
+                    if (++slot == BP_STAGE) {
+                        __syncwarp();
+                        warp_contract<NCG>(mb, st, BP_STAGE, my_acc, row0, lane);
+                        __syncwarp();
+                        row0 += BP_STAGE;
+                        slot = 0;
                     }
-                    ++row;
                 }
                 if (f & BP_SPOIL) mx = my = lx = ly = 0.0f;
+            }
+            if (slot > 0) {
+                __syncwarp();
+                warp_contract<NCG>(mb, st, slot, my_acc, row0, lane);
+                __syncwarp();
             }
             if (active) {
                 a.state[j] = mx;
@@ -205,8 +249,7 @@ __global__ void bp_signal_finish_kernel(const double* __restrict__ raw, const do
 // ---- launch helpers ----
 template <int NCG>
 static size_t fwd_smem_bytes() {
-    return 2 * BP_SEG_MAX * sizeof(SegRec) + (size_t)BP_WARPS * samp_max<NCG>() * 16 * NCG * sizeof(float) +
-           2 * sizeof(uint64_t);
+    return fwd_smem_bytes_t<NCG>();
 }
 
 static int g_num_sms[64];
@@ -289,8 +332,9 @@ extern "C" int bp_forward(const float* spins, const float* sens, int n, int n_co
 
 extern "C" int bp_signal_finish(const double* raw, const double* psi, int n_adc, int n_coils, void* out,
                                 void* stream) {
-    if (n_adc < 0 || n_coils < 1 || !raw || !psi || !out) return BP_E_ARG;
+    if (n_adc < 0 || n_coils < 1) return BP_E_ARG;
     if (n_adc == 0) return BP_OK;
+    if (!raw || !psi || !out) return BP_E_ARG;
     const int64_t total = (int64_t)n_adc * n_coils;
     const int threads = 256;
     const int64_t blocks = (total + threads - 1) / threads;

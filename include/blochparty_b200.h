@@ -27,7 +27,8 @@ extern "C" {
 #define BP_E_SIZE 4     /* a size above a documented maximum */
 
 #define BP_MAX_COILS 32 /* receive coils of the float32 readout */
-#define BP_SEG_MAX 512  /* segments per window (one TMA-staged block) */
+#define BP_SEG_MAX 240  /* segments per window (one TMA-staged block; four CTAs per SM fit in shared memory) */
+#define BP_ADJ_WIN 32   /* segments per adjoint window (recomputed into shared memory) */
 
 /* Window planner (host code, no GPU): cuts `n_segments` segments with per-segment `flags` (bit 1 RF, 2 ADC,
  * 4 spoil) into consecutive windows of at most `seg_max` (<= BP_SEG_MAX) segments and `samp_max` ADC samples;
@@ -59,6 +60,30 @@ int bp_forward(const float* spins, const float* sens, int n, int n_coils, const 
 /* signal[c][t] = raw[t][c] exp(-i psi[t]) in float64, written as complex64 (interleaved float pairs), shape
  * (n_coils, n_adc) (replaces the host-side assembly engines/gpu/driver.py:699-702). */
 int bp_signal_finish(const double* raw, const double* psi, int n_adc, int n_coils, void* out, void* stream);
+
+/* Grid (persistent CTAs) that bp_adjoint uses for n spins: size the first dimension of its `gseg` scratch with
+ * it. Negative on error. */
+int bp_adjoint_grid(int n, int n_coils);
+
+/* Reverse sweep of one checkpoint interval (replaces bloch_adjoint_c<NC>, engines/gpu/cuda/adjoint.cu.in:5-121,
+ * with the per-segment reverse of shaders/adjoint_common.metal:212-315). `windows` are adjoint windows (at most
+ * BP_ADJ_WIN segments, boundaries on multiples of BP_ADJ_WIN), [wa, wb) the interval's, covering segments
+ * [seg0, seg0 + seg_len).
+ *   wstates [wb - wa][6][n] the state at every window start (bp_forward replay of the interval, stride 1)
+ *   h       [n_adc][2C] float32 dL/d(raw coil sums) = dL/dsignal rotated by exp(+i psi), or NULL
+ *   lam     [3][n] in: dL/dm after the interval; out: dL/dm before it
+ *   gs      [8][n] += dL/d(x, y, z, dB0, pd, r1, r2, b1)
+ *   gc      [2C][n] += dL/d(coil c real, imaginary) at rows 2c, 2c+1, or NULL
+ *   gseg    [grid][seg_len][8] scratch: per-CTA segment gradients (w.r.t. the record's dt, -2 pi dt rf_x,
+ *           -2 pi dt rf_y, g dt (3), b0_offset dt), or NULL when no segment gradient is wanted
+ *   grid    bp_adjoint_grid(n, n_coils) */
+int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
+               const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates, const float* h,
+               float* lam, float* gs, float* gc, float* gseg, int grid, void* stream);
+
+/* seg[seg0 + s][k] += sum over the `n_cta` CTAs, in CTA order, of gseg[cta][s][k], in float64 (replaces
+ * seg_reduce, engines/gpu/cuda/seg_reduce.cu:3-11). `seg` is [S][8] float64. */
+int bp_seg_reduce(const float* gseg, int n_cta, int seg_len, int seg0, double* seg, void* stream);
 
 /* Measurement kernel (the roofline denominator): 4 CTAs x 256 threads per SM, each thread `iters` x 128
  * independent FFMAs; `*flops` receives the flop count of the launch, which the caller divides by the launch's

@@ -1,0 +1,146 @@
+"""Gradients through the hand-written adjoint on the GPU (``simulate`` with inputs that require grad).
+
+Mirrors blochparty ``tests/engines/test_gpu_grad.py``: every input's gradient of a fixed random-weight linear loss
+against the float64 core's autograd (golden fixtures written by the reference itself, and the float64 oracle),
+the per-TR flip train of the 2D 128^2 adjoint workload against central finite differences, and bit-identical
+gradients for any ``checkpoint_every`` and across runs (blochparty test_gpu_grad.py:95-102).
+Tolerances: largest relative error (max-norm) per input 2e-4, the reference engines' gradient tolerance
+(blochparty tests/engines/test_engines.py:47 GRAD_TOL).
+"""
+
+from dataclasses import replace
+
+import numpy as np
+import pytest
+import torch
+
+import blochparty_b200 as bpb
+from blochparty_b200 import workloads
+from golden_cases import load, objects
+from oracle import bloch
+
+pytestmark = pytest.mark.gpu
+F64 = torch.float64
+GRAD_TOL = 2e-4
+
+NAMES = ("pos", "pd", "t1", "t2", "db0", "b1", "coils", "dt", "rf", "grad", "adc_phase", "b0_offset", "m_init")
+
+
+def rel(a, b):
+    a = a.to(b.dtype)
+    s = b.abs().max()
+    return float((a - b).abs().max() / s) if s > 0 else float((a - b).abs().max())
+
+
+def gpu_gradients(ph, seq, coils, m_init, loss_fn, names=NAMES, **kw):
+    leaves = {}
+
+    def leaf(k, t):
+        if t is None or k not in names:
+            return t
+        t = t.detach().clone().requires_grad_()
+        leaves[k] = t
+        return t
+
+    gph = bpb.Phantom(leaf("pos", ph.pos), leaf("pd", ph.pd), leaf("t1", ph.t1), leaf("t2", ph.t2),
+                      leaf("db0", ph.db0), b1=leaf("b1", ph.b1))
+    gseq = bpb.Sequence(leaf("dt", seq.dt), leaf("rf", seq.rf), leaf("grad", seq.grad),
+                        leaf("adc_phase", seq.adc_phase), list(seq.is_rf), list(seq.adc), list(seq.spoil),
+                        b0_offset=leaf("b0_offset", seq.b0_offset))
+    r = bpb.simulate(gph, gseq, leaf("coils", coils), m_init=leaf("m_init", m_init), **kw)
+    loss = loss_fn(r.signal, r.m)
+    grads = torch.autograd.grad(loss, list(leaves.values()), allow_unused=True)
+    return float(loss), {k: g for k, g in zip(leaves, grads)}
+
+
+@pytest.mark.parametrize("name", ["grad_rand", "grad_busy"])
+def test_gradients_match_reference_autograd(name):
+    case, _, _, z = load(name)
+    ph, seq, coils, m_init = objects(case)
+    wr, wi, wm = (torch.from_numpy(z[k]) for k in ("w_re", "w_im", "w_m"))
+    loss = lambda s, m: (s.real.double() * wr).sum() + (s.imag.double() * wi).sum() + (m.double() * wm).sum()
+    _, g = gpu_gradients(ph, seq, coils, m_init, loss)
+    errors = {}
+    for k, v in g.items():
+        if v is None:
+            continue
+        ref = (torch.complex(torch.from_numpy(z[f"grad_{k}_re"]), torch.from_numpy(z[f"grad_{k}_im"]))
+               if k == "coils" else torch.from_numpy(z[f"grad_{k}"]))
+        errors[k] = rel(v, ref)
+    assert len(errors) >= 11, errors
+    assert max(errors.values()) < GRAD_TOL, errors
+
+
+def _adjoint_case(n=32):
+    ph, seq, coils, flips, t1_target = workloads.adjoint_2d_128(n)
+    return ph, seq, coils, flips, t1_target
+
+
+def _target(ph, seq, coils, t1_target):
+    with torch.no_grad():
+        return bpb.simulate(replace(ph, t1=t1_target), seq, coils).signal.to(torch.complex128)
+
+
+def test_adjoint_workload_against_oracle_autograd():
+    """The 2D adjoint workload (32^2 here): squared L2 distance to the signal of a perturbed T1 map; gradients
+    w.r.t. T1, T2, PD, B0, B1, the coils and the RF (flip train) against the float64 oracle's autograd."""
+    ph, seq, coils, flips, t1_target = _adjoint_case(32)
+    target = _target(ph, seq, coils, t1_target)
+    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum()
+    names = ("pd", "t1", "t2", "db0", "b1", "coils", "rf")
+    _, g = gpu_gradients(ph, seq, coils, None, loss, names, checkpoint_every=8 * 32)
+    case = bloch.case_from(ph, seq, coils)
+    _, ref = bloch.gradients(case, lambda s, m: ((s - target).abs() ** 2).sum(), names=names)
+    errors = {k: rel(g[k], ref[k]) for k in names}
+    print("adjoint 32^2 relative errors:", {k: f"{v:.1e}" for k, v in errors.items()})
+    assert max(errors.values()) < GRAD_TOL, errors
+
+
+def test_flip_train_against_central_differences():
+    """d loss / d flip_j through the per-TR RF amplitudes, against central differences of the GPU forward
+    (h = 1e-3 relative); the float32 forward limits the agreement to ~1e-3."""
+    ph, seq, coils, flips, t1_target = _adjoint_case(16)
+    target = _target(ph, seq, coils, t1_target)
+    rf_idx = np.flatnonzero(np.asarray(seq.is_rf))
+    assert len(rf_idx) == len(flips)
+
+    def with_flips(f):
+        rf = seq.rf.clone()
+        rf[rf_idx] = seq.rf[rf_idx] * (f / flips)[:, None]
+        return replace(seq, rf=rf)
+
+    def loss_of(f):
+        with torch.no_grad():
+            s = bpb.simulate(ph, with_flips(f), coils).signal.to(torch.complex128)
+        return float(((s - target).abs() ** 2).sum())
+
+    f = flips.clone().requires_grad_()
+    r = bpb.simulate(ph, with_flips(f), coils)
+    loss = ((r.signal.to(torch.complex128) - target).abs() ** 2).sum()
+    (g,) = torch.autograd.grad(loss, [f])
+    for j in (0, 3, len(flips) // 2, len(flips) - 1):
+        h = 1e-3 * float(flips[j])
+        fp, fm = flips.clone(), flips.clone()
+        fp[j] += h
+        fm[j] -= h
+        fd = (loss_of(fp) - loss_of(fm)) / (2 * h)
+        assert abs(float(g[j]) - fd) <= 2e-3 * abs(fd) + 1e-6 * float(loss), (j, float(g[j]), fd)
+
+
+def test_gradients_do_not_depend_on_checkpoint_interval():
+    ph, seq, coils, flips, t1_target = _adjoint_case(16)
+    target = _target(ph, seq, coils, t1_target)
+    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum() + m.double().sum()
+    names = ("pd", "t1", "t2", "db0", "b1", "coils", "rf", "dt", "grad")
+    _, a = gpu_gradients(ph, seq, coils, None, loss, names, checkpoint_every=64)
+    _, b = gpu_gradients(ph, seq, coils, None, loss, names, checkpoint_every=32 * 50)
+    _, c = gpu_gradients(ph, seq, coils, None, loss, names, checkpoint_every=32 * 50)
+    for k in names:
+        assert torch.equal(a[k], b[k]), k
+        assert torch.equal(b[k], c[k]), k
+
+
+def test_checkpoint_every_must_be_window_multiple():
+    ph, seq, coils, _, _ = _adjoint_case(8)
+    with pytest.raises(ValueError, match="multiple of 32"):
+        bpb.simulate(replace(ph, t1=ph.t1.clone().requires_grad_()), seq, coils, checkpoint_every=48)
