@@ -48,13 +48,14 @@ def test_planner_breaks_and_errors():
     flags = np.zeros(10, np.int32)
     br = np.zeros(10, np.uint8)
     br[[3, 7]] = 1
-    w = engine.plan_windows(flags, 4, seg_max=512, breaks=br)
+    w = engine.plan_windows(flags, 4, seg_max=_lib.BP_SEG_MAX, breaks=br)
     assert w[:, 0].tolist() == [0, 3, 7]
     lib = _lib.lib()
     out = np.zeros((1, 4), np.int32)
     nw = np.zeros(1, np.int64)
     assert lib.bp_plan_windows(flags.ctypes.data, 10, 4, 4, None, out.ctypes.data, 1, nw.ctypes.data) == _lib.BP_E_SIZE
-    assert lib.bp_plan_windows(flags.ctypes.data, 10, 513, 4, None, out.ctypes.data, 9, nw.ctypes.data) == _lib.BP_E_ARG
+    assert lib.bp_plan_windows(flags.ctypes.data, 10, _lib.BP_SEG_MAX + 1, 4, None, out.ctypes.data, 9,
+                               nw.ctypes.data) == _lib.BP_E_ARG
     assert lib.bp_forward_samp_max(8) > 0 and lib.bp_forward_samp_max(33) == 0 and lib.bp_forward_samp_max(0) == 0
 
 
