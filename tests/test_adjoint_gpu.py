@@ -50,7 +50,7 @@ def gpu_gradients(ph, seq, coils, m_init, loss_fn, names=NAMES, **kw):
     r = bpb.simulate(gph, gseq, leaf("coils", coils), m_init=leaf("m_init", m_init), **kw)
     loss = loss_fn(r.signal, r.m)
     grads = torch.autograd.grad(loss, list(leaves.values()), allow_unused=True)
-    return float(loss), {k: g for k, g in zip(leaves, grads)}
+    return float(loss.detach()), {k: g for k, g in zip(leaves, grads)}
 
 
 @pytest.mark.parametrize("name", ["grad_rand", "grad_busy"])
@@ -81,19 +81,37 @@ def _target(ph, seq, coils, t1_target):
         return bpb.simulate(replace(ph, t1=t1_target), seq, coils).signal.to(torch.complex128)
 
 
-def test_adjoint_workload_against_oracle_autograd():
-    """The 2D adjoint workload (32^2 here): squared L2 distance to the signal of a perturbed T1 map; gradients
-    w.r.t. T1, T2, PD, B0, B1, the coils and the RF (flip train) against the float64 oracle's autograd."""
+def test_adjoint_workload_vjp_against_oracle():
+    """The 2D adjoint workload (32^2 here) with its cotangent fixed: d/dtheta of Re sum conj(w) s, where w is the
+    GPU's own residual 2 (s - s_target) (so both sides differentiate the same linear form), w.r.t. T1, T2, PD, B0,
+    B1, the coils and the RF train, against the float64 oracle's autograd; the bar is the engines' 2e-4."""
     ph, seq, coils, flips, t1_target = _adjoint_case(32)
     target = _target(ph, seq, coils, t1_target)
-    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum()
+    with torch.no_grad():
+        w = 2 * (bpb.simulate(ph, seq, coils).signal.to(torch.complex128) - target)
+    loss = lambda s, m: (s.to(torch.complex128) * w.conj()).real.sum()
     names = ("pd", "t1", "t2", "db0", "b1", "coils", "rf")
     _, g = gpu_gradients(ph, seq, coils, None, loss, names, checkpoint_every=8 * 32)
-    case = bloch.case_from(ph, seq, coils)
-    _, ref = bloch.gradients(case, lambda s, m: ((s - target).abs() ** 2).sum(), names=names)
+    _, ref = bloch.gradients(bloch.case_from(ph, seq, coils), loss, names=names)
     errors = {k: rel(g[k], ref[k]) for k in names}
-    print("adjoint 32^2 relative errors:", {k: f"{v:.1e}" for k, v in errors.items()})
+    print("\nadjoint 32^2 fixed-cotangent relative errors:", {k: f"{v:.1e}" for k, v in errors.items()})
     assert max(errors.values()) < GRAD_TOL, errors
+
+
+def test_adjoint_workload_loss_against_oracle_autograd():
+    """The workload's own loss, ||s - s_target||^2 with s_target from T1 (1 + 5% noise): both sides use their own
+    forward, so the float32 forward's ~1e-6 relative error enters the small residual (a few % of s) and is
+    amplified ~30x in every gradient; bounded at 2e-3 here (the reference's integration test allows 3e-3 on
+    flip and B1 gradients, blochparty tests/engines/test_integration.py:38-53)."""
+    ph, seq, coils, flips, t1_target = _adjoint_case(32)
+    target = _target(ph, seq, coils, t1_target)
+    names = ("pd", "t1", "t2", "db0", "b1", "coils", "rf")
+    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum()
+    _, g = gpu_gradients(ph, seq, coils, None, loss, names, checkpoint_every=8 * 32)
+    _, ref = bloch.gradients(bloch.case_from(ph, seq, coils), loss, names=names)
+    errors = {k: rel(g[k], ref[k]) for k in names}
+    print("\nadjoint 32^2 workload-loss relative errors:", {k: f"{v:.1e}" for k, v in errors.items()})
+    assert max(errors.values()) < 2e-3, errors
 
 
 def test_flip_train_against_central_differences():
