@@ -18,6 +18,7 @@ BP_OK, BP_E_ARG, BP_E_ALIGN, BP_E_LAUNCH, BP_E_SIZE = 0, 1, 2, 3, 4
 BP_MAX_COILS = 32
 BP_SEG_MAX = 240
 BP_ADJ_WIN = 32
+BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",
@@ -35,6 +36,8 @@ SIGNATURES = {
     "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P,
                            c_int, _P]),
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
+    "bp_adjoint_noalloc": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P,
+                                   _P, _P]),
 }
 
 _lib = None

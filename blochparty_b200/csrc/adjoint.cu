@@ -371,3 +371,57 @@ extern "C" int bp_seg_reduce(const float* gseg, int n_cta, int seg_len, int seg0
         gseg, n_cta, seg_len, seg0, seg);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
+
+// ---- The adjoint sweep for callers that cannot allocate device memory ----
+//
+// bp_adjoint needs a scratch buffer for its per-CTA segment gradients (`gseg`), which its callers allocate. Some
+// callers of this library cannot: a host runtime that hands the library a fixed set of buffers sized at start-up
+// and forbids allocation while it runs, or a foreign-language binding (Go, Java, JavaScript) that passes device
+// pointers in but has no way to call cudaMalloc; and cudaFree synchronises the whole device, which such callers
+// must not trigger. For them this variant keeps that scratch in a file-scope array in device memory, so the call
+// allocates nothing. The array is BP_NOALLOC_SCRATCH_FLOATS floats (8 MiB); every GPU that loads the library
+// holds it until the process exits.
+#define BP_NOALLOC_SCRATCH_FLOATS (2 * 1024 * 1024)
+
+static __device__ __align__(256) float bp_noalloc_scratch[BP_NOALLOC_SCRATCH_FLOATS];
+
+// Device address of the array per device, looked up once with that device current (in host code the array's
+// name is only a host-side stand-in, not a device address).
+static float* g_noalloc_ptr[64];
+
+static int noalloc_scratch(float** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BP_E_LAUNCH;
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, bp_noalloc_scratch) != cudaSuccess || p == nullptr) return BP_E_LAUNCH;
+        g_noalloc_ptr[dev] = static_cast<float*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return BP_OK;
+}
+
+extern "C" int bp_adjoint_noalloc(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                                  const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                                  const float* wstates, const float* h, float* lam, float* gs, float* gc, double* seg,
+                                  void* stream) {
+    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg_len < 0 || seg0 < 0)
+        return BP_E_ARG;
+    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs) return BP_E_ARG;
+    // one CTA needs seg_len * N_SG floats of the array; more CTAs share it up to its size
+    const long long per_cta = (long long)seg_len * N_SG;
+    if (seg && per_cta > BP_NOALLOC_SCRATCH_FLOATS) return BP_E_SIZE;
+    if (wb == wa) return BP_OK;
+    float* scratch = nullptr;
+    int code = noalloc_scratch(&scratch);
+    if (code != BP_OK) return code;
+    int grid = bp_adjoint_grid(n, n_coils);
+    if (grid < 1) return BP_E_LAUNCH;
+    if (seg && per_cta > 0 && (long long)grid * per_cta > BP_NOALLOC_SCRATCH_FLOATS)
+        grid = (int)(BP_NOALLOC_SCRATCH_FLOATS / per_cta);
+    // the kernel clears each CTA's rows of the scratch before accumulating into them
+    code = bp_adjoint(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, lam, gs, gc,
+                      seg ? scratch : nullptr, grid, stream);
+    if (code != BP_OK || !seg) return code;
+    return bp_seg_reduce(scratch, grid, seg_len, seg0, seg, stream);
+}

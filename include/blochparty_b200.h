@@ -85,6 +85,22 @@ int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const 
  * seg_reduce, engines/gpu/cuda/seg_reduce.cu:3-11). `seg` is [S][8] float64. */
 int bp_seg_reduce(const float* gseg, int n_cta, int seg_len, int seg0, double* seg, void* stream);
 
+/* bp_adjoint followed by bp_seg_reduce, without the caller's `gseg` scratch: for callers that cannot allocate
+ * device memory (a host runtime that hands the library fixed buffers and forbids allocation while it runs, or a
+ * foreign-language binding that passes device pointers but cannot call cudaMalloc). No counterpart in the
+ * reference. The scratch lives in one file-scope device array of BP_NOALLOC_SCRATCH_BYTES (8 MiB) that every GPU
+ * loading the library holds until exit; the call allocates nothing. Returns BP_E_SIZE when one CTA's share,
+ * seg_len * 8 floats, exceeds the array; the grid is capped so that all CTAs fit. `seg` ([S][8] float64, +=) may
+ * be NULL (no segment gradients). The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current: make it before any stream capture. Every call uses the same
+ * array: calls that overlap on the GPU (other streams, other host threads) race on it. Results equal bp_adjoint's
+ * for lam, gs, gc, and seg up to the order of the float64 sum over CTAs. */
+#define BP_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+int bp_adjoint_noalloc(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                       const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                       const float* wstates, const float* h, float* lam, float* gs, float* gc, double* seg,
+                       void* stream);
+
 /* Measurement kernel (the roofline denominator): 4 CTAs x 256 threads per SM, each thread `iters` x 128
  * independent FFMAs; `*flops` receives the flop count of the launch, which the caller divides by the launch's
  * CUDA-event duration. `out` needs 4 * SMs * 256 floats (never written in practice). */
