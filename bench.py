@@ -212,9 +212,16 @@ def main():
     inp = bpb.api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad,
                          seq.adc_phase, None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
     pk = engine.pack(inp, dev)
-    samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
-    windows = engine.plan_windows(pk.flags, samp)
-    wdev = torch.from_numpy(windows).to(dev)
+    mma = None
+    if args.readout == "bf16x3":
+        from blochparty_b200.readout_mma import MmaBuffers, run_forward_mma
+
+        mma = MmaBuffers(pk)
+        windows, wdev = mma.windows, mma.windows_dev
+    else:
+        samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
+        windows = engine.plan_windows(pk.flags, samp)
+        wdev = torch.from_numpy(windows).to(dev)
     state0 = engine.initial_state(inp.pd, None, dev)
     state = torch.empty_like(state0)
     raw = torch.zeros(pk.n_adc, 2 * pk.n_coils, dtype=torch.float64, device=dev)
@@ -229,7 +236,10 @@ def main():
         raw.zero_()
         if i is not None:
             kstart[i].record()
-        engine.run_forward(pk, state, wdev, 0, windows.shape[0], raw, status)
+        if mma is not None:
+            run_forward_mma(pk, mma, state, raw, status)
+        else:
+            engine.run_forward(pk, state, wdev, 0, windows.shape[0], raw, status)
         if i is not None:
             kend[i].record()
         sig = engine.finish_signal(pk, raw)
@@ -268,10 +278,11 @@ def main():
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        bpb.simulate(ph, seq, coils)
+        bpb.simulate(ph, seq, coils, readout=args.readout)
         e2e_ms.append((time.perf_counter() - t) * 1e3)
     e2e = world * n * S / (statistics.median(e2e_ms) * 1e-3) if e2e_ms else None
     h2d = sum(t.numel() * t.element_size() for t in (pk.spins, pk.sens, pk.segs, pk.seg64, pk.psi, wdev, state0))
+    _lib.check_status(status, "forward")
     d2h = pk.n_coils * pk.n_adc * 8 + state.numel() * 4
 
     if rank != 0:
@@ -285,12 +296,15 @@ def main():
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "spins_per_gpu": n, "segments": S, "adc_samples": pk.n_adc,
-                   "coils": pk.n_coils, "readout": args.readout, "l2": "inputs larger than L2 (state, spins, coils, "
+                   "coils": pk.n_coils, "readout": args.readout,
+                   "ctas": (_lib.lib().bp_forward_mma_grid(n) if mma is not None
+                            else _lib.lib().bp_forward_grid(n, pk.n_coils)), "l2": "inputs larger than L2 (state, spins, coils, "
                    "segments ~220 MB per GPU) and a 256 MB L2 flush between timed steps"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU; MEASURED_PEAKS.json has no FP32",
-                     "kernel": "bp_forward_kernel", "kernel_ms": kernel_ms,
+                     "kernel": "bp_forward_mma_kernel" if mma is not None else "bp_forward_kernel",
+                     "kernel_ms": kernel_ms,
                      "flops_per_launch": flops},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": statistics.median(e2e_ms) if e2e_ms else None},

@@ -18,6 +18,8 @@ BP_OK, BP_E_ARG, BP_E_ALIGN, BP_E_LAUNCH, BP_E_SIZE = 0, 1, 2, 3, 4
 BP_MAX_COILS = 32
 BP_SEG_MAX = 240
 BP_ADJ_WIN = 32
+BP_MMA_MAX_COILS = 8
+BP_MMA_SAMPLES = 64
 BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
@@ -29,9 +31,14 @@ _P = c_void_p
 SIGNATURES = {
     "bp_plan_windows": (c_int, [_P, c_int64, c_int, c_int, _P, _P, c_int64, _P]),
     "bp_forward_samp_max": (c_int, [c_int]),
+    "bp_forward_grid": (c_int, [c_int, c_int]),
+    "bp_forward_mma_grid": (c_int, [c_int]),
     "bp_forward": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P]),
     "bp_signal_finish": (c_int, [_P, _P, c_int, c_int, _P, _P]),
     "bp_ffma_peak": (c_int, [_P, c_int, _P, _P]),
+    "bp_mma_atiles_bytes": (c_int64, [c_int]),
+    "bp_mma_atiles": (c_int, [_P, c_int, c_int, _P, _P]),
+    "bp_forward_mma": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P]),
     "bp_adjoint_grid": (c_int, [c_int, c_int]),
     "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P,
                            c_int, _P]),

@@ -315,7 +315,9 @@ static int adj_grid(int n) {
     static bool configured[64] = {false};
     if (dev >= 0 && dev < 64 && !configured[dev]) {
         if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)adj_smem<NCG>()) != cudaSuccess)
+                                 (int)adj_smem<NCG>()) != cudaSuccess ||
+            cudaFuncSetAttribute(bp_adjoint_kernel<NCG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return -1;
         configured[dev] = true;
     }

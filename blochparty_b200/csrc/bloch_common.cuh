@@ -12,6 +12,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/blochparty_b200.h"
+
 #define BP_TWO_PI_F 6.283185307179586f
 
 // segment flags (host: blochparty_b200/engine.py pack_segments)
@@ -216,6 +218,15 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// A window record the kernels can run: segments within one staged block, samples within the accumulator.
+__device__ __forceinline__ bool window_ok(const int4& w, int samp_max) {
+    return w.x >= 0 && w.y >= w.x && w.y - w.x <= BP_SEG_MAX && w.z >= 0 && w.w >= 0 && w.w <= samp_max;
 }
 
 // global -> shared bulk copy (cp.async.bulk, the TMA's untiled form): 16-byte aligned addresses, size a multiple

@@ -126,6 +126,11 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
 
     auto issue = [&](int w, int buf) {
         const int4 win = a.windows[w];
+        if (!window_ok(win, samp_max<NCG>())) {  // never copy what does not fit: complete the phase without data
+            atomicOr(a.status, BP_ERR_BAD_WINDOW);
+            mbar_arrive(&bars[buf]);
+            return;
+        }
         const uint32_t bytes = static_cast<uint32_t>(win.y - win.x) * sizeof(SegRec);
         fence_proxy_async_smem();
         mbar_expect_tx(&bars[buf], bytes);
@@ -140,8 +145,9 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
             if (tid == 0) atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
             return;
         }
-        if (tid == 0 && w + 1 < a.w_end) issue(w + 1, buf ^ 1);
         const int4 win = a.windows[w];
+        if (!window_ok(win, samp_max<NCG>())) return;  // uniform; the status bit was set where it was staged
+        if (tid == 0 && w + 1 < a.w_end) issue(w + 1, buf ^ 1);  // after the check: nothing left in flight
         const SegRec* q0 = segbuf + buf * BP_SEG_MAX;
         const int nseg = win.y - win.x;
         const bool readout = a.raw != nullptr && win.w > 0;
@@ -261,14 +267,16 @@ static int num_sms(int dev) {
 }
 
 template <int NCG>
-static int launch_forward(const FwdArgs& a, int max_ctas, cudaStream_t stream) {
+static int forward_grid(int n, int max_ctas, int* grid_out) {
     const size_t smem = fwd_smem_bytes<NCG>();
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
         if (cudaFuncSetAttribute(bp_forward_kernel<NCG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
+                cudaSuccess ||
+            cudaFuncSetAttribute(bp_forward_kernel<NCG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return BP_E_LAUNCH;
         configured[dev] = true;
     }
@@ -277,13 +285,34 @@ static int launch_forward(const FwdArgs& a, int max_ctas, cudaStream_t stream) {
         cudaSuccess)
         return BP_E_LAUNCH;
     if (per_sm < 1) per_sm = 1;
-    const int n_tiles = (a.n + BP_THREADS - 1) / BP_THREADS;
+    const int n_tiles = (n + BP_THREADS - 1) / BP_THREADS;
     int grid = num_sms(dev) * per_sm;
     if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
     if (grid > n_tiles) grid = n_tiles;
     if (grid < 1) grid = 1;
-    bp_forward_kernel<NCG><<<grid, BP_THREADS, smem, stream>>>(a);
+    *grid_out = grid;
+    return BP_OK;
+}
+
+template <int NCG>
+static int launch_forward(const FwdArgs& a, int max_ctas, cudaStream_t stream) {
+    int grid = 0;
+    const int code = forward_grid<NCG>(a.n, max_ctas, &grid);
+    if (code != BP_OK) return code;
+    bp_forward_kernel<NCG><<<grid, BP_THREADS, fwd_smem_bytes<NCG>(), stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+extern "C" int bp_forward_grid(int n, int n_coils) {
+    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS) return -BP_E_ARG;
+    int grid = 0, code = BP_OK;
+    switch ((n_coils + 7) / 8) {
+        case 1: code = forward_grid<1>(n, 0, &grid); break;
+        case 2: code = forward_grid<2>(n, 0, &grid); break;
+        case 3: code = forward_grid<3>(n, 0, &grid); break;
+        default: code = forward_grid<4>(n, 0, &grid); break;
+    }
+    return code == BP_OK ? grid : -code;
 }
 
 extern "C" int bp_forward_samp_max(int n_coils) {

@@ -57,9 +57,31 @@ int bp_forward(const float* spins, const float* sens, int n, int n_coils, const 
                const int32_t* windows, int w_begin, int w_end, float* state, double* raw, float* wstates,
                int wstate_stride, int max_ctas, int32_t* status, void* stream);
 
+/* Persistent grid (CTAs) that bp_forward launches for n spins and n_coils coils; negative on error. */
+int bp_forward_grid(int n, int n_coils);
+
 /* signal[c][t] = raw[t][c] exp(-i psi[t]) in float64, written as complex64 (interleaved float pairs), shape
  * (n_coils, n_adc) (replaces the host-side assembly engines/gpu/driver.py:699-702). */
 int bp_signal_finish(const double* raw, const double* psi, int n_adc, int n_coils, void* out, void* stream);
+
+/* Split-bfloat16 tensor-core readout (tcgen05): at most BP_MMA_MAX_COILS coils. The coil sensitivities are
+ * first converted into per-128-spin-tile operand blocks ("A tiles", bp_mma_atiles_bytes(n) bytes, 16-byte aligned)
+ * by bp_mma_atiles from the same [16][n] `sens` layout as bp_forward. No counterpart in the reference (its CUDA
+ * engine's coil sum is float32 on the CUDA cores, engines/gpu/cuda/common.cuh:91-116; its Metal engine uses
+ * simdgroup matrices, engines/gpu/shaders/common.metal:653-705). */
+#define BP_MMA_MAX_COILS 8
+int64_t bp_mma_atiles_bytes(int n);
+int bp_mma_atiles(const float* sens, int n, int n_coils, void* atiles, void* stream);
+
+/* bp_forward with the coil contraction on the tensor cores: D += A_hi B_hi + A_hi B_lo + A_lo B_hi in float32
+ * (A: coil sensitivities, B: 16 samples' magnetization, both split into bfloat16 high and low parts), summed over
+ * the CTA's tiles in tensor memory and added to the float64 `raw` per window. Windows must hold at most 64 samples
+ * (bp_plan_windows with samp_max = 64). Same arguments as bp_forward otherwise (no window-state output). */
+/* Persistent grid (CTAs) that bp_forward_mma launches for n spins; negative on error. */
+int bp_forward_mma_grid(int n);
+int bp_forward_mma(const float* spins, const void* atiles, int n, int n_coils, const void* segs, const double* seg64,
+                   const int32_t* windows, int w_begin, int w_end, float* state, double* raw, int max_ctas,
+                   int32_t* status, void* stream);
 
 /* Grid (persistent CTAs) that bp_adjoint uses for n spins: size the first dimension of its `gseg` scratch with
  * it. Negative on error. */
