@@ -7,7 +7,7 @@ CUDA device is present, ``lib()`` raises, and nothing computes the simulation an
 from __future__ import annotations
 
 import ctypes
-from ctypes import c_double, c_int, c_int64, c_void_p
+from ctypes import c_double, c_float, c_int, c_int64, c_void_p
 from pathlib import Path
 
 import torch
@@ -19,6 +19,7 @@ BP_MAX_COILS = 32
 BP_SEG_MAX = 240
 BP_ADJ_WIN = 32
 BP_MMA_MAX_COILS = 8
+BP_MLP_PARAMS = 8836
 BP_MMA_SAMPLES = 64
 BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
@@ -43,6 +44,14 @@ SIGNATURES = {
     "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P,
                            c_int, _P]),
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
+    "bp_pulse_quats": (c_int, [_P, c_int, c_double, c_double, c_double, c_double, _P, c_int, _P, _P, _P]),
+    "bp_mlp_grad_ctas": (c_int, [c_int]),
+    "bp_mlp_grad": (c_int, [_P, _P, _P, c_int, _P, _P, _P]),
+    "bp_mlp_reduce": (c_int, [_P, _P, c_int, c_float, _P, _P, _P]),
+    "bp_adam": (c_int, [_P, _P, _P, _P, c_float, c_float, c_float, c_float, c_int, _P]),
+    "bp_mlp_eval": (c_int, [_P, _P, c_int, _P, _P]),
+    "bp_surrogate_pulse": (c_int, [_P, _P, c_int, _P, _P, c_int, c_int, c_double, c_double, c_double, c_double,
+                                   c_double, c_float, _P, _P]),
     "bp_adjoint_noalloc": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P,
                                    _P, _P]),
 }

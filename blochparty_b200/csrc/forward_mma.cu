@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
     // mbarrier phases, tracked identically by every thread
     uint32_t mma_phase[2] = {0u, 0u}, a_phase = 0u;
     bool mma_pending[2] = {false, false};
-    bool fail = false;
+    bool fail = false, err = false;  // fail: leave the window loop; err: this thread saw a failed wait
     auto drain = [&](int b) -> bool {  // wait for the MMAs that read B buffer b (and A) to complete
         if (!mma_pending[b]) return true;
         const bool ok = mbar_wait_bounded(&bars[2 + b], mma_phase[b]);
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
             // the previous tile's MMAs read A: let them finish, then bring this tile's A in
             bool okd = drain(0);
             okd = drain(1) && okd;
-            if (__syncthreads_or(!okd)) {
+            if (__syncthreads_or(!okd || err)) {
                 fail = true;
                 break;
             }
@@ -166,13 +166,9 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
                 }
                 if ((f & BP_ADC) && readout) {
                     const int b = grp & 1;
-                    if (slot == 0) {  // buffer b is free once the MMAs of the block before last have completed
-                        const bool okb = drain(b);
-                        if (__syncthreads_or(!okb)) {
-                            fail = true;
-                            break;
-                        }
-                    }
+                    // buffer b is free once the MMAs of the block before last have completed (each thread waits;
+                    // a failed wait is reported at the next barrier)
+                    if (slot == 0 && !drain(b)) err = true;
                     uint16_t xh, xl, yh, yl;
                     split_bf16(mx + lx, xh, xl);
                     split_bf16(my + ly, yh, yl);
@@ -184,11 +180,13 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
                     ++row;
                     if (slot == MM_BLOCK || row == win.w) {
                         fence_proxy_async_smem();  // this thread's B writes, visible to the tensor cores
-                        __syncthreads();
-                        bool oka = true;
+                        if (__syncthreads_or(err)) {  // the block is complete; and every wait so far succeeded
+                            fail = true;
+                            break;
+                        }
                         if (tid == 0) {
-                            if (!a_waited) oka = mbar_wait_bounded(&bars[4], a_phase);
-                            if (oka) {
+                            if (!a_waited && !mbar_wait_bounded(&bars[4], a_phase)) err = true;
+                            if (!err) {
                                 tc_fence_after();
                                 const uint32_t bh = sB + 2 * b * MM_B_BYTES, bl = bh + MM_B_BYTES;
                                 const uint32_t d = tmem + (uint32_t)(grp * MM_BLOCK);
@@ -211,10 +209,6 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
                         }
                         if (!a_waited) a_phase ^= 1u, a_waited = true;
                         mma_pending[b] = true;
-                        if (__syncthreads_or(!oka)) {
-                            fail = true;
-                            break;
-                        }
                         ++grp;
                         slot = 0;
                     }
@@ -233,7 +227,7 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
         if (readout) {  // the window's coil sums: D rows 0 .. 2C-1 (TMEM lanes of warp 0), columns = samples
             bool okd = drain(0);
             okd = drain(1) && okd;
-            if (__syncthreads_or(!okd)) {
+            if (__syncthreads_or(!okd || err)) {
                 fail = true;
                 break;
             }
@@ -261,7 +255,7 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
     }
     drain(0);
     drain(1);
-    if (fail && tid == 0) atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
+    if ((fail || err) && tid == 0) atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {

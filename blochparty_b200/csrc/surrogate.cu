@@ -1,0 +1,482 @@
+// Learned RF surrogate: a 3 -> 64 -> 64 -> 64 -> 4 GELU network standing in for the sub-stepped integration of
+// one shaped RF pulse, mapping (off-resonance, B1 scale, slice position) to the pulse's rotation.
+//
+// No counterpart in the reference (its nearest part is the exact per-spin map of a reused pulse,
+// engines/gpu/cuda/pulse.cu.in:3-32). Kernels here:
+//  * bp_pulse_quats: training targets from the plain integrator: per sample, the pulse's per-step rotations
+//    w = -2 pi dt (b1 rf_x, b1 rf_y, G z + df) composed as unit quaternions in float64, reduced by the free
+//    precession (R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T) so that the target is smooth in z;
+//  * bp_mlp_grad: fused forward + backward of the network over a batch (per-CTA gradient partials), then
+//    bp_mlp_reduce (fixed-order sum over CTAs) and bp_adam (the optimiser step): training on the GPU;
+//  * bp_surrogate_pulse: one pulse occurrence applied to every spin's state: inside the training domain, the
+//    network's rotation wrapped by half-pulse relaxations (relax T/2, rotate, relax T/2); outside it, the
+//    plain sub-stepped integration of the pulse's segments (the fallback).
+// Quaternions: (q0, q1, q2, q3) = (cos |w|/2, sin |w|/2 w/|w|), composition "q1 then q2" = q2 q1 (Hamilton
+// product); the Cayley-Klein pair of q is alpha = q0 - i q3, beta = -i (q1 + i q2).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bloch_common.cuh"
+#include "../../include/blochparty_b200.h"
+
+#define MLP_H 64
+#define MLP_IN 3
+#define MLP_OUT 4
+// flat parameter layout: W1 (64 x 3), b1 (64), W2 (64 x 64), b2, W3 (64 x 64), b3, W4 (4 x 64), b4 (4)
+#define P_W1 0
+#define P_B1 (P_W1 + MLP_H * MLP_IN)
+#define P_W2 (P_B1 + MLP_H)
+#define P_B2 (P_W2 + MLP_H * MLP_H)
+#define P_W3 (P_B2 + MLP_H)
+#define P_B3 (P_W3 + MLP_H * MLP_H)
+#define P_W4 (P_B3 + MLP_H)
+#define P_B4 (P_W4 + MLP_OUT * MLP_H)
+#define N_PARAMS (P_B4 + MLP_OUT)  // 8836
+
+static_assert(N_PARAMS == BP_MLP_PARAMS, "parameter count");
+
+// input normalisation of the training domain: df in [-200, 200] Hz, b1 in [0.7, 1.3], z_rel in [-2, 2]
+#define DOM_DF 200.0f
+#define DOM_B1 0.3f
+#define DOM_Z 2.0f
+
+struct dq4 {
+    double w, x, y, z;
+};
+
+__device__ __forceinline__ dq4 dq_mul(const dq4& a, const dq4& b) {
+    return {a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z, a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
+            a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x, a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w};
+}
+
+__device__ __forceinline__ dq4 dq_rotvec(double wx, double wy, double wz) {
+    const double phi = sqrt(wx * wx + wy * wy + wz * wz);
+    double s, c;
+    sincos(0.5 * phi, &s, &c);
+    const double k = phi > 1e-300 ? s / phi : 0.5;
+    return {c, k * wx, k * wy, k * wz};
+}
+
+__device__ __forceinline__ dq4 dq_z(double angle) {
+    double s, c;
+    sincos(0.5 * angle, &s, &c);
+    return {c, 0.0, 0.0, s};
+}
+
+// Targets: samples [n][3] (df [Hz], b1, z_rel [slice widths]) -> q~ [n][4] float32 (and q [n][4] if not null).
+__global__ void bp_pulse_quats_kernel(const double2* __restrict__ rf, int k_steps, double dt, double gz,
+                                      double thickness, double z0, const float* __restrict__ samples, int n,
+                                      float* __restrict__ qred, float* __restrict__ qfull) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double df = samples[3 * i], b1 = samples[3 * i + 1], zr = samples[3 * i + 2];
+    const double z = z0 + zr * thickness;
+    const double w = -2.0 * M_PI * dt, wz = w * (gz * z + df);
+    dq4 q{1.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < k_steps; ++k) {
+        const double2 r = rf[k];
+        q = dq_mul(dq_rotvec(w * b1 * r.x, w * b1 * r.y, wz), q);
+    }
+    const dq4 h = dq_z(-0.5 * wz * k_steps);
+    const dq4 qr = dq_mul(dq_mul(h, q), h);
+    qred[4 * i] = (float)qr.w, qred[4 * i + 1] = (float)qr.x, qred[4 * i + 2] = (float)qr.y, qred[4 * i + 3] = (float)qr.z;
+    if (qfull) qfull[4 * i] = (float)q.w, qfull[4 * i + 1] = (float)q.x, qfull[4 * i + 2] = (float)q.y, qfull[4 * i + 3] = (float)q.z;
+}
+
+extern "C" int bp_pulse_quats(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
+                              const float* samples, int n, float* qred, float* qfull, void* stream) {
+    if (!rf || !samples || !qred || k_steps < 1 || n < 0 || dt <= 0 || thickness <= 0) return BP_E_ARG;
+    if (n == 0) return BP_OK;
+    bp_pulse_quats_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const double2*>(rf), k_steps, dt, gz, thickness, z0, samples, n, qred, qfull);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+// GELU in its tanh form, 0.5 x (1 + tanh(c (x + 0.044715 x^3))), c = sqrt(2/pi) (Hendrycks and Gimpel), and its
+// derivative; tanhf is the accurate library function.
+__device__ __forceinline__ float gelu_f(float x) {
+    const float c = 0.7978845608028654f;
+    const float t = tanhf(c * fmaf(0.044715f * x, x * x, x));
+    return 0.5f * x * (1.0f + t);
+}
+
+__device__ __forceinline__ float gelu_d(float x) {
+    const float c = 0.7978845608028654f;
+    const float t = tanhf(c * fmaf(0.044715f * x, x * x, x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * c * fmaf(3.0f * 0.044715f * x, x, 1.0f);
+}
+
+// ---- training: forward + backward over a batch ----
+#define TR_T 128          // samples per CTA (one per thread)
+#define TR_LD 65          // row stride (floats) of the per-sample activation arrays [TR_T][TR_LD]
+#define TR_ARR (TR_T * TR_LD)
+
+// The network's output for normalised input x, and (train) its pre-activations into z1, z2, z3 rows.
+__device__ __forceinline__ void mlp_forward_row(const float* __restrict__ P, const float x[3], float* z1, float* z2,
+                                                float* z3, float y[4]) {
+    float a[MLP_H];
+#pragma unroll
+    for (int k = 0; k < MLP_H; ++k) {
+        const float v = fmaf(P[P_W1 + 3 * k], x[0], fmaf(P[P_W1 + 3 * k + 1], x[1], fmaf(P[P_W1 + 3 * k + 2], x[2], P[P_B1 + k])));
+        if (z1) z1[k] = v;
+        a[k] = gelu_f(v);
+    }
+    float b[MLP_H];
+    for (int k = 0; k < MLP_H; ++k) {
+        float v = P[P_B2 + k];
+#pragma unroll
+        for (int i = 0; i < MLP_H; ++i) v = fmaf(P[P_W2 + MLP_H * k + i], a[i], v);
+        if (z2) z2[k] = v;
+        b[k] = gelu_f(v);
+    }
+    for (int k = 0; k < MLP_H; ++k) {
+        float v = P[P_B3 + k];
+#pragma unroll
+        for (int i = 0; i < MLP_H; ++i) v = fmaf(P[P_W3 + MLP_H * k + i], b[i], v);
+        if (z3) z3[k] = v;
+        a[k] = gelu_f(v);
+    }
+#pragma unroll
+    for (int j = 0; j < MLP_OUT; ++j) {
+        float v = P[P_B4 + j];
+#pragma unroll
+        for (int i = 0; i < MLP_H; ++i) v = fmaf(P[P_W4 + MLP_H * j + i], a[i], v);
+        y[j] = v;
+    }
+}
+
+// Sum over the CTA's samples of dz[t][k] * act[t][i] -> grad[o_w + k * n_in + i], and of dz[t][k] -> grad[o_b + k]:
+// thread (kb, ib) owns an 8 x 4 block of (k, i).
+__device__ __forceinline__ void weight_grads(const float* dz, const float* act, int n_in, int nt, float* grad,
+                                             int o_w, int o_b, int tid) {
+    const int kb = tid >> 4, ib = tid & 15;
+    if (4 * ib < n_in) {
+        float acc[8][4];
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[r][c] = 0.0f;
+        for (int t = 0; t < nt; ++t) {
+            float d[8], v[4];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) d[r] = dz[t * TR_LD + 8 * kb + r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[c] = (4 * ib + c < n_in) ? act[t * TR_LD + 4 * ib + c] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(d[r], v[c], acc[r][c]);
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (4 * ib + c < n_in) grad[o_w + (8 * kb + r) * n_in + 4 * ib + c] = acc[r][c];
+    }
+    if (tid < MLP_H) {
+        float s = 0.0f;
+        for (int t = 0; t < nt; ++t) s += dz[t * TR_LD + tid];
+        grad[o_b + tid] = s;
+    }
+}
+
+// Per CTA: samples [blockIdx.x * 128, +128) of x [n][3] (normalised inputs) and targets [n][4]; writes the CTA's
+// gradient sum (not yet divided by the batch) to gpart[blockIdx.x][N_PARAMS] and its loss sum to lpart.
+__global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __restrict__ params,
+                                                              const float* __restrict__ x, const float* __restrict__ target,
+                                                              int n, float* __restrict__ gpart, float* __restrict__ lpart) {
+    extern __shared__ __align__(16) float sm[];
+    float* P = sm;                       // N_PARAMS (padded to a multiple of 4)
+    float* z1 = P + ((N_PARAMS + 3) & ~3);
+    float* z2 = z1 + TR_ARR;
+    float* z3 = z2 + TR_ARR;
+    float* buf = z3 + TR_ARR;            // activations of the layer below, then x
+    __shared__ float dyb[TR_T][MLP_OUT];
+    __shared__ float lsum[TR_T];
+    const int tid = threadIdx.x;
+    const int t0 = blockIdx.x * TR_T;
+    const int nt = min(TR_T, n - t0);
+    for (int i = tid; i < N_PARAMS; i += TR_T) P[i] = params[i];
+    __syncthreads();
+    float* g = gpart + (size_t)blockIdx.x * N_PARAMS;
+    const bool live = tid < nt;
+    float xin[3] = {0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f};
+    if (live) {
+        xin[0] = x[3 * (t0 + tid)], xin[1] = x[3 * (t0 + tid) + 1], xin[2] = x[3 * (t0 + tid) + 2];
+        mlp_forward_row(P, xin, z1 + tid * TR_LD, z2 + tid * TR_LD, z3 + tid * TR_LD, y);
+    }
+    // loss |y/|y| - target|^2 and dL/dy = (dL/dq - q (q . dL/dq)) / |y|
+    float dy[4] = {0.f, 0.f, 0.f, 0.f}, loss = 0.0f;
+    if (live) {
+        const float r = sqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+        const float inv = 1.0f / r;
+        float q[4], gq[4], qg = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            q[j] = y[j] * inv;
+            const float e = q[j] - target[4 * (t0 + tid) + j];
+            loss = fmaf(e, e, loss);
+            gq[j] = 2.0f * e;
+            qg = fmaf(q[j], gq[j], qg);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dy[j] = (gq[j] - q[j] * qg) * inv;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dyb[tid][j] = dy[j];
+    lsum[tid] = loss;
+    // a3 = gelu(z3) into buf (own row)
+    for (int k = 0; k < MLP_H; ++k) buf[tid * TR_LD + k] = live ? gelu_f(z3[tid * TR_LD + k]) : 0.0f;
+    __syncthreads();
+    if (tid == 0) {
+        float s = 0.0f;
+        for (int t = 0; t < nt; ++t) s += lsum[t];
+        lpart[blockIdx.x] = s;
+    }
+    // layer 4: dW4[j][k] = sum_t dy[t][j] a3[t][k], db4[j] = sum_t dy[t][j]
+    for (int o = tid; o < MLP_OUT * MLP_H + MLP_OUT; o += TR_T) {
+        float s = 0.0f;
+        if (o < MLP_OUT * MLP_H) {
+            const int j = o / MLP_H, k = o % MLP_H;
+            for (int t = 0; t < nt; ++t) s = fmaf(dyb[t][j], buf[t * TR_LD + k], s);
+            g[P_W4 + o] = s;
+        } else {
+            const int j = o - MLP_OUT * MLP_H;
+            for (int t = 0; t < nt; ++t) s += dyb[t][j];
+            g[P_B4 + j] = s;
+        }
+    }
+    // dz3 = (W4^T dy) gelu'(z3), in place of z3
+    if (live) {
+        for (int k = 0; k < MLP_H; ++k) {
+            float d = 0.0f;
+#pragma unroll
+            for (int j = 0; j < MLP_OUT; ++j) d = fmaf(P[P_W4 + MLP_H * j + k], dy[j], d);
+            z3[tid * TR_LD + k] = d * gelu_d(z3[tid * TR_LD + k]);
+        }
+    } else {
+        for (int k = 0; k < MLP_H; ++k) z3[tid * TR_LD + k] = 0.0f;
+    }
+    __syncthreads();  // buf (a3) consumed; dz3 complete
+    for (int k = 0; k < MLP_H; ++k) buf[tid * TR_LD + k] = live ? gelu_f(z2[tid * TR_LD + k]) : 0.0f;  // a2
+    __syncthreads();
+    weight_grads(z3, buf, MLP_H, nt, g, P_W3, P_B3, tid);
+    // dz2 = (W3^T dz3) gelu'(z2), in place of z2
+    if (live) {
+        float d3[MLP_H];
+#pragma unroll
+        for (int k = 0; k < MLP_H; ++k) d3[k] = z3[tid * TR_LD + k];
+        for (int i = 0; i < MLP_H; ++i) {
+            float d = 0.0f;
+#pragma unroll
+            for (int k = 0; k < MLP_H; ++k) d = fmaf(P[P_W3 + MLP_H * k + i], d3[k], d);
+            z2[tid * TR_LD + i] = d * gelu_d(z2[tid * TR_LD + i]);
+        }
+    } else {
+        for (int k = 0; k < MLP_H; ++k) z2[tid * TR_LD + k] = 0.0f;
+    }
+    __syncthreads();  // buf (a2) consumed by the layer-3 gradients; dz2 complete
+    for (int k = 0; k < MLP_H; ++k) buf[tid * TR_LD + k] = live ? gelu_f(z1[tid * TR_LD + k]) : 0.0f;  // a1
+    __syncthreads();
+    weight_grads(z2, buf, MLP_H, nt, g, P_W2, P_B2, tid);
+    if (live) {
+        float d2[MLP_H];
+#pragma unroll
+        for (int k = 0; k < MLP_H; ++k) d2[k] = z2[tid * TR_LD + k];
+        for (int i = 0; i < MLP_H; ++i) {
+            float d = 0.0f;
+#pragma unroll
+            for (int k = 0; k < MLP_H; ++k) d = fmaf(P[P_W2 + MLP_H * k + i], d2[k], d);
+            z1[tid * TR_LD + i] = d * gelu_d(z1[tid * TR_LD + i]);
+        }
+    } else {
+        for (int k = 0; k < MLP_H; ++k) z1[tid * TR_LD + k] = 0.0f;
+    }
+    __syncthreads();  // buf (a1) consumed; dz1 complete
+    buf[tid * TR_LD] = xin[0], buf[tid * TR_LD + 1] = xin[1], buf[tid * TR_LD + 2] = xin[2];
+    __syncthreads();
+    weight_grads(z1, buf, MLP_IN, nt, g, P_W1, P_B1, tid);
+}
+
+// grad[p] = scale * sum over CTAs (in order) of gpart[cta][p]; loss = scale * sum of lpart (float64 sums)
+__global__ void bp_mlp_reduce_kernel(const float* __restrict__ gpart, const float* __restrict__ lpart, int n_cta,
+                                     float scale, float* __restrict__ grad, float* __restrict__ loss) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < N_PARAMS) {
+        double s = 0.0;
+        for (int c = 0; c < n_cta; ++c) s += (double)gpart[(size_t)c * N_PARAMS + p];
+        grad[p] = (float)(s * scale);
+    }
+    if (p == 0 && loss) {
+        double s = 0.0;
+        for (int c = 0; c < n_cta; ++c) s += (double)lpart[c];
+        *loss = (float)(s * scale);
+    }
+}
+
+// Adam (Kingma and Ba): m = b1 m + (1 - b1) g, v = b2 v + (1 - b2) g^2, p -= lr mhat / (sqrt(vhat) + eps) with
+// the bias corrections of step `step` (1-based).
+__global__ void bp_adam_kernel(float* __restrict__ params, const float* __restrict__ grad, float* __restrict__ m,
+                               float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N_PARAMS) return;
+    const float g = grad[p];
+    const float mm = fmaf(b1, m[p], (1.0f - b1) * g), vv = fmaf(b2, v[p], (1.0f - b2) * g * g);
+    m[p] = mm, v[p] = vv;
+    params[p] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+}
+
+extern "C" int bp_mlp_grad_ctas(int n) { return n < 1 ? 0 : (n + TR_T - 1) / TR_T; }
+
+static size_t mlp_grad_smem() { return (((size_t)N_PARAMS + 3) & ~(size_t)3) * 4 + 4 * (size_t)TR_ARR * 4; }
+
+extern "C" int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float* gpart,
+                           float* lpart, void* stream) {
+    if (!params || !x || !target || !gpart || !lpart || n < 1) return BP_E_ARG;
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        if (cudaFuncSetAttribute(bp_mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mlp_grad_smem()) != cudaSuccess)
+            return BP_E_LAUNCH;
+        configured[dev] = true;
+    }
+    bp_mlp_grad_kernel<<<bp_mlp_grad_ctas(n), TR_T, mlp_grad_smem(), static_cast<cudaStream_t>(stream)>>>(
+        params, x, target, n, gpart, lpart);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+extern "C" int bp_mlp_reduce(const float* gpart, const float* lpart, int n_cta, float scale, float* grad, float* loss,
+                             void* stream) {
+    if (!gpart || !lpart || !grad || n_cta < 1) return BP_E_ARG;
+    bp_mlp_reduce_kernel<<<(N_PARAMS + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(gpart, lpart, n_cta,
+                                                                                              scale, grad, loss);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+extern "C" int bp_adam(float* params, const float* grad, float* m, float* v, float lr, float beta1, float beta2,
+                       float eps, int step, void* stream) {
+    if (!params || !grad || !m || !v || step < 1) return BP_E_ARG;
+    const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
+    bp_adam_kernel<<<(N_PARAMS + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(params, grad, m, v, lr, beta1,
+                                                                                       beta2, eps, c1, c2);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+// Network outputs for normalised inputs x [n][3] -> y [n][4] (normalised to unit length): inference for checks.
+__global__ void __launch_bounds__(128) bp_mlp_eval_kernel(const float* __restrict__ params, const float* __restrict__ x,
+                                                         int n, float* __restrict__ y) {
+    __shared__ float P[N_PARAMS];
+    for (int i = threadIdx.x; i < N_PARAMS; i += blockDim.x) P[i] = params[i];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float xin[3] = {x[3 * t], x[3 * t + 1], x[3 * t + 2]};
+    float o[4];
+    mlp_forward_row(P, xin, nullptr, nullptr, nullptr, o);
+    const float inv = rsqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) y[4 * t + j] = o[j] * inv;
+}
+
+extern "C" int bp_mlp_eval(const float* params, const float* x, int n, float* y, void* stream) {
+    if (!params || !x || !y || n < 0) return BP_E_ARG;
+    if (n == 0) return BP_OK;
+    bp_mlp_eval_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(params, x, n, y);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+// ---- inference: one pulse occurrence applied to every spin's state ----
+struct PulseArgs {
+    const float* spins;   // [8][n]
+    float* state;         // [6][n] in/out
+    const float* params;  // the pulse's network
+    const SegRec* segs;   // the occurrence's segments for the fallback: segs[seg0 .. seg0 + k_steps)
+    int seg0, k_steps, n;
+    double T, gz, thickness, z0, phi0;  // duration [s], slice gradient [Hz/m], thickness [m], centre [m], RF phase
+    float b0off;          // the occurrence's uniform off-resonance [Hz]
+    int* counts;          // null or [2]: spins through the network, spins through the fallback
+};
+
+__device__ __forceinline__ void quat_mul_f(const float a[4], const float b[4], float o[4]) {
+    o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+    o[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+    o[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+    o[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+}
+
+__global__ void __launch_bounds__(128) bp_surrogate_pulse_kernel(PulseArgs a) {
+    __shared__ float P[N_PARAMS];
+    for (int i = threadIdx.x; i < N_PARAMS; i += blockDim.x) P[i] = a.params[i];
+    __syncthreads();
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = j < a.n;
+    const int jj = active ? j : 0;
+    const Spin p = load_spin(a.spins, a.n, jj, active);
+    const float df = p.db0 + a.b0off;
+    const float zr = (float)(((double)p.pz - a.z0) / a.thickness);
+    const bool inside = fabsf(df) <= DOM_DF && fabsf(p.b1 - 1.0f) <= DOM_B1 && fabsf(zr) <= DOM_Z;
+    if (a.counts) {
+        const unsigned in_mask = __ballot_sync(0xffffffffu, active && inside);
+        const unsigned out_mask = __ballot_sync(0xffffffffu, active && !inside);
+        if ((threadIdx.x & 31) == 0) {
+            if (in_mask) atomicAdd(&a.counts[0], __popc(in_mask));
+            if (out_mask) atomicAdd(&a.counts[1], __popc(out_mask));
+        }
+    }
+    if (!active) return;
+    float mx = a.state[j], my = a.state[a.n + j], mz = a.state[2 * a.n + j];
+    float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
+    if (inside) {
+        const float xin[3] = {df / DOM_DF, (p.b1 - 1.0f) / DOM_B1, zr / DOM_Z};
+        float y[4];
+        mlp_forward_row(P, xin, nullptr, nullptr, nullptr, y);
+        const float inv = rsqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+        const float qr[4] = {y[0] * inv, y[1] * inv, y[2] * inv, y[3] * inv};
+        // R = Rz(wz/2 + phi0) R~ Rz(wz/2 - phi0), wz = -2 pi (G z + df) T: the half angles in float64
+        const double half = -M_PI * ((double)a.gz * (double)p.pz + (double)df) * a.T;
+        double s1, c1, s2, c2;
+        sincos(0.5 * (half + a.phi0), &s1, &c1);
+        sincos(0.5 * (half - a.phi0), &s2, &c2);
+        const float qa[4] = {(float)c1, 0.f, 0.f, (float)s1}, qb[4] = {(float)c2, 0.f, 0.f, (float)s2};
+        float t[4], q[4];
+        quat_mul_f(qa, qr, t);
+        quat_mul_f(t, qb, q);
+        const float s = q[0], x = q[1], yq = q[2], z = q[3];
+        const float R00 = 1 - 2 * (yq * yq + z * z), R01 = 2 * (x * yq - s * z), R02 = 2 * (x * z + s * yq);
+        const float R10 = 2 * (x * yq + s * z), R11 = 1 - 2 * (x * x + z * z), R12 = 2 * (yq * z - s * x);
+        const float R20 = 2 * (x * z - s * yq), R21 = 2 * (yq * z + s * x), R22 = 1 - 2 * (x * x + yq * yq);
+        // relax T/2, rotate, relax T/2 (relaxation cannot be a pure rotation: it wraps the network's rotation)
+        const float th = (float)(0.5 * a.T);
+        const float e1 = expm1f(-th * p.r1), e2 = expm1f(-th * p.r2);
+        const float ax = (mx + lx) * (1.0f + e2), ay = (my + ly) * (1.0f + e2);
+        const float az = fmaf((mz + lz) - p.pd, e1, mz + lz);
+        const float nx = fmaf(R00, ax, fmaf(R01, ay, R02 * az));
+        const float ny = fmaf(R10, ax, fmaf(R11, ay, R12 * az));
+        const float nz = fmaf(R20, ax, fmaf(R21, ay, R22 * az));
+        mx = nx * (1.0f + e2), my = ny * (1.0f + e2), mz = fmaf(nz - p.pd, e1, nz);
+        lx = ly = lz = 0.0f;
+    } else {  // the fallback: the plain sub-stepped pulse
+        RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+        for (int k = 0; k < a.k_steps; ++k) {
+            const SegRec q = a.segs[a.seg0 + k];
+            if (k == 0 || !(q.flags & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
+            rf_step(q, p, rr, mx, my, mz, lx, ly, lz);
+        }
+    }
+    a.state[j] = mx, a.state[a.n + j] = my, a.state[2 * a.n + j] = mz;
+    a.state[3 * a.n + j] = lx, a.state[4 * a.n + j] = ly, a.state[5 * a.n + j] = lz;
+}
+
+extern "C" int bp_surrogate_pulse(const float* spins, float* state, int n, const float* params, const void* segs,
+                                  int seg0, int k_steps, double T, double gz, double thickness, double z0, double phi0,
+                                  float b0off, int32_t* counts, void* stream) {
+    if (!spins || !state || !params || !segs || n < 1 || seg0 < 0 || k_steps < 1 || T <= 0 || thickness <= 0)
+        return BP_E_ARG;
+    PulseArgs a{spins, state, params, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0, phi0,
+                b0off, counts};
+    bp_surrogate_pulse_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(a);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}

@@ -123,6 +123,42 @@ int bp_adjoint_noalloc(const float* spins, const float* sens, int n, int n_coils
                        const float* wstates, const float* h, float* lam, float* gs, float* gc, double* seg,
                        void* stream);
 
+/* ---- learned RF surrogate (no counterpart in the reference; its nearest part is the exact per-spin map of a
+ * reused pulse, engines/gpu/cuda/pulse.cu.in:3-32) ----
+ * A 3 -> 64 -> 64 -> 64 -> 4 GELU network per shaped pulse: inputs (df / 200 Hz, (b1 - 1) / 0.3, z_rel / 2) with
+ * z_rel = (z - z0) / slice thickness, output a unit quaternion (q0, q1, q2, q3), the Cayley-Klein pair
+ * alpha = q0 - i q3, beta = -i (q1 + i q2), of the pulse's rotation reduced by its free precession:
+ * R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T. Parameters: BP_MLP_PARAMS floats, W1 (64x3), b1, W2 (64x64),
+ * b2, W3 (64x64), b3, W4 (4x64), b4. */
+#define BP_MLP_PARAMS 8836
+
+/* Training targets from the plain integrator: samples [n][3] (df [Hz], b1, z_rel) -> reduced rotations
+ * qred [n][4] (and the whole rotations qfull [n][4] if not NULL); rf [k_steps][2] float64 [Hz], float64 throughout. */
+int bp_pulse_quats(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
+                   const float* samples, int n, float* qred, float* qfull, void* stream);
+
+/* One training step's gradient: x [n][3] normalised inputs, target [n][4]; per-CTA partials gpart
+ * [bp_mlp_grad_ctas(n)][BP_MLP_PARAMS] and loss sums lpart [bp_mlp_grad_ctas(n)] (scratch of the caller). */
+int bp_mlp_grad_ctas(int n);
+int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float* gpart, float* lpart,
+                void* stream);
+/* grad = scale * (sum over CTAs in order of gpart), loss = scale * sum of lpart (scale = 1 / batch). */
+int bp_mlp_reduce(const float* gpart, const float* lpart, int n_cta, float scale, float* grad, float* loss,
+                  void* stream);
+/* Adam step number `step` (1-based) on params with moments m, v. */
+int bp_adam(float* params, const float* grad, float* m, float* v, float lr, float beta1, float beta2, float eps,
+            int step, void* stream);
+/* The network's unit-quaternion outputs y [n][4] for normalised inputs x [n][3]. */
+int bp_mlp_eval(const float* params, const float* x, int n, float* y, void* stream);
+
+/* One pulse occurrence (segments [seg0, seg0 + k_steps) of `segs`, the trained waveform times exp(i phi0), slice
+ * gradient gz along z, uniform offset b0off) applied to every spin's state [6][n]: inside the domain
+ * (|df| <= 200 Hz, |b1 - 1| <= 0.3, |z_rel| <= 2) relax T/2, rotate by the network's rotation, relax T/2; outside,
+ * the plain sub-stepped segments. counts (NULL or [2]) += spins through the network, through the fallback. */
+int bp_surrogate_pulse(const float* spins, float* state, int n, const float* params, const void* segs, int seg0,
+                       int k_steps, double T, double gz, double thickness, double z0, double phi0, float b0off,
+                       int32_t* counts, void* stream);
+
 /* Measurement kernel (the roofline denominator): 4 CTAs x 256 threads per SM, each thread `iters` x 128
  * independent FFMAs; `*flops` receives the flop count of the launch, which the caller divides by the launch's
  * CUDA-event duration. `out` needs 4 * SMs * 256 floats (never written in practice). */

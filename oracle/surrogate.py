@@ -1,0 +1,115 @@
+"""CPU float64 oracles of the learned RF surrogate — TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` may import this module, as the checker.
+The reference (blochparty) has no learned surrogate: its closest parts are the exact per-spin maps of reused
+pulses (``engines/gpu/cuda/pulse.cu.in:3-32``, ``engines/gpu/driver.py:112-164``). What this oracle restates is
+the plain integrator's rotation part (blochparty ``engines/core.py:97-108``: a rotation by
+w = -2 pi dt (b1 rf_x, b1 rf_y, G z + df) per RF segment), composed over a pulse as unit quaternions, and the
+surrogate's network in float64 with autograd (to check the hand-written training kernels' gradients).
+
+Conventions (shared with ``blochparty_b200/csrc/surrogate.cu``):
+
+* a rotation by angle |w| about w/|w| is the unit quaternion (cos |w|/2, sin |w|/2 w/|w|); applying q1 then q2
+  is the Hamilton product q2 q1; the Cayley-Klein pair of q = (q0, q1, q2, q3) is alpha = q0 - i q3,
+  beta = -i (q1 + i q2);
+* the pulse's whole precession without RF is the z rotation by wz = -2 pi (G z + df) T; the network learns
+  the reduced rotation R~ with R = Rz(wz / 2) R~ Rz(wz / 2), smooth in z where R itself winds around z;
+* inputs normalised to [-1, 1]: (df / 200 Hz, (b1 - 1) / 0.3, z_rel / 2), z_rel = z / slice thickness.
+"""
+
+from __future__ import annotations
+
+import math
+
+import torch
+
+F64 = torch.float64
+TWO_PI = 2.0 * math.pi
+
+
+def qmul(a, b):
+    """Hamilton product of quaternion tensors (..., 4)."""
+    a0, a1, a2, a3 = a.unbind(-1)
+    b0, b1, b2, b3 = b.unbind(-1)
+    return torch.stack([a0 * b0 - a1 * b1 - a2 * b2 - a3 * b3,
+                        a0 * b1 + a1 * b0 + a2 * b3 - a3 * b2,
+                        a0 * b2 - a1 * b3 + a2 * b0 + a3 * b1,
+                        a0 * b3 + a1 * b2 - a2 * b1 + a3 * b0], -1)
+
+
+def quat_of_rotvec(w):
+    """(..., 3) rotation vectors -> (..., 4) unit quaternions."""
+    phi = torch.linalg.vector_norm(w, dim=-1, keepdim=True)
+    half = 0.5 * phi
+    s = torch.where(phi > 1e-300, torch.sin(half) / phi.clamp_min(1e-300), torch.full_like(phi, 0.5))
+    return torch.cat([torch.cos(half), s * w], -1)
+
+
+def qz(angle):
+    """Quaternion of the z rotation by ``angle`` (tensor (...,))."""
+    z = torch.zeros_like(angle)
+    return torch.stack([torch.cos(0.5 * angle), z, z, torch.sin(0.5 * angle)], -1)
+
+
+def rotmat(q):
+    """(..., 3, 3) rotation matrices of unit quaternions."""
+    s, x, y, z = q.unbind(-1)
+    return torch.stack([
+        torch.stack([1 - 2 * (y * y + z * z), 2 * (x * y - s * z), 2 * (x * z + s * y)], -1),
+        torch.stack([2 * (x * y + s * z), 1 - 2 * (x * x + z * z), 2 * (y * z - s * x)], -1),
+        torch.stack([2 * (x * z - s * y), 2 * (y * z + s * x), 1 - 2 * (x * x + y * y)], -1)], -2)
+
+
+def pulse_quaternions(rf, dt, gz, z, df, b1):
+    """Whole-pulse rotation q and reduced rotation q~ of every sample (z [m], df [Hz], b1), float64.
+    ``rf`` (K, 2) [Hz] at steps of ``dt`` [s] under the slice gradient ``gz`` [Hz/m]."""
+    rf = torch.as_tensor(rf, dtype=F64)
+    z, df, b1 = (torch.as_tensor(t, dtype=F64) for t in (z, df, b1))
+    q = torch.zeros(z.shape + (4,), dtype=F64)
+    q[..., 0] = 1.0
+    w = -TWO_PI * dt
+    wz = w * (gz * z + df)
+    for k in range(rf.shape[0]):
+        wv = torch.stack([w * b1 * rf[k, 0], w * b1 * rf[k, 1], wz], -1)
+        q = qmul(quat_of_rotvec(wv), q)
+    total = wz * rf.shape[0]
+    qr = qmul(qmul(qz(-0.5 * total), q), qz(-0.5 * total))
+    return q, qr
+
+
+def gelu(x):
+    """GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))) (Hendrycks and Gimpel)."""
+    return 0.5 * x * (1.0 + torch.tanh(math.sqrt(2.0 / math.pi) * (x + 0.044715 * x ** 3)))
+
+
+# parameter layout of the flat vector (as the kernels): W1 (64, 3), b1 (64), W2 (64, 64), b2, W3 (64, 64), b3,
+# W4 (4, 64), b4 (4): 8,836 floats
+SHAPES = ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (4, 64), (4,))
+N_PARAMS = sum(math.prod(s) for s in SHAPES)
+
+
+def unflatten(p):
+    out, o = [], 0
+    for s in SHAPES:
+        k = math.prod(s)
+        out.append(p[o:o + k].reshape(s))
+        o += k
+    return out
+
+
+def mlp(p, x):
+    """Network output (B, 4), normalised to unit length, for normalised inputs x (B, 3)."""
+    w1, b1, w2, b2, w3, b3, w4, b4 = unflatten(p)
+    h = gelu(x @ w1.T + b1)
+    h = gelu(h @ w2.T + b2)
+    h = gelu(h @ w3.T + b3)
+    y = h @ w4.T + b4
+    return y / torch.linalg.vector_norm(y, dim=-1, keepdim=True)
+
+
+def loss_and_grad(p, x, target):
+    """Mean over the batch of |q_pred - q_target|^2 and its gradient w.r.t. the flat parameters (float64)."""
+    p = p.detach().to(F64).clone().requires_grad_()
+    loss = ((mlp(p, x.to(F64)) - target.to(F64)) ** 2).sum(-1).mean()
+    (g,) = torch.autograd.grad(loss, [p])
+    return float(loss), g
