@@ -1,0 +1,270 @@
+"""Learned RF surrogate: a small network per shaped pulse, trained on the GPU, standing in for the pulse's
+sub-stepped integration (``simulate(..., pulses="surrogate", surrogate=[...])``).
+
+The reference has no learned part; its nearest mechanism is the exact per-spin map of a reused pulse
+(blochparty ``engines/gpu/driver.py:112-164``, ``engines/gpu/cuda/pulse.cu.in:3-32``). Here each distinct pulse
+waveform (dt, slice gradient G along z, RF samples) gets a 3 -> 64 -> 64 -> 64 -> 4 GELU network mapping
+(off-resonance df, B1 scale, slice position z_rel = (z - z0) / thickness) to the unit quaternion (the Cayley-Klein
+pair) of the pulse's rotation reduced by its free precession, R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T.
+The targets come from the plain integrator (``bp_pulse_quats``: the per-step rotations composed in float64); the
+network is trained by the hand-written kernels ``bp_mlp_grad`` / ``bp_mlp_reduce`` / ``bp_adam``.
+
+In a simulation, every occurrence of a trained pulse (the same dt and gradient, RF = trained waveform x exp(i phi0),
+uniform b0_offset, no sample or spoil inside) is applied by ``bp_surrogate_pulse``: spins inside the training
+domain (|df| <= 200 Hz, |b1 - 1| <= 0.3, |z_rel| <= 2) take the network's rotation between two half-pulse
+relaxations; the others take the plain sub-stepped segments (the fallback, which is also the judge: the plain
+simulation is the same call without the surrogate).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib, engine
+from ._lib import ptr
+
+F32, F64 = torch.float32, torch.float64
+TWO_PI = 2.0 * math.pi
+DOMAIN = (200.0, 0.3, 2.0)  # |df| [Hz], |b1 - 1|, |z_rel| [slice widths]
+
+
+def _fan_in_init(seed: int) -> torch.Tensor:
+    """Flat initial parameters: weights N(0, 1/fan_in), biases 0 (seeded)."""
+    g = torch.Generator().manual_seed(seed)
+    parts = []
+    for shape in ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (4, 64), (4,)):
+        if len(shape) == 2:
+            parts.append(torch.randn(shape, generator=g, dtype=F64).reshape(-1) / math.sqrt(shape[1]))
+        else:
+            parts.append(torch.zeros(shape, dtype=F64))
+    p = torch.cat(parts)
+    p[-4] = 1.0  # output bias toward the identity rotation (1, 0, 0, 0)
+    return p.to(F32)
+
+
+@dataclass
+class TrainLog:
+    steps: int = 0
+    epochs: int = 0
+    loss: list = field(default_factory=list)  # mean loss per epoch
+
+
+class RFSurrogate:
+    """The network of one shaped pulse: ``rf`` (K, 2) [Hz] on a raster ``dt`` [s] under the slice gradient ``gz``
+    [Hz/m] (along z), slice ``thickness`` [m] centred at ``z0`` [m] (default: from the waveform's phase ramp)."""
+
+    def __init__(self, rf, dt: float, gz: float, thickness: float, z0: float | None = None, device=None, seed=5):
+        self.rf = torch.as_tensor(np.asarray(rf, dtype=np.float64))
+        self.dt, self.gz, self.thickness = float(dt), float(gz), float(thickness)
+        self.K = self.rf.shape[0]
+        self.T = self.K * self.dt
+        self.z0 = self._centre() if z0 is None else float(z0)
+        if device is None:
+            device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+        self.device = torch.device(device)
+        self.params = _fan_in_init(seed).to(self.device)
+        self.seed = seed
+        self.log = TrainLog()
+
+    def _centre(self) -> float:
+        """Slice centre from the waveform's linear phase ramp: RF ~ exp(-i 2 pi G z0 t) (least squares on the phase
+        steps between samples of significant amplitude)."""
+        z = self.rf[:, 0].numpy() + 1j * self.rf[:, 1].numpy()
+        on = np.abs(z) > 1e-3 * np.abs(z).max()
+        steps = np.angle(z[1:] * np.conj(z[:-1]))[on[1:] & on[:-1]]
+        steps = steps[np.abs(steps) < 0.5 * np.pi]  # the sinc's sign flips are pi steps
+        if steps.size == 0 or self.gz == 0:
+            return 0.0
+        f = -float(np.median(steps)) / (TWO_PI * self.dt)
+        return f / self.gz
+
+    # ---- targets and training ----
+    def samples(self, n: int, seed: int) -> torch.Tensor:
+        """n uniform samples (df [Hz], b1, z_rel) of the training domain, (n, 3) float32 on the device."""
+        g = torch.Generator().manual_seed(seed)
+        u = torch.rand(n, 3, generator=g, dtype=F64) * 2 - 1
+        s = torch.stack([u[:, 0] * DOMAIN[0], 1 + u[:, 1] * DOMAIN[1], u[:, 2] * DOMAIN[2]], -1)
+        return s.to(F32).to(self.device).contiguous()
+
+    def targets(self, samples: torch.Tensor, full: bool = False):
+        """Reduced rotations (n, 4) (and the whole rotations) of the samples from the plain integrator."""
+        n = samples.shape[0]
+        rf = self.rf.to(self.device).contiguous()
+        qred = torch.empty(n, 4, dtype=F32, device=self.device)
+        qfull = torch.empty(n, 4, dtype=F32, device=self.device) if full else None
+        code = _lib.lib().bp_pulse_quats(ptr(rf), self.K, self.dt, self.gz, self.thickness, self.z0, ptr(samples), n,
+                                         ptr(qred), ptr(qfull), _lib.stream_ptr())
+        _lib.check(code, "bp_pulse_quats")
+        return (qred, qfull) if full else qred
+
+    @staticmethod
+    def normalise(samples: torch.Tensor) -> torch.Tensor:
+        s = samples
+        return torch.stack([s[:, 0] / DOMAIN[0], (s[:, 1] - 1) / DOMAIN[1], s[:, 2] / DOMAIN[2]], -1).contiguous()
+
+    def gradient(self, x: torch.Tensor, target: torch.Tensor):
+        """(mean loss, gradient) of the batch through the training kernels (x normalised)."""
+        lib, n = _lib.lib(), x.shape[0]
+        ctas = lib.bp_mlp_grad_ctas(n)
+        gpart = torch.empty(ctas, _lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
+        lpart = torch.empty(ctas, dtype=F32, device=self.device)
+        grad = torch.empty(_lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
+        loss = torch.empty(1, dtype=F32, device=self.device)
+        st = _lib.stream_ptr()
+        _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(x), ptr(target), n, ptr(gpart), ptr(lpart), st), "bp_mlp_grad")
+        _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / n, ptr(grad), ptr(loss), st), "bp_mlp_reduce")
+        return loss, grad
+
+    def train(self, n_samples: int = 1 << 20, epochs: int = 60, batch: int = 16384, lr: float = 3e-3,
+              lr_min: float = 3e-5, seed: int | None = None) -> TrainLog:
+        """Adam with a cosine learning-rate decay over ``epochs`` passes of ``n_samples`` plain-integrator targets."""
+        lib, st = _lib.lib(), _lib.stream_ptr()
+        seed = self.seed if seed is None else seed
+        s = self.samples(n_samples, seed + 1)
+        x, y = self.normalise(s), self.targets(s)
+        m = torch.zeros(_lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
+        v = torch.zeros_like(m)
+        ctas = lib.bp_mlp_grad_ctas(batch)
+        gpart = torch.empty(ctas, _lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
+        lpart = torch.empty(ctas, dtype=F32, device=self.device)
+        grad = torch.empty_like(m)
+        loss = torch.zeros(1, dtype=F32, device=self.device)
+        steps_per_epoch = n_samples // batch
+        total = epochs * steps_per_epoch
+        g = torch.Generator(device="cpu").manual_seed(seed + 2)
+        for ep in range(epochs):
+            perm = torch.randperm(n_samples, generator=g).to(self.device)
+            xs, ys = x[perm].contiguous(), y[perm].contiguous()
+            acc = torch.zeros(1, dtype=F32, device=self.device)
+            for b in range(steps_per_epoch):
+                step = self.log.steps + 1
+                frac = (ep * steps_per_epoch + b) / max(total - 1, 1)
+                rate = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * frac))
+                xb, yb = xs[b * batch:(b + 1) * batch], ys[b * batch:(b + 1) * batch]
+                _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(xb), ptr(yb), batch, ptr(gpart), ptr(lpart), st),
+                           "bp_mlp_grad")
+                _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / batch, ptr(grad), ptr(loss), st),
+                           "bp_mlp_reduce")
+                _lib.check(lib.bp_adam(ptr(self.params), ptr(grad), ptr(m), ptr(v), rate, 0.9, 0.999, 1e-8, step, st),
+                           "bp_adam")
+                acc += loss
+                self.log.steps = step
+            self.log.epochs += 1
+            self.log.loss.append(float(acc) / steps_per_epoch)
+        torch.cuda.synchronize(self.device)
+        return self.log
+
+    def predict(self, samples: torch.Tensor) -> torch.Tensor:
+        """The network's reduced rotations (n, 4) for samples (df, b1, z_rel)."""
+        x = self.normalise(samples)
+        y = torch.empty(x.shape[0], 4, dtype=F32, device=self.device)
+        _lib.check(_lib.lib().bp_mlp_eval(ptr(self.params), ptr(x), x.shape[0], ptr(y), _lib.stream_ptr()),
+                   "bp_mlp_eval")
+        return y
+
+    def validate(self, n: int = 1 << 16, seed: int = 99):
+        """Largest and RMS error of the network's reduced rotation against the plain integrator's, on fresh samples
+        (quaternion components; the rotation-matrix error is at most twice as large)."""
+        s = self.samples(n, seed)
+        err = (self.predict(s) - self.targets(s)).abs()
+        return float(err.max()), float(err.pow(2).mean().sqrt())
+
+    # ---- matching occurrences in a sequence ----
+    def match(self, dt, rf, grad, b0, is_rf, adc, spoil, tol: float = 1e-6):
+        """Occurrences [(first segment, phi0, b0_offset)] of this pulse in a sequence (numpy float64 arrays)."""
+        K = self.K
+        z = self.rf[:, 0].numpy() + 1j * self.rf[:, 1].numpy()
+        peak = float(np.abs(z).max())
+        S = len(dt)
+        run_start = is_rf & ~np.concatenate([[False], is_rf[:-1]])
+        out = []
+        for s in np.flatnonzero(run_start):
+            while s + K <= S and is_rf[s:s + K].all():  # back-to-back occurrences within one RF run
+                e = s + K
+                seg = slice(s, e)
+                ok = (not adc[seg].any() and not spoil[seg].any()
+                      and np.abs(dt[seg] - self.dt).max() <= 1e-9 * self.dt
+                      and np.abs(grad[seg, :2]).max() <= 1e-9 * max(abs(self.gz), 1.0)
+                      and np.abs(grad[seg, 2] - self.gz).max() <= 1e-9 * max(abs(self.gz), 1.0)
+                      and np.abs(b0[seg] - b0[s]).max() <= 1e-9)
+                if not ok:
+                    break
+                w = rf[seg, 0] + 1j * rf[seg, 1]
+                c = np.vdot(z, w)
+                phi0 = float(np.angle(c)) if c != 0 else 0.0
+                if np.abs(w - z * np.exp(1j * phi0)).max() > tol * peak:
+                    break
+                out.append((int(s), phi0, float(b0[s])))
+                s = e
+        return out
+
+
+def find_occurrences(surrogates, inp):
+    """[(start, K, surrogate index, phi0, b0)] of every pulse occurrence that one of ``surrogates`` stands in for,
+    sorted, non-overlapping."""
+    d = lambda t: t.detach().to(F64).cpu().numpy()
+    dt, rf, grad = d(inp.dt), d(inp.rf), d(inp.grad)
+    b0 = np.zeros(len(dt)) if inp.b0_offset is None else d(inp.b0_offset)
+    is_rf, adc, spoil = (np.asarray(f, dtype=bool) for f in (inp.is_rf, inp.adc, inp.spoil))
+    occ = []
+    for i, sg in enumerate(surrogates):
+        occ += [(s, sg.K, i, phi0, b) for s, phi0, b in sg.match(dt, rf, grad, b0, is_rf, adc, spoil)]
+    occ.sort()
+    keep, end = [], -1
+    for o in occ:
+        if o[0] >= end:
+            keep.append(o)
+            end = o[0] + o[1]
+    return keep
+
+
+def forward_with_surrogate(inp, device, options):
+    """``simulate(..., pulses="surrogate")``: signal (C, A) complex64 and m (N, 3) float32 on the CPU."""
+    surrogates = options.get("surrogate")
+    if surrogates is None:
+        raise ValueError("pulses='surrogate' needs surrogate=[RFSurrogate, ...] (trained networks)")
+    if isinstance(surrogates, RFSurrogate):
+        surrogates = [surrogates]
+    sig, m, _ = run_with_surrogates(inp, device, surrogates)
+    return sig, m
+
+
+def run_with_surrogates(inp, device, surrogates, counts_out: bool = False):
+    """The forward with every matched pulse occurrence through its surrogate; returns (signal, m, counts)."""
+    pk = engine.pack(inp, device)
+    occ = find_occurrences(surrogates, inp)
+    S = pk.flags.shape[0]
+    breaks = np.zeros(S, dtype=np.uint8)
+    for s, k, *_ in occ:
+        breaks[s] = 1
+        if s + k < S:
+            breaks[s + k] = 1
+    samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
+    windows = engine.plan_windows(pk.flags, samp, breaks=breaks)
+    wdev = torch.from_numpy(windows).to(device)
+    starts = windows[:, 0]
+    state = engine.initial_state(inp.pd, inp.m_init, device)
+    raw = torch.zeros(max(pk.n_adc, 1), 2 * pk.n_coils, dtype=F64, device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    counts = torch.zeros(2, dtype=torch.int32, device=device)
+    lib, st = _lib.lib(), _lib.stream_ptr()
+    w = 0
+    for s, k, i, phi0, b0 in occ:
+        wa = int(np.searchsorted(starts, s))
+        if wa > w:
+            engine.run_forward(pk, state, wdev, w, wa, raw if pk.n_adc else None, status)
+        sg = surrogates[i]
+        code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s, k, sg.T,
+                                      sg.gz, sg.thickness, sg.z0, phi0, b0, ptr(counts), st)
+        _lib.check(code, "bp_surrogate_pulse")
+        w = int(np.searchsorted(starts, s + k))
+    if w < windows.shape[0]:
+        engine.run_forward(pk, state, wdev, w, windows.shape[0], raw if pk.n_adc else None, status)
+    sig = engine.finish_signal(pk, raw)
+    torch.cuda.synchronize(device)
+    _lib.check_status(status, "bp_forward")
+    return sig.cpu(), engine.final_m(state), counts.cpu().tolist()

@@ -11,7 +11,7 @@ Each function returns ``(phantom, seq, coils)`` (plus extras where stated) as fl
 * ``adjoint_2d_128``: 128 x 128 ellipse phantom, 8 coils, 128 per-TR flips drawn uniformly in [5, 30] degrees
   (seed 3), a radial B1+ in [0.8, 1.2]; hard 20 us pulses, TR 10 ms, TE 5 ms; extras: the flips and the target
   T1 map (T1 (1 + 0.05 N(0, 1)), seed 4).
-* ``tse_3slice_128``: 3 slices of 128 x 128 with 8 spins per voxel spread through the slice thickness (393,216
+* ``tse_3slice_128``: 3 contiguous 5 mm slices of 128 x 128 with 8 spins per voxel spread through the slice thickness (393,216
   spins); multi-slice TSE, 90 / 180 windowed sincs (time-bandwidth 4, 3 ms, 300 steps), ETL 16, ESP 12 ms,
   TR 3 s.
 * ``gre3d_128_4echo``: 128^3 head-like phantom (fat, WM, GM, CSF), 4 spins per voxel (8,388,608 spins), B0 smooth
@@ -55,7 +55,7 @@ def adjoint_2d_128(n=128):
     return ph, seq, phantoms.birdcage_sensitivities(ph.pos, 8), flips, t1_target
 
 
-def tse_3slice_128(n=128, slice_thickness=5e-3, slice_gap=10e-3, spins_per_voxel=8):
+def tse_3slice_128(n=128, slice_thickness=5e-3, slice_gap=5e-3, spins_per_voxel=8):
     slices = (-slice_gap, 0.0, slice_gap)
     base = phantoms.ellipse_phantom_2d(n, 0.25, n_ellipses=10, seed=0)
     z_off = (torch.arange(spins_per_voxel, dtype=F64) + 0.5) / spins_per_voxel - 0.5

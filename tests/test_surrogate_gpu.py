@@ -1,0 +1,138 @@
+"""The learned RF surrogate on the GPU: training kernels against the float64 oracle, training, and the TSE
+workload through the surrogate against the float64 plain integrator (the judge).
+
+Bars: targets (float64 composition rounded to float32) within 1e-6 of the oracle; the training kernel's gradient
+within 1e-4 (largest relative error) of float64 autograd; the surrogate signal within 1e-3 relative L2 of the
+float64 oracle (the target for the learned form); and a measured speed-up over plain sub-stepping on the same GPU.
+"""
+
+import math
+import time
+
+import numpy as np
+import pytest
+import torch
+
+import blochparty_b200 as bpb
+from blochparty_b200 import _lib, sequences, surrogate, workloads
+from blochparty_b200._lib import ptr
+from oracle import bloch
+from oracle import surrogate as S
+
+pytestmark = pytest.mark.gpu
+F64 = torch.float64
+
+
+def _pulse(flip=90.0, z0=0.0, phase=0.0):
+    return sequences.sinc_pulse(flip, 3e-3, 300, slice_thickness=5e-3, slice_offset=z0, phase=phase)
+
+
+def test_targets_match_the_float64_oracle():
+    w, dt, gz, _ = _pulse(180.0, 5e-3, 0.5 * math.pi)
+    sg = surrogate.RFSurrogate(w, dt, gz, 5e-3)
+    s = sg.samples(2000, seed=3)
+    qr, qf = sg.targets(s, full=True)
+    sc = s.double().cpu()
+    q_ref, qr_ref = S.pulse_quaternions(w, dt, gz, sg.z0 + sc[:, 2] * 5e-3, sc[:, 0], sc[:, 1])
+    assert float((qr.double().cpu() - qr_ref).abs().max()) < 1e-6
+    assert float((qf.double().cpu() - q_ref).abs().max()) < 1e-6
+
+
+def test_training_gradient_matches_float64_autograd():
+    w, dt, gz, _ = _pulse()
+    sg = surrogate.RFSurrogate(w, dt, gz, 5e-3, seed=11)
+    s = sg.samples(300, seed=4)  # 300: the last CTA is partly empty
+    x, t = sg.normalise(s), sg.targets(s)
+    loss, grad = sg.gradient(x, t)
+    ref_loss, ref_grad = S.loss_and_grad(sg.params.double().cpu(), x.double().cpu(), t.double().cpu())
+    assert abs(float(loss) - ref_loss) < 1e-5 * max(1.0, ref_loss)
+    err = float((grad.double().cpu() - ref_grad).abs().max() / ref_grad.abs().max())
+    assert err < 1e-4, err
+
+
+def test_adam_step():
+    lib = _lib.lib()
+    g = torch.Generator().manual_seed(0)
+    p = torch.randn(_lib.BP_MLP_PARAMS, generator=g).cuda()
+    grad = torch.randn(_lib.BP_MLP_PARAMS, generator=g).cuda()
+    m, v = torch.zeros_like(p), torch.zeros_like(p)
+    ref = p.clone()
+    rm, rv = torch.zeros_like(p), torch.zeros_like(p)
+    for step in (1, 2, 3):
+        _lib.check(lib.bp_adam(ptr(p), ptr(grad), ptr(m), ptr(v), 1e-3, 0.9, 0.999, 1e-8, step, _lib.stream_ptr()),
+                   "bp_adam")
+        rm = 0.9 * rm + 0.1 * grad
+        rv = 0.999 * rv + 0.001 * grad * grad
+        ref -= 1e-3 * (rm / (1 - 0.9 ** step)) / ((rv / (1 - 0.999 ** step)).sqrt() + 1e-8)
+    torch.cuda.synchronize()
+    assert float((p - ref).abs().max()) < 1e-6
+
+
+def test_training_lowers_the_loss_and_the_error():
+    w, dt, gz, _ = _pulse()
+    sg = surrogate.RFSurrogate(w, dt, gz, 5e-3)
+    before = sg.validate(1 << 14)
+    log = sg.train(n_samples=1 << 17, epochs=20, batch=8192)
+    after = sg.validate(1 << 14)
+    print("\nshort training: loss %.2e -> %.2e, max error %.2e -> %.2e" % (log.loss[0], log.loss[-1], before[0],
+                                                                           after[0]))
+    assert log.loss[-1] < 0.05 * log.loss[0]
+    assert after[1] < 0.1 * before[1]
+
+
+@pytest.fixture(scope="module")
+def tse_surrogates():
+    """Networks for the six TSE pulses (3 slices x excitation / refocusing), trained on 2^20 samples each."""
+    out, info = [], []
+    for z0 in (-5e-3, 0.0, 5e-3):
+        for flip, phase in ((90.0, 0.0), (180.0, 0.5 * math.pi)):
+            w, dt, gz, _ = _pulse(flip, z0, phase)
+            sg = surrogate.RFSurrogate(w, dt, gz, 5e-3)
+            t = time.perf_counter()
+            sg.train(n_samples=1 << 20, epochs=40, batch=16384)
+            info.append((flip, z0, time.perf_counter() - t, sg.validate()))
+            out.append(sg)
+    for flip, z0, sec, (mx, rms) in info:
+        print(f"\nsurrogate {flip:.0f} deg at {z0 * 1e3:+.0f} mm: trained in {sec:.1f} s, max {mx:.1e}, rms {rms:.1e}")
+    return out
+
+
+def test_tse_through_the_surrogate_against_the_float64_oracle(tse_surrogates):
+    ph, seq, coils = workloads.tse_3slice_128(16)
+    sig64, m64 = bloch.simulate(bloch.case_from(ph, seq, coils))
+    plain = bpb.simulate(ph, seq, coils)
+    sur = bpb.simulate(ph, seq, coils, pulses="surrogate", surrogate=tse_surrogates)
+    l2 = lambda a: float(torch.linalg.vector_norm(a.to(sig64.dtype) - sig64) / torch.linalg.vector_norm(sig64))
+    e_sur, e_plain = l2(sur.signal), l2(plain.signal)
+    print(f"\nTSE 16^2 x 3 slices: surrogate rel L2 {e_sur:.2e}, plain sub-stepping {e_plain:.2e} (vs float64)")
+    assert e_plain < 1e-5
+    assert e_sur < 1e-3
+
+
+def test_surrogate_gain_on_the_tse_workload(tse_surrogates):
+    """What the trained networks gain over the method without them: the full 3-slice TSE (393,216 spins), the
+    same GPU, plain sub-stepped pulses against the surrogate (timed after a warm-up run of each)."""
+    from blochparty_b200.api import Inputs
+
+    ph, seq, coils = workloads.tse_3slice_128()
+    inp = Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad, seq.adc_phase, None,
+                 list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
+    dev = torch.device("cuda", 0)
+    from blochparty_b200 import engine
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t, out
+
+    t_plain, (s_plain, _) = timed(lambda: engine.forward(inp, dev))
+    t_sur, (s_sur, _, counts) = timed(lambda: surrogate.run_with_surrogates(inp, dev, tse_surrogates))
+    rel = float(torch.linalg.vector_norm(s_sur - s_plain) / torch.linalg.vector_norm(s_plain))
+    frac = counts[0] / max(1, sum(counts))
+    print(f"\nTSE 393,216 spins: plain {t_plain:.3f} s, surrogate {t_sur:.3f} s, speed-up {t_plain / t_sur:.2f}x; "
+          f"{100 * frac:.1f}% of spin-pulse pairs through the networks; signal difference {rel:.1e}")
+    assert t_sur < t_plain
+    assert rel < 1e-3

@@ -1,0 +1,73 @@
+"""Host-side checks of the learned RF surrogate (no GPU): the float64 rotation oracle against closed forms, the
+frame relations the surrogate relies on, the network oracle's gradient, and the matching of pulse occurrences."""
+
+import math
+
+import numpy as np
+import torch
+
+from blochparty_b200 import api, sequences, surrogate, workloads
+from oracle import surrogate as S
+
+F64 = torch.float64
+
+
+def test_hard_pulse_quaternion_is_a_rotation_about_x():
+    """A constant RF of amplitude a for time T on resonance is the rotation by -2 pi a T about x."""
+    a, n, dt = 500.0, 50, 1e-5
+    rf = np.tile([[a, 0.0]], (n, 1))
+    q, qr = S.pulse_quaternions(rf, dt, 0.0, torch.zeros(1), torch.zeros(1), torch.ones(1))
+    angle = -2 * math.pi * a * n * dt
+    expect = torch.tensor([[math.cos(angle / 2), math.sin(angle / 2), 0.0, 0.0]], dtype=F64)
+    assert torch.allclose(q, expect, atol=1e-12) and torch.allclose(qr, expect, atol=1e-12)
+
+
+def test_reduced_rotation_without_rf_is_the_identity():
+    rf = np.zeros((30, 2))
+    z, df = torch.tensor([0.01, -0.02]), torch.tensor([30.0, -150.0])
+    q, qr = S.pulse_quaternions(rf, 1e-5, 2e5, z, df, torch.ones(2))
+    assert torch.allclose(qr, torch.tensor([[1.0, 0, 0, 0]] * 2, dtype=F64), atol=1e-12)
+    assert float((S.rotmat(q)[:, 2, 2] - 1).abs().max()) < 1e-12  # a pure z rotation
+
+
+def test_rf_phase_conjugates_the_reduced_rotation():
+    """RF x exp(i phi0): R = Rz(wz/2 + phi0) R~ Rz(wz/2 - phi0) with R~ the unshifted pulse's, exactly."""
+    base, dt, gz, _ = sequences.sinc_pulse(90.0, 3e-3, 300, slice_thickness=5e-3)
+    shifted, *_ = sequences.sinc_pulse(90.0, 3e-3, 300, slice_thickness=5e-3, phase=1.1)
+    z = torch.tensor([-0.004, 0.0, 0.002], dtype=F64)
+    df, b1 = torch.tensor([20.0, -80.0, 150.0], dtype=F64), torch.tensor([0.8, 1.0, 1.25], dtype=F64)
+    q, _ = S.pulse_quaternions(shifted, dt, gz, z, df, b1)
+    _, qr = S.pulse_quaternions(base, dt, gz, z, df, b1)
+    a = -2 * math.pi * (gz * z + df) * 300 * dt
+    cand = S.qmul(S.qmul(S.qz(0.5 * a + 1.1), qr), S.qz(0.5 * a - 1.1))
+    assert float((S.rotmat(q) - S.rotmat(cand)).abs().max()) < 1e-12
+
+
+def test_network_oracle_gradient_against_central_differences():
+    g = torch.Generator().manual_seed(0)
+    p = torch.randn(S.N_PARAMS, generator=g, dtype=F64) * 0.1
+    x = torch.rand(16, 3, generator=g, dtype=F64) * 2 - 1
+    t = torch.nn.functional.normalize(torch.randn(16, 4, generator=g, dtype=F64), dim=-1)
+    loss, grad = S.loss_and_grad(p, x, t)
+    for i in (0, 100, 300, 5000, 8832):
+        e = torch.zeros_like(p)
+        e[i] = 1e-6
+        fd = (S.loss_and_grad(p + e, x, t)[0] - S.loss_and_grad(p - e, x, t)[0]) / 2e-6
+        assert abs(fd - float(grad[i])) < 1e-6 * max(1.0, abs(fd))
+
+
+def test_occurrences_of_the_tse_pulses_are_found():
+    ph, seq, coils = workloads.tse_3slice_128(16)
+    sur = []
+    for z0 in (-5e-3, 0.0, 5e-3):
+        for flip, phase in ((90.0, 0.0), (180.0, 0.5 * math.pi)):
+            w, dt, gz, _ = sequences.sinc_pulse(flip, 3e-3, 300, slice_thickness=5e-3, slice_offset=z0, phase=phase)
+            sur.append(surrogate.RFSurrogate(w, dt, gz, 5e-3, device="cpu"))
+    assert [round(s.z0 * 1e3, 6) for s in sur] == [-5.0, -5.0, 0.0, 0.0, 5.0, 5.0]
+    inp = api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad, seq.adc_phase,
+                     None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
+    occ = surrogate.find_occurrences(sur, inp)
+    assert len(occ) == sum(seq.is_rf) // 300
+    starts = [o[0] for o in occ]
+    assert all(seq.is_rf[s] and (s == 0 or not seq.is_rf[s - 1]) for s in starts)
+    assert all(abs(o[3]) < 1e-9 for o in occ)  # every occurrence is one of the trained waveforms itself
