@@ -119,7 +119,7 @@ class RFSurrogate:
         _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / n, ptr(grad), ptr(loss), st), "bp_mlp_reduce")
         return loss, grad
 
-    def train(self, n_samples: int = 1 << 20, epochs: int = 60, batch: int = 16384, lr: float = 3e-3,
+    def train(self, n_samples: int = 1 << 20, epochs: int = 400, batch: int = 16384, lr: float = 2e-3,
               lr_min: float = 3e-5, seed: int | None = None) -> TrainLog:
         """Adam with a cosine learning-rate decay over ``epochs`` passes of ``n_samples`` plain-integrator targets."""
         lib, st = _lib.lib(), _lib.stream_ptr()
@@ -174,52 +174,62 @@ class RFSurrogate:
         return float(err.max()), float(err.pow(2).mean().sqrt())
 
     # ---- matching occurrences in a sequence ----
-    def match(self, dt, rf, grad, b0, is_rf, adc, spoil, tol: float = 1e-6):
-        """Occurrences [(first segment, phi0, b0_offset)] of this pulse in a sequence (numpy float64 arrays)."""
-        K = self.K
+    def match_at(self, s, dt, rf, grad, b0, is_rf, adc, spoil, tol: float = 1e-6):
+        """phi0 if segments [s, s + K) are an occurrence of this pulse (the same dt and slice gradient, RF = trained
+        waveform x exp(i phi0), uniform b0_offset, no sample or spoil), else None."""
+        K, e = self.K, s + self.K
+        if e > len(dt) or not is_rf[s:e].all():
+            return None
+        seg = slice(s, e)
+        scale = max(abs(self.gz), 1.0)
+        if (adc[seg].any() or spoil[seg].any() or np.abs(dt[seg] - self.dt).max() > 1e-9 * self.dt
+                or np.abs(grad[seg, :2]).max() > 1e-9 * scale or np.abs(grad[seg, 2] - self.gz).max() > 1e-9 * scale
+                or np.abs(b0[seg] - b0[s]).max() > 1e-9):
+            return None
         z = self.rf[:, 0].numpy() + 1j * self.rf[:, 1].numpy()
-        peak = float(np.abs(z).max())
-        S = len(dt)
-        run_start = is_rf & ~np.concatenate([[False], is_rf[:-1]])
-        out = []
-        for s in np.flatnonzero(run_start):
-            while s + K <= S and is_rf[s:s + K].all():  # back-to-back occurrences within one RF run
-                e = s + K
-                seg = slice(s, e)
-                ok = (not adc[seg].any() and not spoil[seg].any()
-                      and np.abs(dt[seg] - self.dt).max() <= 1e-9 * self.dt
-                      and np.abs(grad[seg, :2]).max() <= 1e-9 * max(abs(self.gz), 1.0)
-                      and np.abs(grad[seg, 2] - self.gz).max() <= 1e-9 * max(abs(self.gz), 1.0)
-                      and np.abs(b0[seg] - b0[s]).max() <= 1e-9)
-                if not ok:
-                    break
-                w = rf[seg, 0] + 1j * rf[seg, 1]
-                c = np.vdot(z, w)
-                phi0 = float(np.angle(c)) if c != 0 else 0.0
-                if np.abs(w - z * np.exp(1j * phi0)).max() > tol * peak:
-                    break
-                out.append((int(s), phi0, float(b0[s])))
-                s = e
-        return out
+        w = rf[seg, 0] + 1j * rf[seg, 1]
+        c = np.vdot(z, w)
+        phi0 = float(np.angle(c)) if c != 0 else 0.0
+        if np.abs(w - z * np.exp(1j * phi0)).max() > tol * float(np.abs(z).max()):
+            return None
+        return phi0
+
+
+def pulse_pieces(rf, dt, gz, thickness, pieces: int = 1, device=None, seed=5):
+    """Surrogates for a pulse cut into ``pieces`` consecutive equal parts (each a shorter shaped pulse with its own
+    network; the relaxation is then split around every piece, which shrinks the splitting error ~pieces^2)."""
+    rf = np.asarray(rf, dtype=np.float64)
+    k = rf.shape[0]
+    if k % pieces:
+        raise ValueError(f"{k} steps do not split into {pieces} equal pieces")
+    m = k // pieces
+    return [RFSurrogate(rf[i * m:(i + 1) * m], dt, gz, thickness, device=device, seed=seed + 17 * i)
+            for i in range(pieces)]
 
 
 def find_occurrences(surrogates, inp):
-    """[(start, K, surrogate index, phi0, b0)] of every pulse occurrence that one of ``surrogates`` stands in for,
-    sorted, non-overlapping."""
+    """[(start, K, surrogate index, phi0, b0)] of every pulse occurrence (or piece) that one of ``surrogates`` stands
+    in for: within every run of RF segments, from its start, the first surrogate that matches at the current
+    position takes it and the scan continues after it; at a position no surrogate matches, the rest of the run is
+    left to the plain integrator."""
     d = lambda t: t.detach().to(F64).cpu().numpy()
     dt, rf, grad = d(inp.dt), d(inp.rf), d(inp.grad)
     b0 = np.zeros(len(dt)) if inp.b0_offset is None else d(inp.b0_offset)
     is_rf, adc, spoil = (np.asarray(f, dtype=bool) for f in (inp.is_rf, inp.adc, inp.spoil))
+    run_start = is_rf & ~np.concatenate([[False], is_rf[:-1]])
     occ = []
-    for i, sg in enumerate(surrogates):
-        occ += [(s, sg.K, i, phi0, b) for s, phi0, b in sg.match(dt, rf, grad, b0, is_rf, adc, spoil)]
-    occ.sort()
-    keep, end = [], -1
-    for o in occ:
-        if o[0] >= end:
-            keep.append(o)
-            end = o[0] + o[1]
-    return keep
+    for s in np.flatnonzero(run_start):
+        s = int(s)
+        while True:
+            for i, sg in enumerate(surrogates):
+                phi0 = sg.match_at(s, dt, rf, grad, b0, is_rf, adc, spoil)
+                if phi0 is not None:
+                    occ.append((s, sg.K, i, phi0, float(b0[s])))
+                    s += sg.K
+                    break
+            else:
+                break
+    return occ
 
 
 def forward_with_surrogate(inp, device, options):

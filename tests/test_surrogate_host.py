@@ -71,3 +71,10 @@ def test_occurrences_of_the_tse_pulses_are_found():
     starts = [o[0] for o in occ]
     assert all(seq.is_rf[s] and (s == 0 or not seq.is_rf[s - 1]) for s in starts)
     assert all(abs(o[3]) < 1e-9 for o in occ)  # every occurrence is one of the trained waveforms itself
+    # the same pulses cut into two pieces each: twice the occurrences, back to back within every pulse
+    halves = [h for z0 in (-5e-3, 0.0, 5e-3) for flip, phase in ((90.0, 0.0), (180.0, 0.5 * math.pi))
+              for h in surrogate.pulse_pieces(sequences.sinc_pulse(flip, 3e-3, 300, slice_thickness=5e-3,
+                                                                   slice_offset=z0, phase=phase)[0],
+                                              1e-5, sur[0].gz, 5e-3, pieces=2, device="cpu")]
+    occ2 = surrogate.find_occurrences(halves, inp)
+    assert len(occ2) == 2 * len(occ) and all(o[1] == 150 for o in occ2)
