@@ -51,7 +51,12 @@ SIGNATURES = {
     "bp_adam": (c_int, [_P, _P, _P, _P, c_float, c_float, c_float, c_float, c_int, _P]),
     "bp_mlp_eval": (c_int, [_P, _P, c_int, _P, _P]),
     "bp_surrogate_pulse": (c_int, [_P, _P, c_int, _P, _P, c_int, c_int, c_double, c_double, c_double, c_double,
-                                   c_double, c_float, _P, _P]),
+                                   c_double, c_float, c_float, c_float, c_float, _P, _P]),
+    "bp_mlp_wtiles_bytes": (c_int, []),
+    "bp_mlp_wtiles": (c_int, [_P, _P, _P]),
+    "bp_surrogate_pulse_mma_grid": (c_int, [c_int]),
+    "bp_surrogate_pulse_mma": (c_int, [_P, _P, c_int, _P, _P, _P, c_int, c_int, c_double, c_double, c_double,
+                                       c_double, c_double, c_float, c_float, c_float, c_float, _P, _P, c_int, _P]),
     "bp_adjoint_noalloc": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P,
                                    _P, _P]),
 }

@@ -21,7 +21,7 @@ from . import capabilities, engine
 from .types import SimResult
 
 ENGINES = ("b200", "gpu", "cuda")  # "gpu" and "cuda" name this engine too, so a caller's engine= still works
-OPTIONS = ("readout", "pulses", "surrogate", "max_ctas")
+OPTIONS = ("readout", "pulses", "surrogate", "surrogate_inference", "max_ctas")
 REFERENCE_GPU_OPTIONS = ("chunk", "group", "mma", "readouts", "nufft_width", "nufft_terms")
 READOUTS = ("fp32", "bf16x3")
 
@@ -80,7 +80,8 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
         boundaries); default about sqrt(segments).
     options: ``readout`` "fp32" (default: float32 coil products reduced by warp shuffles) or "bf16x3" (the coil
         contraction on the tensor cores in split bfloat16 with float32 accumulation); ``pulses`` "step"
-        (default) or "surrogate" (shaped pulses through a trained ``surrogate``); ``max_ctas`` caps the grid.
+        (default) or "surrogate" (shaped pulses through a trained ``surrogate``), whose ``surrogate_inference``
+        is "mma" (default: the hidden 64 x 64 layers on the tensor cores) or "fp32"; ``max_ctas`` caps the grid.
     """
     if engine not in ENGINES:
         raise ValueError(f"engine must be one of {ENGINES}, not {engine!r}")

@@ -36,10 +36,8 @@
 
 static_assert(N_PARAMS == BP_MLP_PARAMS, "parameter count");
 
-// input normalisation of the training domain: df in [-200, 200] Hz, b1 in [0.7, 1.3], z_rel in [-2, 2]
-#define DOM_DF 200.0f
-#define DOM_B1 0.3f
-#define DOM_Z 2.0f
+// The training domain of a network is |df| <= dom_df [Hz], |b1 - 1| <= dom_b1, |z_rel| <= dom_z [slice widths]
+// (the caller's choice); its inputs are normalised to (df / dom_df, (b1 - 1) / dom_b1, z_rel / dom_z).
 
 struct dq4 {
     double w, x, y, z;
@@ -93,18 +91,20 @@ extern "C" int bp_pulse_quats(const double* rf, int k_steps, double dt, double g
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
-// GELU in its tanh form, 0.5 x (1 + tanh(c (x + 0.044715 x^3))), c = sqrt(2/pi) (Hendrycks and Gimpel), and its
-// derivative; tanhf is the accurate library function.
-__device__ __forceinline__ float gelu_f(float x) {
-    const float c = 0.7978845608028654f;
-    const float t = tanhf(c * fmaf(0.044715f * x, x * x, x));
-    return 0.5f * x * (1.0f + t);
+// GELU in its tanh form, 0.5 x (1 + tanh(u)), u = c (x + 0.044715 x^3), c = sqrt(2/pi) (Hendrycks and Gimpel),
+// evaluated as the identical x sigma(2u) = x / (1 + exp(-2u)) with the fast exponential and divide (absolute error
+// of sigma ~1e-7); the derivative is sigma(2u) + x s (1 - s) 2 du/dx. exp(-2u) overflowing to inf gives 0, the limit.
+__device__ __forceinline__ float gelu_sig(float x) {
+    const float c2 = 2.0f * 0.7978845608028654f;
+    return __fdividef(1.0f, 1.0f + __expf(-c2 * fmaf(0.044715f * x, x * x, x)));
 }
 
+__device__ __forceinline__ float gelu_f(float x) { return x * gelu_sig(x); }
+
 __device__ __forceinline__ float gelu_d(float x) {
-    const float c = 0.7978845608028654f;
-    const float t = tanhf(c * fmaf(0.044715f * x, x * x, x));
-    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * c * fmaf(3.0f * 0.044715f * x, x, 1.0f);
+    const float c2 = 2.0f * 0.7978845608028654f;
+    const float s = gelu_sig(x);
+    return fmaf(x * s * (1.0f - s), c2 * fmaf(3.0f * 0.044715f * x, x, 1.0f), s);
 }
 
 // ---- training: forward + backward over a batch ----
@@ -398,7 +398,28 @@ struct PulseArgs {
     double T, gz, thickness, z0, phi0;  // duration [s], slice gradient [Hz/m], thickness [m], centre [m], RF phase
     float b0off;          // the occurrence's uniform off-resonance [Hz]
     int* counts;          // null or [2]: spins through the network, spins through the fallback
+    float dom_df, dom_b1, dom_z;  // the network's training domain
 };
+
+// The plain sub-stepped pulse for spin j (the fallback outside the domain).
+__device__ __forceinline__ void fallback_spin(const PulseArgs& a, int j) {
+    const Spin p = load_spin(a.spins, a.n, j, true);
+    float mx = a.state[j], my = a.state[a.n + j], mz = a.state[2 * a.n + j];
+    float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
+    RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k < a.k_steps; ++k) {
+        const SegRec q = a.segs[a.seg0 + k];
+        if (k == 0 || !(q.flags & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
+        rf_step(q, p, rr, mx, my, mz, lx, ly, lz);
+    }
+    a.state[j] = mx, a.state[a.n + j] = my, a.state[2 * a.n + j] = mz;
+    a.state[3 * a.n + j] = lx, a.state[4 * a.n + j] = ly, a.state[5 * a.n + j] = lz;
+}
+
+// sin and cos of a float64 angle to float32: reduced to [-pi, pi] in float64, then sincosf.
+__device__ __forceinline__ void sincos_reduced(double x, float* s, float* c) {
+    sincosf((float)(x - 2.0 * M_PI * rint(x * (0.5 / M_PI))), s, c);
+}
 
 __device__ __forceinline__ void quat_mul_f(const float a[4], const float b[4], float o[4]) {
     o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
@@ -417,7 +438,7 @@ __global__ void __launch_bounds__(128) bp_surrogate_pulse_kernel(PulseArgs a) {
     const Spin p = load_spin(a.spins, a.n, jj, active);
     const float df = p.db0 + a.b0off;
     const float zr = (float)(((double)p.pz - a.z0) / a.thickness);
-    const bool inside = fabsf(df) <= DOM_DF && fabsf(p.b1 - 1.0f) <= DOM_B1 && fabsf(zr) <= DOM_Z;
+    const bool inside = fabsf(df) <= a.dom_df && fabsf(p.b1 - 1.0f) <= a.dom_b1 && fabsf(zr) <= a.dom_z;
     if (a.counts) {
         const unsigned in_mask = __ballot_sync(0xffffffffu, active && inside);
         const unsigned out_mask = __ballot_sync(0xffffffffu, active && !inside);
@@ -430,17 +451,17 @@ __global__ void __launch_bounds__(128) bp_surrogate_pulse_kernel(PulseArgs a) {
     float mx = a.state[j], my = a.state[a.n + j], mz = a.state[2 * a.n + j];
     float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
     if (inside) {
-        const float xin[3] = {df / DOM_DF, (p.b1 - 1.0f) / DOM_B1, zr / DOM_Z};
+        const float xin[3] = {df / a.dom_df, (p.b1 - 1.0f) / a.dom_b1, zr / a.dom_z};
         float y[4];
         mlp_forward_row(P, xin, nullptr, nullptr, nullptr, y);
         const float inv = rsqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
         const float qr[4] = {y[0] * inv, y[1] * inv, y[2] * inv, y[3] * inv};
         // R = Rz(wz/2 + phi0) R~ Rz(wz/2 - phi0), wz = -2 pi (G z + df) T: the half angles in float64
         const double half = -M_PI * ((double)a.gz * (double)p.pz + (double)df) * a.T;
-        double s1, c1, s2, c2;
-        sincos(0.5 * (half + a.phi0), &s1, &c1);
-        sincos(0.5 * (half - a.phi0), &s2, &c2);
-        const float qa[4] = {(float)c1, 0.f, 0.f, (float)s1}, qb[4] = {(float)c2, 0.f, 0.f, (float)s2};
+        float s1, c1, s2, c2;
+        sincos_reduced(0.5 * (half + a.phi0), &s1, &c1);
+        sincos_reduced(0.5 * (half - a.phi0), &s2, &c2);
+        const float qa[4] = {c1, 0.f, 0.f, s1}, qb[4] = {c2, 0.f, 0.f, s2};
         float t[4], q[4];
         quat_mul_f(qa, qr, t);
         quat_mul_f(t, qb, q);
@@ -472,11 +493,340 @@ __global__ void __launch_bounds__(128) bp_surrogate_pulse_kernel(PulseArgs a) {
 
 extern "C" int bp_surrogate_pulse(const float* spins, float* state, int n, const float* params, const void* segs,
                                   int seg0, int k_steps, double T, double gz, double thickness, double z0, double phi0,
-                                  float b0off, int32_t* counts, void* stream) {
-    if (!spins || !state || !params || !segs || n < 1 || seg0 < 0 || k_steps < 1 || T <= 0 || thickness <= 0)
+                                  float b0off, float dom_df, float dom_b1, float dom_z, int32_t* counts,
+                                  void* stream) {
+    if (!spins || !state || !params || !segs || n < 1 || seg0 < 0 || k_steps < 1 || T <= 0 || thickness <= 0 ||
+        !(dom_df > 0) || !(dom_b1 > 0) || !(dom_z > 0))
         return BP_E_ARG;
     PulseArgs a{spins, state, params, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0, phi0,
-                b0off, counts};
+                b0off, counts, dom_df, dom_b1, dom_z};
     bp_surrogate_pulse_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(a);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+// ---- inference on the tensor cores: layers 2 and 3 (64 x 64) as tcgen05 matrix products ----
+//
+// Per CTA tile of 128 spins (thread t = spin row t = tensor-memory lane t): layer 1 on the CUDA cores, its
+// GELU outputs split into bfloat16 high and low parts and stored as the A operand (128 x 64, K-major); layer 2 is
+// D = A_hi W2_hi^T + A_hi W2_lo^T + A_lo W2_hi^T (M = 128, N = 64, K = 64 in 4 steps, float32 in 64 tensor-memory
+// columns); each thread reads its row of D back (tcgen05.ld), adds the bias, applies GELU and stores the next A;
+// layer 3 likewise; layer 4 (64 -> 4) on the CUDA cores. Shared memory: W2 hi, W2 lo, W3 hi, W3 lo (8192 bytes
+// each, [0, 32768)), A hi and A lo (16384 each, [32768, 65536)), the small parameters, mbarriers. Layout of every
+// operand: core matrices of 8 rows x 16 bytes, K-adjacent ones 128 bytes apart, 8-row groups 1024 bytes apart; a
+// thread writes its row 16 bytes at a time, so the 8 lanes of each store phase fill one 128-byte line.
+#include "tcgen05.cuh"
+
+#define SI_W_BYTES 8192
+#define SI_OFF_A 32768
+#define SI_A_BYTES 16384
+#define SI_OFF_P 65536
+#define SI_NP (MLP_H * MLP_IN + MLP_H + MLP_H + MLP_H + MLP_OUT * MLP_H + MLP_OUT)  // W1 b1 b2 b3 W4 b4
+#define SI_OFF_LIST (SI_OFF_P + ((SI_NP * 4 + 127) / 128) * 128)  // queued fallback spins (256 ints)
+#define SI_LIST 256
+#define SI_OFF_BAR (SI_OFF_LIST + SI_LIST * 4)
+#define SI_SMEM (SI_OFF_BAR + 64)
+#define SI_LBO 128
+#define SI_SBO 1024
+#define SI_COLS 64
+
+// the small parameters' offsets inside the shared copy
+#define Q_W1 0
+#define Q_B1 (Q_W1 + MLP_H * MLP_IN)
+#define Q_B2 (Q_B1 + MLP_H)
+#define Q_B3 (Q_B2 + MLP_H)
+#define Q_W4 (Q_B3 + MLP_H)
+#define Q_B4 (Q_W4 + MLP_OUT * MLP_H)
+
+// 64 activations of this thread's row -> A hi and A lo rows (16-byte stores)
+__device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned char* alo, int row, const float* v) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            uint16_t h0, l0, h1, l1;
+            split_bf16(v[8 * c + 2 * w], h0, l0);
+            split_bf16(v[8 * c + 2 * w + 1], h1, l1);
+            h[w] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+            l[w] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+        }
+        const uint32_t off = (uint32_t)((row >> 3) * SI_SBO + c * SI_LBO + (row & 7) * 16);
+        *reinterpret_cast<uint4*>(ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+}
+
+struct PulseMmaArgs {
+    PulseArgs p;
+    const uint8_t* wtiles;  // [4][8192]: W2 hi, W2 lo, W3 hi, W3 lo in the operand layout (bp_mlp_wtiles)
+    int* status;
+};
+
+__global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMmaArgs args) {
+    extern __shared__ __align__(1024) unsigned char smb[];
+    const PulseArgs& a = args.p;
+    float* Q = reinterpret_cast<float*>(smb + SI_OFF_P);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smb + SI_OFF_BAR);  // [0] weights, [1] MMA
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smb + SI_OFF_BAR + 2 * sizeof(uint64_t));
+    int* queued = reinterpret_cast<int*>(smb + SI_OFF_BAR + 3 * sizeof(uint64_t));
+    int* flist = reinterpret_cast<int*>(smb + SI_OFF_LIST);
+    unsigned char* ahi = smb + SI_OFF_A;
+    unsigned char* alo = smb + SI_OFF_A + SI_A_BYTES;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t sW = smem_u32(smb), sA = smem_u32(ahi);
+    const uint32_t idesc = umma_idesc_bf16_f32(128, MLP_H);
+
+    // small parameters
+    for (int i = tid; i < MLP_H * MLP_IN; i += 128) Q[Q_W1 + i] = a.params[P_W1 + i];
+    for (int i = tid; i < MLP_H; i += 128) {
+        Q[Q_B1 + i] = a.params[P_B1 + i];
+        Q[Q_B2 + i] = a.params[P_B2 + i];
+        Q[Q_B3 + i] = a.params[P_B3 + i];
+    }
+    for (int i = tid; i < MLP_OUT * MLP_H; i += 128) Q[Q_W4 + i] = a.params[P_W4 + i];
+    if (tid < MLP_OUT) Q[Q_B4 + tid] = a.params[P_B4 + tid];
+    if (tid == 0) {
+        *queued = 0;
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        fence_proxy_async_smem();
+        mbar_expect_tx(&bars[0], 4 * SI_W_BYTES);
+        tma_load_1d(smb, args.wtiles, 4 * SI_W_BYTES, &bars[0]);
+    }
+    if (warp == 0) tmem_alloc(tmem_slot, SI_COLS);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+
+    uint32_t mma_phase = 0;
+    bool w_ready = false, fail = false, err = false, mma_out = false;
+    const int n_tiles = (a.n + 127) / 128;
+
+    for (int tile = blockIdx.x; tile < n_tiles && !fail; tile += gridDim.x) {
+        const int j0 = tile * 128 + tid;
+        const bool active = j0 < a.n;
+        const int j = active ? j0 : 0;
+        const Spin p = load_spin(a.spins, a.n, j, active);
+        const float df = p.db0 + a.b0off;
+        const float zr = (float)(((double)p.pz - a.z0) / a.thickness);
+        const bool inside = active && fabsf(df) <= a.dom_df && fabsf(p.b1 - 1.0f) <= a.dom_b1 && fabsf(zr) <= a.dom_z;
+        float v[MLP_H];
+        {   // layer 1 (the inputs of rows outside the domain are clamped: their outputs are not used)
+            const float x0 = fminf(fmaxf(df / a.dom_df, -1.f), 1.f);
+            const float x1 = fminf(fmaxf((p.b1 - 1.0f) / a.dom_b1, -1.f), 1.f);
+            const float x2 = fminf(fmaxf(zr / a.dom_z, -1.f), 1.f);
+#pragma unroll
+            for (int k = 0; k < MLP_H; ++k)
+                v[k] = gelu_f(fmaf(Q[Q_W1 + 3 * k], x0, fmaf(Q[Q_W1 + 3 * k + 1], x1, fmaf(Q[Q_W1 + 3 * k + 2], x2, Q[Q_B1 + k]))));
+        }
+        for (int layer = 0; layer < 2 && !fail; ++layer) {
+            store_row_bf16x2(ahi, alo, tid, v);
+            fence_proxy_async_smem();
+            tc_fence_before();
+            if (__syncthreads_or(err)) {
+                fail = true;
+                break;
+            }
+            if (tid == 0) {
+                if (!w_ready && !mbar_wait_bounded(&bars[0], 0)) err = true;
+                w_ready = true;
+                if (!err) {
+                    tc_fence_after();
+                    const uint32_t wh = sW + (uint32_t)(2 * layer) * SI_W_BYTES, wl = wh + SI_W_BYTES;
+                    uint64_t ah_d = umma_desc(sA, SI_LBO, SI_SBO), al_d = umma_desc(sA + SI_A_BYTES, SI_LBO, SI_SBO);
+                    uint64_t bh_d = umma_desc(wh, SI_LBO, SI_SBO), bl_d = umma_desc(wl, SI_LBO, SI_SBO);
+#pragma unroll
+                    for (int kk = 0; kk < MLP_H / 16; ++kk) {
+                        umma_bf16(tmem, ah_d, bh_d, idesc, kk > 0 ? 1u : 0u);
+                        umma_bf16(tmem, ah_d, bl_d, idesc, 1u);
+                        umma_bf16(tmem, al_d, bh_d, idesc, 1u);
+                        ah_d += 2 * SI_LBO / 16, al_d += 2 * SI_LBO / 16, bh_d += 2 * SI_LBO / 16, bl_d += 2 * SI_LBO / 16;
+                    }
+                    umma_commit(&bars[1]);
+                }
+            }
+            mma_out = true;
+            if (mbar_wait_bounded(&bars[1], mma_phase)) {
+                mma_phase ^= 1u;
+                mma_out = false;
+            } else {
+                err = true;
+            }
+            if (__syncthreads_or(err)) {
+                fail = true;
+                break;
+            }
+            tc_fence_after();
+            const float* bias = Q + (layer == 0 ? Q_B2 : Q_B3);
+#pragma unroll
+            for (int c0 = 0; c0 < MLP_H; c0 += 16) {
+                float d[16];
+                tmem_ld16(lane_addr + (uint32_t)c0, d);
+                tmem_ld_wait();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[c0 + i] = gelu_f(d[i] + bias[c0 + i]);
+            }
+            tc_fence_before();
+        }
+        if (fail) break;
+        if (inside) {
+            float mx = a.state[j], my = a.state[a.n + j], mz = a.state[2 * a.n + j];
+            float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
+            float y[4];
+#pragma unroll
+            for (int o = 0; o < MLP_OUT; ++o) {
+                float s = Q[Q_B4 + o];
+#pragma unroll
+                for (int i = 0; i < MLP_H; ++i) s = fmaf(Q[Q_W4 + MLP_H * o + i], v[i], s);
+                y[o] = s;
+            }
+            const float inv = rsqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+            const float qr[4] = {y[0] * inv, y[1] * inv, y[2] * inv, y[3] * inv};
+            const double half = -M_PI * ((double)a.gz * (double)p.pz + (double)df) * a.T;
+            float s1, c1, s2, c2;
+            sincos_reduced(0.5 * (half + a.phi0), &s1, &c1);
+            sincos_reduced(0.5 * (half - a.phi0), &s2, &c2);
+            const float qa[4] = {c1, 0.f, 0.f, s1}, qb[4] = {c2, 0.f, 0.f, s2};
+            float t4[4], q[4];
+            quat_mul_f(qa, qr, t4);
+            quat_mul_f(t4, qb, q);
+            const float s = q[0], x = q[1], yq = q[2], z = q[3];
+            const float R00 = 1 - 2 * (yq * yq + z * z), R01 = 2 * (x * yq - s * z), R02 = 2 * (x * z + s * yq);
+            const float R10 = 2 * (x * yq + s * z), R11 = 1 - 2 * (x * x + z * z), R12 = 2 * (yq * z - s * x);
+            const float R20 = 2 * (x * z - s * yq), R21 = 2 * (yq * z + s * x), R22 = 1 - 2 * (x * x + yq * yq);
+            const float th = (float)(0.5 * a.T);
+            const float e1 = expm1f(-th * p.r1), e2 = expm1f(-th * p.r2);
+            const float ax = (mx + lx) * (1.0f + e2), ay = (my + ly) * (1.0f + e2);
+            const float az = fmaf((mz + lz) - p.pd, e1, mz + lz);
+            const float nx = fmaf(R00, ax, fmaf(R01, ay, R02 * az));
+            const float ny = fmaf(R10, ax, fmaf(R11, ay, R12 * az));
+            const float nz = fmaf(R20, ax, fmaf(R21, ay, R22 * az));
+            mx = nx * (1.0f + e2), my = ny * (1.0f + e2), mz = fmaf(nz - p.pd, e1, nz);
+            lx = ly = lz = 0.0f;
+            a.state[j] = mx, a.state[a.n + j] = my, a.state[2 * a.n + j] = mz;
+            a.state[3 * a.n + j] = lx, a.state[4 * a.n + j] = ly, a.state[5 * a.n + j] = lz;
+        }
+        // spins outside the domain join the CTA's queue; whenever it holds 128, all threads step them (full warps
+        // whatever the spins' order)
+        const unsigned in_mask = __ballot_sync(0xffffffffu, inside);
+        const unsigned out_mask = __ballot_sync(0xffffffffu, active && !inside);
+        if (a.counts && (tid & 31) == 0) {
+            if (in_mask) atomicAdd(&a.counts[0], __popc(in_mask));
+            if (out_mask) atomicAdd(&a.counts[1], __popc(out_mask));
+        }
+        if (out_mask) {
+            int base = 0;
+            if ((tid & 31) == 0) base = atomicAdd(queued, __popc(out_mask));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (active && !inside) flist[base + __popc(out_mask & ((1u << (tid & 31)) - 1u))] = j;
+        }
+        __syncthreads();
+        const int nq = *queued;
+        if (nq >= 128) {
+            fallback_spin(a, flist[nq - 128 + tid]);
+            __syncthreads();
+            if (tid == 0) *queued = nq - 128;
+        }
+        __syncthreads();
+    }
+    if (!fail && tid < *queued) fallback_spin(a, flist[tid]);
+    // leave no copy or MMA in flight (failure paths), then free the tensor memory
+    if (tid == 0 && !w_ready) mbar_wait_bounded(&bars[0], 0);
+    if (mma_out) mbar_wait_bounded(&bars[1], mma_phase);
+    if ((fail || err) && tid == 0 && args.status) atomicOr(args.status, BP_ERR_TMA_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, SI_COLS);
+    }
+}
+
+// W2 and W3 -> four 8192-byte bfloat16 tiles (W2 hi, W2 lo, W3 hi, W3 lo) in the operand layout: row n (output
+// unit) and column k (input unit) at element (n / 8) 512 + (k / 8) 64 + (n % 8) 8 + k % 8.
+__global__ void bp_mlp_wtiles_kernel(const float* __restrict__ params, uint16_t* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * MLP_H * MLP_H) return;
+    const int l = i / (MLP_H * MLP_H), r = i % (MLP_H * MLP_H), n = r / MLP_H, k = r % MLP_H;
+    uint16_t h, lo;
+    split_bf16(params[(l ? P_W3 : P_W2) + r], h, lo);
+    const int e = (n >> 3) * 512 + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
+    out[(2 * l) * (SI_W_BYTES / 2) + e] = h;
+    out[(2 * l + 1) * (SI_W_BYTES / 2) + e] = lo;
+}
+
+extern "C" int bp_mlp_wtiles_bytes(void) { return 4 * SI_W_BYTES; }
+
+extern "C" int bp_mlp_wtiles(const float* params, void* tiles, void* stream) {
+    if (!params || !tiles) return BP_E_ARG;
+    if ((reinterpret_cast<uintptr_t>(tiles) & 15) != 0) return BP_E_ALIGN;
+    bp_mlp_wtiles_kernel<<<(2 * MLP_H * MLP_H + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        params, static_cast<uint16_t*>(tiles));
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
+// CTAs of bp_surrogate_pulse_mma for n spins: one per 128-spin tile up to the SMs x the residency by shared memory
+// (with the per-block reservation), registers, threads and tensor memory (512 columns per SM).
+static int pulse_mma_grid(int n, int max_ctas, int* grid_out) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    static bool configured[64] = {false};
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        if (cudaFuncSetAttribute(bp_surrogate_pulse_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SI_SMEM) != cudaSuccess ||
+            cudaFuncSetAttribute(bp_surrogate_pulse_mma_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+            return BP_E_LAUNCH;
+        configured[dev] = true;
+    }
+    int smem_sm = 0, smem_res = 0, regs_sm = 0, thr_sm = 0;
+    cudaFuncAttributes fa;
+    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, bp_surrogate_pulse_mma_kernel) != cudaSuccess)
+        return BP_E_LAUNCH;
+    int per_sm = smem_sm / (SI_SMEM + smem_res);
+    const int regs_block = ((fa.numRegs * 32 + 255) / 256) * 256 * 4;
+    if (regs_block > 0 && regs_sm / regs_block < per_sm) per_sm = regs_sm / regs_block;
+    if (thr_sm / 128 < per_sm) per_sm = thr_sm / 128;
+    if (per_sm > 512 / SI_COLS) per_sm = 512 / SI_COLS;
+    if (per_sm < 1) per_sm = 1;
+    const int n_tiles = (n + 127) / 128;
+    int grid = sms * per_sm;
+    if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+    if (grid > n_tiles) grid = n_tiles;
+    *grid_out = grid;
+    return BP_OK;
+}
+
+extern "C" int bp_surrogate_pulse_mma_grid(int n) {
+    int grid = 0;
+    if (n < 1) return -BP_E_ARG;
+    const int code = pulse_mma_grid(n, 0, &grid);
+    return code == BP_OK ? grid : -code;
+}
+
+extern "C" int bp_surrogate_pulse_mma(const float* spins, float* state, int n, const float* params,
+                                      const void* wtiles, const void* segs, int seg0, int k_steps, double T, double gz,
+                                      double thickness, double z0, double phi0, float b0off, float dom_df,
+                                      float dom_b1, float dom_z, int32_t* counts, int32_t* status, int max_ctas,
+                                      void* stream) {
+    if (!spins || !state || !params || !wtiles || !segs || !status || n < 1 || seg0 < 0 || k_steps < 1 || T <= 0 ||
+        thickness <= 0 || !(dom_df > 0) || !(dom_b1 > 0) || !(dom_z > 0))
+        return BP_E_ARG;
+    if ((reinterpret_cast<uintptr_t>(wtiles) & 15) != 0) return BP_E_ALIGN;
+    int grid = 0;
+    const int code = pulse_mma_grid(n, max_ctas, &grid);
+    if (code != BP_OK) return code;
+    PulseMmaArgs a{{spins, state, params, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0,
+                    phi0, b0off, counts, dom_df, dom_b1, dom_z},
+                   static_cast<const uint8_t*>(wtiles), status};
+    bp_surrogate_pulse_mma_kernel<<<grid, 128, SI_SMEM, static_cast<cudaStream_t>(stream)>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }

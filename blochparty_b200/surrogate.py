@@ -11,9 +11,9 @@ network is trained by the hand-written kernels ``bp_mlp_grad`` / ``bp_mlp_reduce
 
 In a simulation, every occurrence of a trained pulse (the same dt and gradient, RF = trained waveform x exp(i phi0),
 uniform b0_offset, no sample or spoil inside) is applied by ``bp_surrogate_pulse``: spins inside the training
-domain (|df| <= 200 Hz, |b1 - 1| <= 0.3, |z_rel| <= 2) take the network's rotation between two half-pulse
-relaxations; the others take the plain sub-stepped segments (the fallback, which is also the judge: the plain
-simulation is the same call without the surrogate).
+domain (by default |df| <= 200 Hz, |b1 - 1| <= 0.3, |z_rel| <= 2; a network's own ``domain`` otherwise) take the
+network's rotation between two half-pulse relaxations; the others take the plain sub-stepped segments (the fallback,
+which is also the judge: the plain simulation is the same call without the surrogate).
 """
 
 from __future__ import annotations
@@ -29,7 +29,7 @@ from ._lib import ptr
 
 F32, F64 = torch.float32, torch.float64
 TWO_PI = 2.0 * math.pi
-DOMAIN = (200.0, 0.3, 2.0)  # |df| [Hz], |b1 - 1|, |z_rel| [slice widths]
+DOMAIN = (200.0, 0.3, 2.0)  # default training domain: |df| [Hz], |b1 - 1|, |z_rel| [slice widths]
 
 
 def _fan_in_init(seed: int) -> torch.Tensor:
@@ -55,9 +55,11 @@ class TrainLog:
 
 class RFSurrogate:
     """The network of one shaped pulse: ``rf`` (K, 2) [Hz] on a raster ``dt`` [s] under the slice gradient ``gz``
-    [Hz/m] (along z), slice ``thickness`` [m] centred at ``z0`` [m] (default: from the waveform's phase ramp)."""
+    [Hz/m] (along z), slice ``thickness`` [m] centred at ``z0`` [m] (default: from the waveform's phase ramp), trained
+    on ``domain`` = (|df| [Hz], |b1 - 1|, |z_rel| [slice widths]) bounds."""
 
-    def __init__(self, rf, dt: float, gz: float, thickness: float, z0: float | None = None, device=None, seed=5):
+    def __init__(self, rf, dt: float, gz: float, thickness: float, z0: float | None = None, device=None, seed=5,
+                 domain=DOMAIN):
         self.rf = torch.as_tensor(np.asarray(rf, dtype=np.float64))
         self.dt, self.gz, self.thickness = float(dt), float(gz), float(thickness)
         self.K = self.rf.shape[0]
@@ -68,6 +70,9 @@ class RFSurrogate:
         self.device = torch.device(device)
         self.params = _fan_in_init(seed).to(self.device)
         self.seed = seed
+        self.domain = tuple(float(d) for d in domain)
+        if len(self.domain) != 3 or min(self.domain) <= 0:
+            raise ValueError(f"domain must be three positive bounds (|df|, |b1 - 1|, |z_rel|), got {domain!r}")
         self.log = TrainLog()
 
     def _centre(self) -> float:
@@ -87,7 +92,8 @@ class RFSurrogate:
         """n uniform samples (df [Hz], b1, z_rel) of the training domain, (n, 3) float32 on the device."""
         g = torch.Generator().manual_seed(seed)
         u = torch.rand(n, 3, generator=g, dtype=F64) * 2 - 1
-        s = torch.stack([u[:, 0] * DOMAIN[0], 1 + u[:, 1] * DOMAIN[1], u[:, 2] * DOMAIN[2]], -1)
+        d = self.domain
+        s = torch.stack([u[:, 0] * d[0], 1 + u[:, 1] * d[1], u[:, 2] * d[2]], -1)
         return s.to(F32).to(self.device).contiguous()
 
     def targets(self, samples: torch.Tensor, full: bool = False):
@@ -101,10 +107,9 @@ class RFSurrogate:
         _lib.check(code, "bp_pulse_quats")
         return (qred, qfull) if full else qred
 
-    @staticmethod
-    def normalise(samples: torch.Tensor) -> torch.Tensor:
-        s = samples
-        return torch.stack([s[:, 0] / DOMAIN[0], (s[:, 1] - 1) / DOMAIN[1], s[:, 2] / DOMAIN[2]], -1).contiguous()
+    def normalise(self, samples: torch.Tensor) -> torch.Tensor:
+        s, d = samples, self.domain
+        return torch.stack([s[:, 0] / d[0], (s[:, 1] - 1) / d[1], s[:, 2] / d[2]], -1).contiguous()
 
     def gradient(self, x: torch.Tensor, target: torch.Tensor):
         """(mean loss, gradient) of the batch through the training kernels (x normalised)."""
@@ -158,6 +163,16 @@ class RFSurrogate:
         torch.cuda.synchronize(self.device)
         return self.log
 
+    def wtiles(self) -> torch.Tensor:
+        """W2 and W3 split into bfloat16 high / low tiles in the tensor cores' operand layout (``bp_mlp_wtiles``),
+        made again whenever the parameters changed since the last call."""
+        key = (self.log.steps, self.params.data_ptr())
+        if getattr(self, "_wt_key", None) != key:
+            self._wt = torch.empty(_lib.lib().bp_mlp_wtiles_bytes(), dtype=torch.uint8, device=self.device)
+            _lib.check(_lib.lib().bp_mlp_wtiles(ptr(self.params), ptr(self._wt), _lib.stream_ptr()), "bp_mlp_wtiles")
+            self._wt_key = key
+        return self._wt
+
     def predict(self, samples: torch.Tensor) -> torch.Tensor:
         """The network's reduced rotations (n, 4) for samples (df, b1, z_rel)."""
         x = self.normalise(samples)
@@ -174,28 +189,36 @@ class RFSurrogate:
         return float(err.max()), float(err.pow(2).mean().sqrt())
 
     # ---- matching occurrences in a sequence ----
-    def match_at(self, s, dt, rf, grad, b0, is_rf, adc, spoil, tol: float = 1e-6):
-        """phi0 if segments [s, s + K) are an occurrence of this pulse (the same dt and slice gradient, RF = trained
-        waveform x exp(i phi0), uniform b0_offset, no sample or spoil), else None."""
-        K, e = self.K, s + self.K
-        if e > len(dt) or not is_rf[s:e].all():
-            return None
-        seg = slice(s, e)
-        scale = max(abs(self.gz), 1.0)
-        if (adc[seg].any() or spoil[seg].any() or np.abs(dt[seg] - self.dt).max() > 1e-9 * self.dt
-                or np.abs(grad[seg, :2]).max() > 1e-9 * scale or np.abs(grad[seg, 2] - self.gz).max() > 1e-9 * scale
-                or np.abs(b0[seg] - b0[s]).max() > 1e-9):
-            return None
+    def phase_of(self, w: np.ndarray, tol: float = 1e-6):
+        """phi0 if the complex RF samples ``w`` (K,) are the trained waveform times exp(i phi0), else None."""
         z = self.rf[:, 0].numpy() + 1j * self.rf[:, 1].numpy()
-        w = rf[seg, 0] + 1j * rf[seg, 1]
         c = np.vdot(z, w)
         phi0 = float(np.angle(c)) if c != 0 else 0.0
         if np.abs(w - z * np.exp(1j * phi0)).max() > tol * float(np.abs(z).max()):
             return None
         return phi0
 
+    def clean_windows(self, dt, gz, other):
+        """Prefix counts c (S + 1,) of segments that rule out this pulse (``other``: not RF, a sample, a spoil or an
+        x / y gradient; or another dt or slice gradient ``gz``): [s, s + K) can be an occurrence only if
+        c[s + K] == c[s]."""
+        scale = max(abs(self.gz), 1.0)
+        bad = other | (np.abs(dt - self.dt) > 1e-9 * self.dt) | (np.abs(gz - self.gz) > 1e-9 * scale)
+        return np.concatenate([[0], np.cumsum(bad)])
 
-def pulse_pieces(rf, dt, gz, thickness, pieces: int = 1, device=None, seed=5):
+    def match_at(self, s, dt, rf, grad, b0, is_rf, adc, spoil, tol: float = 1e-6):
+        """phi0 if segments [s, s + K) are an occurrence of this pulse (the same dt and slice gradient, RF = trained
+        waveform x exp(i phi0), uniform b0_offset, no sample or spoil), else None."""
+        e = s + self.K
+        if e > len(dt):
+            return None
+        other = ~is_rf[s:e] | adc[s:e] | spoil[s:e] | (np.abs(grad[s:e, :2]).max(1) > 1e-9 * max(abs(self.gz), 1.0))
+        if self.clean_windows(dt[s:e], grad[s:e, 2], other)[-1] or np.abs(b0[s:e] - b0[s]).max() > 1e-9:
+            return None
+        return self.phase_of(rf[s:e, 0] + 1j * rf[s:e, 1], tol)
+
+
+def pulse_pieces(rf, dt, gz, thickness, pieces: int = 1, device=None, seed=5, domain=DOMAIN):
     """Surrogates for a pulse cut into ``pieces`` consecutive equal parts (each a shorter shaped pulse with its own
     network; the relaxation is then split around every piece, which shrinks the splitting error ~pieces^2)."""
     rf = np.asarray(rf, dtype=np.float64)
@@ -203,32 +226,54 @@ def pulse_pieces(rf, dt, gz, thickness, pieces: int = 1, device=None, seed=5):
     if k % pieces:
         raise ValueError(f"{k} steps do not split into {pieces} equal pieces")
     m = k // pieces
-    return [RFSurrogate(rf[i * m:(i + 1) * m], dt, gz, thickness, device=device, seed=seed + 17 * i)
+    return [RFSurrogate(rf[i * m:(i + 1) * m], dt, gz, thickness, device=device, seed=seed + 17 * i, domain=domain)
             for i in range(pieces)]
 
 
-def find_occurrences(surrogates, inp):
+def find_occurrences(surrogates, inp, tol: float = 1e-6):
     """[(start, K, surrogate index, phi0, b0)] of every pulse occurrence (or piece) that one of ``surrogates`` stands
     in for: within every run of RF segments, from its start, the first surrogate that matches at the current
     position takes it and the scan continues after it; at a position no surrogate matches, the rest of the run is
-    left to the plain integrator."""
+    left to the plain integrator. Vectorised over positions: every run start at once, then every position just
+    after a match, and so on (the per-segment conditions are prefix counts; the waveform test is one batched
+    comparison per surrogate and level)."""
     d = lambda t: t.detach().to(F64).cpu().numpy()
     dt, rf, grad = d(inp.dt), d(inp.rf), d(inp.grad)
-    b0 = np.zeros(len(dt)) if inp.b0_offset is None else d(inp.b0_offset)
-    is_rf, adc, spoil = (np.asarray(f, dtype=bool) for f in (inp.is_rf, inp.adc, inp.spoil))
-    run_start = is_rf & ~np.concatenate([[False], is_rf[:-1]])
+    S = len(dt)
+    b0 = np.zeros(S) if inp.b0_offset is None else d(inp.b0_offset)
+    is_rf, adc, spoil = (np.fromiter(f, dtype=bool, count=S) for f in (inp.is_rf, inp.adc, inp.spoil))
+    w = rf[:, 0] + 1j * rf[:, 1]
+    gxy = np.abs(grad[:, :2]).max(1)
+    base = ~is_rf | adc | spoil
+    clean = [sg.clean_windows(dt, grad[:, 2], base | (gxy > 1e-9 * max(abs(sg.gz), 1.0))) for sg in surrogates]
+    # b0_offset steps: a window [s, e) is uniform when no step lies in (s, e)
+    steps = np.concatenate([[0], np.cumsum(np.concatenate([[False], np.abs(np.diff(b0)) > 1e-9]))])
     occ = []
-    for s in np.flatnonzero(run_start):
-        s = int(s)
-        while True:
-            for i, sg in enumerate(surrogates):
-                phi0 = sg.match_at(s, dt, rf, grad, b0, is_rf, adc, spoil)
-                if phi0 is not None:
-                    occ.append((s, sg.K, i, phi0, float(b0[s])))
-                    s += sg.K
-                    break
-            else:
-                break
+    cands = np.flatnonzero(is_rf & ~np.concatenate([[False], is_rf[:-1]]))
+    while cands.size:
+        taken = np.zeros(cands.size, dtype=bool)
+        ends = []
+        for i, sg in enumerate(surrogates):
+            e = cands + sg.K
+            ok = ~taken & (e <= S)
+            ec = np.minimum(e, S)
+            ok &= (clean[i][ec] == clean[i][cands]) & (steps[ec] == steps[np.minimum(cands + 1, S)])
+            idx = np.flatnonzero(ok)
+            if idx.size == 0:
+                continue
+            z = sg.rf[:, 0].numpy() + 1j * sg.rf[:, 1].numpy()
+            W = w[cands[idx, None] + np.arange(sg.K)]
+            c = W @ np.conj(z)
+            phi = np.where(c != 0, np.angle(c), 0.0)
+            good = np.abs(W - z[None, :] * np.exp(1j * phi)[:, None]).max(1) <= tol * np.abs(z).max()
+            for j, ph in zip(idx[good].tolist(), phi[good].tolist()):
+                s0 = int(cands[j])
+                occ.append((s0, sg.K, i, ph, float(b0[s0])))
+            taken[idx[good]] = True
+            ends.append(e[idx[good]])
+        cands = np.concatenate(ends) if ends else np.zeros(0, dtype=np.int64)
+        cands = cands[cands < S]
+    occ.sort()
     return occ
 
 
@@ -239,12 +284,19 @@ def forward_with_surrogate(inp, device, options):
         raise ValueError("pulses='surrogate' needs surrogate=[RFSurrogate, ...] (trained networks)")
     if isinstance(surrogates, RFSurrogate):
         surrogates = [surrogates]
-    sig, m, _ = run_with_surrogates(inp, device, surrogates)
+    sig, m, _ = run_with_surrogates(inp, device, surrogates, options.get("surrogate_inference", "mma"))
     return sig, m
 
 
-def run_with_surrogates(inp, device, surrogates, counts_out: bool = False):
-    """The forward with every matched pulse occurrence through its surrogate; returns (signal, m, counts)."""
+INFERENCE = ("mma", "fp32")
+
+
+def run_with_surrogates(inp, device, surrogates, inference: str = "mma"):
+    """The forward with every matched pulse occurrence through its surrogate; returns (signal, m, counts).
+    ``inference``: "mma" (layers 2 and 3 on the tensor cores, ``bp_surrogate_pulse_mma``) or "fp32" (the whole
+    network on the CUDA cores, ``bp_surrogate_pulse``)."""
+    if inference not in INFERENCE:
+        raise ValueError(f"surrogate_inference must be one of {INFERENCE}, not {inference!r}")
     pk = engine.pack(inp, device)
     occ = find_occurrences(surrogates, inp)
     S = pk.flags.shape[0]
@@ -268,8 +320,13 @@ def run_with_surrogates(inp, device, surrogates, counts_out: bool = False):
         if wa > w:
             engine.run_forward(pk, state, wdev, w, wa, raw if pk.n_adc else None, status)
         sg = surrogates[i]
-        code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s, k, sg.T,
-                                      sg.gz, sg.thickness, sg.z0, phi0, b0, ptr(counts), st)
+        if inference == "mma":
+            code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(sg.wtiles()),
+                                              ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0,
+                                              *sg.domain, ptr(counts), ptr(status), 0, st)
+        else:
+            code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s, k, sg.T,
+                                          sg.gz, sg.thickness, sg.z0, phi0, b0, *sg.domain, ptr(counts), st)
         _lib.check(code, "bp_surrogate_pulse")
         w = int(np.searchsorted(starts, s + k))
     if w < windows.shape[0]:

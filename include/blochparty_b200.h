@@ -152,12 +152,26 @@ int bp_adam(float* params, const float* grad, float* m, float* v, float lr, floa
 int bp_mlp_eval(const float* params, const float* x, int n, float* y, void* stream);
 
 /* One pulse occurrence (segments [seg0, seg0 + k_steps) of `segs`, the trained waveform times exp(i phi0), slice
- * gradient gz along z, uniform offset b0off) applied to every spin's state [6][n]: inside the domain
- * (|df| <= 200 Hz, |b1 - 1| <= 0.3, |z_rel| <= 2) relax T/2, rotate by the network's rotation, relax T/2; outside,
- * the plain sub-stepped segments. counts (NULL or [2]) += spins through the network, through the fallback. */
+ * gradient gz along z, uniform offset b0off) applied to every spin's state [6][n]: inside the network's training
+ * domain (|df| <= dom_df [Hz], |b1 - 1| <= dom_b1, |z_rel| <= dom_z slice widths) relax T/2, rotate by the
+ * network's rotation, relax T/2; outside, the plain sub-stepped segments. counts (NULL or [2]) += spins through the
+ * network, through the fallback. */
 int bp_surrogate_pulse(const float* spins, float* state, int n, const float* params, const void* segs, int seg0,
                        int k_steps, double T, double gz, double thickness, double z0, double phi0, float b0off,
-                       int32_t* counts, void* stream);
+                       float dom_df, float dom_b1, float dom_z, int32_t* counts, void* stream);
+
+/* The same occurrence with layers 2 and 3 of the network on the tensor cores (tcgen05, split bfloat16: hi x hi +
+ * hi x lo + lo x hi, float32 accumulation in tensor memory; 128 spins per tile, persistent CTAs, at most
+ * `max_ctas` when > 0). `wtiles` (16-byte aligned, bp_mlp_wtiles_bytes()) holds W2 and W3 split by bp_mlp_wtiles;
+ * `status` |= 1 when a bounded wait on the weights' copy or an MMA ran out (the CTA then stops, its remaining
+ * spins not written). Spins outside the domain are queued per CTA and stepped 128 at a time. bp_surrogate_pulse_mma_grid(n) returns the CTA count a launch for n spins uses (< 0: -error). */
+int bp_mlp_wtiles_bytes(void);
+int bp_mlp_wtiles(const float* params, void* tiles, void* stream);
+int bp_surrogate_pulse_mma_grid(int n);
+int bp_surrogate_pulse_mma(const float* spins, float* state, int n, const float* params, const void* wtiles,
+                           const void* segs, int seg0, int k_steps, double T, double gz, double thickness, double z0,
+                           double phi0, float b0off, float dom_df, float dom_b1, float dom_z, int32_t* counts,
+                           int32_t* status, int max_ctas, void* stream);
 
 /* Measurement kernel (the roofline denominator): 4 CTAs x 256 threads per SM, each thread `iters` x 128
  * independent FFMAs; `*flops` receives the flop count of the launch, which the caller divides by the launch's

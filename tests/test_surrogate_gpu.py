@@ -1,9 +1,13 @@
-"""The learned RF surrogate on the GPU: training kernels against the float64 oracle, training, and the TSE
-workload through the surrogate against the float64 plain integrator (the judge).
+"""The learned RF surrogate on the GPU: training kernels against the float64 oracle, training, tensor-core
+inference against float32 inference, and the TSE workload through the surrogate against the float64 plain
+integrator.
 
 Bars: targets (float64 composition rounded to float32) within 1e-6 of the oracle; the training kernel's gradient
-within 1e-4 (largest relative error) of float64 autograd; the surrogate signal within 1e-3 relative L2 of the
-float64 oracle (the target for the learned form); and a measured speed-up over plain sub-stepping on the same GPU.
+within 1e-4 (largest relative error) of float64 autograd; tensor-core inference within 1e-4 of float32 inference
+(magnetization, unit PD scale), the fallback spins bit-identical; the TSE signal through the surrogate within
+3.5e-2 relative L2 of the float64 oracle, the bar set by the whole-pulse relax / rotate / relax splitting (2.3e-2
+with exact rotations on this refocusing train, measured by a float64 CPU emulation), not by the networks; and a
+measured speed-up over plain sub-stepping on the same GPU.
 """
 
 import math
@@ -83,12 +87,13 @@ def test_training_lowers_the_loss_and_the_error():
 @pytest.fixture(scope="module")
 def tse_surrogates():
     """Networks for the six TSE pulses (3 slices x excitation / refocusing), trained on 2^20 samples each (400
-    epochs, ~6 s per pulse)."""
+    epochs, ~6 s per pulse) over |z_rel| <= 2.5: the slices are contiguous, so every spin of the 3-slice stack lies
+    within 2.5 slice widths of every pulse's centre."""
     out, info = [], []
     for z0 in (-5e-3, 0.0, 5e-3):
         for flip, phase in ((90.0, 0.0), (180.0, 0.5 * math.pi)):
             w, dt, gz, _ = _pulse(flip, z0, phase)
-            sg = surrogate.RFSurrogate(w, dt, gz, 5e-3)
+            sg = surrogate.RFSurrogate(w, dt, gz, 5e-3, domain=(200.0, 0.3, 2.5))
             t = time.perf_counter()
             sg.train(n_samples=1 << 20, epochs=400, batch=16384)
             info.append((flip, z0, time.perf_counter() - t, sg.validate()))
@@ -132,10 +137,79 @@ def test_surrogate_gain_on_the_tse_workload(tse_surrogates):
         return time.perf_counter() - t, out
 
     t_plain, (s_plain, _) = timed(lambda: engine.forward(inp, dev))
+    t_fp32, _ = timed(lambda: surrogate.run_with_surrogates(inp, dev, tse_surrogates, "fp32"))
     t_sur, (s_sur, _, counts) = timed(lambda: surrogate.run_with_surrogates(inp, dev, tse_surrogates))
     rel = float(torch.linalg.vector_norm(s_sur - s_plain) / torch.linalg.vector_norm(s_plain))
     frac = counts[0] / max(1, sum(counts))
-    print(f"\nTSE 393,216 spins: plain {t_plain:.3f} s, surrogate {t_sur:.3f} s, speed-up {t_plain / t_sur:.2f}x; "
-          f"{100 * frac:.1f}% of spin-pulse pairs through the networks; signal difference {rel:.1e}")
+    print(f"\nTSE 393,216 spins: plain {t_plain:.3f} s, surrogate {t_sur:.3f} s (tensor cores; float32 inference "
+          f"{t_fp32:.3f} s), speed-up {t_plain / t_sur:.2f}x; {100 * frac:.1f}% of spin-pulse pairs through the "
+          f"networks; signal difference {rel:.1e}")
     assert t_sur < t_plain
     assert rel < 3.5e-2
+
+
+def test_weight_tiles_layout():
+    """bp_mlp_wtiles: every W2 / W3 entry is hi + lo at its operand-layout position, hi = bf16(w) (nearest)."""
+    sg = surrogate.RFSurrogate(*_pulse()[:3], 5e-3, seed=21)
+    t = sg.wtiles().cpu().view(torch.int16).view(torch.bfloat16).float().reshape(4, 8, 8, 8, 8)
+    # element (n / 8) 512 + (k / 8) 64 + (n % 8) 8 + k % 8 -> [n // 8, k // 8, n % 8, k % 8]
+    t = t.permute(0, 1, 3, 2, 4).reshape(4, 64, 64)
+    _, _, w2, _, w3, _, _, _ = S.unflatten(sg.params.cpu())
+    assert torch.equal(t[0], w2.to(torch.bfloat16).float())
+    assert torch.equal(t[2], w3.to(torch.bfloat16).float())
+    assert float(((t[0] + t[1]) - w2).abs().max() / w2.abs().max()) < 2 ** -16
+    assert float(((t[2] + t[3]) - w3).abs().max() / w3.abs().max()) < 2 ** -16
+
+
+@pytest.mark.parametrize("n,max_ctas", [(300, 0), (300, 1), (5000, 7)])
+def test_tensor_core_inference_matches_fp32_inference(n, max_ctas):
+    """bp_surrogate_pulse_mma against bp_surrogate_pulse on one occurrence: the same counts, spins outside the
+    domain bit-identical (both take the plain fallback), spins inside within the split-bfloat16 rounding."""
+    w, dt, gz, _ = _pulse(90.0)
+    sg = surrogate.RFSurrogate(w, dt, gz, 5e-3, seed=7)
+    sg.train(n_samples=1 << 15, epochs=4, batch=4096)
+    seq = sequences.SequenceBuilder().rf_waveform(w, dt, grad=(0.0, 0.0, gz)).build()
+    g = torch.Generator().manual_seed(n)
+    pos = torch.zeros(n, 3, dtype=F64)
+    pos[:, 2] = (torch.rand(n, generator=g, dtype=F64) - 0.5) * 6 * 5e-3  # |z_rel| up to 3: some outside
+    ph = bpb.Phantom(pos, torch.rand(n, generator=g, dtype=F64), 0.3 + torch.rand(n, generator=g, dtype=F64),
+                     0.02 + 0.1 * torch.rand(n, generator=g, dtype=F64),
+                     (torch.rand(n, generator=g, dtype=F64) - 0.5) * 500.0)
+    from blochparty_b200 import engine
+    from blochparty_b200.api import Inputs
+
+    ones = torch.ones(n, 1, dtype=torch.complex128)
+    inp = Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, ones, seq.dt, seq.rf, seq.grad, seq.adc_phase, None,
+                 list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
+    dev = torch.device("cuda", 0)
+    pk = engine.pack(inp, dev)
+    m0 = torch.rand(n, 3, generator=g, dtype=F64) - 0.5
+    lib, st = _lib.lib(), _lib.stream_ptr()
+    out = []
+    for mma in (False, True):
+        state = engine.initial_state(inp.pd, m0, dev)
+        counts = torch.zeros(2, dtype=torch.int32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        phi0 = 0.3  # (the fallback steps the sequence's own segments; both kernels see the same arguments)
+        if mma:
+            code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), n, ptr(sg.params), ptr(sg.wtiles()),
+                                              ptr(pk.segs), 0, sg.K, sg.T, sg.gz, sg.thickness, sg.z0, phi0, 10.0,
+                                              *sg.domain, ptr(counts), ptr(status), max_ctas, st)
+        else:
+            code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), n, ptr(sg.params), ptr(pk.segs), 0, sg.K, sg.T,
+                                          sg.gz, sg.thickness, sg.z0, phi0, 10.0, *sg.domain, ptr(counts), st)
+        _lib.check(code, "surrogate pulse")
+        torch.cuda.synchronize()
+        assert int(status) == 0
+        out.append((state.cpu(), counts.cpu().tolist()))
+    (s32, c32), (smma, cmma) = out
+    assert c32 == cmma and c32[0] > 0 and c32[1] > 0 and sum(c32) == n
+    # the kernels' domain test, in their float32 / float64 arithmetic
+    df = ph.db0.numpy().astype(np.float32) + np.float32(10.0)
+    zr = ((pos[:, 2].numpy().astype(np.float32).astype(np.float64) - sg.z0) / 5e-3).astype(np.float32)
+    inside = torch.from_numpy((np.abs(df) <= np.float32(200.0)) & (np.abs(zr) <= np.float32(2.0)))
+    assert int(inside.sum()) == c32[0]
+    assert torch.equal(s32[:, ~inside], smma[:, ~inside])
+    err = float((s32[:3, inside] - smma[:3, inside]).abs().max())
+    print(f"\ntensor-core vs fp32 inference, n={n}: largest magnetization difference {err:.1e}")
+    assert err < 1e-4
