@@ -125,8 +125,9 @@ int bp_adjoint_noalloc(const float* spins, const float* sens, int n, int n_coils
 
 /* ---- learned RF surrogate (no counterpart in the reference; its nearest part is the exact per-spin map of a
  * reused pulse, engines/gpu/cuda/pulse.cu.in:3-32) ----
- * A 3 -> 64 -> 64 -> 64 -> 4 GELU network per shaped pulse: inputs (df / 200 Hz, (b1 - 1) / 0.3, z_rel / 2) with
- * z_rel = (z - z0) / slice thickness, output a unit quaternion (q0, q1, q2, q3), the Cayley-Klein pair
+ * A 3 -> 64 -> 64 -> 64 -> 4 GELU network per shaped pulse: inputs (df / dom_df, (b1 - 1) / dom_b1, z_rel / dom_z)
+ * with z_rel = (z - z0) / slice thickness and the network's training domain (dom_df, dom_b1, dom_z) (the host
+ * side's default: 200 Hz, 0.3, 2), output a unit quaternion (q0, q1, q2, q3), the Cayley-Klein pair
  * alpha = q0 - i q3, beta = -i (q1 + i q2), of the pulse's rotation reduced by its free precession:
  * R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T. Parameters: BP_MLP_PARAMS floats, W1 (64x3), b1, W2 (64x64),
  * b2, W3 (64x64), b3, W4 (4x64), b4. */

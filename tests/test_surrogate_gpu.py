@@ -147,6 +147,42 @@ def test_surrogate_gain_on_the_tse_workload(tse_surrogates):
     assert t_sur < t_plain
     assert rel < 3.5e-2
 
+    # one pulse occurrence at kernel level (CUDA events, 20 repetitions): the plain forward over the pulse's
+    # windows against both inference kernels, on the same state
+    pk = engine.pack(inp, dev)
+    s, k, i, phi0, b0 = surrogate.find_occurrences(tse_surrogates, inp)[1]
+    breaks = np.zeros(pk.flags.shape[0], dtype=np.uint8)
+    breaks[s] = breaks[s + k] = 1
+    windows = engine.plan_windows(pk.flags, _lib.lib().bp_forward_samp_max(pk.n_coils), breaks=breaks)
+    wdev = torch.from_numpy(windows).to(dev)
+    wa, wb = int(np.searchsorted(windows[:, 0], s)), int(np.searchsorted(windows[:, 0], s + k))
+    state = engine.initial_state(inp.pd, None, dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    lib, st, sg = _lib.lib(), _lib.stream_ptr(), tse_surrogates[i]
+    wt = sg.wtiles()
+
+    def events(fn, reps=20):
+        fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    p_plain = events(lambda: engine.run_forward(pk, state, wdev, wa, wb, None, status))
+    p_fp32 = events(lambda: lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s,
+                                                   k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0, *sg.domain, None,
+                                                   st))
+    p_mma = events(lambda: lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(wt),
+                                                      ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0,
+                                                      *sg.domain, None, ptr(status), 0, st))
+    assert int(status) == 0
+    print(f"one {k}-step pulse over {pk.n:,} spins: plain {p_plain:.3f} ms, float32 network {p_fp32:.3f} ms, "
+          f"tensor-core network {p_mma:.3f} ms ({p_plain / p_mma:.1f}x)")
+    assert p_mma < 0.5 * p_plain
+
 
 def test_weight_tiles_layout():
     """bp_mlp_wtiles: every W2 / W3 entry is hi + lo at its operand-layout position, hi = bf16(w) (nearest)."""
