@@ -55,6 +55,24 @@ def flops_per_spin(flags: np.ndarray, n_coils: int) -> int:
             + (FLOP_ADC_PER_COIL * n_coils + FLOP_ADC) * n_adc)
 
 
+# the backward's work per spin and segment (counted from blochparty_b200/csrc/adjoint.cu; fixed): the interval
+# replay and the in-window recompute each repeat the forward's propagation (no coil contraction), then the
+# reverse sweep: RF segment 227 flops (rf_reverse with its rotation factors and offset gradients), free segment
+# 58 (free_reverse), ADC sample 16 per coil (signal and coil gradients) + 2.
+FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 227, 58, 16, 2
+
+
+def grad_flops_per_spin(flags: np.ndarray, n_coils: int) -> tuple[int, int]:
+    """(forward, backward) algorithmic flops per spin of a simulation with gradients."""
+    rf = (flags & 1) != 0
+    n_rf, n_free = int(rf.sum()), int((~rf).sum())
+    n_adc = int(((flags & 2) != 0).sum())
+    fwd = flops_per_spin(flags, n_coils)
+    prop = flops_per_spin(flags, 0) - FLOP_ADC * n_adc
+    rev = FLOP_RF_REV * n_rf + FLOP_FREE_REV * n_free + (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc
+    return fwd, 2 * prop + rev
+
+
 class Clocks:
     """nvidia-smi samples (every 200 ms) of the GPU's SM clock and throttle reasons during the timed region."""
 
@@ -178,6 +196,71 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_grad(args, dev):
+    """Forward + adjoint through the public API (gradients w.r.t. T1 and the RF waveform of a seeded linear loss
+    of the signal), one GPU: isochromat-steps/s of the pair, timed by CUDA events around the forward call and the
+    backward call."""
+    import blochparty_b200 as bpb
+    from blochparty_b200 import adjoint, engine, workloads
+
+    ph, seq, coils = workloads.gre3d_64(args.n)
+    n, S = len(ph.pd), len(seq)
+    g = torch.Generator().manual_seed(7)
+    n_adc = int(sum(seq.adc))
+    wr, wi = torch.randn(coils.shape[1], n_adc, generator=g), torch.randn(coils.shape[1], n_adc, generator=g)
+    t1 = ph.t1.clone().requires_grad_()
+    rf = seq.rf.clone().requires_grad_()
+    phg = bpb.Phantom(ph.pos, ph.pd, t1, ph.t2, ph.db0)
+    seqg = bpb.Sequence(seq.dt, rf, seq.grad, seq.adc_phase, list(seq.is_rf), list(seq.adc), list(seq.spoil))
+
+    def step():
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        t1.grad = rf.grad = None
+        torch.cuda.synchronize()
+        e0.record()
+        r = bpb.simulate(phg, seqg, coils)
+        e1.record()
+        loss = (r.signal.real * wr).sum() + (r.signal.imag * wi).sum()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+    for _ in range(args.warmup):
+        step()
+    clocks = Clocks(dev.index or 0)
+    times = []
+    with clocks:
+        for _ in range(args.steps):
+            times.append(step())
+    f_ms = statistics.mean(t[0] for t in times)
+    b_ms = statistics.mean(t[1] for t in times)
+    ms = f_ms + b_ms
+    flags = engine.pack_segments(seq.dt, seq.rf, seq.grad, None, seq.adc_phase, list(seq.is_rf), list(seq.adc),
+                                 list(seq.spoil), "cpu")[3]
+    fwd, bwd = grad_flops_per_spin(flags, coils.shape[1])
+    every = adjoint.default_checkpoint_every(S)
+    intervals = math.ceil(S / every)
+    peak = ffma_peak_tflops(dev)
+    achieved = n * (fwd + bwd) / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "isochromat-steps/s (fwd+adjoint)", "value": n * S / (ms * 1e-3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD if args.n == 64 else f"gre3d_{args.n}", "spins": n, "segments": S,
+                   "coils": coils.shape[1], "grad_wrt": ["t1", "rf"], "checkpoint_every": every,
+                   "forward_ms": f_ms, "backward_ms": b_ms,
+                   "l2": "inputs larger than L2; the forward starts from host tensors (packing and copies inside)"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU",
+                     "kernel": "bp_forward_kernel (forward, replay) + bp_adjoint_kernel",
+                     "flops_per_spin": {"forward": fwd, "backward": bwd}},
+        "gpu_launches": intervals * 4 + 1,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -188,6 +271,7 @@ def main():
     ap.add_argument("--n", type=int, default=64, help="grid size of the 3D GRE (64: the measured workload)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grad", action="store_true", help="forward + adjoint (gradients of T1 and the RF), one GPU")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -202,6 +286,11 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.grad:
+        if world > 1:
+            raise SystemExit("--grad measures one GPU")
+        run_grad(args, dev)
+        return
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 

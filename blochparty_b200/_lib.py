@@ -22,6 +22,7 @@ BP_MMA_MAX_COILS = 8
 BP_MLP_PARAMS = 8836
 BP_MMA_SAMPLES = 64
 BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
+BP_PULSE_MAP_BYTES = 96
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",
@@ -52,6 +53,8 @@ SIGNATURES = {
     "bp_mlp_eval": (c_int, [_P, _P, c_int, _P, _P]),
     "bp_surrogate_pulse": (c_int, [_P, _P, c_int, _P, _P, c_int, c_int, c_double, c_double, c_double, c_double,
                                    c_double, c_float, c_float, c_float, c_float, _P, _P]),
+    "bp_pulse_maps": (c_int, [_P, c_int, _P, _P, c_int, c_int, _P, _P]),
+    "bp_pulse_apply": (c_int, [_P, c_int, _P, c_double, _P]),
     "bp_mlp_wtiles_bytes": (c_int, []),
     "bp_mlp_wtiles": (c_int, [_P, _P, _P]),
     "bp_surrogate_pulse_mma_grid": (c_int, [c_int]),

@@ -187,6 +187,8 @@ def simulate_grad(inp, dev, checkpoint_every, options) -> SimResult:
     if options.get("readout", "fp32") != "fp32":
         raise NotImplementedError("b200 engine: gradients through readout='bf16x3' are not implemented; use the "
                                   "default float32 readout (or torch.no_grad())")
+    if options.get("pulses", "step") == "reuse":
+        raise ValueError("pulses='reuse' is forward only")
     if options.get("pulses", "step") != "step":
         raise NotImplementedError("b200 engine: gradients through pulses='surrogate' are not implemented; use "
                                   "pulses='step' (or torch.no_grad())")

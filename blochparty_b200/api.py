@@ -22,6 +22,7 @@ from .types import SimResult
 
 ENGINES = ("b200", "gpu", "cuda")  # "gpu" and "cuda" name this engine too, so a caller's engine= still works
 OPTIONS = ("readout", "pulses", "surrogate", "surrogate_inference", "max_ctas")
+PULSES = ("step", "reuse", "surrogate")
 REFERENCE_GPU_OPTIONS = ("chunk", "group", "mma", "readouts", "nufft_width", "nufft_terms")
 READOUTS = ("fp32", "bf16x3")
 
@@ -80,8 +81,9 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
         boundaries); default about sqrt(segments).
     options: ``readout`` "fp32" (default: float32 coil products reduced by warp shuffles) or "bf16x3" (the coil
         contraction on the tensor cores in split bfloat16 with float32 accumulation); ``pulses`` "step"
-        (default) or "surrogate" (shaped pulses through a trained ``surrogate``), whose ``surrogate_inference``
-        is "mma" (default: the hidden 64 x 64 layers on the tensor cores) or "fp32"; ``max_ctas`` caps the grid.
+        (default), "reuse" (every recurring pulse through its exact per-spin map, forward only) or "surrogate"
+        (shaped pulses through a trained ``surrogate``), whose ``surrogate_inference`` is "mma" (default: the
+        hidden 64 x 64 layers on the tensor cores) or "fp32"; ``max_ctas`` caps the grid.
     """
     if engine not in ENGINES:
         raise ValueError(f"engine must be one of {ENGINES}, not {engine!r}")
@@ -94,8 +96,10 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
     if readout not in READOUTS:
         raise ValueError(f"readout must be one of {READOUTS}, not {readout!r}")
     pulses = options.get("pulses", "step")
-    if pulses not in ("step", "surrogate"):
-        raise ValueError(f"pulses must be 'step' or 'surrogate', not {pulses!r}")
+    if pulses not in PULSES:
+        raise ValueError(f"pulses must be one of {PULSES}, not {pulses!r}")
+    if pulses == "reuse" and readout != "fp32":
+        raise ValueError("pulses='reuse' takes the float32 readout (readout='fp32')")
     n = len(phantom.pd)
     if coils is not None and (coils.dim() != 2 or coils.shape[0] != n):
         raise ValueError(f"coils must be (N, C) = ({n}, C), got {tuple(coils.shape)}")
@@ -121,6 +125,10 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
 
 
 def _forward(inp: Inputs, dev, options):
+    if options.get("pulses", "step") == "reuse":
+        from .pulses import forward_with_reuse
+
+        return forward_with_reuse(inp, dev, options.get("max_ctas", 0))
     if options.get("pulses", "step") == "surrogate":
         from .surrogate import forward_with_surrogate
 

@@ -250,14 +250,12 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
                     cached_free = s;
                     free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
                 }
-                if (need_seg) {
+                if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
+                    float v[N_SG];
 #pragma unroll
-                    for (int k = 0; k < 7; ++k) {
-                        float v = active ? sg.v[k] : 0.0f;
-#pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                        if (lane == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + k] = v;
-                    }
+                    for (int k = 0; k < N_SG; ++k) v[k] = active ? sg.v[k] : 0.0f;
+                    const float t = warp_reduce_scatter8(v, lane);
+                    if ((lane & 3) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + ((lane >> 2) & 7)] = t;
                 }
             }
             __syncthreads();  // segacc complete; every thread is done reading this window's slots

@@ -22,6 +22,7 @@
 #define BP_SPOIL 4       // zero Mxy at the end of the segment (after its sample)
 #define BP_SAME_FREE 8   // free segment identical (dt, moment, offset) to the free segment just before it
 #define BP_SAME_RFDT 16  // RF segment with the dt of the RF segment just before it
+#define BP_SAME_OFF 32   // RF segment with the dt, moment and offset of the RF segment just before it (same G.r)
 
 // status bits written by the kernels (read by the host after the launch)
 #define BP_ERR_TMA_TIMEOUT 1
@@ -64,11 +65,17 @@ __device__ __forceinline__ void two_sum(float& hi, float& lo, float d) {
 }
 
 // Rodrigues coefficients of a rotation by |w|, from p2 = |w|^2: s1 = sin(phi)/phi, s2 = (1 - cos phi)/phi^2.
-// Below phi = 1 both are their Taylor series in p2 (sum_k (-1)^k p2^k / (2k+1)! and / (2k+2)!), truncated after
-// p2^5: the first dropped terms are below 2e-10, far under a float32 ulp, and the series costs five FMAs each
-// on the FMA pipe with no square root. Above, the accurate sine of the angle and of its half.
+// Below phi = 1 both are their Taylor series in p2 (sum_k (-1)^k p2^k / (2k+1)! and / (2k+2)!): truncated after
+// p2^3 below phi = 1/4 (the usual RF step; first dropped terms p2^4 / 9! < 4.3e-11) and after p2^5 below phi = 1
+// (first dropped terms below 2e-10), far under a float32 ulp, on the FMA pipe with no square root. Above, the
+// accurate sine of the angle and of its half.
 __device__ __forceinline__ void rodrigues_coeffs(float p2, float& s1, float& s2) {
-    if (p2 < 1.0f) {
+    if (p2 < 0.0625f) {
+        s1 = fmaf(p2, fmaf(p2, fmaf(p2, -1.9841269841269841e-04f, 8.3333333333333333e-03f), -1.6666666666666667e-01f),
+                  1.0f);
+        s2 = fmaf(p2, fmaf(p2, fmaf(p2, -2.4801587301587302e-05f, 1.3888888888888889e-03f), -4.1666666666666667e-02f),
+                  0.5f);
+    } else if (p2 < 1.0f) {
         s1 = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -2.5052108385441720e-08f, 2.7557319223985893e-06f),
                                               -1.9841269841269841e-04f), 8.3333333333333333e-03f),
                            -1.6666666666666667e-01f), 1.0f);
@@ -119,10 +126,13 @@ __device__ __forceinline__ RfRelax rf_relax(float dt, const Spin& p) {
 // relax dt/2 (E n + c), composed into one increment of m: (E E - I) m + E (R - I) m1 + (E + I) c, with
 // (R - I) m1 = s1 (w x m1) + s2 w x (w x m1). The increment is small next to m and computed from m directly,
 // so one two-sum per component (instead of one per sub-step) keeps the float32 state compensated.
-__device__ __forceinline__ void rf_step(const SegRec& q, const Spin& p, const RfRelax& r, float& mx, float& my,
-                                        float& mz, float& lx, float& ly, float& lz) {
-    const float cyc = fmaf(q.kx, p.px, fmaf(q.ky, p.py, fmaf(q.kz, p.pz, fmaf(q.dt, p.db0, q.beta))));
-    const float wz = -BP_TWO_PI_F * cyc;
+// The z component of an RF segment's rotation vector: -2 pi (k.r + dt dB0 + beta) (its off-resonance in cycles).
+__device__ __forceinline__ float rf_wz(const SegRec& q, const Spin& p) {
+    return -BP_TWO_PI_F * fmaf(q.kx, p.px, fmaf(q.ky, p.py, fmaf(q.kz, p.pz, fmaf(q.dt, p.db0, q.beta))));
+}
+
+__device__ __forceinline__ void rf_step_wz(const SegRec& q, const Spin& p, const RfRelax& r, float wz, float& mx,
+                                           float& my, float& mz, float& lx, float& ly, float& lz) {
     const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
     const float m1x = mx * r.a2, m1y = my * r.a2, m1z = fmaf(-p.pd, r.e1h, mz * r.a1);
     const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
@@ -134,6 +144,11 @@ __device__ __forceinline__ void rf_step(const SegRec& q, const Spin& p, const Rf
     two_sum(mx, lx, fmaf(r.d2, mx, r.a2 * qx));
     two_sum(my, ly, fmaf(r.d2, my, r.a2 * qy));
     two_sum(mz, lz, fmaf(r.d1, mz, fmaf(r.a1, qz, r.cz2)));
+}
+
+__device__ __forceinline__ void rf_step(const SegRec& q, const Spin& p, const RfRelax& r, float& mx, float& my,
+                                        float& mz, float& lx, float& ly, float& lz) {
+    rf_step_wz(q, p, r, rf_wz(q, p), mx, my, mz, lx, ly, lz);
 }
 
 // Free-precession factors of one segment: the rotation (c, s) by -2 pi (k.r + dt dB0 + beta), evaluated in
@@ -158,6 +173,37 @@ __device__ __forceinline__ FreeFactors free_factors(const SegRec& q, const doubl
     f.e1 = expm1f(-q.dt * p.r1);
     f.e2 = expm1f(-q.dt * p.r2);
     return f;
+}
+
+// The factors of `reps` consecutive copies of one free segment merged into one: the phase of reps x (k.r + dt dB0
+// + beta) cycles, taken in float64 before the reduction to [-1/2, 1/2], and the relaxation over reps x dt.
+__device__ __forceinline__ FreeFactors free_factors_merged(const SegRec& q, const double4& k64, const Spin& p,
+                                                           int reps) {
+    FreeFactors f;
+    const double cyc = fma(k64.x, (double)p.px,
+                           fma(k64.y, (double)p.py, fma(k64.z, (double)p.pz, fma((double)q.dt, (double)p.db0, k64.w))));
+    const double tot = cyc * (double)reps;
+    const double fr = tot - rint(tot);
+    double sd, cd;
+    sincospi(-2.0 * fr, &sd, &cd);
+    f.ch = (float)cd;
+    f.cl = (float)(cd - (double)f.ch);
+    f.sh = (float)sd;
+    f.sl = (float)(sd - (double)f.sh);
+    const float t = (float)((double)q.dt * (double)reps);
+    f.e1 = expm1f(-t * p.r1);
+    f.e2 = expm1f(-t * p.r2);
+    return f;
+}
+
+// One sample of a readout run from the previous one: z (e2 + 1) (c + i s), the rotation's low part folded into
+// the products and the relaxation applied with one rounding (float32; the run's state is rebuilt exactly after it).
+__device__ __forceinline__ void readout_advance(const FreeFactors& f, float& zr, float& zi) {
+    const float tr = fmaf(f.cl, zr, -f.sl * zi), ti = fmaf(f.cl, zi, f.sl * zr);
+    const float nr = fmaf(f.ch, zr, fmaf(-f.sh, zi, tr));
+    const float ni = fmaf(f.ch, zi, fmaf(f.sh, zr, ti));
+    zr = fmaf(nr, f.e2, nr);
+    zi = fmaf(ni, f.e2, ni);
 }
 
 // hi + lo renormalised so that lo is below half an ulp of hi (requires |hi| >= |lo|).
@@ -258,36 +304,31 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
-// Sixteen values per lane summed over the warp and scattered (a butterfly reduce-scatter): afterwards every
-// lane holds the warp's total of value index (lane >> 1) & 15. Each stage exchanges the half of the remaining
-// values that the partner lane keeps: 8 + 4 + 2 + 1 + 1 shuffles.
-__device__ __forceinline__ float warp_reduce_scatter16(float* v, int lane) {
+// Eight values per lane summed over the warp and scattered (a butterfly reduce-scatter): afterwards every lane
+// holds the warp's total of value index (lane >> 2) & 7. Each stage exchanges the half of the remaining values
+// that the partner lane keeps: 4 + 2 + 1 shuffles, then 2 for the last value's four copies (9 instead of the
+// 40 of eight separate butterflies).
+__device__ __forceinline__ float warp_reduce_scatter8(float* v, int lane) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < 4; ++k) {
         const bool up = lane & 16;
-        const float send = up ? v[k] : v[k + 8];
-        const float keep = up ? v[k + 8] : v[k];
+        const float send = up ? v[k] : v[k + 4];
+        const float keep = up ? v[k + 4] : v[k];
         v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const bool up = lane & 8;
-        const float send = up ? v[k] : v[k + 4];
-        const float keep = up ? v[k + 4] : v[k];
-        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-#pragma unroll
     for (int k = 0; k < 2; ++k) {
-        const bool up = lane & 4;
+        const bool up = lane & 8;
         const float send = up ? v[k] : v[k + 2];
         const float keep = up ? v[k + 2] : v[k];
-        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
     }
     {
-        const bool up = lane & 2;
+        const bool up = lane & 4;
         const float send = up ? v[0] : v[1];
         const float keep = up ? v[1] : v[0];
-        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
     }
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
     return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }

@@ -184,28 +184,58 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
             }
             FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+            float wz = 0.0f;
             int slot = 0, row0 = 0;
+            auto stage = [&](float x, float y) {
+                mb[slot * BP_MB_STRIDE + lane] = make_float2(x, y);
+                if (++slot == BP_STAGE) {
+                    __syncwarp();
+                    warp_contract<NCG>(mb, st, BP_STAGE, my_acc, row0, lane);
+                    __syncwarp();
+                    row0 += BP_STAGE;
+                    slot = 0;
+                }
+            };
             for (int s = 0; s < nseg; ++s) {
                 const SegRec q = q0[s];
                 const int f = q.flags;
                 if (f & BP_RF) {
                     if (s == 0 || !(f & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
-                    rf_step(q, p, rr, mx, my, mz, lx, ly, lz);
+                    if (s == 0 || !(f & BP_SAME_OFF)) wz = rf_wz(q, p);
+                    rf_step_wz(q, p, rr, wz, mx, my, mz, lx, ly, lz);
                 } else {
                     if (s == 0 || !(f & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
                     free_step(ff, p, mx, my, mz, lx, ly, lz);
-                }
-                if ((f & BP_ADC) && readout) {
-                    mb[slot * BP_MB_STRIDE + lane] = make_float2(mx + lx, my + ly);
-                    if (++slot == BP_STAGE) {
-                        __syncwarp();
-                        warp_contract<NCG>(mb, st, BP_STAGE, my_acc, row0, lane);
-                        __syncwarp();
-                        row0 += BP_STAGE;
-                        slot = 0;
+                    if ((f & (BP_ADC | BP_SPOIL)) == BP_ADC) {
+                        // a readout run: the following samples with this segment's factors (the last may spoil),
+                        // within this window and this block of BP_ADJ_WIN segments (so that the runs are cut at
+                        // the same segments whatever the window plan). Their values come from a float32
+                        // recurrence; the state after the run is this one advanced by the merged factors (exact
+                        // phase in float64), as if stepped one by one.
+                        const int block_end = min(nseg, (win.x + s) / BP_ADJ_WIN * BP_ADJ_WIN + BP_ADJ_WIN - win.x);
+                        int e = s + 1;
+                        float zr = mx + lx, zi = my + ly;
+                        if (readout) stage(zr, zi);
+                        while (e < block_end && (q0[e].flags & ~BP_SPOIL) == (BP_ADC | BP_SAME_FREE)) {
+                            if (readout) {
+                                readout_advance(ff, zr, zi);
+                                stage(zr, zi);
+                            }
+                            if (q0[e++].flags & BP_SPOIL) break;
+                        }
+                        if (e > s + 1) {
+                            const FreeFactors fr = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
+                            free_step(fr, p, mx, my, mz, lx, ly, lz);
+                            if (q0[e - 1].flags & BP_SPOIL) mx = my = lx = ly = 0.0f;
+                        }
+                        s = e - 1;
+                        continue;
                     }
                 }
-                if (f & BP_SPOIL) mx = my = lx = ly = 0.0f;
+                if (f & (BP_ADC | BP_SPOIL)) {
+                    if ((f & BP_ADC) && readout) stage(mx + lx, my + ly);
+                    if (f & BP_SPOIL) mx = my = lx = ly = 0.0f;
+                }
             }
             if (slot > 0) {
                 __syncwarp();

@@ -11,12 +11,23 @@ extern "C" int bp_plan_windows(const int32_t* flags, int64_t n_segments, int seg
     while (s < n_segments) {
         const int64_t start = s, row0 = row;
         int64_t samples = 0;
-        while (s < n_segments && s - start < seg_max) {
+        bool limited = false;  // cut by seg_max or samp_max (not by a break or the sequence's end)
+        while (s < n_segments) {
             if (s > start && breaks && breaks[s]) break;
             const bool adc = (flags[s] & 2) != 0;
-            if (adc && samples == samp_max) break;
+            if (s - start == seg_max || (adc && samples == samp_max)) {
+                limited = true;
+                break;
+            }
             samples += adc ? 1 : 0;
             ++s;
+        }
+        // a limit's cut moves back to a multiple of BP_ADJ_WIN segments when the window keeps one: the cuts then
+        // fall on the same segments whatever the breaks before them
+        const int64_t aligned = (s / BP_ADJ_WIN) * BP_ADJ_WIN;
+        if (limited && aligned > start) {
+            for (int64_t t = aligned; t < s; ++t) samples -= (flags[t] & 2) ? 1 : 0;
+            s = aligned;
         }
         row += samples;
         if (nw >= max_windows) return BP_E_SIZE;

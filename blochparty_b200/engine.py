@@ -29,7 +29,7 @@ from ._lib import ptr
 TWO_PI = 2.0 * math.pi
 F32, F64 = torch.float32, torch.float64
 
-RF, ADC, SPOIL, SAME_FREE, SAME_RFDT = 1, 2, 4, 8, 16
+RF, ADC, SPOIL, SAME_FREE, SAME_RFDT, SAME_OFF = 1, 2, 4, 8, 16, 32
 
 
 @dataclass
@@ -92,7 +92,9 @@ def pack_segments(dt, rf, grad, b0_offset, adc_phase, is_rf, adc, spoil, device)
         same_dt = rec[1:, 0] == rec[:-1, 0]
         same_free = free[1:] & free[:-1] & same_dt & (seg64[1:] == seg64[:-1]).all(1)
         same_rf = is_rf[1:] & is_rf[:-1] & same_dt
-        flags[1:] |= (same_free.astype(np.int32) << 3) | (same_rf.astype(np.int32) << 4)
+        same_off = same_rf & (rec[1:, 3:7] == rec[:-1, 3:7]).all(1)  # the same G.r + dt dB0 + beta per spin
+        flags[1:] |= ((same_free.astype(np.int32) << 3) | (same_rf.astype(np.int32) << 4)
+                      | (same_off.astype(np.int32) << 5))
     rec.view(np.int32)[:, 7] = flags
     psi = np.remainder(_np64(adc_phase)[adc_b], TWO_PI)
     return (torch.from_numpy(rec).to(device).contiguous(), torch.from_numpy(seg64).to(device).contiguous(),
@@ -104,13 +106,17 @@ def plan_windows(flags: np.ndarray, samp_max: int, seg_max: int = _lib.BP_SEG_MA
     S = flags.shape[0]
     n_adc = int(((flags & ADC) != 0).sum())
     n_breaks = 0 if breaks is None else int(breaks.sum())
-    cap = S // seg_max + n_adc // samp_max + n_breaks + 2
-    out = np.zeros((cap, 4), dtype=np.int32)
+    cap = 2 * (S // seg_max + n_adc // samp_max + n_breaks) + 2  # (grown below if the aligned cuts need more)
     nw = np.zeros(1, dtype=np.int64)
     fl = np.ascontiguousarray(flags, dtype=np.int32)
     br = None if breaks is None else np.ascontiguousarray(breaks, dtype=np.uint8)
-    code = _lib.lib().bp_plan_windows(fl.ctypes.data, S, seg_max, samp_max, None if br is None else br.ctypes.data,
-                                      out.ctypes.data, cap, nw.ctypes.data)
+    while True:
+        out = np.zeros((cap, 4), dtype=np.int32)
+        code = _lib.lib().bp_plan_windows(fl.ctypes.data, S, seg_max, samp_max,
+                                          None if br is None else br.ctypes.data, out.ctypes.data, cap, nw.ctypes.data)
+        if code != _lib.BP_E_SIZE or cap >= S + 1:
+            break
+        cap = min(2 * cap, S + 1)
     _lib.check(code, "bp_plan_windows")
     return out[: int(nw[0])].copy()
 
@@ -154,6 +160,53 @@ def finish_signal(pk: Packed, raw: torch.Tensor) -> torch.Tensor:
     code = _lib.lib().bp_signal_finish(ptr(raw), ptr(pk.psi), pk.n_adc, pk.n_coils, ptr(out), _lib.stream_ptr())
     _lib.check(code, "bp_signal_finish")
     return out[:, : pk.n_adc]
+
+
+def plan_replacing(pk: Packed, spans):
+    """Windows (host array and device copy) with breaks at every span's start and end, and the window ranges
+    [(w_begin, w_end)] stepped before each span and after the last, for ``forward_replacing``."""
+    S = pk.flags.shape[0]
+    breaks = np.zeros(S, dtype=np.uint8)
+    for s, k in spans:
+        breaks[s] = 1
+        if s + k < S:
+            breaks[s + k] = 1
+    samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
+    windows = plan_windows(pk.flags, samp, breaks=breaks)
+    starts = windows[:, 0]
+    ranges, w = [], 0
+    for s, k in spans:
+        wa = int(np.searchsorted(starts, s))
+        ranges.append((w, wa))
+        w = int(np.searchsorted(starts, s + k))
+    ranges.append((w, windows.shape[0]))
+    return windows, torch.from_numpy(windows).to(pk.device), ranges
+
+
+def forward_replacing(pk: Packed, state: torch.Tensor, spans, apply, raw: torch.Tensor | None,
+                      status: torch.Tensor, max_ctas: int = 0, plan=None, events=None) -> None:
+    """The forward over all segments, where each span ``(start, length)`` of ``spans`` (sorted, disjoint, no ADC
+    inside) is not stepped but replaced by ``apply(i)`` (launching the replacement of span i on the state).
+    Windows are planned with breaks at every span's start and end (``plan_replacing``, or ``plan`` when given), so
+    a span is a whole run of windows. ``events``: a list that receives a (start, end) pair of recorded CUDA events
+    around every forward launch (the stepped part's device time)."""
+    _, wdev, ranges = plan or plan_replacing(pk, spans)
+
+    def step(wa, wb):
+        if wb <= wa:
+            return
+        if events is not None:
+            e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            e[0].record()
+        run_forward(pk, state, wdev, wa, wb, raw, status, max_ctas=max_ctas)
+        if events is not None:
+            e[1].record()
+            events.append(e)
+
+    for i in range(len(spans)):
+        step(*ranges[i])
+        apply(i)
+    step(*ranges[-1])
 
 
 def forward(case, device, max_ctas: int = 0):

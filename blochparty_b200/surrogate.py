@@ -299,27 +299,15 @@ def run_with_surrogates(inp, device, surrogates, inference: str = "mma"):
         raise ValueError(f"surrogate_inference must be one of {INFERENCE}, not {inference!r}")
     pk = engine.pack(inp, device)
     occ = find_occurrences(surrogates, inp)
-    S = pk.flags.shape[0]
-    breaks = np.zeros(S, dtype=np.uint8)
-    for s, k, *_ in occ:
-        breaks[s] = 1
-        if s + k < S:
-            breaks[s + k] = 1
-    samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
-    windows = engine.plan_windows(pk.flags, samp, breaks=breaks)
-    wdev = torch.from_numpy(windows).to(device)
-    starts = windows[:, 0]
     state = engine.initial_state(inp.pd, inp.m_init, device)
     raw = torch.zeros(max(pk.n_adc, 1), 2 * pk.n_coils, dtype=F64, device=device)
     status = torch.zeros(1, dtype=torch.int32, device=device)
     counts = torch.zeros(2, dtype=torch.int32, device=device)
     lib, st = _lib.lib(), _lib.stream_ptr()
-    w = 0
-    for s, k, i, phi0, b0 in occ:
-        wa = int(np.searchsorted(starts, s))
-        if wa > w:
-            engine.run_forward(pk, state, wdev, w, wa, raw if pk.n_adc else None, status)
-        sg = surrogates[i]
+
+    def apply(i):
+        s, k, isg, phi0, b0 = occ[i]
+        sg = surrogates[isg]
         if inference == "mma":
             code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(sg.wtiles()),
                                               ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0,
@@ -328,9 +316,8 @@ def run_with_surrogates(inp, device, surrogates, inference: str = "mma"):
             code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s, k, sg.T,
                                           sg.gz, sg.thickness, sg.z0, phi0, b0, *sg.domain, ptr(counts), st)
         _lib.check(code, "bp_surrogate_pulse")
-        w = int(np.searchsorted(starts, s + k))
-    if w < windows.shape[0]:
-        engine.run_forward(pk, state, wdev, w, windows.shape[0], raw if pk.n_adc else None, status)
+
+    engine.forward_replacing(pk, state, [(s, k) for s, k, *_ in occ], apply, raw if pk.n_adc else None, status)
     sig = engine.finish_signal(pk, raw)
     torch.cuda.synchronize(device)
     _lib.check_status(status, "bp_forward")

@@ -34,8 +34,10 @@ extern "C" {
  * 4 spoil) into consecutive windows of at most `seg_max` (<= BP_SEG_MAX) segments and `samp_max` ADC samples;
  * `breaks` (optional, n_segments bytes) forces a window to start at every segment whose byte is nonzero.
  * Writes 4 ints per window (first segment, end segment, first ADC row, samples) into `windows` (room for
- * `max_windows`) and the count into `*n_windows`. Replaces the dispatch boundaries of
- * engines/gpu/driver.py:617-627. Returns BP_E_SIZE when `max_windows` is too small. */
+ * `max_windows`) and the count into `*n_windows`. A window cut by one of the two limits ends on a multiple of
+ * BP_ADJ_WIN segments whenever it still holds one (always for samp_max >= BP_ADJ_WIN), so limit cuts do not depend
+ * on the breaks before them. Replaces the dispatch boundaries of engines/gpu/driver.py:617-627. Returns
+ * BP_E_SIZE when `max_windows` is too small. */
 int bp_plan_windows(const int32_t* flags, int64_t n_segments, int seg_max, int samp_max, const uint8_t* breaks,
                     int32_t* windows, int64_t max_windows, int64_t* n_windows);
 
@@ -122,6 +124,17 @@ int bp_adjoint_noalloc(const float* spins, const float* sens, int n, int n_coils
                        const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
                        const float* wstates, const float* h, float* lam, float* gs, float* gc, double* seg,
                        void* stream);
+
+/* ---- reused pulses (replace the pulse maps of engines/gpu/cuda/pulse.cu.in:3-32 and the reuse branch of
+ * engines/gpu/cuda/kernels.cu.in:141-165) ----
+ * bp_pulse_maps: per spin, the affine map m -> M m + v of the k_steps RF segments [seg0, seg0 + k_steps) of `segs`
+ * (plain RF steps composed in float64), into maps [12][n] float64 (M row-major, then v): BP_PULSE_MAP_BYTES per
+ * spin. bp_pulse_apply: one occurrence of that pulse with its RF times exp(i phase) applied to the state [6][n]:
+ * m -> Rz(phase) (M Rz(-phase) m + v), in float64 on the compensated state. */
+#define BP_PULSE_MAP_BYTES 96
+int bp_pulse_maps(const float* spins, int n, const void* segs, const double* seg64, int seg0, int k_steps,
+                  double* maps, void* stream);
+int bp_pulse_apply(const double* maps, int n, float* state, double phase, void* stream);
 
 /* ---- learned RF surrogate (no counterpart in the reference; its nearest part is the exact per-spin map of a
  * reused pulse, engines/gpu/cuda/pulse.cu.in:3-32) ----

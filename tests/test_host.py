@@ -38,6 +38,10 @@ def test_planner_windows_cover_the_sequence():
         assert w[0, 0] == 0 and w[-1, 1] == 5000
         assert (w[1:, 0] == w[:-1, 1]).all()
         assert ((w[:, 1] - w[:, 0]) <= 100).all() and (w[:, 3] <= samp).all()
+        # cuts by a limit fall on multiples of BP_ADJ_WIN segments whenever the window keeps one
+        limited = w[:-1, 1]
+        assert all(e % _lib.BP_ADJ_WIN == 0 or e - a < _lib.BP_ADJ_WIN or e // _lib.BP_ADJ_WIN * _lib.BP_ADJ_WIN <= a
+                   for a, e in zip(w[:-1, 0], limited))
         adc = (flags & 2) != 0
         counts = np.array([adc[a:b].sum() for a, b in w[:, :2]])
         assert (counts == w[:, 3]).all()
@@ -67,7 +71,8 @@ def test_segment_records():
     rec, seg64, psi, flags, n_adc = engine.pack_segments(seq.dt, seq.rf, seq.grad, seq.b0_offset, seq.adc_phase,
                                                          seq.is_rf, seq.adc, seq.spoil, "cpu")
     assert rec.shape == (len(seq), 8) and rec.dtype == torch.float32 and n_adc == 4
-    assert flags.tolist() == [1, 1 | 16, 2, 2, 2 | 8, 2 | 8, 0, 4]  # first sample half a dwell: not "same"
+    # the second RF step has the first's dt and offset; the first sample is half a dwell: not "same"
+    assert flags.tolist() == [1, 1 | 16 | 32, 2, 2, 2 | 8, 2 | 8, 0, 4]
     assert abs(float(rec[0, 1]) - (-2 * np.pi * 5e-5 * float(seq.rf[0, 0]))) < 1e-6
     assert float(seg64[3, 0]) == 1000.0 * 1e-5 and float(seg64[3, 3]) == 3.0 * 1e-5
     assert rec.view(torch.int32)[:, 7].tolist() == flags.tolist()
