@@ -35,6 +35,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "isochromat-steps/s (fwd)"
 UNIT = "isochromat-steps/s"
 WORKLOAD = "gre3d_64: 3D spoiled GRE 64^3, 1,048,576 spins, 8 coils, 200-step sinc slab, TR 8 ms"
+WORKLOAD_128 = ("gre3d_128_4echo: 4-echo 3D GRE 128^3 head phantom, 8,388,608 spins, 8 coils, 200-step sinc slab, "
+                "TR 20 ms")
 
 # algorithmic FP32 flops per spin and segment of the forward kernel (counted from its formulas in
 # blochparty_b200/csrc/bloch_common.cuh; kept fixed across versions): RF segment, free segment with cached
@@ -272,6 +274,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grad", action="store_true", help="forward + adjoint (gradients of T1 and the RF), one GPU")
+    ap.add_argument("--workload", default="gre3d_64", choices=("gre3d_64", "gre3d_128_4echo"))
+    ap.add_argument("--max-segments", type=int, default=0,
+                    help="time the workload's first whole TRs only, up to this many segments (0: all)")
+    ap.add_argument("--pulses", default="step", choices=("step", "reuse"),
+                    help="reuse: recurring pulses through their exact per-spin maps (composed inside every step)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -297,12 +304,25 @@ def main():
     import blochparty_b200 as bpb
     from blochparty_b200 import _lib, engine, workloads
 
-    ph, seq, coils = workloads.gre3d_64(args.n) if rank == 0 else _rank_workload(args.n, rank)
+    if args.workload == "gre3d_128_4echo":
+        ph, seq, coils = workloads.gre3d_128_4echo()
+        workload = WORKLOAD_128
+    else:
+        ph, seq, coils = workloads.gre3d_64(args.n) if rank == 0 else _rank_workload(args.n, rank)
+        workload = WORKLOAD if args.n == 64 else f"gre3d_{args.n}"
+    if args.max_segments:
+        seq = workloads.first_trs(seq, args.max_segments)
+        workload += f"; its first {len(seq)} segments (whole TRs)"
     inp = bpb.api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad,
                          seq.adc_phase, None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
     pk = engine.pack(inp, dev)
-    mma = None
-    if args.readout == "bf16x3":
+    mma = reuse = None
+    if args.pulses == "reuse":
+        from blochparty_b200.pulses import Reuse
+
+        reuse = Reuse(inp, pk)
+        windows, wdev = reuse.plan[0], reuse.plan[1]
+    elif args.readout == "bf16x3":
         from blochparty_b200.readout_mma import MmaBuffers, run_forward_mma
 
         mma = MmaBuffers(pk)
@@ -320,12 +340,17 @@ def main():
     kstart = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     kend = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
 
+    fwd_events = [[] for _ in range(args.steps)]  # reused pulses: the forward launches between occurrences
+
     def step(i=None):
         state.copy_(state0)
         raw.zero_()
         if i is not None:
             kstart[i].record()
-        if mma is not None:
+        if reuse is not None:
+            reuse.make_maps(pk)
+            reuse.run(pk, state, raw, status, events=None if i is None else fwd_events[i])
+        elif mma is not None:
             run_forward_mma(pk, mma, state, raw, status)
         else:
             engine.run_forward(pk, state, wdev, 0, windows.shape[0], raw, status)
@@ -360,6 +385,8 @@ def main():
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     ms = float(ms)
     kernel_ms = statistics.mean(kstart[i].elapsed_time(kend[i]) for i in range(args.steps))
+    if reuse is not None:  # the forward kernel's own time (the maps and their applications excluded)
+        kernel_ms = statistics.mean(sum(a.elapsed_time(b) for a, b in ev) for ev in fwd_events)
     value = world * n * S / (ms * 1e-3)
 
     # end to end: the public simulate() call with host inputs (packing, copies, kernels, result read-back)
@@ -367,7 +394,7 @@ def main():
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        bpb.simulate(ph, seq, coils, readout=args.readout)
+        bpb.simulate(ph, seq, coils, readout=args.readout, pulses=args.pulses)
         e2e_ms.append((time.perf_counter() - t) * 1e3)
     e2e = world * n * S / (statistics.median(e2e_ms) * 1e-3) if e2e_ms else None
     h2d = sum(t.numel() * t.element_size() for t in (pk.spins, pk.sens, pk.segs, pk.seg64, pk.psi, wdev, state0))
@@ -378,14 +405,20 @@ def main():
         dist.destroy_process_group() if world > 1 else None
         return
     peak = ffma_peak_tflops(dev)
-    flops = n * flops_per_spin(pk.flags, pk.n_coils)
+    stepped = pk.flags
+    if reuse is not None:  # the flops of the segments the forward kernel stepped
+        keep = np.ones(pk.flags.shape[0], dtype=bool)
+        for s0, k in reuse.spans:
+            keep[s0:s0 + k] = False
+        stepped = pk.flags[keep]
+    flops = n * flops_per_spin(stepped, pk.n_coils)
     achieved = flops / (kernel_ms * 1e-3) / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "spins_per_gpu": n, "segments": S, "adc_samples": pk.n_adc,
-                   "coils": pk.n_coils, "readout": args.readout,
+        "config": {"workload": workload, "spins_per_gpu": n, "segments": S, "adc_samples": pk.n_adc,
+                   "coils": pk.n_coils, "readout": args.readout, "pulses": args.pulses,
                    "ctas": (_lib.lib().bp_forward_mma_grid(n) if mma is not None
                             else _lib.lib().bp_forward_grid(n, pk.n_coils)), "l2": "inputs larger than L2 (state, spins, coils, "
                    "segments ~220 MB per GPU) and a 256 MB L2 flush between timed steps"},
@@ -397,11 +430,13 @@ def main():
                      "flops_per_launch": flops},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": statistics.median(e2e_ms) if e2e_ms else None},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": (2 * args.steps if reuse is None else
+                         args.steps * (len(reuse.pulses) + len(reuse.spans) + len(fwd_events[0]) + 1)),
         "clocks": clocks.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        case, sample = cpu_sample(workloads.gre3d_64)
+        case, sample = cpu_sample(workloads.gre3d_128_4echo if args.workload == "gre3d_128_4echo"
+                                  else workloads.gre3d_64)
         v, cores = time_cpu(case)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     print(json.dumps(line), flush=True)

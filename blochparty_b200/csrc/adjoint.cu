@@ -167,13 +167,18 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
         const int j = active ? j0 : 0;
         const Spin p = load_spin(a.spins, n, j, active);
         float lx = active ? a.lam[j] : 0.0f, ly = active ? a.lam[n + j] : 0.0f, lz = active ? a.lam[2 * n + j] : 0.0f;
+        // per-spin gradients: running totals carried in registers through the interval (loaded here, stored after
+        // its last window): every contribution is added to the total in segment order, so the results do not
+        // depend on where the checkpoint intervals fall
         float g[N_GS];
 #pragma unroll
-        for (int k = 0; k < N_GS; ++k) g[k] = 0.0f;
+        for (int k = 0; k < N_GS; ++k) g[k] = active ? a.gs[k * n + j] : 0.0f;
+        const bool want_gc = a.gc != nullptr && active;
         float gcr[8 * NCG], gci[8 * NCG], sr[8 * NCG], si[8 * NCG];
 #pragma unroll
         for (int c = 0; c < 8 * NCG; ++c) {
-            gcr[c] = gci[c] = 0.0f;
+            gcr[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c) * n + j] : 0.0f;
+            gci[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c + 1) * n + j] : 0.0f;
             sr[c] = active ? a.sens[(2 * c) * n + j] : 0.0f;
             si[c] = active ? a.sens[(2 * c + 1) * n + j] : 0.0f;
         }
@@ -268,25 +273,22 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
                     dst[i] += t;
                 }
             }
-            // per-spin gradients flushed at every window end: windows fall on multiples of BP_ADJ_WIN segments
-            // whatever the checkpoint interval, so the sums (and the result) do not depend on it
-            if (active) {
+            __syncthreads();
+        }
+        if (active) {
+            a.lam[j] = lx, a.lam[n + j] = ly, a.lam[2 * n + j] = lz;
 #pragma unroll
-                for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] += g[k], g[k] = 0.0f;
-                if (a.gc != nullptr) {
+            for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] = g[k];
+            if (want_gc) {
 #pragma unroll
-                    for (int c = 0; c < 8 * NCG; ++c) {
-                        if (c < a.n_coils) {
-                            a.gc[(2 * c) * n + j] += gcr[c];
-                            a.gc[(2 * c + 1) * n + j] += gci[c];
-                        }
-                        gcr[c] = gci[c] = 0.0f;
+                for (int c = 0; c < 8 * NCG; ++c) {
+                    if (c < a.n_coils) {
+                        a.gc[(2 * c) * n + j] = gcr[c];
+                        a.gc[(2 * c + 1) * n + j] = gci[c];
                     }
                 }
             }
-            __syncthreads();
         }
-        if (active) a.lam[j] = lx, a.lam[n + j] = ly, a.lam[2 * n + j] = lz;
     }
 }
 

@@ -13,11 +13,12 @@
 //    through the window: the tile's state is loaded from HBM, propagated in registers, and stored back.
 //  * ADC samples: each warp stages the (mx, my) of its 32 spins for 16 samples in shared memory, then contracts
 //    them with the spins' coil sensitivities (an FMA chain over the 32 spins per lane: a small matrix product)
-//    into its own slice of a per-window accumulator in shared memory, summed over all of the CTA's tiles. At
-//    the window's end the warps' slices are added in fixed order and the CTA's
-//    partial is added to the float64 signal with one float64 atomic per (sample, coil, re/im): the cross-block
-//    sum is float64, and the CTA-level sum covers thousands of spins, so the number of atomics does not grow
-//    with the spin count.
+//    and adds the results into the CTA's window accumulator in shared memory (shared-memory atomics: one
+//    accumulator per CTA, summed over all of its tiles and warps). At the window's end the CTA's partial is added
+//    to the float64 signal with one float64 atomic per (sample, coil, re/im): the cross-block sum is float64, and
+//    the CTA-level sum covers thousands of spins, so the number of atomics does not grow with the spin count.
+//  * Readout runs (samples with one segment's factors): the samples come from a float32 recurrence, the state
+//    after the run from the float64 merged factors (see bloch_common.cuh), within blocks of BP_ADJ_WIN segments.
 //  * Demodulation by exp(-i adc_phase) is the same for every spin and is applied after the sum, in float64
 //    (bp_signal_finish).
 #include <cuda_runtime.h>
@@ -54,9 +55,9 @@ __host__ __device__ constexpr int samp_max() {
 }
 
 // The warp's staged samples (mb: [BP_STAGE][BP_MB_STRIDE] (mx, my) of its 32 spins) contracted with the coil
-// sensitivities of those spins (st: [32][16 NCG], coil c real at 2c, imaginary at 2c + 1) and added to the warp's
-// accumulator rows acc[row0 + s]. Lane l computes sample l & 15, coils 4 (l >> 4) .. + 3 of every coil group:
-// a chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles).
+// sensitivities of those spins (st: [32][16 NCG], coil c real at 2c, imaginary at 2c + 1) and added to the CTA's
+// accumulator rows acc[row0 + s] (shared-memory atomics). Lane l computes sample l & 15, coils 4 (l >> 4) .. + 3
+// of every coil group: a chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles).
 template <int NCG>
 __device__ __forceinline__ void warp_contract(const float2* mb, const float* st, int nslot, float* acc, int row0,
                                               int lane) {
@@ -81,30 +82,31 @@ __device__ __forceinline__ void warp_contract(const float2* mb, const float* st,
             re[3] = fmaf(m.x, b.z, fmaf(-m.y, b.w, re[3]));
             im[3] = fmaf(m.x, b.w, fmaf(m.y, b.z, im[3]));
         }
-        float4* dst = reinterpret_cast<float4*>(acc + (row0 + smp) * VG + 16 * g + 8 * half);
-        float4 d0 = dst[0], d1 = dst[1];
-        d0.x += re[0], d0.y += im[0], d0.z += re[1], d0.w += im[1];
-        d1.x += re[2], d1.y += im[2], d1.z += re[3], d1.w += im[3];
-        dst[0] = d0, dst[1] = d1;
+        float* dst = acc + (row0 + smp) * VG + 16 * g + 8 * half;  // the CTA's accumulator: every warp adds here
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            atomicAdd(dst + 2 * c, re[c]);
+            atomicAdd(dst + 2 * c + 1, im[c]);
+        }
     }
 }
 
 template <int NCG>
 __host__ __device__ constexpr size_t fwd_smem_bytes_t() {
     return 2 * BP_SEG_MAX * sizeof(SegRec)                                   // segment blocks
-           + (size_t)BP_WARPS * samp_max<NCG>() * 16 * NCG * sizeof(float)   // window accumulators
+           + (size_t)samp_max<NCG>() * 16 * NCG * sizeof(float)              // the window's accumulator
            + (size_t)BP_WARPS * BP_STAGE * BP_MB_STRIDE * sizeof(float2)     // staged samples
            + (size_t)BP_WARPS * 32 * 16 * NCG * sizeof(float)                // coil sensitivities of the tile
            + 2 * sizeof(uint64_t);
 }
 
 template <int NCG>
-__global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
+__global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kernel(FwdArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int VG = 16 * NCG;  // accumulator values per sample (coil groups of 8, padded)
     SegRec* segbuf = reinterpret_cast<SegRec*>(smem_raw);                                   // [2][BP_SEG_MAX]
     float* acc = reinterpret_cast<float*>(segbuf + 2 * BP_SEG_MAX);                         // [W][samp][VG]
-    float2* mball = reinterpret_cast<float2*>(acc + BP_WARPS * samp_max<NCG>() * VG);       // [W][16][33]
+    float2* mball = reinterpret_cast<float2*>(acc + samp_max<NCG>() * VG);                  // [W][16][33]
     float* stall = reinterpret_cast<float*>(mball + BP_WARPS * BP_STAGE * BP_MB_STRIDE);    // [W][32][VG]
     uint64_t* bars = reinterpret_cast<uint64_t*>(stall + BP_WARPS * 32 * VG);
 
@@ -112,7 +114,6 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
     const int n = a.n;
     const int n_tiles = (n + BP_THREADS - 1) / BP_THREADS;
     const int nv = 2 * a.n_coils;
-    float* my_acc = acc + warp * samp_max<NCG>() * VG;
     float2* mb = mball + warp * BP_STAGE * BP_MB_STRIDE;
     float* st = stall + warp * 32 * VG;
 
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
         mbar_init(&bars[1], 1);
         fence_mbar_init();
     }
-    for (int i = tid; i < BP_WARPS * samp_max<NCG>() * VG; i += BP_THREADS) acc[i] = 0.0f;
+    for (int i = tid; i < samp_max<NCG>() * VG; i += BP_THREADS) acc[i] = 0.0f;
     __syncthreads();
 
     auto issue = [&](int w, int buf) {
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
                 mb[slot * BP_MB_STRIDE + lane] = make_float2(x, y);
                 if (++slot == BP_STAGE) {
                     __syncwarp();
-                    warp_contract<NCG>(mb, st, BP_STAGE, my_acc, row0, lane);
+                    warp_contract<NCG>(mb, st, BP_STAGE, acc, row0, lane);
                     __syncwarp();
                     row0 += BP_STAGE;
                     slot = 0;
@@ -203,6 +204,17 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
                     if (s == 0 || !(f & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
                     if (s == 0 || !(f & BP_SAME_OFF)) wz = rf_wz(q, p);
                     rf_step_wz(q, p, rr, wz, mx, my, mz, lx, ly, lz);
+                    if (!(f & (BP_ADC | BP_SPOIL))) {
+                        // the rest of a pulse with this dt and offset: only the RF changes from step to step
+                        constexpr int kRun = BP_RF | BP_SAME_RFDT | BP_SAME_OFF;
+                        while (s + 1 < nseg) {
+                            const SegRec& qn = q0[s + 1];
+                            if ((qn.flags & (kRun | BP_ADC | BP_SPOIL)) != kRun) break;
+                            ++s;
+                            rf_step_wz(qn, p, rr, wz, mx, my, mz, lx, ly, lz);
+                        }
+                        continue;
+                    }
                 } else {
                     if (s == 0 || !(f & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
                     free_step(ff, p, mx, my, mz, lx, ly, lz);
@@ -239,7 +251,7 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
             }
             if (slot > 0) {
                 __syncwarp();
-                warp_contract<NCG>(mb, st, slot, my_acc, row0, lane);
+                warp_contract<NCG>(mb, st, slot, acc, row0, lane);
                 __syncwarp();
             }
             if (active) {
@@ -253,16 +265,12 @@ __global__ void __launch_bounds__(BP_THREADS, 4) bp_forward_kernel(FwdArgs a) {
         }
         __syncthreads();
         if (readout) {
-            // the warps' slices in fixed order, then one float64 atomic per value; slots are cleared as read
+            // the CTA's sums, one float64 atomic per value; slots are cleared as read
             for (int k = tid; k < win.w * nv; k += BP_THREADS) {
                 const int r = k / nv, v = k % nv;
                 const int slot = r * VG + v;
-                float t = 0.0f;
-#pragma unroll
-                for (int ww = 0; ww < BP_WARPS; ++ww) {
-                    t += acc[ww * samp_max<NCG>() * VG + slot];
-                    acc[ww * samp_max<NCG>() * VG + slot] = 0.0f;
-                }
+                const float t = acc[slot];
+                acc[slot] = 0.0f;
                 atomicAdd(a.raw + (size_t)(win.z + r) * nv + v, (double)t);
             }
             __syncthreads();

@@ -153,68 +153,113 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
             }
             FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+            float wz = 0.0f;
             int slot = 0, grp = 0, row = 0;
-            for (int s = 0; s < nseg; ++s) {
+            // one sample (x, y) into the B block; a full block (or the window's last sample) goes to the tensor
+            // cores. Returns false when a wait failed (the CTA stops).
+            auto stage = [&](float x, float y) -> bool {
+                const int b = grp & 1;
+                // buffer b is free once the MMAs of the block before last have completed (each thread waits; a
+                // failed wait is reported at the next barrier)
+                if (slot == 0 && !drain(b)) err = true;
+                uint16_t xh, xl, yh, yl;
+                split_bf16(x, xh, xl);
+                split_bf16(y, yh, yl);
+                const uint32_t off = kmajor_off(slot, 2 * tid, MM_B_LBO, MM_B_SBO);
+                unsigned char* bb = sm + MM_OFF_B + 2 * b * MM_B_BYTES;
+                *reinterpret_cast<uint32_t*>(bb + off) = (uint32_t)xh | ((uint32_t)yh << 16);
+                *reinterpret_cast<uint32_t*>(bb + MM_B_BYTES + off) = (uint32_t)xl | ((uint32_t)yl << 16);
+                ++slot;
+                ++row;
+                if (slot == MM_BLOCK || row == win.w) {
+                    fence_proxy_async_smem();  // this thread's B writes, visible to the tensor cores
+                    if (__syncthreads_or(err)) return false;  // the block is complete; every wait so far succeeded
+                    if (tid == 0) {
+                        if (!a_waited && !mbar_wait_bounded(&bars[4], a_phase)) err = true;
+                        if (!err) {
+                            tc_fence_after();
+                            const uint32_t bh = sB + 2 * b * MM_B_BYTES, bl = bh + MM_B_BYTES;
+                            const uint32_t d = tmem + (uint32_t)(grp * MM_BLOCK);
+                            // K step kk starts 2 kk core matrices further along K: the descriptors' start field
+                            // (address >> 4, low 14 bits) advances by 2 LBO / 16 per step
+                            uint64_t ah_d = umma_desc(sA, MM_A_LBO, MM_A_SBO);
+                            uint64_t al_d = umma_desc(sA + MM_A_BYTES, MM_A_LBO, MM_A_SBO);
+                            uint64_t bh_d = umma_desc(bh, MM_B_LBO, MM_B_SBO);
+                            uint64_t bl_d = umma_desc(bl, MM_B_LBO, MM_B_SBO);
+#pragma unroll
+                            for (int kk = 0; kk < 16; ++kk) {
+                                umma_bf16(d, ah_d, bh_d, idesc, (kk == 0 && first_tile) ? 0u : 1u);
+                                umma_bf16(d, ah_d, bl_d, idesc, 1u);
+                                umma_bf16(d, al_d, bh_d, idesc, 1u);
+                                ah_d += 2 * MM_A_LBO / 16, al_d += 2 * MM_A_LBO / 16;
+                                bh_d += 2 * MM_B_LBO / 16, bl_d += 2 * MM_B_LBO / 16;
+                            }
+                            umma_commit(&bars[2 + b]);
+                        }
+                    }
+                    if (!a_waited) a_phase ^= 1u, a_waited = true;
+                    mma_pending[b] = true;
+                    ++grp;
+                    slot = 0;
+                }
+                return true;
+            };
+            for (int s = 0; s < nseg && !fail; ++s) {
                 const SegRec q = q0[s];
                 const int f = q.flags;
                 if (f & BP_RF) {
                     if (s == 0 || !(f & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
-                    rf_step(q, p, rr, mx, my, mz, lx, ly, lz);
+                    if (s == 0 || !(f & BP_SAME_OFF)) wz = rf_wz(q, p);
+                    rf_step_wz(q, p, rr, wz, mx, my, mz, lx, ly, lz);
+                    if (!(f & (BP_ADC | BP_SPOIL))) {  // the rest of the pulse, as in bp_forward
+                        constexpr int kRun = BP_RF | BP_SAME_RFDT | BP_SAME_OFF;
+                        while (s + 1 < nseg) {
+                            const SegRec& qn = q0[s + 1];
+                            if ((qn.flags & (kRun | BP_ADC | BP_SPOIL)) != kRun) break;
+                            ++s;
+                            rf_step_wz(qn, p, rr, wz, mx, my, mz, lx, ly, lz);
+                        }
+                        continue;
+                    }
                 } else {
                     if (s == 0 || !(f & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
                     free_step(ff, p, mx, my, mz, lx, ly, lz);
-                }
-                if ((f & BP_ADC) && readout) {
-                    const int b = grp & 1;
-                    // buffer b is free once the MMAs of the block before last have completed (each thread waits;
-                    // a failed wait is reported at the next barrier)
-                    if (slot == 0 && !drain(b)) err = true;
-                    uint16_t xh, xl, yh, yl;
-                    split_bf16(mx + lx, xh, xl);
-                    split_bf16(my + ly, yh, yl);
-                    const uint32_t off = kmajor_off(slot, 2 * tid, MM_B_LBO, MM_B_SBO);
-                    unsigned char* bb = sm + MM_OFF_B + 2 * b * MM_B_BYTES;
-                    *reinterpret_cast<uint32_t*>(bb + off) = (uint32_t)xh | ((uint32_t)yh << 16);
-                    *reinterpret_cast<uint32_t*>(bb + MM_B_BYTES + off) = (uint32_t)xl | ((uint32_t)yl << 16);
-                    ++slot;
-                    ++row;
-                    if (slot == MM_BLOCK || row == win.w) {
-                        fence_proxy_async_smem();  // this thread's B writes, visible to the tensor cores
-                        if (__syncthreads_or(err)) {  // the block is complete; and every wait so far succeeded
-                            fail = true;
-                            break;
-                        }
-                        if (tid == 0) {
-                            if (!a_waited && !mbar_wait_bounded(&bars[4], a_phase)) err = true;
-                            if (!err) {
-                                tc_fence_after();
-                                const uint32_t bh = sB + 2 * b * MM_B_BYTES, bl = bh + MM_B_BYTES;
-                                const uint32_t d = tmem + (uint32_t)(grp * MM_BLOCK);
-                                // K step kk starts 2 kk core matrices further along K: the descriptors' start
-                                // field (address >> 4, low 14 bits) advances by 2 LBO / 16 per step
-                                uint64_t ah_d = umma_desc(sA, MM_A_LBO, MM_A_SBO);
-                                uint64_t al_d = umma_desc(sA + MM_A_BYTES, MM_A_LBO, MM_A_SBO);
-                                uint64_t bh_d = umma_desc(bh, MM_B_LBO, MM_B_SBO);
-                                uint64_t bl_d = umma_desc(bl, MM_B_LBO, MM_B_SBO);
-#pragma unroll
-                                for (int kk = 0; kk < 16; ++kk) {
-                                    umma_bf16(d, ah_d, bh_d, idesc, (kk == 0 && first_tile) ? 0u : 1u);
-                                    umma_bf16(d, ah_d, bl_d, idesc, 1u);
-                                    umma_bf16(d, al_d, bh_d, idesc, 1u);
-                                    ah_d += 2 * MM_A_LBO / 16, al_d += 2 * MM_A_LBO / 16;
-                                    bh_d += 2 * MM_B_LBO / 16, bl_d += 2 * MM_B_LBO / 16;
+                    if ((f & (BP_ADC | BP_SPOIL)) == BP_ADC) {
+                        // a readout run, as in bp_forward: the samples by a float32 recurrence within this window
+                        // and block of BP_ADJ_WIN segments, the state after it from the merged factors
+                        const int block_end = min(nseg, (win.x + s) / BP_ADJ_WIN * BP_ADJ_WIN + BP_ADJ_WIN - win.x);
+                        int e = s + 1;
+                        float zr = mx + lx, zi = my + ly;
+                        if (readout && !stage(zr, zi)) fail = true;
+                        while (!fail && e < block_end && (q0[e].flags & ~BP_SPOIL) == (BP_ADC | BP_SAME_FREE)) {
+                            if (readout) {
+                                readout_advance(ff, zr, zi);
+                                if (!stage(zr, zi)) {
+                                    fail = true;
+                                    break;
                                 }
-                                umma_commit(&bars[2 + b]);
                             }
+                            if (q0[e++].flags & BP_SPOIL) break;
                         }
-                        if (!a_waited) a_phase ^= 1u, a_waited = true;
-                        mma_pending[b] = true;
-                        ++grp;
-                        slot = 0;
+                        if (fail) break;
+                        if (e > s + 1) {
+                            const FreeFactors fr = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
+                            free_step(fr, p, mx, my, mz, lx, ly, lz);
+                            if (q0[e - 1].flags & BP_SPOIL) mx = my = lx = ly = 0.0f;
+                        }
+                        s = e - 1;
+                        continue;
                     }
                 }
-                if (f & BP_SPOIL) mx = my = lx = ly = 0.0f;
+                if (f & (BP_ADC | BP_SPOIL)) {
+                    if ((f & BP_ADC) && readout && !stage(mx + lx, my + ly)) {
+                        fail = true;
+                        break;
+                    }
+                    if (f & BP_SPOIL) mx = my = lx = ly = 0.0f;
+                }
             }
+            // (on a failure the tile loop ends below, after the A-tile copy has been waited for)
             if (active) {
                 a.state[j] = mx, a.state[n + j] = my, a.state[2 * n + j] = mz;
                 a.state[3 * n + j] = lx, a.state[4 * n + j] = ly, a.state[5 * n + j] = lz;

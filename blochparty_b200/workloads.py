@@ -20,10 +20,11 @@ Each function returns ``(phantom, seq, coils)`` (plus extras where stated) as fl
 
 from __future__ import annotations
 
+import numpy as np
 import torch
 
 from . import phantoms, sequences
-from .types import Phantom
+from .types import Phantom, Sequence
 
 F64 = torch.float64
 
@@ -76,3 +77,17 @@ def gre3d_128_4echo(n=128):
                         rf_duration=2e-3, rf_steps=200, slab_thickness=0.2, n_echoes=4, echo_spacing=2.6e-3,
                         spoiling="rf")
     return ph, seq, phantoms.birdcage_sensitivities(ph.pos, 8)
+
+
+def first_trs(seq, max_segments: int):
+    """The sequence's first segments, up to the last RF pulse that starts at or before ``max_segments`` (whole TRs
+    of a TR-periodic sequence): a bounded sample of a long workload with its per-TR structure."""
+    is_rf = np.asarray(seq.is_rf, dtype=bool)
+    starts = np.flatnonzero(is_rf & ~np.concatenate([[False], is_rf[:-1]]))
+    cut = int(starts[starts <= max_segments].max()) if (starts <= max_segments).any() else len(seq)
+    if cut == 0:
+        cut = len(seq)
+    sl = slice(0, cut)
+    return Sequence(seq.dt[sl], seq.rf[sl], seq.grad[sl], seq.adc_phase[sl], list(seq.is_rf[:cut]),
+                    list(seq.adc[:cut]), list(seq.spoil[:cut]), dict(seq.meta, first_segments=cut),
+                    None if seq.b0_offset is None else seq.b0_offset[sl])
