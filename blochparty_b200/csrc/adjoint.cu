@@ -84,11 +84,10 @@ __device__ __forceinline__ void offset_grads(float gcyc, const SegRec& q, const 
 }
 
 // Reverse of an RF segment from its input state (x0, y0, z0): lambda in/out, gradients accumulated.
-__device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, float e1h, float e2h, float x0, float y0,
-                                           float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
+__device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, float e1h, float e2h, float wz, float x0,
+                                           float y0, float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
     const float h = 0.5f * q.dt;
-    const float cyc = fmaf(q.kx, p.px, fmaf(q.ky, p.py, fmaf(q.kz, p.pz, fmaf(q.dt, p.db0, q.beta))));
-    const float wz = -BP_TWO_PI_F * cyc, wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
+    const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;  // wz = rf_wz(q, p)
     const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
     float c, s1, s2, f1, f2;
     rot_factors(p2, c, s1, s2, f1, f2);
@@ -148,10 +147,12 @@ __device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, con
 }
 
 template <int NCG>
-__global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
+__global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kernel(AdjArgs a) {
     extern __shared__ __align__(16) float sm[];
     float* slots = sm;                                     // [ADJ_SLOTS][3][ADJ_THREADS]
     float* segacc = slots + ADJ_SLOTS * 3 * ADJ_THREADS;  // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
+    SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * N_SG);  // [BP_ADJ_WIN] the window's
+    double4* wk64 = reinterpret_cast<double4*>(wrec + BP_ADJ_WIN);                     // records and moments
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
     const int nv = 2 * a.n_coils;
@@ -185,6 +186,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
         for (int w = a.wb - 1; w >= a.wa; --w) {
             const int4 win = a.windows[w];
             const int nseg = win.y - win.x;
+            if (nseg < 0 || nseg > BP_ADJ_WIN) continue;  // not an adjoint window (uniform): never index past the slots
+            // the window's records into shared memory (every warp of the CTA sweeps the same window); the barrier
+            // at the end of the previous window ended its reads
+            for (int i = tid; i < nseg * 8; i += ADJ_THREADS)
+                reinterpret_cast<float*>(wrec)[i] = reinterpret_cast<const float*>(a.segs + win.x)[i];
+            for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
+                reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
+            __syncthreads();
             // recompute the window: slot k = state after segment k-1 (before its spoil), slot 0 = window start
             const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
             float mx = 0.f, my = 0.f, mz = 0.f, llx = 0.f, lly = 0.f, llz = 0.f;
@@ -195,14 +204,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
             slots[tid] = mx + llx, slots[ADJ_THREADS + tid] = my + lly, slots[2 * ADJ_THREADS + tid] = mz + llz;
             FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
-            float e1h = 0.f, e2h = 0.f;
+            float e1h = 0.f, e2h = 0.f, wz = 0.f;
             for (int s = 0; s < nseg; ++s) {
-                const SegRec q = a.segs[win.x + s];
+                const SegRec q = wrec[s];
                 if (q.flags & BP_RF) {
                     if (s == 0 || !(q.flags & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
-                    rf_step(q, p, rr, mx, my, mz, llx, lly, llz);
+                    if (s == 0 || !(q.flags & BP_SAME_OFF)) wz = rf_wz(q, p);
+                    rf_step_wz(q, p, rr, wz, mx, my, mz, llx, lly, llz);
                 } else {
-                    if (s == 0 || !(q.flags & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
+                    if (s == 0 || !(q.flags & BP_SAME_FREE)) ff = free_factors(q, wk64[s], p);
                     free_step(ff, p, mx, my, mz, llx, lly, llz);
                 }
                 float* sl = slots + (s + 1) * 3 * ADJ_THREADS;
@@ -213,7 +223,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
             int row = win.z + win.w;
             int cached_free = -1, cached_rf = -1;
             for (int s = nseg - 1; s >= 0; --s) {
-                const SegRec q = a.segs[win.x + s];
+                const SegRec q = wrec[s];
                 const int f = q.flags;
                 if (f & BP_SPOIL) lx = ly = 0.0f;
                 if ((f & BP_ADC) && a.h != nullptr) {
@@ -238,20 +248,22 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) bp_adjoint_kernel(AdjArgs a) {
                 const float* in = slots + s * 3 * ADJ_THREADS;
                 float x0 = in[tid], y0 = in[ADJ_THREADS + tid];
                 const float z0 = in[2 * ADJ_THREADS + tid];
-                if (s > 0 && (a.segs[win.x + s - 1].flags & BP_SPOIL)) x0 = y0 = 0.0f;
+                if (s > 0 && (wrec[s - 1].flags & BP_SPOIL)) x0 = y0 = 0.0f;
                 SegGrad sg;
 #pragma unroll
                 for (int k = 0; k < N_SG; ++k) sg.v[k] = 0.0f;
                 if (f & BP_RF) {
-                    if (cached_rf != s + 1 || !(a.segs[win.x + s + 1].flags & BP_SAME_RFDT)) {
+                    // the factors of the segment after this one (swept just before) when they are the same
+                    if (cached_rf != s + 1 || !(wrec[s + 1].flags & BP_SAME_RFDT)) {
                         e1h = expm1f(-0.5f * q.dt * p.r1);
                         e2h = expm1f(-0.5f * q.dt * p.r2);
                     }
+                    if (cached_rf != s + 1 || !(wrec[s + 1].flags & BP_SAME_OFF)) wz = rf_wz(q, p);
                     cached_rf = s;
-                    rf_reverse(q, p, e1h, e2h, x0, y0, z0, lx, ly, lz, g, sg);
+                    rf_reverse(q, p, e1h, e2h, wz, x0, y0, z0, lx, ly, lz, g, sg);
                 } else {
-                    if (cached_free != s + 1 || !(a.segs[win.x + s + 1].flags & BP_SAME_FREE))
-                        ff = free_factors(q, a.seg64[win.x + s], p);
+                    if (cached_free != s + 1 || !(wrec[s + 1].flags & BP_SAME_FREE))
+                        ff = free_factors(q, wk64[s], p);
                     cached_free = s;
                     free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
                 }
@@ -304,7 +316,8 @@ __global__ void bp_seg_reduce_kernel(const float* __restrict__ gseg, int n_cta, 
 
 template <int NCG>
 static size_t adj_smem() {
-    return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float);
+    return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) +
+           (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4));
 }
 
 template <int NCG>

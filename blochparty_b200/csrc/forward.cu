@@ -13,10 +13,11 @@
 //    through the window: the tile's state is loaded from HBM, propagated in registers, and stored back.
 //  * ADC samples: each warp stages the (mx, my) of its 32 spins for 16 samples in shared memory, then contracts
 //    them with the spins' coil sensitivities (an FMA chain over the 32 spins per lane: a small matrix product)
-//    and adds the results into the CTA's window accumulator in shared memory (shared-memory atomics: one
-//    accumulator per CTA, summed over all of its tiles and warps). At the window's end the CTA's partial is added
-//    to the float64 signal with one float64 atomic per (sample, coil, re/im): the cross-block sum is float64, and
-//    the CTA-level sum covers thousands of spins, so the number of atomics does not grow with the spin count.
+//    into its own slice of the window accumulator in shared memory, summed over all of the CTA's tiles. At the
+//    window's end the warps' slices are added in fixed order and the CTA's partial is added to the float64 signal
+//    with one float64 atomic per (sample, coil, re/im): the cross-block sum is float64 (float32 partials added in
+//    float64 are exact in practice, so the result does not depend on the CTAs' order), and the CTA-level sum
+//    covers thousands of spins, so the number of atomics does not grow with the spin count.
 //  * Readout runs (samples with one segment's factors): the samples come from a float32 recurrence, the state
 //    after the run from the float64 merged factors (see bloch_common.cuh), within blocks of BP_ADJ_WIN segments.
 //  * Demodulation by exp(-i adc_phase) is the same for every spin and is applied after the sum, in float64
@@ -30,7 +31,7 @@
 
 #define BP_THREADS 128
 #define BP_WARPS (BP_THREADS / 32)
-#define BP_ACC_SAMPLES 64  // accumulator capacity in samples at 8 coils (one coil group)
+#define BP_ACC_SAMPLES 64  // accumulator capacity in samples x coil groups above 8 coils
 #define BP_STAGE 16        // samples staged per warp before they are contracted
 #define BP_MB_STRIDE 33    // float2 per staged sample row (32 spins + 1: conflict-free column reads)
 
@@ -51,13 +52,13 @@ struct FwdArgs {
 
 template <int NCG>
 __host__ __device__ constexpr int samp_max() {
-    return BP_ACC_SAMPLES / NCG;
+    return NCG == 1 ? 32 : BP_ACC_SAMPLES / NCG;  // up to 8 coils: 32 samples (five CTAs per SM fit)
 }
 
 // The warp's staged samples (mb: [BP_STAGE][BP_MB_STRIDE] (mx, my) of its 32 spins) contracted with the coil
-// sensitivities of those spins (st: [32][16 NCG], coil c real at 2c, imaginary at 2c + 1) and added to the CTA's
-// accumulator rows acc[row0 + s] (shared-memory atomics). Lane l computes sample l & 15, coils 4 (l >> 4) .. + 3
-// of every coil group: a chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles).
+// sensitivities of those spins (st: [32][16 NCG], coil c real at 2c, imaginary at 2c + 1) and added to the warp's
+// accumulator rows acc[row0 + s]. Lane l computes sample l & 15, coils 4 (l >> 4) .. + 3 of every coil group: a
+// chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles).
 template <int NCG>
 __device__ __forceinline__ void warp_contract(const float2* mb, const float* st, int nslot, float* acc, int row0,
                                               int lane) {
@@ -82,19 +83,18 @@ __device__ __forceinline__ void warp_contract(const float2* mb, const float* st,
             re[3] = fmaf(m.x, b.z, fmaf(-m.y, b.w, re[3]));
             im[3] = fmaf(m.x, b.w, fmaf(m.y, b.z, im[3]));
         }
-        float* dst = acc + (row0 + smp) * VG + 16 * g + 8 * half;  // the CTA's accumulator: every warp adds here
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            atomicAdd(dst + 2 * c, re[c]);
-            atomicAdd(dst + 2 * c + 1, im[c]);
-        }
+        float4* dst = reinterpret_cast<float4*>(acc + (row0 + smp) * VG + 16 * g + 8 * half);
+        float4 d0 = dst[0], d1 = dst[1];
+        d0.x += re[0], d0.y += im[0], d0.z += re[1], d0.w += im[1];
+        d1.x += re[2], d1.y += im[2], d1.z += re[3], d1.w += im[3];
+        dst[0] = d0, dst[1] = d1;
     }
 }
 
 template <int NCG>
 __host__ __device__ constexpr size_t fwd_smem_bytes_t() {
     return 2 * BP_SEG_MAX * sizeof(SegRec)                                   // segment blocks
-           + (size_t)samp_max<NCG>() * 16 * NCG * sizeof(float)              // the window's accumulator
+           + (size_t)BP_WARPS * samp_max<NCG>() * 16 * NCG * sizeof(float)   // window accumulators, one per warp
            + (size_t)BP_WARPS * BP_STAGE * BP_MB_STRIDE * sizeof(float2)     // staged samples
            + (size_t)BP_WARPS * 32 * 16 * NCG * sizeof(float)                // coil sensitivities of the tile
            + 2 * sizeof(uint64_t);
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
     constexpr int VG = 16 * NCG;  // accumulator values per sample (coil groups of 8, padded)
     SegRec* segbuf = reinterpret_cast<SegRec*>(smem_raw);                                   // [2][BP_SEG_MAX]
     float* acc = reinterpret_cast<float*>(segbuf + 2 * BP_SEG_MAX);                         // [W][samp][VG]
-    float2* mball = reinterpret_cast<float2*>(acc + samp_max<NCG>() * VG);                  // [W][16][33]
+    float2* mball = reinterpret_cast<float2*>(acc + BP_WARPS * samp_max<NCG>() * VG);       // [W][16][33]
     float* stall = reinterpret_cast<float*>(mball + BP_WARPS * BP_STAGE * BP_MB_STRIDE);    // [W][32][VG]
     uint64_t* bars = reinterpret_cast<uint64_t*>(stall + BP_WARPS * 32 * VG);
 
@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
     const int n = a.n;
     const int n_tiles = (n + BP_THREADS - 1) / BP_THREADS;
     const int nv = 2 * a.n_coils;
+    float* my_acc = acc + warp * samp_max<NCG>() * VG;
     float2* mb = mball + warp * BP_STAGE * BP_MB_STRIDE;
     float* st = stall + warp * 32 * VG;
 
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
         mbar_init(&bars[1], 1);
         fence_mbar_init();
     }
-    for (int i = tid; i < samp_max<NCG>() * VG; i += BP_THREADS) acc[i] = 0.0f;
+    for (int i = tid; i < BP_WARPS * samp_max<NCG>() * VG; i += BP_THREADS) acc[i] = 0.0f;
     __syncthreads();
 
     auto issue = [&](int w, int buf) {
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                 mb[slot * BP_MB_STRIDE + lane] = make_float2(x, y);
                 if (++slot == BP_STAGE) {
                     __syncwarp();
-                    warp_contract<NCG>(mb, st, BP_STAGE, acc, row0, lane);
+                    warp_contract<NCG>(mb, st, BP_STAGE, my_acc, row0, lane);
                     __syncwarp();
                     row0 += BP_STAGE;
                     slot = 0;
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
             }
             if (slot > 0) {
                 __syncwarp();
-                warp_contract<NCG>(mb, st, slot, acc, row0, lane);
+                warp_contract<NCG>(mb, st, slot, my_acc, row0, lane);
                 __syncwarp();
             }
             if (active) {
@@ -265,12 +266,17 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
         }
         __syncthreads();
         if (readout) {
-            // the CTA's sums, one float64 atomic per value; slots are cleared as read
+            // the warps' slices in fixed order (the CTA's sum does not depend on timing), then one float64 atomic
+            // per value; slots are cleared as read
             for (int k = tid; k < win.w * nv; k += BP_THREADS) {
                 const int r = k / nv, v = k % nv;
                 const int slot = r * VG + v;
-                const float t = acc[slot];
-                acc[slot] = 0.0f;
+                float t = 0.0f;
+#pragma unroll
+                for (int ww = 0; ww < BP_WARPS; ++ww) {
+                    t += acc[ww * samp_max<NCG>() * VG + slot];
+                    acc[ww * samp_max<NCG>() * VG + slot] = 0.0f;
+                }
                 atomicAdd(a.raw + (size_t)(win.z + r) * nv + v, (double)t);
             }
             __syncthreads();
