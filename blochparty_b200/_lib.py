@@ -16,7 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libblochparty_b200.so"
 
 BP_OK, BP_E_ARG, BP_E_ALIGN, BP_E_LAUNCH, BP_E_SIZE = 0, 1, 2, 3, 4
 BP_MAX_COILS = 32
-BP_SEG_MAX = 192
+BP_SEG_MAX = 160
 BP_ADJ_WIN = 32
 BP_MMA_MAX_COILS = 8
 BP_MLP_PARAMS = 8836

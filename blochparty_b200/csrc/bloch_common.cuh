@@ -64,6 +64,17 @@ __device__ __forceinline__ void two_sum(float& hi, float& lo, float d) {
     hi = t;
 }
 
+// hi + lo += d for an increment that does not outgrow hi (an RF step's increment next to the state it turns):
+// Dekker's fast two-sum, exact when the exponent of hi is at least that of d + lo (and whenever hi is 0), in four
+// operations instead of seven. Where a component crosses zero the condition can fail for a step, and that step's
+// rounding error (an ulp of the small increment) is not kept.
+__device__ __forceinline__ void quick_two_sum(float& hi, float& lo, float d) {
+    d = __fadd_rn(d, lo);
+    const float t = __fadd_rn(hi, d);
+    lo = __fsub_rn(d, __fsub_rn(t, hi));
+    hi = t;
+}
+
 // Rodrigues coefficients of a rotation by |w|, from p2 = |w|^2: s1 = sin(phi)/phi, s2 = (1 - cos phi)/phi^2.
 // Below phi = 1 both are their Taylor series in p2 (sum_k (-1)^k p2^k / (2k+1)! and / (2k+2)!): truncated after
 // p2^3 below phi = 1/4 (the usual RF step; first dropped terms p2^4 / 9! < 4.3e-11) and after p2^5 below phi = 1
@@ -122,15 +133,15 @@ __device__ __forceinline__ RfRelax rf_relax(float dt, const Spin& p) {
     return r;
 }
 
-// An RF segment: relax dt/2 (m1 = E m + c, E = diag(a2, a2, a1), c = (0, 0, -pd e1h)), rotate about w (n = R m1),
-// relax dt/2 (E n + c), composed into one increment of m: (E E - I) m + E (R - I) m1 + (E + I) c, with
-// (R - I) m1 = s1 (w x m1) + s2 w x (w x m1). The increment is small next to m and computed from m directly,
-// so one two-sum per component (instead of one per sub-step) keeps the float32 state compensated.
 // The z component of an RF segment's rotation vector: -2 pi (k.r + dt dB0 + beta) (its off-resonance in cycles).
 __device__ __forceinline__ float rf_wz(const SegRec& q, const Spin& p) {
     return -BP_TWO_PI_F * fmaf(q.kx, p.px, fmaf(q.ky, p.py, fmaf(q.kz, p.pz, fmaf(q.dt, p.db0, q.beta))));
 }
 
+// An RF segment: relax dt/2 (m1 = E m + c, E = diag(a2, a2, a1), c = (0, 0, -pd e1h)), rotate about w (n = R m1),
+// relax dt/2 (E n + c), composed into one increment of m: (E E - I) m + E (R - I) m1 + (E + I) c, with
+// (R - I) m1 = s1 (w x m1) + s2 w x (w x m1). The increment is small next to m and computed from m directly,
+// so one (fast) two-sum per component (instead of one per sub-step) keeps the float32 state compensated.
 __device__ __forceinline__ void rf_step_wz(const SegRec& q, const Spin& p, const RfRelax& r, float wz, float& mx,
                                            float& my, float& mz, float& lx, float& ly, float& lz) {
     const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
@@ -141,9 +152,9 @@ __device__ __forceinline__ void rf_step_wz(const SegRec& q, const Spin& p, const
     const float cx = wy * m1z - wz * m1y, cy = wz * m1x - wx * m1z, cz = wx * m1y - wy * m1x;
     const float dx = wy * cz - wz * cy, dy = wz * cx - wx * cz, dz = wx * cy - wy * cx;
     const float qx = fmaf(s1, cx, s2 * dx), qy = fmaf(s1, cy, s2 * dy), qz = fmaf(s1, cz, s2 * dz);
-    two_sum(mx, lx, fmaf(r.d2, mx, r.a2 * qx));
-    two_sum(my, ly, fmaf(r.d2, my, r.a2 * qy));
-    two_sum(mz, lz, fmaf(r.d1, mz, fmaf(r.a1, qz, r.cz2)));
+    quick_two_sum(mx, lx, fmaf(r.d2, mx, r.a2 * qx));
+    quick_two_sum(my, ly, fmaf(r.d2, my, r.a2 * qy));
+    quick_two_sum(mz, lz, fmaf(r.d1, mz, fmaf(r.a1, qz, r.cz2)));
 }
 
 __device__ __forceinline__ void rf_step(const SegRec& q, const Spin& p, const RfRelax& r, float& mx, float& my,

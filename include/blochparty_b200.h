@@ -27,7 +27,7 @@ extern "C" {
 #define BP_E_SIZE 4     /* a size above a documented maximum */
 
 #define BP_MAX_COILS 32 /* receive coils of the float32 readout */
-#define BP_SEG_MAX 192  /* segments per window (one TMA-staged block; five CTAs per SM fit in shared memory) */
+#define BP_SEG_MAX 160  /* segments per window (one TMA-staged block; five CTAs per SM fit in shared memory) */
 #define BP_ADJ_WIN 32   /* segments per adjoint window (recomputed into shared memory) */
 
 /* Window planner (host code, no GPU): cuts `n_segments` segments with per-segment `flags` (bit 1 RF, 2 ADC,
