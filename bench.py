@@ -277,8 +277,9 @@ def main():
     ap.add_argument("--workload", default="gre3d_64", choices=("gre3d_64", "gre3d_128_4echo"))
     ap.add_argument("--max-segments", type=int, default=0,
                     help="time the workload's first whole TRs only, up to this many segments (0: all)")
-    ap.add_argument("--pulses", default="step", choices=("step", "reuse"),
-                    help="reuse: recurring pulses through their exact per-spin maps (composed inside every step)")
+    ap.add_argument("--pulses", default="step", choices=("step", "reuse", "surrogate"),
+                    help="reuse: recurring pulses through their exact per-spin maps (composed inside every step); "
+                         "surrogate: the slab pulse through a network trained before the timed region")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -316,12 +317,27 @@ def main():
     inp = bpb.api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad,
                          seq.adc_phase, None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
     pk = engine.pack(inp, dev)
-    mma = reuse = None
+    mma = reuse = sur = None
+    sur_info = {}
     if args.pulses == "reuse":
         from blochparty_b200.pulses import Reuse
 
         reuse = Reuse(inp, pk)
         windows, wdev = reuse.plan[0], reuse.plan[1]
+    elif args.pulses == "surrogate":
+        # one network for the workload's slab pulse (trained before the timed region; speed does not depend on it)
+        from blochparty_b200 import surrogate
+
+        is_rf = np.asarray(seq.is_rf, dtype=bool)
+        a = int(np.flatnonzero(is_rf)[0])
+        k = int(np.flatnonzero(~is_rf[a:])[0])
+        sg = surrogate.RFSurrogate(seq.rf[a:a + k].numpy(), float(seq.dt[a]), float(seq.grad[a, 2]),
+                                   float(seq.meta["slab_thickness"]), device=dev)
+        t0 = time.perf_counter()
+        sg.train()
+        sur_info = {"train_s": time.perf_counter() - t0, "network_error_max_rms": sg.validate()}
+        sur = surrogate.SurrogateRun(inp, pk, [sg])
+        windows, wdev = sur.plan[0], sur.plan[1]
     elif args.readout == "bf16x3":
         from blochparty_b200.readout_mma import MmaBuffers, run_forward_mma
 
@@ -350,6 +366,8 @@ def main():
         if reuse is not None:
             reuse.make_maps(pk)
             reuse.run(pk, state, raw, status, events=None if i is None else fwd_events[i])
+        elif sur is not None:
+            sur.run(pk, state, raw, status, events=None if i is None else fwd_events[i])
         elif mma is not None:
             run_forward_mma(pk, mma, state, raw, status)
         else:
@@ -385,7 +403,8 @@ def main():
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     ms = float(ms)
     kernel_ms = statistics.mean(kstart[i].elapsed_time(kend[i]) for i in range(args.steps))
-    if reuse is not None:  # the forward kernel's own time (the maps and their applications excluded)
+    replaced = reuse or sur
+    if replaced is not None:  # the forward kernel's own time (the maps or networks and their launches excluded)
         kernel_ms = statistics.mean(sum(a.elapsed_time(b) for a, b in ev) for ev in fwd_events)
     value = world * n * S / (ms * 1e-3)
 
@@ -394,7 +413,8 @@ def main():
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        bpb.simulate(ph, seq, coils, readout=args.readout, pulses=args.pulses)
+        bpb.simulate(ph, seq, coils, readout=args.readout, pulses=args.pulses,
+                     **({"surrogate": sur.surrogates} if sur is not None else {}))
         e2e_ms.append((time.perf_counter() - t) * 1e3)
     e2e = world * n * S / (statistics.median(e2e_ms) * 1e-3) if e2e_ms else None
     h2d = sum(t.numel() * t.element_size() for t in (pk.spins, pk.sens, pk.segs, pk.seg64, pk.psi, wdev, state0))
@@ -406,11 +426,21 @@ def main():
         return
     peak = ffma_peak_tflops(dev)
     stepped = pk.flags
-    if reuse is not None:  # the flops of the segments the forward kernel stepped
+    if replaced is not None:  # the flops of the segments the forward kernel stepped
         keep = np.ones(pk.flags.shape[0], dtype=bool)
-        for s0, k in reuse.spans:
+        for s0, k in replaced.spans:
             keep[s0:s0 + k] = False
         stepped = pk.flags[keep]
+    if sur is not None:  # the networks' signal against plain stepping on the same inputs
+        sig_sur = step().clone()
+        state.copy_(state0)
+        raw.zero_()
+        plain = engine.plan_windows(pk.flags, _lib.lib().bp_forward_samp_max(pk.n_coils))
+        engine.run_forward(pk, state, torch.from_numpy(plain).to(dev), 0, plain.shape[0], raw, status)
+        sig_plain = engine.finish_signal(pk, raw)
+        torch.cuda.synchronize()
+        sur_info["signal_rel_l2_vs_stepping"] = float(torch.linalg.vector_norm(sig_sur - sig_plain)
+                                                      / torch.linalg.vector_norm(sig_plain))
     flops = n * flops_per_spin(stepped, pk.n_coils)
     achieved = flops / (kernel_ms * 1e-3) / 1e12
     line = {
@@ -418,7 +448,8 @@ def main():
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": workload, "spins_per_gpu": n, "segments": S, "adc_samples": pk.n_adc,
-                   "coils": pk.n_coils, "readout": args.readout, "pulses": args.pulses,
+                   "coils": pk.n_coils, "readout": args.readout, "pulses": args.pulses, **({"surrogate": sur_info}
+                                                                                               if sur_info else {}),
                    "ctas": (_lib.lib().bp_forward_mma_grid(n) if mma is not None
                             else _lib.lib().bp_forward_grid(n, pk.n_coils)), "l2": "inputs larger than L2 (state, spins, coils, "
                    "segments ~220 MB per GPU) and a 256 MB L2 flush between timed steps"},
@@ -430,8 +461,9 @@ def main():
                      "flops_per_launch": flops},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": statistics.median(e2e_ms) if e2e_ms else None},
-        "gpu_launches": (2 * args.steps if reuse is None else
-                         args.steps * (len(reuse.pulses) + len(reuse.spans) + len(fwd_events[0]) + 1)),
+        "gpu_launches": (2 * args.steps if replaced is None else
+                         args.steps * ((len(reuse.pulses) if reuse is not None else 0) + len(replaced.spans)
+                                       + len(fwd_events[0]) + 1)),
         "clocks": clocks.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -31,8 +31,8 @@
 
 #define BP_THREADS 128
 #define BP_WARPS (BP_THREADS / 32)
-#define BP_ACC_SAMPLES 64  // accumulator capacity in samples x coil groups above 8 coils
-#define BP_STAGE 16        // samples staged per warp before they are contracted
+#define BP_ACC_SAMPLES 64  // accumulator capacity in samples at 8 coils (one coil group)
+#define BP_STAGE 8         // samples staged per warp before they are contracted
 #define BP_MB_STRIDE 33    // float2 per staged sample row (32 spins + 1: conflict-free column reads)
 
 struct FwdArgs {
@@ -52,42 +52,38 @@ struct FwdArgs {
 
 template <int NCG>
 __host__ __device__ constexpr int samp_max() {
-    return NCG == 1 ? 32 : BP_ACC_SAMPLES / NCG;  // up to 8 coils: 32 samples (five CTAs per SM fit)
+    return BP_ACC_SAMPLES / NCG;
 }
 
 // The warp's staged samples (mb: [BP_STAGE][BP_MB_STRIDE] (mx, my) of its 32 spins) contracted with the coil
 // sensitivities of those spins (st: [32][16 NCG], coil c real at 2c, imaginary at 2c + 1) and added to the warp's
-// accumulator rows acc[row0 + s]. Lane l computes sample l & 15, coils 4 (l >> 4) .. + 3 of every coil group: a
-// chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles).
+// accumulator rows acc[row0 + s]. Lane l computes sample l & 7, coils 2 (l >> 3) and 2 (l >> 3) + 1 of every coil
+// group: a chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles). Reads are
+// conflict-free: the 8 samples' rows start 33 float2 apart, and every lane of a sample reads the same spin's
+// sensitivities (a broadcast of 4 float4s).
 template <int NCG>
 __device__ __forceinline__ void warp_contract(const float2* mb, const float* st, int nslot, float* acc, int row0,
                                               int lane) {
     constexpr int VG = 16 * NCG;
-    const int smp = lane & 15, half = lane >> 4;
+    const int smp = lane & 7, quarter = lane >> 3;
     if (smp >= nslot) return;
     const float2* row = mb + smp * BP_MB_STRIDE;
 #pragma unroll
     for (int g = 0; g < NCG; ++g) {
-        float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
+        float r0 = 0.f, i0 = 0.f, r1 = 0.f, i1 = 0.f;
 #pragma unroll 8
         for (int j = 0; j < 32; ++j) {
             const float2 m = row[j];
-            const float4* sj = reinterpret_cast<const float4*>(st + j * VG + 16 * g + 8 * half);
-            const float4 a = sj[0], b = sj[1];  // (r0 i0 r1 i1), (r2 i2 r3 i3)
-            re[0] = fmaf(m.x, a.x, fmaf(-m.y, a.y, re[0]));
-            im[0] = fmaf(m.x, a.y, fmaf(m.y, a.x, im[0]));
-            re[1] = fmaf(m.x, a.z, fmaf(-m.y, a.w, re[1]));
-            im[1] = fmaf(m.x, a.w, fmaf(m.y, a.z, im[1]));
-            re[2] = fmaf(m.x, b.x, fmaf(-m.y, b.y, re[2]));
-            im[2] = fmaf(m.x, b.y, fmaf(m.y, b.x, im[2]));
-            re[3] = fmaf(m.x, b.z, fmaf(-m.y, b.w, re[3]));
-            im[3] = fmaf(m.x, b.w, fmaf(m.y, b.z, im[3]));
+            const float4 a = *reinterpret_cast<const float4*>(st + j * VG + 16 * g + 4 * quarter);  // (r0 i0 r1 i1)
+            r0 = fmaf(m.x, a.x, fmaf(-m.y, a.y, r0));
+            i0 = fmaf(m.x, a.y, fmaf(m.y, a.x, i0));
+            r1 = fmaf(m.x, a.z, fmaf(-m.y, a.w, r1));
+            i1 = fmaf(m.x, a.w, fmaf(m.y, a.z, i1));
         }
-        float4* dst = reinterpret_cast<float4*>(acc + (row0 + smp) * VG + 16 * g + 8 * half);
-        float4 d0 = dst[0], d1 = dst[1];
-        d0.x += re[0], d0.y += im[0], d0.z += re[1], d0.w += im[1];
-        d1.x += re[2], d1.y += im[2], d1.z += re[3], d1.w += im[3];
-        dst[0] = d0, dst[1] = d1;
+        float4* dst = reinterpret_cast<float4*>(acc + (row0 + smp) * VG + 16 * g + 4 * quarter);
+        float4 d = *dst;
+        d.x += r0, d.y += i0, d.z += r1, d.w += i1;
+        *dst = d;
     }
 }
 

@@ -177,7 +177,7 @@ def gre(shape, fov, *, flip_deg=15.0, tr=10e-3, te=5e-3, n_dummy=0, dwell=10e-6,
         b.delay(t_spoil, grad=((spoil_x - k_end_x) / t_spoil, -ky / t_spoil, -kz / t_spoil))
         b.delay(t_fill)
     return b.build(kspace_shape=tuple(shape), fov=fov, tr=tr, te=te, n_echoes=n_echoes, dwell=dwell,
-                   n_tr=n_tr, n_dummy=n_dummy)
+                   n_tr=n_tr, n_dummy=n_dummy, rf=rf, slab_thickness=slab_thickness)
 
 
 def tse_2d(n, fov, *, slices=(0.0,), slice_thickness=5e-3, etl=16, esp=12e-3, tr=3.0, dwell=10e-6,

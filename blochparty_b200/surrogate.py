@@ -291,33 +291,48 @@ def forward_with_surrogate(inp, device, options):
 INFERENCE = ("mma", "fp32")
 
 
+class SurrogateRun:
+    """The occurrences of one packed case that ``surrogates`` stand in for, with the window plan around them."""
+
+    def __init__(self, inp, pk, surrogates, inference: str = "mma"):
+        if inference not in INFERENCE:
+            raise ValueError(f"surrogate_inference must be one of {INFERENCE}, not {inference!r}")
+        self.surrogates, self.inference = surrogates, inference
+        self.occ = find_occurrences(surrogates, inp)
+        self.spans = [(s, k) for s, k, *_ in self.occ]
+        self.plan = engine.plan_replacing(pk, self.spans)
+
+    def run(self, pk, state, raw, status, counts=None, events=None):
+        """The forward with every occurrence through its network; counts (None or int32 [2]) += spins through the
+        networks, through the fallback."""
+        lib, st = _lib.lib(), _lib.stream_ptr()
+
+        def apply(i):
+            s, k, isg, phi0, b0 = self.occ[i]
+            sg = self.surrogates[isg]
+            if self.inference == "mma":
+                code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(sg.wtiles()),
+                                                  ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0,
+                                                  *sg.domain, ptr(counts), ptr(status), 0, st)
+            else:
+                code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s, k,
+                                              sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0, *sg.domain, ptr(counts), st)
+            _lib.check(code, "bp_surrogate_pulse")
+
+        engine.forward_replacing(pk, state, self.spans, apply, raw, status, plan=self.plan, events=events)
+
+
 def run_with_surrogates(inp, device, surrogates, inference: str = "mma"):
     """The forward with every matched pulse occurrence through its surrogate; returns (signal, m, counts).
     ``inference``: "mma" (layers 2 and 3 on the tensor cores, ``bp_surrogate_pulse_mma``) or "fp32" (the whole
     network on the CUDA cores, ``bp_surrogate_pulse``)."""
-    if inference not in INFERENCE:
-        raise ValueError(f"surrogate_inference must be one of {INFERENCE}, not {inference!r}")
     pk = engine.pack(inp, device)
-    occ = find_occurrences(surrogates, inp)
+    plan = SurrogateRun(inp, pk, surrogates, inference)
     state = engine.initial_state(inp.pd, inp.m_init, device)
     raw = torch.zeros(max(pk.n_adc, 1), 2 * pk.n_coils, dtype=F64, device=device)
     status = torch.zeros(1, dtype=torch.int32, device=device)
     counts = torch.zeros(2, dtype=torch.int32, device=device)
-    lib, st = _lib.lib(), _lib.stream_ptr()
-
-    def apply(i):
-        s, k, isg, phi0, b0 = occ[i]
-        sg = surrogates[isg]
-        if inference == "mma":
-            code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(sg.wtiles()),
-                                              ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0,
-                                              *sg.domain, ptr(counts), ptr(status), 0, st)
-        else:
-            code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s, k, sg.T,
-                                          sg.gz, sg.thickness, sg.z0, phi0, b0, *sg.domain, ptr(counts), st)
-        _lib.check(code, "bp_surrogate_pulse")
-
-    engine.forward_replacing(pk, state, [(s, k) for s, k, *_ in occ], apply, raw if pk.n_adc else None, status)
+    plan.run(pk, state, raw if pk.n_adc else None, status, counts)
     sig = engine.finish_signal(pk, raw)
     torch.cuda.synchronize(device)
     _lib.check_status(status, "bp_forward")
