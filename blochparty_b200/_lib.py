@@ -14,6 +14,17 @@ import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "libblochparty_b200.so"
 
+BP_SPAN_MAP, BP_SPAN_NET_MMA, BP_SPAN_NET_F32 = 0, 1, 2
+
+
+class BpSpan(ctypes.Structure):
+    """``BpSpan`` of the C ABI: one replaced pulse occurrence for ``bp_forward_spans``."""
+
+    _fields_ = [("kind", ctypes.c_int32), ("seg0", ctypes.c_int32), ("k_steps", ctypes.c_int32),
+                ("phase", c_double), ("b0off", c_float), ("map", c_void_p), ("params", c_void_p),
+                ("wtiles", c_void_p), ("T", c_double), ("gz", c_double), ("thickness", c_double), ("z0", c_double),
+                ("dom_df", c_float), ("dom_b1", c_float), ("dom_z", c_float), ("counts", c_void_p)]
+
 BP_OK, BP_E_ARG, BP_E_ALIGN, BP_E_LAUNCH, BP_E_SIZE = 0, 1, 2, 3, 4
 BP_MAX_COILS = 32
 BP_SEG_MAX = 160
@@ -36,6 +47,7 @@ SIGNATURES = {
     "bp_forward_grid": (c_int, [c_int, c_int]),
     "bp_forward_mma_grid": (c_int, [c_int]),
     "bp_forward": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P]),
+    "bp_forward_spans": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, _P, c_int, _P, _P, _P, c_int, _P, _P]),
     "bp_signal_finish": (c_int, [_P, _P, c_int, c_int, _P, _P]),
     "bp_ffma_peak": (c_int, [_P, c_int, _P, _P]),
     "bp_mma_atiles_bytes": (c_int64, [c_int]),

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "bloch_common.cuh"
 #include "../../include/blochparty_b200.h"
@@ -511,7 +512,8 @@ extern "C" int bp_surrogate_pulse(const float* spins, float* state, int n, const
 // D = A_hi W2_hi^T + A_hi W2_lo^T + A_lo W2_hi^T (M = 128, N = 64, K = 64 in 4 steps, float32 in 64 tensor-memory
 // columns); each thread reads its row of D back (tcgen05.ld), adds the bias, applies GELU and stores the next A;
 // layer 3 likewise; layer 4 (64 -> 4) on the CUDA cores. Shared memory: W2 hi, W2 lo, W3 hi, W3 lo (8192 bytes
-// each, [0, 32768)), A hi and A lo (16384 each, [32768, 65536)), the small parameters, mbarriers. Layout of every
+// each, [0, 32768)), A hi and A lo (16384 each, [32768, 65536)), the fallback queue, mbarriers. W1, W4 and the
+// biases travel in the kernel's arguments (the constant bank). Layout of every
 // operand: core matrices of 8 rows x 16 bytes, K-adjacent ones 128 bytes apart, 8-row groups 1024 bytes apart; a
 // thread writes its row 16 bytes at a time, so the 8 lanes of each store phase fill one 128-byte line.
 #include "tcgen05.cuh"
@@ -519,9 +521,7 @@ extern "C" int bp_surrogate_pulse(const float* spins, float* state, int n, const
 #define SI_W_BYTES 8192
 #define SI_OFF_A 32768
 #define SI_A_BYTES 16384
-#define SI_OFF_P 65536
-#define SI_NP (MLP_H * MLP_IN + MLP_H + MLP_H + MLP_H + MLP_OUT * MLP_H + MLP_OUT)  // W1 b1 b2 b3 W4 b4
-#define SI_OFF_LIST (SI_OFF_P + ((SI_NP * 4 + 127) / 128) * 128)  // queued fallback spins (256 ints)
+#define SI_OFF_LIST 65536  // queued fallback spins (256 ints), after the A operand
 #define SI_LIST 256
 #define SI_OFF_BAR (SI_OFF_LIST + SI_LIST * 4)
 #define SI_SMEM (SI_OFF_BAR + 64)
@@ -529,26 +529,19 @@ extern "C" int bp_surrogate_pulse(const float* spins, float* state, int n, const
 #define SI_SBO 1024
 #define SI_COLS 64
 
-// the small parameters' offsets inside the shared copy
-#define Q_W1 0
-#define Q_B1 (Q_W1 + MLP_H * MLP_IN)
-#define Q_B2 (Q_B1 + MLP_H)
-#define Q_B3 (Q_B2 + MLP_H)
-#define Q_W4 (Q_B3 + MLP_H)
-#define Q_B4 (Q_W4 + MLP_OUT * MLP_H)
-
 // 64 activations of this thread's row -> A hi and A lo rows (16-byte stores)
 __device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned char* alo, int row, const float* v) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         uint32_t h[4], l[4];
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            uint16_t h0, l0, h1, l1;
-            split_bf16(v[8 * c + 2 * w], h0, l0);
-            split_bf16(v[8 * c + 2 * w + 1], h1, l1);
-            h[w] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-            l[w] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+        for (int w = 0; w < 4; ++w) {  // a pair: hi = bf16(v) (nearest), lo = bf16(v - hi), two values per conversion
+            const float v0 = v[8 * c + 2 * w], v1 = v[8 * c + 2 * w + 1];
+            const __nv_bfloat162 hp = __floats2bfloat162_rn(v0, v1);
+            const float2 hf = __bfloat1622float2(hp);
+            const __nv_bfloat162 lp = __floats2bfloat162_rn(v0 - hf.x, v1 - hf.y);
+            h[w] = *reinterpret_cast<const uint32_t*>(&hp);
+            l[w] = *reinterpret_cast<const uint32_t*>(&lp);
         }
         const uint32_t off = (uint32_t)((row >> 3) * SI_SBO + c * SI_LBO + (row & 7) * 16);
         *reinterpret_cast<uint4*>(ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
@@ -556,16 +549,22 @@ __device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned ch
     }
 }
 
+// The network's small parameters, passed by value in the kernel's arguments (2,576 bytes of the constant bank):
+// every thread reads the same weight at the same time, so the FMAs take them as constant operands, no loads.
+struct SmallNet {
+    float w1[MLP_H * MLP_IN], b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_OUT * MLP_H], b4[MLP_OUT];
+};
+
 struct PulseMmaArgs {
-    PulseArgs p;
+    PulseArgs p;            // (p.params unused: the small parameters are in net, W2 and W3 in wtiles)
     const uint8_t* wtiles;  // [4][8192]: W2 hi, W2 lo, W3 hi, W3 lo in the operand layout (bp_mlp_wtiles)
     int* status;
+    SmallNet net;
 };
 
 __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMmaArgs args) {
     extern __shared__ __align__(1024) unsigned char smb[];
     const PulseArgs& a = args.p;
-    float* Q = reinterpret_cast<float*>(smb + SI_OFF_P);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smb + SI_OFF_BAR);  // [0] weights, [1] MMA
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smb + SI_OFF_BAR + 2 * sizeof(uint64_t));
     int* queued = reinterpret_cast<int*>(smb + SI_OFF_BAR + 3 * sizeof(uint64_t));
@@ -576,15 +575,7 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
     const uint32_t sW = smem_u32(smb), sA = smem_u32(ahi);
     const uint32_t idesc = umma_idesc_bf16_f32(128, MLP_H);
 
-    // small parameters
-    for (int i = tid; i < MLP_H * MLP_IN; i += 128) Q[Q_W1 + i] = a.params[P_W1 + i];
-    for (int i = tid; i < MLP_H; i += 128) {
-        Q[Q_B1 + i] = a.params[P_B1 + i];
-        Q[Q_B2 + i] = a.params[P_B2 + i];
-        Q[Q_B3 + i] = a.params[P_B3 + i];
-    }
-    for (int i = tid; i < MLP_OUT * MLP_H; i += 128) Q[Q_W4 + i] = a.params[P_W4 + i];
-    if (tid < MLP_OUT) Q[Q_B4 + tid] = a.params[P_B4 + tid];
+    const SmallNet& net = args.net;
     if (tid == 0) {
         *queued = 0;
         mbar_init(&bars[0], 1);
@@ -620,9 +611,10 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
             const float x2 = fminf(fmaxf(zr / a.dom_z, -1.f), 1.f);
 #pragma unroll
             for (int k = 0; k < MLP_H; ++k)
-                v[k] = gelu_f(fmaf(Q[Q_W1 + 3 * k], x0, fmaf(Q[Q_W1 + 3 * k + 1], x1, fmaf(Q[Q_W1 + 3 * k + 2], x2, Q[Q_B1 + k]))));
+                v[k] = gelu_f(fmaf(net.w1[3 * k], x0, fmaf(net.w1[3 * k + 1], x1, fmaf(net.w1[3 * k + 2], x2, net.b1[k]))));
         }
-        for (int layer = 0; layer < 2 && !fail; ++layer) {
+#pragma unroll
+        for (int layer = 0; layer < 2; ++layer) {  // unrolled: the biases are indexed by constants
             store_row_bf16x2(ahi, alo, tid, v);
             fence_proxy_async_smem();
             tc_fence_before();
@@ -660,14 +652,13 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
                 break;
             }
             tc_fence_after();
-            const float* bias = Q + (layer == 0 ? Q_B2 : Q_B3);
 #pragma unroll
             for (int c0 = 0; c0 < MLP_H; c0 += 16) {
                 float d[16];
                 tmem_ld16(lane_addr + (uint32_t)c0, d);
                 tmem_ld_wait();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) v[c0 + i] = gelu_f(d[i] + bias[c0 + i]);
+                for (int i = 0; i < 16; ++i) v[c0 + i] = gelu_f(d[i] + (layer == 0 ? net.b2[c0 + i] : net.b3[c0 + i]));
             }
             tc_fence_before();
         }
@@ -678,9 +669,9 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
             float y[4];
 #pragma unroll
             for (int o = 0; o < MLP_OUT; ++o) {
-                float s = Q[Q_B4 + o];
+                float s = net.b4[o];
 #pragma unroll
-                for (int i = 0; i < MLP_H; ++i) s = fmaf(Q[Q_W4 + MLP_H * o + i], v[i], s);
+                for (int i = 0; i < MLP_H; ++i) s = fmaf(net.w4[MLP_H * o + i], v[i], s);
                 y[o] = s;
             }
             const float inv = rsqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
@@ -812,21 +803,27 @@ extern "C" int bp_surrogate_pulse_mma_grid(int n) {
     return code == BP_OK ? grid : -code;
 }
 
-extern "C" int bp_surrogate_pulse_mma(const float* spins, float* state, int n, const float* params,
+extern "C" int bp_surrogate_pulse_mma(const float* spins, float* state, int n, const float* params_host,
                                       const void* wtiles, const void* segs, int seg0, int k_steps, double T, double gz,
                                       double thickness, double z0, double phi0, float b0off, float dom_df,
                                       float dom_b1, float dom_z, int32_t* counts, int32_t* status, int max_ctas,
                                       void* stream) {
-    if (!spins || !state || !params || !wtiles || !segs || !status || n < 1 || seg0 < 0 || k_steps < 1 || T <= 0 ||
-        thickness <= 0 || !(dom_df > 0) || !(dom_b1 > 0) || !(dom_z > 0))
+    if (!spins || !state || !params_host || !wtiles || !segs || !status || n < 1 || seg0 < 0 || k_steps < 1 ||
+        T <= 0 || thickness <= 0 || !(dom_df > 0) || !(dom_b1 > 0) || !(dom_z > 0))
         return BP_E_ARG;
     if ((reinterpret_cast<uintptr_t>(wtiles) & 15) != 0) return BP_E_ALIGN;
     int grid = 0;
     const int code = pulse_mma_grid(n, max_ctas, &grid);
     if (code != BP_OK) return code;
-    PulseMmaArgs a{{spins, state, params, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0,
+    PulseMmaArgs a{{spins, state, nullptr, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0,
                     phi0, b0off, counts, dom_df, dom_b1, dom_z},
-                   static_cast<const uint8_t*>(wtiles), status};
+                   static_cast<const uint8_t*>(wtiles), status, {}};
+    std::memcpy(a.net.w1, params_host + P_W1, sizeof(a.net.w1));
+    std::memcpy(a.net.b1, params_host + P_B1, sizeof(a.net.b1));
+    std::memcpy(a.net.b2, params_host + P_B2, sizeof(a.net.b2));
+    std::memcpy(a.net.b3, params_host + P_B3, sizeof(a.net.b3));
+    std::memcpy(a.net.w4, params_host + P_W4, sizeof(a.net.w4));
+    std::memcpy(a.net.b4, params_host + P_B4, sizeof(a.net.b4));
     bp_surrogate_pulse_mma_kernel<<<grid, 128, SI_SMEM, static_cast<cudaStream_t>(stream)>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }

@@ -17,6 +17,7 @@ Device buffers (float32 unless stated; N spins, S segments, C coils, A ADC sampl
 
 from __future__ import annotations
 
+import ctypes
 import math
 from dataclasses import dataclass
 
@@ -207,6 +208,19 @@ def forward_replacing(pk: Packed, state: torch.Tensor, spans, apply, raw: torch.
         step(*ranges[i])
         apply(i)
     step(*ranges[-1])
+
+
+def forward_spans(pk: Packed, state: torch.Tensor, plan, spans, raw: torch.Tensor | None, status: torch.Tensor,
+                  max_ctas: int = 0) -> None:
+    """``forward_replacing`` in one native call: ``spans`` is a ctypes array of ``_lib.BpSpan`` (one per span of
+    ``plan``, from ``plan_replacing``), launched in order by ``bp_forward_spans``."""
+    _, wdev, ranges = plan
+    rng = np.ascontiguousarray(np.asarray(ranges, dtype=np.int32).reshape(-1, 2))
+    n_spans = rng.shape[0] - 1
+    code = _lib.lib().bp_forward_spans(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
+                                       ptr(wdev), rng.ctypes.data, n_spans, ctypes.addressof(spans) if n_spans else None,
+                                       ptr(state), ptr(raw), max_ctas, ptr(status), _lib.stream_ptr())
+    _lib.check(code, "bp_forward_spans")
 
 
 def forward(case, device, max_ctas: int = 0):

@@ -99,8 +99,21 @@ class Reuse:
             _lib.check(lib.bp_pulse_maps(ptr(pk.spins), pk.n, ptr(pk.segs), ptr(pk.seg64), a, k, ptr(self.maps[pid]),
                                          st), "bp_pulse_maps")
 
+    def descriptors(self):
+        """The occurrences as ``BpSpan`` descriptors for ``bp_forward_spans`` (map pointers into ``self.maps``)."""
+        arr = (_lib.BpSpan * max(1, len(self.occ)))()
+        for i, (s, k, pid, ph) in enumerate(self.occ):
+            arr[i] = _lib.BpSpan(kind=_lib.BP_SPAN_MAP, seg0=s, k_steps=k, phase=ph, map=ptr(self.maps[pid]))
+        return arr
+
     def run(self, pk, state, raw, status, max_ctas: int = 0, events=None):
-        """The forward with every occurrence through its pulse's map (``make_maps`` first)."""
+        """The forward with every occurrence through its pulse's map (``make_maps`` first): one native call, or the
+        launches one by one from Python when ``events`` collects the forward launches' CUDA events."""
+        if events is None:
+            if not hasattr(self, "_desc"):
+                self._desc = self.descriptors()
+            engine.forward_spans(pk, state, self.plan, self._desc, raw, status, max_ctas)
+            return
         lib, st = _lib.lib(), _lib.stream_ptr()
 
         def apply(i):

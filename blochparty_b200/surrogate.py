@@ -173,6 +173,15 @@ class RFSurrogate:
             self._wt_key = key
         return self._wt
 
+    def params_host(self) -> np.ndarray:
+        """A float32 host copy of the parameters (the tensor-core inference passes the small ones by value), made
+        again whenever the parameters changed since the last call."""
+        key = (self.log.steps, self.params.data_ptr())
+        if getattr(self, "_ph_key", None) != key:
+            self._ph = np.ascontiguousarray(self.params.detach().float().cpu().numpy())
+            self._ph_key = key
+        return self._ph
+
     def predict(self, samples: torch.Tensor) -> torch.Tensor:
         """The network's reduced rotations (n, 4) for samples (df, b1, z_rel)."""
         x = self.normalise(samples)
@@ -302,17 +311,40 @@ class SurrogateRun:
         self.spans = [(s, k) for s, k, *_ in self.occ]
         self.plan = engine.plan_replacing(pk, self.spans)
 
+    def descriptors(self, counts=None):
+        """The occurrences as ``BpSpan`` descriptors for ``bp_forward_spans`` (the networks' host parameters and
+        weight tiles are made here and kept by the surrogates)."""
+        arr = (_lib.BpSpan * max(1, len(self.occ)))()
+        for i, (s, k, isg, phi0, b0) in enumerate(self.occ):
+            sg = self.surrogates[isg]
+            mma = self.inference == "mma"
+            arr[i] = _lib.BpSpan(kind=_lib.BP_SPAN_NET_MMA if mma else _lib.BP_SPAN_NET_F32, seg0=s, k_steps=k,
+                                 phase=phi0, b0off=b0,
+                                 params=sg.params_host().ctypes.data if mma else ptr(sg.params),
+                                 wtiles=ptr(sg.wtiles()) if mma else None, T=sg.T, gz=sg.gz, thickness=sg.thickness,
+                                 z0=sg.z0, dom_df=sg.domain[0], dom_b1=sg.domain[1], dom_z=sg.domain[2],
+                                 counts=ptr(counts))
+        return arr
+
     def run(self, pk, state, raw, status, counts=None, events=None):
         """The forward with every occurrence through its network; counts (None or int32 [2]) += spins through the
-        networks, through the fallback."""
+        networks, through the fallback. One native call, or the launches one by one from Python when ``events``
+        collects the forward launches' CUDA events."""
+        if events is None:
+            key = None if counts is None else counts.data_ptr()
+            if getattr(self, "_desc_key", -1) != key:
+                self._desc, self._desc_key = self.descriptors(counts), key
+            engine.forward_spans(pk, state, self.plan, self._desc, raw, status)
+            return
         lib, st = _lib.lib(), _lib.stream_ptr()
 
         def apply(i):
             s, k, isg, phi0, b0 = self.occ[i]
             sg = self.surrogates[isg]
             if self.inference == "mma":
-                code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(sg.wtiles()),
-                                                  ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0,
+                code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, sg.params_host().ctypes.data,
+                                                  ptr(sg.wtiles()), ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness,
+                                                  sg.z0, phi0, b0,
                                                   *sg.domain, ptr(counts), ptr(status), 0, st)
             else:
                 code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s, k,

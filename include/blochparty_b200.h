@@ -176,16 +176,46 @@ int bp_surrogate_pulse(const float* spins, float* state, int n, const float* par
 
 /* The same occurrence with layers 2 and 3 of the network on the tensor cores (tcgen05, split bfloat16: hi x hi +
  * hi x lo + lo x hi, float32 accumulation in tensor memory; 128 spins per tile, persistent CTAs, at most
- * `max_ctas` when > 0). `wtiles` (16-byte aligned, bp_mlp_wtiles_bytes()) holds W2 and W3 split by bp_mlp_wtiles;
+ * `max_ctas` when > 0). `params_host` is the network in HOST memory (BP_MLP_PARAMS floats): W1, W4 and the biases
+ * travel by value in the launch's arguments; `wtiles` (device, 16-byte aligned, bp_mlp_wtiles_bytes()) holds W2
+ * and W3 split by bp_mlp_wtiles;
  * `status` |= 1 when a bounded wait on the weights' copy or an MMA ran out (the CTA then stops, its remaining
  * spins not written). Spins outside the domain are queued per CTA and stepped 128 at a time. bp_surrogate_pulse_mma_grid(n) returns the CTA count a launch for n spins uses (< 0: -error). */
 int bp_mlp_wtiles_bytes(void);
 int bp_mlp_wtiles(const float* params, void* tiles, void* stream);
 int bp_surrogate_pulse_mma_grid(int n);
-int bp_surrogate_pulse_mma(const float* spins, float* state, int n, const float* params, const void* wtiles,
+int bp_surrogate_pulse_mma(const float* spins, float* state, int n, const float* params_host, const void* wtiles,
                            const void* segs, int seg0, int k_steps, double T, double gz, double thickness, double z0,
                            double phi0, float b0off, float dom_df, float dom_b1, float dom_z, int32_t* counts,
                            int32_t* status, int max_ctas, void* stream);
+
+/* ---- a forward with pulse occurrences replaced (the launch loop of pulses="reuse" / "surrogate") ----
+ * bp_forward_spans steps windows ranges[0] = [w0, w1), then replaces span 0, steps ranges[1], replaces span 1, ...,
+ * and steps ranges[n_spans] last: 2 n_spans + 1 launches issued from host code in one call (ranges: host int32
+ * [n_spans + 1][2]; spans: host array). Every span replaces the segments [seg0, seg0 + k_steps) it names, which
+ * the windows leave out. A span is one of:
+ *   BP_SPAN_MAP      bp_pulse_apply(map, n, state, phase)                 (map: device [12][n] float64)
+ *   BP_SPAN_NET_MMA  bp_surrogate_pulse_mma(..., params (host), wtiles, ...)
+ *   BP_SPAN_NET_F32  bp_surrogate_pulse(..., params (device), ...)
+ * with phase = the RF phase (phi0 of a network), and the network fields as in those calls. Returns the first
+ * failing call's status (launches before it stay queued). */
+#define BP_SPAN_MAP 0
+#define BP_SPAN_NET_MMA 1
+#define BP_SPAN_NET_F32 2
+typedef struct {
+    int32_t kind, seg0, k_steps;
+    double phase;
+    float b0off;
+    const double* map;
+    const float* params;
+    const void* wtiles;
+    double T, gz, thickness, z0;
+    float dom_df, dom_b1, dom_z;
+    int32_t* counts;
+} BpSpan;
+int bp_forward_spans(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                     const double* seg64, const int32_t* windows, const int32_t* ranges, int n_spans,
+                     const BpSpan* spans, float* state, double* raw, int max_ctas, int32_t* status, void* stream);
 
 /* Measurement kernel (the roofline denominator): 4 CTAs x 256 threads per SM, each thread `iters` x 128
  * independent FFMAs; `*flops` receives the flop count of the launch, which the caller divides by the launch's

@@ -127,3 +127,24 @@ def test_no_gpu_fails_loudly():
     ph, seq = _tiny()
     with pytest.raises(RuntimeError, match="needs a CUDA device"):
         bpb.simulate(ph, seq)
+
+
+def test_span_descriptor_layout_matches_the_header(tmp_path):
+    """The ctypes ``BpSpan`` has the C struct's size and field offsets (compiled against the header with gcc)."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    fields = [f for f, _ in _lib.BpSpan._fields_]
+    src = tmp_path / "span.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "blochparty_b200.h"\nint main(void) {\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(BpSpan, {f}));\n' for f in fields)
+                   + '  printf("%zu\\n", sizeof(BpSpan));\n  return 0;\n}\n')
+    exe = tmp_path / "span"
+    inc = Path(__file__).resolve().parents[1] / "include"
+    subprocess.run(["gcc", f"-I{inc}", str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [getattr(_lib.BpSpan, f).offset for f in fields] + [ctypes.sizeof(_lib.BpSpan)]
+    assert got == want

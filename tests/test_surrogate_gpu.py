@@ -175,9 +175,10 @@ def test_surrogate_gain_on_the_tse_workload(tse_surrogates):
     p_fp32 = events(lambda: lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(pk.segs), s,
                                                    k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0, *sg.domain, None,
                                                    st))
-    p_mma = events(lambda: lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, ptr(sg.params), ptr(wt),
-                                                      ptr(pk.segs), s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0,
-                                                      *sg.domain, None, ptr(status), 0, st))
+    host = sg.params_host().ctypes.data
+    p_mma = events(lambda: lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), pk.n, host, ptr(wt), ptr(pk.segs),
+                                                      s, k, sg.T, sg.gz, sg.thickness, sg.z0, phi0, b0, *sg.domain,
+                                                      None, ptr(status), 0, st))
     assert int(status) == 0
     print(f"one {k}-step pulse over {pk.n:,} spins: plain {p_plain:.3f} ms, float32 network {p_fp32:.3f} ms, "
           f"tensor-core network {p_mma:.3f} ms ({p_plain / p_mma:.1f}x)")
@@ -228,8 +229,9 @@ def test_tensor_core_inference_matches_fp32_inference(n, max_ctas):
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         phi0 = 0.3  # (the fallback steps the sequence's own segments; both kernels see the same arguments)
         if mma:
-            code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), n, ptr(sg.params), ptr(sg.wtiles()),
-                                              ptr(pk.segs), 0, sg.K, sg.T, sg.gz, sg.thickness, sg.z0, phi0, 10.0,
+            code = lib.bp_surrogate_pulse_mma(ptr(pk.spins), ptr(state), n, sg.params_host().ctypes.data,
+                                              ptr(sg.wtiles()), ptr(pk.segs), 0, sg.K, sg.T, sg.gz, sg.thickness,
+                                              sg.z0, phi0, 10.0,
                                               *sg.domain, ptr(counts), ptr(status), max_ctas, st)
         else:
             code = lib.bp_surrogate_pulse(ptr(pk.spins), ptr(state), n, ptr(sg.params), ptr(pk.segs), 0, sg.K, sg.T,
