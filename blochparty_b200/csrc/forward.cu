@@ -222,15 +222,16 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                         // recurrence; the state after the run is this one advanced by the merged factors (exact
                         // phase in float64), as if stepped one by one.
                         const int block_end = min(nseg, (win.x + s) / BP_ADJ_WIN * BP_ADJ_WIN + BP_ADJ_WIN - win.x);
-                        int e = s + 1;
-                        float zr = mx + lx, zi = my + ly;
-                        if (readout) stage(zr, zi);
-                        while (e < block_end && (q0[e].flags & ~BP_SPOIL) == (BP_ADC | BP_SAME_FREE)) {
-                            if (readout) {
+                        int e = s + 1;  // the run's end: one scan of the flags, then a tight loop over its samples
+                        while (e < block_end && (q0[e].flags & ~BP_SPOIL) == (BP_ADC | BP_SAME_FREE))
+                            if (q0[e++].flags & BP_SPOIL) break;
+                        if (readout) {
+                            float zr = mx + lx, zi = my + ly;
+                            stage(zr, zi);
+                            for (int t = s + 1; t < e; ++t) {
                                 readout_advance(ff, zr, zi);
                                 stage(zr, zi);
                             }
-                            if (q0[e++].flags & BP_SPOIL) break;
                         }
                         if (e > s + 1) {
                             const FreeFactors fr = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
