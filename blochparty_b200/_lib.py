@@ -34,6 +34,8 @@ BP_MLP_PARAMS = 8836
 BP_MMA_SAMPLES = 64
 BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 BP_PULSE_MAP_BYTES = 96
+BP_SEG_DT, BP_SEG_WX, BP_SEG_WY, BP_SEG_KX, BP_SEG_KY, BP_SEG_KZ, BP_SEG_BETA = (1 << k for k in range(7))
+BP_SEG_ALL = 0x7F
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",
@@ -55,7 +57,7 @@ SIGNATURES = {
     "bp_forward_mma": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P]),
     "bp_adjoint_grid": (c_int, [c_int, c_int]),
     "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P,
-                           c_int, _P]),
+                           c_int, c_int, _P]),
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
     "bp_pulse_quats": (c_int, [_P, c_int, c_double, c_double, c_double, c_double, _P, c_int, _P, _P, _P]),
     "bp_mlp_grad_ctas": (c_int, [c_int]),

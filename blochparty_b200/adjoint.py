@@ -116,6 +116,11 @@ class _Simulate(torch.autograd.Function):
         gs = torch.zeros(8, n, dtype=F32, device=dev)
         gc = torch.zeros(2 * C, n, dtype=F32, device=dev) if (need[7] and h is not None) else None
         need_seg = any(need[i] for i in (8, 9, 10, 12))
+        # the segment gradients the chain rules below use: dt needs all of them (the record's every field scales
+        # with dt), the RF its two components, the gradient the moments, b0_offset its phase
+        seg_mask = (_lib.BP_SEG_ALL if need[8] else 0) | ((_lib.BP_SEG_WX | _lib.BP_SEG_WY) if need[9] else 0) | (
+            (_lib.BP_SEG_KX | _lib.BP_SEG_KY | _lib.BP_SEG_KZ) if need[10] else 0) | (
+            _lib.BP_SEG_BETA if need[12] else 0)
         grid = _lib.lib().bp_adjoint_grid(n, C)
         if grid < 1:
             raise RuntimeError("bp_adjoint_grid failed")
@@ -132,7 +137,7 @@ class _Simulate(torch.autograd.Function):
             engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, status, wstates=wstates, wstate_stride=1)
             code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
                                   aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
-                                  grid, stream)
+                                  seg_mask, grid, stream)
             _lib.check(code, "bp_adjoint")
             if need_seg:
                 _lib.check(lib.bp_seg_reduce(ptr(gseg), grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")

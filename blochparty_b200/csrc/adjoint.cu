@@ -47,6 +47,7 @@ struct AdjArgs {
     float* gs;            // [N_GS][n] += per-spin gradients
     float* gc;            // [2C][n] += coil gradients (rows 2c real, 2c+1 imaginary), or null
     float* gseg;          // [gridDim.x][seg_len][N_SG] per-CTA segment gradients, or null
+    int seg_mask;         // which of the N_SG segment gradients are reduced (bit k: component k)
 };
 
 // Rodrigues rotation factors with the derivative factors f1 = (c - s1)/phi^2, f2 = (s1 - 2 s2)/phi^2 (the
@@ -157,6 +158,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
     const int nv = 2 * a.n_coils;
     const bool need_seg = a.gseg != nullptr;
+    const bool rf_only = need_seg && (a.seg_mask & ~((1 << S_WX) | (1 << S_WY))) == 0;
     for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) segacc[i] = 0.0f;
     if (need_seg)
         for (int i = tid; i < a.seg_len * N_SG; i += ADJ_THREADS) a.gseg[(size_t)blockIdx.x * a.seg_len * N_SG + i] = 0.0f;
@@ -267,7 +269,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     cached_free = s;
                     free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
                 }
-                if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
+                if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0 and 16 hold them)
+                    const bool up = lane & 16;
+                    const float v0 = active ? sg.v[S_WX] : 0.0f, v1 = active ? sg.v[S_WY] : 0.0f;
+                    float t = (up ? v1 : v0) + __shfl_xor_sync(0xffffffffu, up ? v0 : v1, 16);
+#pragma unroll
+                    for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                    if ((lane & 15) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + (up ? S_WY : S_WX)] = t;
+                } else if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
                     float v[N_SG];
 #pragma unroll
                     for (int k = 0; k < N_SG; ++k) v[k] = active ? sg.v[k] : 0.0f;
@@ -361,14 +370,14 @@ static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
 extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs,
                           const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
                           const float* wstates, const float* h, float* lam, float* gs, float* gc, float* gseg,
-                          int grid, void* stream) {
+                          int seg_mask, int grid, void* stream) {
     if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg_len < 0 || grid < 1)
         return BP_E_ARG;
     if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs) return BP_E_ARG;
     if (wb == wa) return BP_OK;
     AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
               reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, lam, gs, gc,
-              gseg};
+              gseg, seg_mask};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch ((n_coils + 7) / 8) {
         case 1: return launch_adj<1>(a, grid, st);
@@ -436,7 +445,7 @@ extern "C" int bp_adjoint_noalloc(const float* spins, const float* sens, int n, 
         grid = (int)(BP_NOALLOC_SCRATCH_FLOATS / per_cta);
     // the kernel clears each CTA's rows of the scratch before accumulating into them
     code = bp_adjoint(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, lam, gs, gc,
-                      seg ? scratch : nullptr, grid, stream);
+                      seg ? scratch : nullptr, BP_SEG_ALL, grid, stream);
     if (code != BP_OK || !seg) return code;
     return bp_seg_reduce(scratch, grid, seg_len, seg0, seg, stream);
 }

@@ -100,10 +100,20 @@ int bp_adjoint_grid(int n, int n_coils);
  *   gc      [2C][n] += dL/d(coil c real, imaginary) at rows 2c, 2c+1, or NULL
  *   gseg    [grid][seg_len][8] scratch: per-CTA segment gradients (w.r.t. the record's dt, -2 pi dt rf_x,
  *           -2 pi dt rf_y, g dt (3), b0_offset dt), or NULL when no segment gradient is wanted
+ *   seg_mask  the segment gradients wanted (BP_SEG_* bits; the others in gseg are left 0 or unreduced): only
+ *           BP_SEG_WX | BP_SEG_WY (the RF alone) takes a cheaper reduction
  *   grid    bp_adjoint_grid(n, n_coils) */
+#define BP_SEG_DT 1
+#define BP_SEG_WX 2
+#define BP_SEG_WY 4
+#define BP_SEG_KX 8
+#define BP_SEG_KY 16
+#define BP_SEG_KZ 32
+#define BP_SEG_BETA 64
+#define BP_SEG_ALL 127
 int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
                const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates, const float* h,
-               float* lam, float* gs, float* gc, float* gseg, int grid, void* stream);
+               float* lam, float* gs, float* gc, float* gseg, int seg_mask, int grid, void* stream);
 
 /* seg[seg0 + s][k] += sum over the `n_cta` CTAs, in CTA order, of gseg[cta][s][k], in float64 (replaces
  * seg_reduce, engines/gpu/cuda/seg_reduce.cu:3-11). `seg` is [S][8] float64. */

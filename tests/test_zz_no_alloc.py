@@ -69,7 +69,7 @@ def test_noalloc_adjoint_matches_the_allocating_entry_point():
     gs_ref, gc_ref, seg_ref = _outputs(pk, S)
     _lib.check(lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
                               ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), ptr(lam_ref),
-                              ptr(gs_ref), ptr(gc_ref), ptr(gseg), grid, stream), "bp_adjoint")
+                              ptr(gs_ref), ptr(gc_ref), ptr(gseg), _lib.BP_SEG_ALL, grid, stream), "bp_adjoint")
     _lib.check(lib.bp_seg_reduce(ptr(gseg), grid, s1 - s0, s0, ptr(seg_ref), stream), "bp_seg_reduce")
     torch.cuda.synchronize()
     assert seg_ref.abs().max() > 0 and gs_ref.abs().max() > 0
