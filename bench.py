@@ -274,6 +274,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grad", action="store_true", help="forward + adjoint (gradients of T1 and the RF), one GPU")
+    ap.add_argument("--surrogate-pieces", type=int, default=1, help="networks per slab pulse (--pulses surrogate)")
     ap.add_argument("--workload", default="gre3d_64", choices=("gre3d_64", "gre3d_128_4echo"))
     ap.add_argument("--max-segments", type=int, default=0,
                     help="time the workload's first whole TRs only, up to this many segments (0: all)")
@@ -331,12 +332,14 @@ def main():
         is_rf = np.asarray(seq.is_rf, dtype=bool)
         a = int(np.flatnonzero(is_rf)[0])
         k = int(np.flatnonzero(~is_rf[a:])[0])
-        sg = surrogate.RFSurrogate(seq.rf[a:a + k].numpy(), float(seq.dt[a]), float(seq.grad[a, 2]),
-                                   float(seq.meta["slab_thickness"]), device=dev)
+        sgs = surrogate.pulse_pieces(seq.rf[a:a + k].numpy(), float(seq.dt[a]), float(seq.grad[a, 2]),
+                                     float(seq.meta["slab_thickness"]), pieces=args.surrogate_pieces, device=dev)
         t0 = time.perf_counter()
-        sg.train()
-        sur_info = {"train_s": time.perf_counter() - t0, "network_error_max_rms": sg.validate()}
-        sur = surrogate.SurrogateRun(inp, pk, [sg])
+        for sg in sgs:
+            sg.train()
+        sur_info = {"pieces": args.surrogate_pieces, "train_s": time.perf_counter() - t0,
+                    "network_error_max_rms": [sg.validate() for sg in sgs]}
+        sur = surrogate.SurrogateRun(inp, pk, sgs)
         windows, wdev = sur.plan[0], sur.plan[1]
     elif args.readout == "bf16x3":
         from blochparty_b200.readout_mma import MmaBuffers, run_forward_mma
