@@ -61,7 +61,7 @@ SIGNATURES = {
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
     "bp_pulse_quats": (c_int, [_P, c_int, c_double, c_double, c_double, c_double, _P, c_int, _P, _P, _P]),
     "bp_mlp_grad_ctas": (c_int, [c_int]),
-    "bp_mlp_grad": (c_int, [_P, _P, _P, c_int, _P, _P, _P]),
+    "bp_mlp_grad": (c_int, [_P, _P, _P, c_int, c_float, _P, _P, _P]),
     "bp_mlp_reduce": (c_int, [_P, _P, c_int, c_float, _P, _P, _P]),
     "bp_adam": (c_int, [_P, _P, _P, _P, c_float, c_float, c_float, c_float, c_int, _P]),
     "bp_mlp_eval": (c_int, [_P, _P, c_int, _P, _P]),

@@ -186,7 +186,8 @@ __device__ __forceinline__ void weight_grads(const float* dz, const float* act, 
 // gradient sum (not yet divided by the batch) to gpart[blockIdx.x][N_PARAMS] and its loss sum to lpart.
 __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __restrict__ params,
                                                               const float* __restrict__ x, const float* __restrict__ target,
-                                                              int n, float* __restrict__ gpart, float* __restrict__ lpart) {
+                                                              int n, float vw, float* __restrict__ gpart,
+                                                              float* __restrict__ lpart) {
     extern __shared__ __align__(16) float sm[];
     float* P = sm;                       // N_PARAMS (padded to a multiple of 4)
     float* z1 = P + ((N_PARAMS + 3) & ~3);
@@ -207,7 +208,8 @@ __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __res
         xin[0] = x[3 * (t0 + tid)], xin[1] = x[3 * (t0 + tid) + 1], xin[2] = x[3 * (t0 + tid) + 2];
         mlp_forward_row(P, xin, z1 + tid * TR_LD, z2 + tid * TR_LD, z3 + tid * TR_LD, y);
     }
-    // loss |y/|y| - target|^2 and dL/dy = (dL/dq - q (q . dL/dq)) / |y|
+    // loss (q0 - t0)^2 + vw |q_vec - t_vec|^2 with q = y/|y| (vw weights the vector part: relative precision for
+    // small rotations), and dL/dy = (dL/dq - q (q . dL/dq)) / |y|
     float dy[4] = {0.f, 0.f, 0.f, 0.f}, loss = 0.0f;
     if (live) {
         const float r = sqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
@@ -217,8 +219,9 @@ __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __res
         for (int j = 0; j < 4; ++j) {
             q[j] = y[j] * inv;
             const float e = q[j] - target[4 * (t0 + tid) + j];
-            loss = fmaf(e, e, loss);
-            gq[j] = 2.0f * e;
+            const float w = j == 0 ? 1.0f : vw;
+            loss = fmaf(w * e, e, loss);
+            gq[j] = 2.0f * w * e;
             qg = fmaf(q[j], gq[j], qg);
         }
 #pragma unroll
@@ -332,9 +335,9 @@ extern "C" int bp_mlp_grad_ctas(int n) { return n < 1 ? 0 : (n + TR_T - 1) / TR_
 
 static size_t mlp_grad_smem() { return (((size_t)N_PARAMS + 3) & ~(size_t)3) * 4 + 4 * (size_t)TR_ARR * 4; }
 
-extern "C" int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float* gpart,
-                           float* lpart, void* stream) {
-    if (!params || !x || !target || !gpart || !lpart || n < 1) return BP_E_ARG;
+extern "C" int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float vweight,
+                           float* gpart, float* lpart, void* stream) {
+    if (!params || !x || !target || !gpart || !lpart || n < 1 || !(vweight > 0)) return BP_E_ARG;
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -345,7 +348,7 @@ extern "C" int bp_mlp_grad(const float* params, const float* x, const float* tar
         configured[dev] = true;
     }
     bp_mlp_grad_kernel<<<bp_mlp_grad_ctas(n), TR_T, mlp_grad_smem(), static_cast<cudaStream_t>(stream)>>>(
-        params, x, target, n, gpart, lpart);
+        params, x, target, n, vweight, gpart, lpart);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 

@@ -70,6 +70,7 @@ class RFSurrogate:
         self.device = torch.device(device)
         self.params = _fan_in_init(seed).to(self.device)
         self.seed = seed
+        self.vweight = 1.0  # the loss weight of the quaternion's vector part (set by train)
         self.domain = tuple(float(d) for d in domain)
         if len(self.domain) != 3 or min(self.domain) <= 0:
             raise ValueError(f"domain must be three positive bounds (|df|, |b1 - 1|, |z_rel|), got {domain!r}")
@@ -111,8 +112,9 @@ class RFSurrogate:
         s, d = samples, self.domain
         return torch.stack([s[:, 0] / d[0], (s[:, 1] - 1) / d[1], s[:, 2] / d[2]], -1).contiguous()
 
-    def gradient(self, x: torch.Tensor, target: torch.Tensor):
-        """(mean loss, gradient) of the batch through the training kernels (x normalised)."""
+    def gradient(self, x: torch.Tensor, target: torch.Tensor, vweight: float = 1.0):
+        """(mean loss, gradient) of the batch through the training kernels (x normalised; ``vweight`` weights the
+        quaternion's vector part in the loss)."""
         lib, n = _lib.lib(), x.shape[0]
         ctas = lib.bp_mlp_grad_ctas(n)
         gpart = torch.empty(ctas, _lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
@@ -120,17 +122,23 @@ class RFSurrogate:
         grad = torch.empty(_lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
         loss = torch.empty(1, dtype=F32, device=self.device)
         st = _lib.stream_ptr()
-        _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(x), ptr(target), n, ptr(gpart), ptr(lpart), st), "bp_mlp_grad")
+        _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(x), ptr(target), n, vweight, ptr(gpart), ptr(lpart), st),
+                   "bp_mlp_grad")
         _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / n, ptr(grad), ptr(loss), st), "bp_mlp_reduce")
         return loss, grad
 
     def train(self, n_samples: int = 1 << 20, epochs: int = 400, batch: int = 16384, lr: float = 2e-3,
               lr_min: float = 3e-5, seed: int | None = None) -> TrainLog:
-        """Adam with a cosine learning-rate decay over ``epochs`` passes of ``n_samples`` plain-integrator targets."""
+        """Adam with a cosine learning-rate decay over ``epochs`` passes of ``n_samples`` plain-integrator targets.
+        The loss weights the quaternion's vector part by 1 / s^2, s its largest magnitude among the targets (clipped
+        to [1e-2, 1]): a small rotation (a 10-degree excitation) is then learned to a relative, not an absolute,
+        precision."""
         lib, st = _lib.lib(), _lib.stream_ptr()
         seed = self.seed if seed is None else seed
         s = self.samples(n_samples, seed + 1)
         x, y = self.normalise(s), self.targets(s)
+        vmax = float(torch.linalg.vector_norm(y[:, 1:], dim=1).max())
+        self.vweight = 1.0 / min(1.0, max(1e-2, vmax)) ** 2
         m = torch.zeros(_lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
         v = torch.zeros_like(m)
         ctas = lib.bp_mlp_grad_ctas(batch)
@@ -150,8 +158,8 @@ class RFSurrogate:
                 frac = (ep * steps_per_epoch + b) / max(total - 1, 1)
                 rate = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * frac))
                 xb, yb = xs[b * batch:(b + 1) * batch], ys[b * batch:(b + 1) * batch]
-                _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(xb), ptr(yb), batch, ptr(gpart), ptr(lpart), st),
-                           "bp_mlp_grad")
+                _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(xb), ptr(yb), batch, self.vweight, ptr(gpart),
+                                           ptr(lpart), st), "bp_mlp_grad")
                 _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / batch, ptr(grad), ptr(loss), st),
                            "bp_mlp_reduce")
                 _lib.check(lib.bp_adam(ptr(self.params), ptr(grad), ptr(m), ptr(v), rate, 0.9, 0.999, 1e-8, step, st),

@@ -161,11 +161,13 @@ int bp_pulse_apply(const double* maps, int n, float* state, double phase, void* 
 int bp_pulse_quats(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
                    const float* samples, int n, float* qred, float* qfull, void* stream);
 
-/* One training step's gradient: x [n][3] normalised inputs, target [n][4]; per-CTA partials gpart
- * [bp_mlp_grad_ctas(n)][BP_MLP_PARAMS] and loss sums lpart [bp_mlp_grad_ctas(n)] (scratch of the caller). */
+/* One training step's gradient: x [n][3] normalised inputs, target [n][4]; loss (q0 - t0)^2 + vweight |q_vec -
+ * t_vec|^2 per sample (vweight > 0 weights the vector part: relative precision for small rotations); per-CTA
+ * partials gpart [bp_mlp_grad_ctas(n)][BP_MLP_PARAMS] and loss sums lpart [bp_mlp_grad_ctas(n)] (scratch of the
+ * caller). */
 int bp_mlp_grad_ctas(int n);
-int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float* gpart, float* lpart,
-                void* stream);
+int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float vweight, float* gpart,
+                float* lpart, void* stream);
 /* grad = scale * (sum over CTAs in order of gpart), loss = scale * sum of lpart (scale = 1 / batch). */
 int bp_mlp_reduce(const float* gpart, const float* lpart, int n_cta, float scale, float* grad, float* loss,
                   void* stream);

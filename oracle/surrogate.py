@@ -107,9 +107,11 @@ def mlp(p, x):
     return y / torch.linalg.vector_norm(y, dim=-1, keepdim=True)
 
 
-def loss_and_grad(p, x, target):
-    """Mean over the batch of |q_pred - q_target|^2 and its gradient w.r.t. the flat parameters (float64)."""
+def loss_and_grad(p, x, target, vweight: float = 1.0):
+    """Mean over the batch of (q0 - t0)^2 + vweight |q_vec - t_vec|^2 and its gradient w.r.t. the flat parameters
+    (float64)."""
     p = p.detach().to(F64).clone().requires_grad_()
-    loss = ((mlp(p, x.to(F64)) - target.to(F64)) ** 2).sum(-1).mean()
+    w = torch.tensor([1.0, vweight, vweight, vweight], dtype=F64)
+    loss = (w * (mlp(p, x.to(F64)) - target.to(F64)) ** 2).sum(-1).mean()
     (g,) = torch.autograd.grad(loss, [p])
     return float(loss), g

@@ -42,13 +42,14 @@ def test_targets_match_the_float64_oracle():
     assert float((qf.double().cpu() - q_ref).abs().max()) < 1e-6
 
 
-def test_training_gradient_matches_float64_autograd():
+@pytest.mark.parametrize("vweight", [1.0, 130.0])
+def test_training_gradient_matches_float64_autograd(vweight):
     w, dt, gz, _ = _pulse()
     sg = surrogate.RFSurrogate(w, dt, gz, 5e-3, seed=11)
     s = sg.samples(300, seed=4)  # 300: the last CTA is partly empty
     x, t = sg.normalise(s), sg.targets(s)
-    loss, grad = sg.gradient(x, t)
-    ref_loss, ref_grad = S.loss_and_grad(sg.params.double().cpu(), x.double().cpu(), t.double().cpu())
+    loss, grad = sg.gradient(x, t, vweight)
+    ref_loss, ref_grad = S.loss_and_grad(sg.params.double().cpu(), x.double().cpu(), t.double().cpu(), vweight)
     assert abs(float(loss) - ref_loss) < 1e-5 * max(1.0, ref_loss)
     err = float((grad.double().cpu() - ref_grad).abs().max() / ref_grad.abs().max())
     assert err < 1e-4, err
