@@ -30,7 +30,8 @@ BP_MAX_COILS = 32
 BP_SEG_MAX = 160
 BP_ADJ_WIN = 32
 BP_MMA_MAX_COILS = 8
-BP_MLP_PARAMS = 8836
+BP_MLP_PARAMS = 9616
+BP_MLP_OUTPUTS = 16
 BP_MMA_SAMPLES = 64
 BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 BP_PULSE_MAP_BYTES = 96
@@ -59,9 +60,9 @@ SIGNATURES = {
     "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P,
                            c_int, c_int, _P]),
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
-    "bp_pulse_quats": (c_int, [_P, c_int, c_double, c_double, c_double, c_double, _P, c_int, _P, _P, _P]),
+    "bp_pulse_targets": (c_int, [_P, c_int, c_double, c_double, c_double, c_double, _P, c_int, _P, _P, _P]),
     "bp_mlp_grad_ctas": (c_int, [c_int]),
-    "bp_mlp_grad": (c_int, [_P, _P, _P, c_int, c_float, _P, _P, _P]),
+    "bp_mlp_grad": (c_int, [_P, _P, _P, c_int, c_float, c_float, _P, _P, _P]),
     "bp_mlp_reduce": (c_int, [_P, _P, c_int, c_float, _P, _P, _P]),
     "bp_adam": (c_int, [_P, _P, _P, _P, c_float, c_float, c_float, c_float, c_int, _P]),
     "bp_mlp_eval": (c_int, [_P, _P, c_int, _P, _P]),

@@ -3,14 +3,15 @@
 //
 // No counterpart in the reference (its nearest part is the exact per-spin map of a reused pulse,
 // engines/gpu/cuda/pulse.cu.in:3-32). Kernels here:
-//  * bp_pulse_quats: training targets from the plain integrator: per sample, the pulse's per-step rotations
+//  * bp_pulse_targets: training targets from the plain integrator: per sample, the pulse's per-step rotations
 //    w = -2 pi dt (b1 rf_x, b1 rf_y, G z + df) composed as unit quaternions in float64, reduced by the free
-//    precession (R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T) so that the target is smooth in z;
+//    precession (R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T) so that the target is smooth in z, with the
+//    first-order relaxation terms the whole-pulse splitting misses;
 //  * bp_mlp_grad: fused forward + backward of the network over a batch (per-CTA gradient partials), then
 //    bp_mlp_reduce (fixed-order sum over CTAs) and bp_adam (the optimiser step): training on the GPU;
 //  * bp_surrogate_pulse: one pulse occurrence applied to every spin's state: inside the training domain, the
-//    network's rotation wrapped by half-pulse relaxations (relax T/2, rotate, relax T/2); outside it, the
-//    plain sub-stepped integration of the pulse's segments (the fallback).
+//    network's rotation wrapped by half-pulse relaxations (relax T/2, rotate, relax T/2) with its first-order
+//    relaxation correction; outside it, the plain sub-stepped integration of the pulse's segments (the fallback).
 // Quaternions: (q0, q1, q2, q3) = (cos |w|/2, sin |w|/2 w/|w|), composition "q1 then q2" = q2 q1 (Hamilton
 // product); the Cayley-Klein pair of q is alpha = q0 - i q3, beta = -i (q1 + i q2).
 #include <cuda_runtime.h>
@@ -23,8 +24,8 @@
 
 #define MLP_H 64
 #define MLP_IN 3
-#define MLP_OUT 4
-// flat parameter layout: W1 (64 x 3), b1 (64), W2 (64 x 64), b2, W3 (64 x 64), b3, W4 (4 x 64), b4 (4)
+#define MLP_OUT 16  // the reduced quaternion (4), dA~ / T (9) and dC~ / T (3)
+// flat parameter layout: W1 (64 x 3), b1 (64), W2 (64 x 64), b2, W3 (64 x 64), b3, W4 (16 x 64), b4 (16)
 #define P_W1 0
 #define P_B1 (P_W1 + MLP_H * MLP_IN)
 #define P_W2 (P_B1 + MLP_H)
@@ -33,7 +34,7 @@
 #define P_B3 (P_W3 + MLP_H * MLP_H)
 #define P_W4 (P_B3 + MLP_H)
 #define P_B4 (P_W4 + MLP_OUT * MLP_H)
-#define N_PARAMS (P_B4 + MLP_OUT)  // 8836
+#define N_PARAMS (P_B4 + MLP_OUT)  // 9616
 
 static_assert(N_PARAMS == BP_MLP_PARAMS, "parameter count");
 
@@ -63,32 +64,88 @@ __device__ __forceinline__ dq4 dq_z(double angle) {
     return {c, 0.0, 0.0, s};
 }
 
-// Targets: samples [n][3] (df [Hz], b1, z_rel [slice widths]) -> q~ [n][4] float32 (and q [n][4] if not null).
-__global__ void bp_pulse_quats_kernel(const double2* __restrict__ rf, int k_steps, double dt, double gz,
-                                      double thickness, double z0, const float* __restrict__ samples, int n,
-                                      float* __restrict__ qred, float* __restrict__ qfull) {
+// 3 x 3 float64 matrices, row-major
+struct dm3 {
+    double m[9];
+};
+
+__device__ __forceinline__ dm3 dm_of_quat(const dq4& q) {
+    const double s = q.w, x = q.x, y = q.y, z = q.z;
+    return {{1 - 2 * (y * y + z * z), 2 * (x * y - s * z), 2 * (x * z + s * y),
+             2 * (x * y + s * z), 1 - 2 * (x * x + z * z), 2 * (y * z - s * x),
+             2 * (x * z - s * y), 2 * (y * z + s * x), 1 - 2 * (x * x + y * y)}};
+}
+
+__device__ __forceinline__ dm3 dm_mul(const dm3& a, const dm3& b) {
+    dm3 c;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            c.m[3 * r + k] = a.m[3 * r] * b.m[k] + a.m[3 * r + 1] * b.m[3 + k] + a.m[3 * r + 2] * b.m[6 + k];
+    return c;
+}
+
+// Targets: samples [n][3] (df [Hz], b1, z_rel [slice widths]) -> targets [n][16] float32 (and q [n][4] if not null):
+// the reduced rotation q~ (4), dA~ / T (9, row-major) and dC~ / T (3), from the plain integrator's Strang steps
+// E(h) R_k E(h), h = dt / 2, expanded to first order in the relaxation rates:
+//   A <- R_k A + h (P R_k + R_k P) R,  C <- R_k C + h (R_k e_z + e_z),  R <- R_k R   (P = diag(1, 1, 0)),
+// then dA = A - (T/2)(P R + R P), dC = C - (T/2)(R e_z + e_z), reduced by Rz(-wz/2) like the rotation.
+__global__ void bp_pulse_targets_kernel(const double2* __restrict__ rf, int k_steps, double dt, double gz,
+                                        double thickness, double z0, const float* __restrict__ samples, int n,
+                                        float* __restrict__ targets, float* __restrict__ qfull) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double df = samples[3 * i], b1 = samples[3 * i + 1], zr = samples[3 * i + 2];
     const double z = z0 + zr * thickness;
-    const double w = -2.0 * M_PI * dt, wz = w * (gz * z + df);
+    const double w = -2.0 * M_PI * dt, wz = w * (gz * z + df), h = 0.5 * dt;
     dq4 q{1.0, 0.0, 0.0, 0.0};
+    dm3 R{{1, 0, 0, 0, 1, 0, 0, 0, 1}}, A{{0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    double C[3] = {0.0, 0.0, 0.0};
     for (int k = 0; k < k_steps; ++k) {
         const double2 r = rf[k];
-        q = dq_mul(dq_rotvec(w * b1 * r.x, w * b1 * r.y, wz), q);
+        const dq4 qk = dq_rotvec(w * b1 * r.x, w * b1 * r.y, wz);
+        const dm3 Rk = dm_of_quat(qk);
+        // (P R_k + R_k P) R: P zeroes row 2 of R_k (left) or column 2 of R_k (right)
+        dm3 S;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) S.m[e] = Rk.m[e] * ((e / 3 < 2 ? 1.0 : 0.0) + (e % 3 < 2 ? 1.0 : 0.0));
+        const dm3 RA = dm_mul(Rk, A), SR = dm_mul(S, R);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) A.m[e] = RA.m[e] + h * SR.m[e];
+        const double c0 = Rk.m[0] * C[0] + Rk.m[1] * C[1] + Rk.m[2] * C[2];
+        const double c1 = Rk.m[3] * C[0] + Rk.m[4] * C[1] + Rk.m[5] * C[2];
+        const double c2 = Rk.m[6] * C[0] + Rk.m[7] * C[1] + Rk.m[8] * C[2];
+        C[0] = c0 + h * Rk.m[2], C[1] = c1 + h * Rk.m[5], C[2] = c2 + h * (Rk.m[8] + 1.0);
+        R = dm_mul(Rk, R);
+        q = dq_mul(qk, q);
     }
-    const dq4 h = dq_z(-0.5 * wz * k_steps);
-    const dq4 qr = dq_mul(dq_mul(h, q), h);
-    qred[4 * i] = (float)qr.w, qred[4 * i + 1] = (float)qr.x, qred[4 * i + 2] = (float)qr.y, qred[4 * i + 3] = (float)qr.z;
+    const double T = k_steps * dt;
+    dm3 dA;
+#pragma unroll
+    for (int e = 0; e < 9; ++e)  // (P R + R P)_{rc} = R_{rc} ((r < 2) + (c < 2))
+        dA.m[e] = A.m[e] - 0.5 * T * R.m[e] * ((e / 3 < 2 ? 1.0 : 0.0) + (e % 3 < 2 ? 1.0 : 0.0));
+    const double dC[3] = {C[0] - 0.5 * T * R.m[2], C[1] - 0.5 * T * R.m[5], C[2] - 0.5 * T * (R.m[8] + 1.0)};
+    const dq4 hq = dq_z(-0.5 * wz * k_steps);
+    const dq4 qr = dq_mul(dq_mul(hq, q), hq);
+    const dm3 Rh = dm_of_quat(hq);
+    const dm3 dAr = dm_mul(dm_mul(Rh, dA), Rh);
+    float* t = targets + 16 * (size_t)i;
+    t[0] = (float)qr.w, t[1] = (float)qr.x, t[2] = (float)qr.y, t[3] = (float)qr.z;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) t[4 + e] = (float)(dAr.m[e] / T);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        t[13 + r] = (float)((Rh.m[3 * r] * dC[0] + Rh.m[3 * r + 1] * dC[1] + Rh.m[3 * r + 2] * dC[2]) / T);
     if (qfull) qfull[4 * i] = (float)q.w, qfull[4 * i + 1] = (float)q.x, qfull[4 * i + 2] = (float)q.y, qfull[4 * i + 3] = (float)q.z;
 }
 
-extern "C" int bp_pulse_quats(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
-                              const float* samples, int n, float* qred, float* qfull, void* stream) {
-    if (!rf || !samples || !qred || k_steps < 1 || n < 0 || dt <= 0 || thickness <= 0) return BP_E_ARG;
+extern "C" int bp_pulse_targets(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
+                                const float* samples, int n, float* targets, float* qfull, void* stream) {
+    if (!rf || !samples || !targets || k_steps < 1 || n < 0 || dt <= 0 || thickness <= 0) return BP_E_ARG;
     if (n == 0) return BP_OK;
-    bp_pulse_quats_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<const double2*>(rf), k_steps, dt, gz, thickness, z0, samples, n, qred, qfull);
+    bp_pulse_targets_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const double2*>(rf), k_steps, dt, gz, thickness, z0, samples, n, targets, qfull);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
@@ -115,7 +172,7 @@ __device__ __forceinline__ float gelu_d(float x) {
 
 // The network's output for normalised input x, and (train) its pre-activations into z1, z2, z3 rows.
 __device__ __forceinline__ void mlp_forward_row(const float* __restrict__ P, const float x[3], float* z1, float* z2,
-                                                float* z3, float y[4]) {
+                                                float* z3, float y[MLP_OUT]) {
     float a[MLP_H];
 #pragma unroll
     for (int k = 0; k < MLP_H; ++k) {
@@ -186,7 +243,7 @@ __device__ __forceinline__ void weight_grads(const float* dz, const float* act, 
 // gradient sum (not yet divided by the batch) to gpart[blockIdx.x][N_PARAMS] and its loss sum to lpart.
 __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __restrict__ params,
                                                               const float* __restrict__ x, const float* __restrict__ target,
-                                                              int n, float vw, float* __restrict__ gpart,
+                                                              int n, float vw, float cw, float* __restrict__ gpart,
                                                               float* __restrict__ lpart) {
     extern __shared__ __align__(16) float sm[];
     float* P = sm;                       // N_PARAMS (padded to a multiple of 4)
@@ -203,22 +260,28 @@ __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __res
     __syncthreads();
     float* g = gpart + (size_t)blockIdx.x * N_PARAMS;
     const bool live = tid < nt;
-    float xin[3] = {0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f};
+    float xin[3] = {0.f, 0.f, 0.f}, y[MLP_OUT];
+#pragma unroll
+    for (int j = 0; j < MLP_OUT; ++j) y[j] = 0.0f;
     if (live) {
         xin[0] = x[3 * (t0 + tid)], xin[1] = x[3 * (t0 + tid) + 1], xin[2] = x[3 * (t0 + tid) + 2];
         mlp_forward_row(P, xin, z1 + tid * TR_LD, z2 + tid * TR_LD, z3 + tid * TR_LD, y);
     }
-    // loss (q0 - t0)^2 + vw |q_vec - t_vec|^2 with q = y/|y| (vw weights the vector part: relative precision for
-    // small rotations), and dL/dy = (dL/dq - q (q . dL/dq)) / |y|
-    float dy[4] = {0.f, 0.f, 0.f, 0.f}, loss = 0.0f;
+    // loss (q0 - t0)^2 + vw |q_vec - t_vec|^2 + cw |c - t_c|^2 with q = y[0:4]/|y[0:4]| (vw weights the vector
+    // part: relative precision for small rotations) and c = y[4:16] the first-order corrections;
+    // dL/dy[0:4] = (dL/dq - q (q . dL/dq)) / |y[0:4]|, dL/dy[4:16] = 2 cw (c - t_c)
+    float dy[MLP_OUT], loss = 0.0f;
+#pragma unroll
+    for (int j = 0; j < MLP_OUT; ++j) dy[j] = 0.0f;
     if (live) {
+        const float* tg = target + (size_t)MLP_OUT * (t0 + tid);
         const float r = sqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
         const float inv = 1.0f / r;
         float q[4], gq[4], qg = 0.0f;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             q[j] = y[j] * inv;
-            const float e = q[j] - target[4 * (t0 + tid) + j];
+            const float e = q[j] - tg[j];
             const float w = j == 0 ? 1.0f : vw;
             loss = fmaf(w * e, e, loss);
             gq[j] = 2.0f * w * e;
@@ -226,9 +289,15 @@ __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __res
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) dy[j] = (gq[j] - q[j] * qg) * inv;
+#pragma unroll
+        for (int j = 4; j < MLP_OUT; ++j) {
+            const float e = y[j] - tg[j];
+            loss = fmaf(cw * e, e, loss);
+            dy[j] = 2.0f * cw * e;
+        }
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) dyb[tid][j] = dy[j];
+    for (int j = 0; j < MLP_OUT; ++j) dyb[tid][j] = dy[j];
     lsum[tid] = loss;
     // a3 = gelu(z3) into buf (own row)
     for (int k = 0; k < MLP_H; ++k) buf[tid * TR_LD + k] = live ? gelu_f(z3[tid * TR_LD + k]) : 0.0f;
@@ -336,8 +405,8 @@ extern "C" int bp_mlp_grad_ctas(int n) { return n < 1 ? 0 : (n + TR_T - 1) / TR_
 static size_t mlp_grad_smem() { return (((size_t)N_PARAMS + 3) & ~(size_t)3) * 4 + 4 * (size_t)TR_ARR * 4; }
 
 extern "C" int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float vweight,
-                           float* gpart, float* lpart, void* stream) {
-    if (!params || !x || !target || !gpart || !lpart || n < 1 || !(vweight > 0)) return BP_E_ARG;
+                           float cweight, float* gpart, float* lpart, void* stream) {
+    if (!params || !x || !target || !gpart || !lpart || n < 1 || !(vweight > 0) || !(cweight >= 0)) return BP_E_ARG;
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -348,7 +417,7 @@ extern "C" int bp_mlp_grad(const float* params, const float* x, const float* tar
         configured[dev] = true;
     }
     bp_mlp_grad_kernel<<<bp_mlp_grad_ctas(n), TR_T, mlp_grad_smem(), static_cast<cudaStream_t>(stream)>>>(
-        params, x, target, n, vweight, gpart, lpart);
+        params, x, target, n, vweight, cweight, gpart, lpart);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
@@ -378,11 +447,11 @@ __global__ void __launch_bounds__(128) bp_mlp_eval_kernel(const float* __restric
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const float xin[3] = {x[3 * t], x[3 * t + 1], x[3 * t + 2]};
-    float o[4];
+    float o[MLP_OUT];
     mlp_forward_row(P, xin, nullptr, nullptr, nullptr, o);
     const float inv = rsqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) y[4 * t + j] = o[j] * inv;
+    for (int j = 0; j < MLP_OUT; ++j) y[MLP_OUT * (size_t)t + j] = j < 4 ? o[j] * inv : o[j];
 }
 
 extern "C" int bp_mlp_eval(const float* params, const float* x, int n, float* y, void* stream) {
@@ -432,6 +501,60 @@ __device__ __forceinline__ void quat_mul_f(const float a[4], const float b[4], f
     o[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
 }
 
+// The network's outputs y (the reduced quaternion, dA~ / T, dC~ / T) applied to one spin's state (m + l):
+// R = Rz(a1) R~ Rz(a2), dA = Rz(a1) dA~ Rz(a2), dC = Rz(a1) dC~ with a1 = wz/2 + phi0, a2 = wz/2 - phi0 and
+// wz = -2 pi (G z + df) T (half angles in float64); then m -> E (R - (r2 - r1) dA)(E m + c) + c + r1 pd dC, E and c
+// the exact relaxation and recovery of half the pulse: the pulse's map to first order in the relaxation rates
+// beyond the relax / rotate / relax splitting (exact in the splitting's exponentials).
+__device__ __forceinline__ void apply_pulse_map(const float* y, const PulseArgs& a, const Spin& p, float df,
+                                                float& mx, float& my, float& mz, float& lx, float& ly, float& lz) {
+    const float inv = rsqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+    const float qr[4] = {y[0] * inv, y[1] * inv, y[2] * inv, y[3] * inv};
+    const double half = -M_PI * ((double)a.gz * (double)p.pz + (double)df) * a.T;
+    float s1, c1, s2, c2;
+    sincos_reduced(0.5 * (half + a.phi0), &s1, &c1);
+    sincos_reduced(0.5 * (half - a.phi0), &s2, &c2);
+    const float qa[4] = {c1, 0.f, 0.f, s1}, qb[4] = {c2, 0.f, 0.f, s2};
+    float t4[4], q[4];
+    quat_mul_f(qa, qr, t4);
+    quat_mul_f(t4, qb, q);
+    const float s = q[0], x = q[1], yq = q[2], z = q[3];
+    float R[9] = {1 - 2 * (yq * yq + z * z), 2 * (x * yq - s * z), 2 * (x * z + s * yq),
+                  2 * (x * yq + s * z), 1 - 2 * (x * x + z * z), 2 * (yq * z - s * x),
+                  2 * (x * z - s * yq), 2 * (yq * z + s * x), 1 - 2 * (x * x + yq * yq)};
+    // the full angles' cos / sin from the half angles
+    const float C1 = fmaf(c1, c1, -s1 * s1), S1 = 2.0f * s1 * c1, C2 = fmaf(c2, c2, -s2 * s2), S2 = 2.0f * s2 * c2;
+    const float T = (float)a.T;
+    const float k = -(p.r2 - p.r1) * T;  // M = R + k dA~' (dA~' = Rz(a1) (dA~ / T) Rz(a2))
+    float X[9];  // X = (dA~ / T) Rz(a2): columns 0 and 1 turn
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const float d0 = y[4 + 3 * r], d1 = y[5 + 3 * r];
+        X[3 * r] = fmaf(d0, C2, d1 * S2);
+        X[3 * r + 1] = fmaf(-d0, S2, d1 * C2);
+        X[3 * r + 2] = y[6 + 3 * r];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {  // Rz(a1) X: rows 0 and 1 turn; M = R + k Rz(a1) X
+        const float a0 = fmaf(C1, X[c], -S1 * X[3 + c]), a1 = fmaf(S1, X[c], C1 * X[3 + c]);
+        R[c] = fmaf(k, a0, R[c]);
+        R[3 + c] = fmaf(k, a1, R[3 + c]);
+        R[6 + c] = fmaf(k, X[6 + c], R[6 + c]);
+    }
+    const float th = 0.5f * T;
+    const float e1 = expm1f(-th * p.r1), e2 = expm1f(-th * p.r2);
+    const float ax = (mx + lx) * (1.0f + e2), ay = (my + ly) * (1.0f + e2);
+    const float az = fmaf((mz + lz) - p.pd, e1, mz + lz);
+    const float nx = fmaf(R[0], ax, fmaf(R[1], ay, R[2] * az));
+    const float ny = fmaf(R[3], ax, fmaf(R[4], ay, R[5] * az));
+    const float nz = fmaf(R[6], ax, fmaf(R[7], ay, R[8] * az));
+    const float g = p.r1 * p.pd * T;  // r1 pd dC = r1 pd T Rz(a1) (dC~ / T)
+    mx = fmaf(g, fmaf(C1, y[13], -S1 * y[14]), nx * (1.0f + e2));
+    my = fmaf(g, fmaf(S1, y[13], C1 * y[14]), ny * (1.0f + e2));
+    mz = fmaf(g, y[15], fmaf(nz - p.pd, e1, nz));
+    lx = ly = lz = 0.0f;
+}
+
 __global__ void __launch_bounds__(128) bp_surrogate_pulse_kernel(PulseArgs a) {
     __shared__ float P[N_PARAMS];
     for (int i = threadIdx.x; i < N_PARAMS; i += blockDim.x) P[i] = a.params[i];
@@ -456,33 +579,9 @@ __global__ void __launch_bounds__(128) bp_surrogate_pulse_kernel(PulseArgs a) {
     float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
     if (inside) {
         const float xin[3] = {df / a.dom_df, (p.b1 - 1.0f) / a.dom_b1, zr / a.dom_z};
-        float y[4];
+        float y[MLP_OUT];
         mlp_forward_row(P, xin, nullptr, nullptr, nullptr, y);
-        const float inv = rsqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
-        const float qr[4] = {y[0] * inv, y[1] * inv, y[2] * inv, y[3] * inv};
-        // R = Rz(wz/2 + phi0) R~ Rz(wz/2 - phi0), wz = -2 pi (G z + df) T: the half angles in float64
-        const double half = -M_PI * ((double)a.gz * (double)p.pz + (double)df) * a.T;
-        float s1, c1, s2, c2;
-        sincos_reduced(0.5 * (half + a.phi0), &s1, &c1);
-        sincos_reduced(0.5 * (half - a.phi0), &s2, &c2);
-        const float qa[4] = {c1, 0.f, 0.f, s1}, qb[4] = {c2, 0.f, 0.f, s2};
-        float t[4], q[4];
-        quat_mul_f(qa, qr, t);
-        quat_mul_f(t, qb, q);
-        const float s = q[0], x = q[1], yq = q[2], z = q[3];
-        const float R00 = 1 - 2 * (yq * yq + z * z), R01 = 2 * (x * yq - s * z), R02 = 2 * (x * z + s * yq);
-        const float R10 = 2 * (x * yq + s * z), R11 = 1 - 2 * (x * x + z * z), R12 = 2 * (yq * z - s * x);
-        const float R20 = 2 * (x * z - s * yq), R21 = 2 * (yq * z + s * x), R22 = 1 - 2 * (x * x + yq * yq);
-        // relax T/2, rotate, relax T/2 (relaxation cannot be a pure rotation: it wraps the network's rotation)
-        const float th = (float)(0.5 * a.T);
-        const float e1 = expm1f(-th * p.r1), e2 = expm1f(-th * p.r2);
-        const float ax = (mx + lx) * (1.0f + e2), ay = (my + ly) * (1.0f + e2);
-        const float az = fmaf((mz + lz) - p.pd, e1, mz + lz);
-        const float nx = fmaf(R00, ax, fmaf(R01, ay, R02 * az));
-        const float ny = fmaf(R10, ax, fmaf(R11, ay, R12 * az));
-        const float nz = fmaf(R20, ax, fmaf(R21, ay, R22 * az));
-        mx = nx * (1.0f + e2), my = ny * (1.0f + e2), mz = fmaf(nz - p.pd, e1, nz);
-        lx = ly = lz = 0.0f;
+        apply_pulse_map(y, a, p, df, mx, my, mz, lx, ly, lz);
     } else {  // the fallback: the plain sub-stepped pulse
         RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
         for (int k = 0; k < a.k_steps; ++k) {
@@ -669,7 +768,7 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
         if (inside) {
             float mx = a.state[j], my = a.state[a.n + j], mz = a.state[2 * a.n + j];
             float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
-            float y[4];
+            float y[MLP_OUT];
 #pragma unroll
             for (int o = 0; o < MLP_OUT; ++o) {
                 float s = net.b4[o];
@@ -677,29 +776,7 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
                 for (int i = 0; i < MLP_H; ++i) s = fmaf(net.w4[MLP_H * o + i], v[i], s);
                 y[o] = s;
             }
-            const float inv = rsqrtf(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
-            const float qr[4] = {y[0] * inv, y[1] * inv, y[2] * inv, y[3] * inv};
-            const double half = -M_PI * ((double)a.gz * (double)p.pz + (double)df) * a.T;
-            float s1, c1, s2, c2;
-            sincos_reduced(0.5 * (half + a.phi0), &s1, &c1);
-            sincos_reduced(0.5 * (half - a.phi0), &s2, &c2);
-            const float qa[4] = {c1, 0.f, 0.f, s1}, qb[4] = {c2, 0.f, 0.f, s2};
-            float t4[4], q[4];
-            quat_mul_f(qa, qr, t4);
-            quat_mul_f(t4, qb, q);
-            const float s = q[0], x = q[1], yq = q[2], z = q[3];
-            const float R00 = 1 - 2 * (yq * yq + z * z), R01 = 2 * (x * yq - s * z), R02 = 2 * (x * z + s * yq);
-            const float R10 = 2 * (x * yq + s * z), R11 = 1 - 2 * (x * x + z * z), R12 = 2 * (yq * z - s * x);
-            const float R20 = 2 * (x * z - s * yq), R21 = 2 * (yq * z + s * x), R22 = 1 - 2 * (x * x + yq * yq);
-            const float th = (float)(0.5 * a.T);
-            const float e1 = expm1f(-th * p.r1), e2 = expm1f(-th * p.r2);
-            const float ax = (mx + lx) * (1.0f + e2), ay = (my + ly) * (1.0f + e2);
-            const float az = fmaf((mz + lz) - p.pd, e1, mz + lz);
-            const float nx = fmaf(R00, ax, fmaf(R01, ay, R02 * az));
-            const float ny = fmaf(R10, ax, fmaf(R11, ay, R12 * az));
-            const float nz = fmaf(R20, ax, fmaf(R21, ay, R22 * az));
-            mx = nx * (1.0f + e2), my = ny * (1.0f + e2), mz = fmaf(nz - p.pd, e1, nz);
-            lx = ly = lz = 0.0f;
+            apply_pulse_map(y, a, p, df, mx, my, mz, lx, ly, lz);
             a.state[j] = mx, a.state[a.n + j] = my, a.state[2 * a.n + j] = mz;
             a.state[3 * a.n + j] = lx, a.state[4 * a.n + j] = ly, a.state[5 * a.n + j] = lz;
         }

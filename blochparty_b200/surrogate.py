@@ -36,13 +36,13 @@ def _fan_in_init(seed: int) -> torch.Tensor:
     """Flat initial parameters: weights N(0, 1/fan_in), biases 0 (seeded)."""
     g = torch.Generator().manual_seed(seed)
     parts = []
-    for shape in ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (4, 64), (4,)):
+    for shape in ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (16, 64), (16,)):
         if len(shape) == 2:
             parts.append(torch.randn(shape, generator=g, dtype=F64).reshape(-1) / math.sqrt(shape[1]))
         else:
             parts.append(torch.zeros(shape, dtype=F64))
     p = torch.cat(parts)
-    p[-4] = 1.0  # output bias toward the identity rotation (1, 0, 0, 0)
+    p[-16] = 1.0  # output bias toward the identity rotation (1, 0, 0, 0) (then the 12 first-order terms: 0)
     return p.to(F32)
 
 
@@ -71,6 +71,9 @@ class RFSurrogate:
         self.params = _fan_in_init(seed).to(self.device)
         self.seed = seed
         self.vweight = 1.0  # the loss weight of the quaternion's vector part (set by train)
+        # the loss weight of the first-order terms: their effect on the magnetization is about (r2 - r1) T times
+        # their error (a few hundredths for T of a few ms), so they need far less precision than the rotation
+        self.cweight = 0.01
         self.domain = tuple(float(d) for d in domain)
         if len(self.domain) != 3 or min(self.domain) <= 0:
             raise ValueError(f"domain must be three positive bounds (|df|, |b1 - 1|, |z_rel|), got {domain!r}")
@@ -98,23 +101,24 @@ class RFSurrogate:
         return s.to(F32).to(self.device).contiguous()
 
     def targets(self, samples: torch.Tensor, full: bool = False):
-        """Reduced rotations (n, 4) (and the whole rotations) of the samples from the plain integrator."""
+        """The network's targets (n, 16) for the samples from the plain integrator: the reduced rotation, dA~ / T
+        and dC~ / T (and the whole rotations (n, 4) when ``full``)."""
         n = samples.shape[0]
         rf = self.rf.to(self.device).contiguous()
-        qred = torch.empty(n, 4, dtype=F32, device=self.device)
+        tg = torch.empty(n, _lib.BP_MLP_OUTPUTS, dtype=F32, device=self.device)
         qfull = torch.empty(n, 4, dtype=F32, device=self.device) if full else None
-        code = _lib.lib().bp_pulse_quats(ptr(rf), self.K, self.dt, self.gz, self.thickness, self.z0, ptr(samples), n,
-                                         ptr(qred), ptr(qfull), _lib.stream_ptr())
-        _lib.check(code, "bp_pulse_quats")
-        return (qred, qfull) if full else qred
+        code = _lib.lib().bp_pulse_targets(ptr(rf), self.K, self.dt, self.gz, self.thickness, self.z0, ptr(samples),
+                                           n, ptr(tg), ptr(qfull), _lib.stream_ptr())
+        _lib.check(code, "bp_pulse_targets")
+        return (tg, qfull) if full else tg
 
     def normalise(self, samples: torch.Tensor) -> torch.Tensor:
         s, d = samples, self.domain
         return torch.stack([s[:, 0] / d[0], (s[:, 1] - 1) / d[1], s[:, 2] / d[2]], -1).contiguous()
 
-    def gradient(self, x: torch.Tensor, target: torch.Tensor, vweight: float = 1.0):
+    def gradient(self, x: torch.Tensor, target: torch.Tensor, vweight: float = 1.0, cweight: float = 1.0):
         """(mean loss, gradient) of the batch through the training kernels (x normalised; ``vweight`` weights the
-        quaternion's vector part in the loss)."""
+        quaternion's vector part in the loss, ``cweight`` the first-order terms)."""
         lib, n = _lib.lib(), x.shape[0]
         ctas = lib.bp_mlp_grad_ctas(n)
         gpart = torch.empty(ctas, _lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
@@ -122,8 +126,8 @@ class RFSurrogate:
         grad = torch.empty(_lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
         loss = torch.empty(1, dtype=F32, device=self.device)
         st = _lib.stream_ptr()
-        _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(x), ptr(target), n, vweight, ptr(gpart), ptr(lpart), st),
-                   "bp_mlp_grad")
+        _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(x), ptr(target), n, vweight, cweight, ptr(gpart),
+                                   ptr(lpart), st), "bp_mlp_grad")
         _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / n, ptr(grad), ptr(loss), st), "bp_mlp_reduce")
         return loss, grad
 
@@ -137,7 +141,7 @@ class RFSurrogate:
         seed = self.seed if seed is None else seed
         s = self.samples(n_samples, seed + 1)
         x, y = self.normalise(s), self.targets(s)
-        vmax = float(torch.linalg.vector_norm(y[:, 1:], dim=1).max())
+        vmax = float(torch.linalg.vector_norm(y[:, 1:4], dim=1).max())
         self.vweight = 1.0 / min(1.0, max(1e-2, vmax)) ** 2
         m = torch.zeros(_lib.BP_MLP_PARAMS, dtype=F32, device=self.device)
         v = torch.zeros_like(m)
@@ -158,8 +162,8 @@ class RFSurrogate:
                 frac = (ep * steps_per_epoch + b) / max(total - 1, 1)
                 rate = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * frac))
                 xb, yb = xs[b * batch:(b + 1) * batch], ys[b * batch:(b + 1) * batch]
-                _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(xb), ptr(yb), batch, self.vweight, ptr(gpart),
-                                           ptr(lpart), st), "bp_mlp_grad")
+                _lib.check(lib.bp_mlp_grad(ptr(self.params), ptr(xb), ptr(yb), batch, self.vweight, self.cweight,
+                                           ptr(gpart), ptr(lpart), st), "bp_mlp_grad")
                 _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / batch, ptr(grad), ptr(loss), st),
                            "bp_mlp_reduce")
                 _lib.check(lib.bp_adam(ptr(self.params), ptr(grad), ptr(m), ptr(v), rate, 0.9, 0.999, 1e-8, step, st),
@@ -191,19 +195,21 @@ class RFSurrogate:
         return self._ph
 
     def predict(self, samples: torch.Tensor) -> torch.Tensor:
-        """The network's reduced rotations (n, 4) for samples (df, b1, z_rel)."""
+        """The network's outputs (n, 16) for samples (df, b1, z_rel)."""
         x = self.normalise(samples)
-        y = torch.empty(x.shape[0], 4, dtype=F32, device=self.device)
+        y = torch.empty(x.shape[0], _lib.BP_MLP_OUTPUTS, dtype=F32, device=self.device)
         _lib.check(_lib.lib().bp_mlp_eval(ptr(self.params), ptr(x), x.shape[0], ptr(y), _lib.stream_ptr()),
                    "bp_mlp_eval")
         return y
 
     def validate(self, n: int = 1 << 16, seed: int = 99):
-        """Largest and RMS error of the network's reduced rotation against the plain integrator's, on fresh samples
-        (quaternion components; the rotation-matrix error is at most twice as large)."""
+        """(largest, RMS) error of the network's reduced rotation against the plain integrator's (quaternion
+        components; the rotation-matrix error is at most twice as large), then (largest, RMS) error of its
+        first-order terms dA~ / T, dC~ / T, on fresh samples."""
         s = self.samples(n, seed)
         err = (self.predict(s) - self.targets(s)).abs()
-        return float(err.max()), float(err.pow(2).mean().sqrt())
+        q, c = err[:, :4], err[:, 4:]
+        return (float(q.max()), float(q.pow(2).mean().sqrt()), float(c.max()), float(c.pow(2).mean().sqrt()))
 
     # ---- matching occurrences in a sequence ----
     def phase_of(self, w: np.ndarray, tol: float = 1e-6):

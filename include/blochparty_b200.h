@@ -148,33 +148,37 @@ int bp_pulse_apply(const double* maps, int n, float* state, double phase, void* 
 
 /* ---- learned RF surrogate (no counterpart in the reference; its nearest part is the exact per-spin map of a
  * reused pulse, engines/gpu/cuda/pulse.cu.in:3-32) ----
- * A 3 -> 64 -> 64 -> 64 -> 4 GELU network per shaped pulse: inputs (df / dom_df, (b1 - 1) / dom_b1, z_rel / dom_z)
- * with z_rel = (z - z0) / slice thickness and the network's training domain (dom_df, dom_b1, dom_z) (the host
- * side's default: 200 Hz, 0.3, 2), output a unit quaternion (q0, q1, q2, q3), the Cayley-Klein pair
- * alpha = q0 - i q3, beta = -i (q1 + i q2), of the pulse's rotation reduced by its free precession:
- * R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T. Parameters: BP_MLP_PARAMS floats, W1 (64x3), b1, W2 (64x64),
- * b2, W3 (64x64), b3, W4 (4x64), b4. */
-#define BP_MLP_PARAMS 8836
+ * A 3 -> 64 -> 64 -> 64 -> 16 GELU network per shaped pulse: inputs (df / dom_df, (b1 - 1) / dom_b1,
+ * z_rel / dom_z) with z_rel = (z - z0) / slice thickness and the network's training domain (dom_df, dom_b1, dom_z)
+ * (the host side's default: 200 Hz, 0.3, 2). Outputs:
+ *   [0, 4)   a unit quaternion (q0, q1, q2, q3), the Cayley-Klein pair alpha = q0 - i q3, beta = -i (q1 + i q2), of
+ *            the pulse's rotation reduced by its free precession: R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T;
+ *   [4, 13)  dA~ / T (row-major), [13, 16) dC~ / T: the pulse's first-order relaxation terms beyond the relax (T/2)
+ *            / rotate / relax (T/2) splitting, reduced like R (the pulse maps m to E (R - (r2 - r1) dA)(E m + c) +
+ *            c + r1 pd dC, E and c the half-pulse relaxation and recovery).
+ * Parameters: BP_MLP_PARAMS floats, W1 (64x3), b1, W2 (64x64), b2, W3 (64x64), b3, W4 (16x64), b4 (16). */
+#define BP_MLP_PARAMS 9616
+#define BP_MLP_OUTPUTS 16
 
-/* Training targets from the plain integrator: samples [n][3] (df [Hz], b1, z_rel) -> reduced rotations
- * qred [n][4] (and the whole rotations qfull [n][4] if not NULL); rf [k_steps][2] float64 [Hz], float64 throughout. */
-int bp_pulse_quats(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
-                   const float* samples, int n, float* qred, float* qfull, void* stream);
+/* Training targets from the plain integrator: samples [n][3] (df [Hz], b1, z_rel) -> targets [n][16] (the outputs
+ * above; and the whole rotations qfull [n][4] if not NULL); rf [k_steps][2] float64 [Hz], float64 throughout. */
+int bp_pulse_targets(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
+                     const float* samples, int n, float* targets, float* qfull, void* stream);
 
-/* One training step's gradient: x [n][3] normalised inputs, target [n][4]; loss (q0 - t0)^2 + vweight |q_vec -
- * t_vec|^2 per sample (vweight > 0 weights the vector part: relative precision for small rotations); per-CTA
- * partials gpart [bp_mlp_grad_ctas(n)][BP_MLP_PARAMS] and loss sums lpart [bp_mlp_grad_ctas(n)] (scratch of the
- * caller). */
+/* One training step's gradient: x [n][3] normalised inputs, target [n][16]; loss (q0 - t0)^2 + vweight |q_vec -
+ * t_vec|^2 + cweight |c - t_c|^2 per sample (q the normalised quaternion, c the 12 correction outputs; vweight > 0
+ * weights the vector part: relative precision for small rotations); per-CTA partials gpart
+ * [bp_mlp_grad_ctas(n)][BP_MLP_PARAMS] and loss sums lpart [bp_mlp_grad_ctas(n)] (scratch of the caller). */
 int bp_mlp_grad_ctas(int n);
-int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float vweight, float* gpart,
-                float* lpart, void* stream);
+int bp_mlp_grad(const float* params, const float* x, const float* target, int n, float vweight, float cweight,
+                float* gpart, float* lpart, void* stream);
 /* grad = scale * (sum over CTAs in order of gpart), loss = scale * sum of lpart (scale = 1 / batch). */
 int bp_mlp_reduce(const float* gpart, const float* lpart, int n_cta, float scale, float* grad, float* loss,
                   void* stream);
 /* Adam step number `step` (1-based) on params with moments m, v. */
 int bp_adam(float* params, const float* grad, float* m, float* v, float lr, float beta1, float beta2, float eps,
             int step, void* stream);
-/* The network's unit-quaternion outputs y [n][4] for normalised inputs x [n][3]. */
+/* The network's outputs y [n][16] (the quaternion normalised) for normalised inputs x [n][3]. */
 int bp_mlp_eval(const float* params, const float* x, int n, float* y, void* stream);
 
 /* One pulse occurrence (segments [seg0, seg0 + k_steps) of `segs`, the trained waveform times exp(i phi0), slice

@@ -14,7 +14,12 @@ Conventions (shared with ``blochparty_b200/csrc/surrogate.cu``):
   beta = -i (q1 + i q2);
 * the pulse's whole precession without RF is the z rotation by wz = -2 pi (G z + df) T; the network learns
   the reduced rotation R~ with R = Rz(wz / 2) R~ Rz(wz / 2), smooth in z where R itself winds around z;
-* inputs normalised to [-1, 1]: (df / 200 Hz, (b1 - 1) / 0.3, z_rel / 2), z_rel = z / slice thickness.
+* inputs normalised to [-1, 1]: (df / 200 Hz, (b1 - 1) / 0.3, z_rel / 2), z_rel = z / slice thickness;
+* relaxation during the pulse, to first order in the rates: the plain integrator's pulse is the affine map
+  m -> M m + v with M = R - r2 A - r1 B + O(r^2), v = r1 pd C + O(r^2); A + B = T R, so the network learns what
+  the relax (T/2) / rotate / relax (T/2) splitting misses, dA = A - (T/2)(P R + R P) (P = diag(1, 1, 0)) and
+  dC = C - (T/2)(R e_z + e_z), reduced like R (dA~ = Rz(-wz/2) dA Rz(-wz/2), dC~ = Rz(-wz/2) dC) and divided by
+  T. The pulse is then m -> E (R - (r2 - r1) dA) (E m + c) + c + r1 pd dC, E and c the exact half-pulse relaxation.
 """
 
 from __future__ import annotations
@@ -74,7 +79,41 @@ def pulse_quaternions(rf, dt, gz, z, df, b1):
         q = qmul(quat_of_rotvec(wv), q)
     total = wz * rf.shape[0]
     qr = qmul(qmul(qz(-0.5 * total), q), qz(-0.5 * total))
-    return q, qr
+    return q, qr  # (the rotation alone; pulse_targets adds the first-order relaxation terms)
+
+
+def pulse_targets(rf, dt, gz, z, df, b1):
+    """(q (n, 4), targets (n, 16)): the whole-pulse rotation q and the network's targets of every sample, float64:
+    the reduced rotation q~ (4), dA~ / T (9, row-major) and dC~ / T (3), from the discrete first-order expansion of
+    the plain Strang steps (each step E(h) R_k E(h) with h = dt / 2)."""
+    rf = torch.as_tensor(rf, dtype=F64)
+    z, df, b1 = (torch.as_tensor(t, dtype=F64) for t in (z, df, b1))
+    K, h = rf.shape[0], 0.5 * dt
+    q = torch.zeros(z.shape + (4,), dtype=F64)
+    q[..., 0] = 1.0
+    R = torch.eye(3, dtype=F64).expand(z.shape + (3, 3)).clone()
+    A = torch.zeros(z.shape + (3, 3), dtype=F64)
+    C = torch.zeros(z.shape + (3,), dtype=F64)
+    P = torch.diag(torch.tensor([1.0, 1.0, 0.0], dtype=F64))
+    ez = torch.tensor([0.0, 0.0, 1.0], dtype=F64)
+    w = -TWO_PI * dt
+    wz = w * (gz * z + df)
+    for k in range(K):
+        qk = quat_of_rotvec(torch.stack([w * b1 * rf[k, 0], w * b1 * rf[k, 1], wz], -1))
+        Rk = rotmat(qk)
+        A = Rk @ A + h * (P @ Rk + Rk @ P) @ R
+        C = (Rk @ C[..., None])[..., 0] + h * (Rk @ ez + ez)
+        R = Rk @ R
+        q = qmul(qk, q)
+    T = K * dt
+    dA = A - 0.5 * T * (P @ R + R @ P)
+    dC = C - 0.5 * T * (R @ ez + ez)
+    half = qz(-0.5 * wz * K)
+    Rh = rotmat(half)
+    qr = qmul(qmul(half, q), half)
+    dAr = Rh @ dA @ Rh / T
+    dCr = (Rh @ dC[..., None])[..., 0] / T
+    return q, torch.cat([qr, dAr.reshape(z.shape + (9,)), dCr], -1)
 
 
 def gelu(x):
@@ -83,8 +122,8 @@ def gelu(x):
 
 
 # parameter layout of the flat vector (as the kernels): W1 (64, 3), b1 (64), W2 (64, 64), b2, W3 (64, 64), b3,
-# W4 (4, 64), b4 (4): 8,836 floats
-SHAPES = ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (4, 64), (4,))
+# W4 (16, 64), b4 (16): 9,616 floats
+SHAPES = ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (16, 64), (16,))
 N_PARAMS = sum(math.prod(s) for s in SHAPES)
 
 
@@ -98,20 +137,21 @@ def unflatten(p):
 
 
 def mlp(p, x):
-    """Network output (B, 4), normalised to unit length, for normalised inputs x (B, 3)."""
+    """Network output (B, 16) for normalised inputs x (B, 3): the quaternion (normalised to unit length), then the
+    12 correction outputs as they are."""
     w1, b1, w2, b2, w3, b3, w4, b4 = unflatten(p)
     h = gelu(x @ w1.T + b1)
     h = gelu(h @ w2.T + b2)
     h = gelu(h @ w3.T + b3)
     y = h @ w4.T + b4
-    return y / torch.linalg.vector_norm(y, dim=-1, keepdim=True)
+    return torch.cat([y[:, :4] / torch.linalg.vector_norm(y[:, :4], dim=-1, keepdim=True), y[:, 4:]], -1)
 
 
-def loss_and_grad(p, x, target, vweight: float = 1.0):
-    """Mean over the batch of (q0 - t0)^2 + vweight |q_vec - t_vec|^2 and its gradient w.r.t. the flat parameters
-    (float64)."""
+def loss_and_grad(p, x, target, vweight: float = 1.0, cweight: float = 1.0):
+    """Mean over the batch of (q0 - t0)^2 + vweight |q_vec - t_vec|^2 + cweight |corrections - their targets|^2
+    and its gradient w.r.t. the flat parameters (float64)."""
     p = p.detach().to(F64).clone().requires_grad_()
-    w = torch.tensor([1.0, vweight, vweight, vweight], dtype=F64)
+    w = torch.tensor([1.0, vweight, vweight, vweight] + [cweight] * 12, dtype=F64)
     loss = (w * (mlp(p, x.to(F64)) - target.to(F64)) ** 2).sum(-1).mean()
     (g,) = torch.autograd.grad(loss, [p])
     return float(loss), g
