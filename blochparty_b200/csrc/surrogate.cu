@@ -438,7 +438,8 @@ extern "C" int bp_adam(float* params, const float* grad, float* m, float* v, flo
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
-// Network outputs for normalised inputs x [n][3] -> y [n][4] (normalised to unit length): inference for checks.
+// Network outputs for normalised inputs x [n][3] -> y [n][16] (the quaternion part normalised to unit length):
+// inference for checks.
 __global__ void __launch_bounds__(128) bp_mlp_eval_kernel(const float* __restrict__ params, const float* __restrict__ x,
                                                          int n, float* __restrict__ y) {
     __shared__ float P[N_PARAMS];
@@ -651,7 +652,7 @@ __device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned ch
     }
 }
 
-// The network's small parameters, passed by value in the kernel's arguments (2,576 bytes of the constant bank):
+// The network's small parameters, passed by value in the kernel's arguments (5,696 bytes of the constant bank):
 // every thread reads the same weight at the same time, so the FMAs take them as constant operands, no loads.
 struct SmallNet {
     float w1[MLP_H * MLP_IN], b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_OUT * MLP_H], b4[MLP_OUT];
