@@ -30,7 +30,8 @@ BP_MAX_COILS = 32
 BP_SEG_MAX = 160
 BP_ADJ_WIN = 32
 BP_MMA_MAX_COILS = 8
-BP_MLP_PARAMS = 9616
+BP_MLP_PARAMS = 10320
+BP_MLP_INPUTS = 2
 BP_MLP_OUTPUTS = 16
 BP_MMA_SAMPLES = 64
 BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024

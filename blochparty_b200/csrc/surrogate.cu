@@ -1,5 +1,6 @@
-// Learned RF surrogate: a 3 -> 64 -> 64 -> 64 -> 4 GELU network standing in for the sub-stepped integration of
-// one shaped RF pulse, mapping (off-resonance, B1 scale, slice position) to the pulse's rotation.
+// Learned RF surrogate: a 14 -> 64 -> 64 -> 64 -> 16 GELU network standing in for the sub-stepped integration of
+// one shaped RF pulse, mapping (off-resonance in the slice gradient, B1 scale) to the pulse's rotation and its
+// first-order relaxation terms.
 //
 // No counterpart in the reference (its nearest part is the exact per-spin map of a reused pulse,
 // engines/gpu/cuda/pulse.cu.in:3-32). Kernels here:
@@ -23,9 +24,11 @@
 #include "../../include/blochparty_b200.h"
 
 #define MLP_H 64
-#define MLP_IN 3
+#define MLP_X 2                        // the inputs (f^, b^)
+#define MLP_NF 6                       // Fourier orders of f^
+#define MLP_IN (MLP_X + 2 * MLP_NF)    // the first layer's features
 #define MLP_OUT 16  // the reduced quaternion (4), dA~ / T (9) and dC~ / T (3)
-// flat parameter layout: W1 (64 x 3), b1 (64), W2 (64 x 64), b2, W3 (64 x 64), b3, W4 (16 x 64), b4 (16)
+// flat parameter layout: W1 (64 x 14), b1 (64), W2 (64 x 64), b2, W3 (64 x 64), b3, W4 (16 x 64), b4 (16)
 #define P_W1 0
 #define P_B1 (P_W1 + MLP_H * MLP_IN)
 #define P_W2 (P_B1 + MLP_H)
@@ -34,12 +37,16 @@
 #define P_B3 (P_W3 + MLP_H * MLP_H)
 #define P_W4 (P_B3 + MLP_H)
 #define P_B4 (P_W4 + MLP_OUT * MLP_H)
-#define N_PARAMS (P_B4 + MLP_OUT)  // 9616
+#define N_PARAMS (P_B4 + MLP_OUT)  // 10320
 
 static_assert(N_PARAMS == BP_MLP_PARAMS, "parameter count");
 
 // The training domain of a network is |df| <= dom_df [Hz], |b1 - 1| <= dom_b1, |z_rel| <= dom_z [slice widths]
-// (the caller's choice); its inputs are normalised to (df / dom_df, (b1 - 1) / dom_b1, z_rel / dom_z).
+// (the caller's choice). The pulse acts on a spin through its off-resonance in the slice gradient,
+// f = df + G (z - z0) [Hz], and its B1 scale alone, so the inputs are f^ = f / F with F = dom_df + |G| dom_z
+// thickness (the largest |f| in the domain) and b^ = (b1 - 1) / dom_b1; the first layer sees them with the
+// Fourier features sin(k pi f^), cos(k pi f^), k = 1..6, which let a small network follow the slice profile's sharp
+// edges (Tancik et al., "Fourier features let networks learn high frequency functions", 2020).
 
 struct dq4 {
     double w, x, y, z;
@@ -170,13 +177,32 @@ __device__ __forceinline__ float gelu_d(float x) {
 #define TR_LD 65          // row stride (floats) of the per-sample activation arrays [TR_T][TR_LD]
 #define TR_ARR (TR_T * TR_LD)
 
-// The network's output for normalised input x, and (train) its pre-activations into z1, z2, z3 rows.
-__device__ __forceinline__ void mlp_forward_row(const float* __restrict__ P, const float x[3], float* z1, float* z2,
-                                                float* z3, float y[MLP_OUT]) {
+// The first layer's features of inputs (f^, b^): f^, b^, then sin(k pi f^), cos(k pi f^) for k = 1..6 (from
+// sincospi(f^), the higher orders by the angle-addition formulas: about k float32 roundings each).
+__device__ __forceinline__ void mlp_features(float fh, float bh, float g[MLP_IN]) {
+    float s1, c1;
+    sincospif(fh, &s1, &c1);
+    g[0] = fh, g[1] = bh;
+    float s = s1, c = c1;
+#pragma unroll
+    for (int k = 0; k < MLP_NF; ++k) {
+        g[MLP_X + 2 * k] = s, g[MLP_X + 2 * k + 1] = c;
+        const float sn = fmaf(s, c1, c * s1), cn = fmaf(c, c1, -s * s1);
+        s = sn, c = cn;
+    }
+}
+
+// The network's output for inputs x = (f^, b^), and (train) its pre-activations into z1, z2, z3 rows.
+__device__ __forceinline__ void mlp_forward_row(const float* __restrict__ P, const float x[MLP_X], float* z1,
+                                                float* z2, float* z3, float y[MLP_OUT]) {
+    float g[MLP_IN];
+    mlp_features(x[0], x[1], g);
     float a[MLP_H];
 #pragma unroll
     for (int k = 0; k < MLP_H; ++k) {
-        const float v = fmaf(P[P_W1 + 3 * k], x[0], fmaf(P[P_W1 + 3 * k + 1], x[1], fmaf(P[P_W1 + 3 * k + 2], x[2], P[P_B1 + k])));
+        float v = P[P_B1 + k];
+#pragma unroll
+        for (int i = 0; i < MLP_IN; ++i) v = fmaf(P[P_W1 + MLP_IN * k + i], g[i], v);
         if (z1) z1[k] = v;
         a[k] = gelu_f(v);
     }
@@ -239,7 +265,7 @@ __device__ __forceinline__ void weight_grads(const float* dz, const float* act, 
     }
 }
 
-// Per CTA: samples [blockIdx.x * 128, +128) of x [n][3] (normalised inputs) and targets [n][4]; writes the CTA's
+// Per CTA: samples [blockIdx.x * 128, +128) of x [n][2] (inputs f^, b^) and targets [n][16]; writes the CTA's
 // gradient sum (not yet divided by the batch) to gpart[blockIdx.x][N_PARAMS] and its loss sum to lpart.
 __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __restrict__ params,
                                                               const float* __restrict__ x, const float* __restrict__ target,
@@ -260,11 +286,11 @@ __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __res
     __syncthreads();
     float* g = gpart + (size_t)blockIdx.x * N_PARAMS;
     const bool live = tid < nt;
-    float xin[3] = {0.f, 0.f, 0.f}, y[MLP_OUT];
+    float xin[MLP_X] = {0.f, 0.f}, y[MLP_OUT];
 #pragma unroll
     for (int j = 0; j < MLP_OUT; ++j) y[j] = 0.0f;
     if (live) {
-        xin[0] = x[3 * (t0 + tid)], xin[1] = x[3 * (t0 + tid) + 1], xin[2] = x[3 * (t0 + tid) + 2];
+        xin[0] = x[MLP_X * (t0 + tid)], xin[1] = x[MLP_X * (t0 + tid) + 1];
         mlp_forward_row(P, xin, z1 + tid * TR_LD, z2 + tid * TR_LD, z3 + tid * TR_LD, y);
     }
     // loss (q0 - t0)^2 + vw |q_vec - t_vec|^2 + cw |c - t_c|^2 with q = y[0:4]/|y[0:4]| (vw weights the vector
@@ -367,7 +393,12 @@ __global__ void __launch_bounds__(TR_T, 1) bp_mlp_grad_kernel(const float* __res
         for (int k = 0; k < MLP_H; ++k) z1[tid * TR_LD + k] = 0.0f;
     }
     __syncthreads();  // buf (a1) consumed; dz1 complete
-    buf[tid * TR_LD] = xin[0], buf[tid * TR_LD + 1] = xin[1], buf[tid * TR_LD + 2] = xin[2];
+    {
+        float gf[MLP_IN];
+        mlp_features(xin[0], xin[1], gf);
+#pragma unroll
+        for (int i = 0; i < MLP_IN; ++i) buf[tid * TR_LD + i] = live ? gf[i] : 0.0f;
+    }
     __syncthreads();
     weight_grads(z1, buf, MLP_IN, nt, g, P_W1, P_B1, tid);
 }
@@ -438,7 +469,7 @@ extern "C" int bp_adam(float* params, const float* grad, float* m, float* v, flo
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
-// Network outputs for normalised inputs x [n][3] -> y [n][16] (the quaternion part normalised to unit length):
+// Network outputs for inputs x [n][2] (f^, b^) -> y [n][16] (the quaternion part normalised to unit length):
 // inference for checks.
 __global__ void __launch_bounds__(128) bp_mlp_eval_kernel(const float* __restrict__ params, const float* __restrict__ x,
                                                          int n, float* __restrict__ y) {
@@ -447,7 +478,7 @@ __global__ void __launch_bounds__(128) bp_mlp_eval_kernel(const float* __restric
     __syncthreads();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const float xin[3] = {x[3 * t], x[3 * t + 1], x[3 * t + 2]};
+    const float xin[MLP_X] = {x[MLP_X * t], x[MLP_X * t + 1]};
     float o[MLP_OUT];
     mlp_forward_row(P, xin, nullptr, nullptr, nullptr, o);
     const float inv = rsqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
@@ -473,7 +504,16 @@ struct PulseArgs {
     float b0off;          // the occurrence's uniform off-resonance [Hz]
     int* counts;          // null or [2]: spins through the network, spins through the fallback
     float dom_df, dom_b1, dom_z;  // the network's training domain
+    double fmax;                  // dom_df + |gz| dom_z thickness: the scale of the input f^
 };
+
+// The network's inputs (f^, b^) of a spin (f^ clamped to [-1, 1]: rows outside the domain, whose outputs are not
+// used, stay finite).
+__device__ __forceinline__ void pulse_inputs(const PulseArgs& a, const Spin& p, float df, float x[MLP_X]) {
+    const float fh = (float)(((double)df + a.gz * ((double)p.pz - a.z0)) / a.fmax);
+    x[0] = fminf(fmaxf(fh, -1.f), 1.f);
+    x[1] = fminf(fmaxf((p.b1 - 1.0f) / a.dom_b1, -1.f), 1.f);
+}
 
 // The plain sub-stepped pulse for spin j (the fallback outside the domain).
 __device__ __forceinline__ void fallback_spin(const PulseArgs& a, int j) {
@@ -579,7 +619,8 @@ __global__ void __launch_bounds__(128) bp_surrogate_pulse_kernel(PulseArgs a) {
     float mx = a.state[j], my = a.state[a.n + j], mz = a.state[2 * a.n + j];
     float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
     if (inside) {
-        const float xin[3] = {df / a.dom_df, (p.b1 - 1.0f) / a.dom_b1, zr / a.dom_z};
+        float xin[MLP_X];
+        pulse_inputs(a, p, df, xin);
         float y[MLP_OUT];
         mlp_forward_row(P, xin, nullptr, nullptr, nullptr, y);
         apply_pulse_map(y, a, p, df, mx, my, mz, lx, ly, lz);
@@ -603,39 +644,54 @@ extern "C" int bp_surrogate_pulse(const float* spins, float* state, int n, const
         !(dom_df > 0) || !(dom_b1 > 0) || !(dom_z > 0))
         return BP_E_ARG;
     PulseArgs a{spins, state, params, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0, phi0,
-                b0off, counts, dom_df, dom_b1, dom_z};
+                b0off, counts, dom_df, dom_b1, dom_z, dom_df + fabs(gz) * dom_z * thickness};
     bp_surrogate_pulse_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
-// ---- inference on the tensor cores: layers 2 and 3 (64 x 64) as tcgen05 matrix products ----
+// ---- inference on the tensor cores: all four layers as tcgen05 matrix products ----
 //
-// Per CTA tile of 128 spins (thread t = spin row t = tensor-memory lane t): layer 1 on the CUDA cores, its
-// GELU outputs split into bfloat16 high and low parts and stored as the A operand (128 x 64, K-major); layer 2 is
-// D = A_hi W2_hi^T + A_hi W2_lo^T + A_lo W2_hi^T (M = 128, N = 64, K = 64 in 4 steps, float32 in 64 tensor-memory
-// columns); each thread reads its row of D back (tcgen05.ld), adds the bias, applies GELU and stores the next A;
-// layer 3 likewise; layer 4 (64 -> 4) on the CUDA cores. Shared memory: W2 hi, W2 lo, W3 hi, W3 lo (8192 bytes
-// each, [0, 32768)), A hi and A lo (16384 each, [32768, 65536)), the fallback queue, mbarriers. W1, W4 and the
-// biases travel in the kernel's arguments (the constant bank). Layout of every
-// operand: core matrices of 8 rows x 16 bytes, K-adjacent ones 128 bytes apart, 8-row groups 1024 bytes apart; a
-// thread writes its row 16 bytes at a time, so the 8 lanes of each store phase fill one 128-byte line.
+// Per CTA tile of 128 spins (thread t = spin row t = tensor-memory lane t), four rounds, one per layer: every
+// thread stores its row of the layer's input, split into bfloat16 high and low parts, as the A operand (K-major),
+// one thread issues D = A_hi W_hi^T + A_hi W_lo^T + A_lo W_hi^T (M = 128, float32 accumulation in tensor memory),
+// and every thread reads its row of D back (tcgen05.ld) and adds the bias (and GELU for layers 1 to 3):
+//   layer 1: the 14 input features, zero-padded to K = 16 (one K step), N = 64, D in columns [0, 64);
+//   layers 2 and 3: K = 64 (4 steps), N = 64, D in columns [0, 64);
+//   layer 4: K = 64, N = 16, D in columns [64, 80).
+// Shared memory: W2 hi, W2 lo, W3 hi, W3 lo (8192 bytes each, [0, 32768)), W1 hi, W1 lo ([32768, 36864)), W4 hi,
+// W4 lo ([36864, 40960)), A hi and A lo (16384 each, [40960, 73728)), the fallback queue, mbarriers. The biases
+// travel in the kernel's arguments (the constant bank). Layout of every operand: core matrices of 8 rows x 16
+// bytes, K-adjacent ones 128 bytes apart, 8-row groups 1024 bytes apart (W1: 256, its rows being 16 wide); a thread
+// writes its row 16 bytes at a time, so the 8 lanes of each store phase fill one 128-byte line.
 #include "tcgen05.cuh"
 
-#define SI_W_BYTES 8192
-#define SI_OFF_A 32768
+#define SI_W_BYTES 8192                         // W2 or W3, one half (hi or lo)
+#define SI_W1_BYTES 2048                        // W1 (64 x 16), one half
+#define SI_W4_BYTES 2048                        // W4 (16 x 64), one half
+#define SI_OFF_W1 (4 * SI_W_BYTES)              // 32768
+#define SI_OFF_W4 (SI_OFF_W1 + 2 * SI_W1_BYTES) // 36864
+#define SI_WT_BYTES (SI_OFF_W4 + 2 * SI_W4_BYTES)  // 40960: every weight tile, one bulk copy
+#define SI_OFF_A SI_WT_BYTES
 #define SI_A_BYTES 16384
-#define SI_OFF_LIST 65536  // queued fallback spins (256 ints), after the A operand
+#define SI_OFF_LIST (SI_OFF_A + 2 * SI_A_BYTES)  // queued fallback spins (256 ints), after the A operand
 #define SI_LIST 256
 #define SI_OFF_BAR (SI_OFF_LIST + SI_LIST * 4)
 #define SI_SMEM (SI_OFF_BAR + 64)
 #define SI_LBO 128
 #define SI_SBO 1024
-#define SI_COLS 64
+#define SI_SBO_W1 256
+#define SI_COLS 128   // tensor-memory columns: D of layers 1 to 3 in [0, 64), of layer 4 in [64, 80)
+#define SI_D4 64
+#define SI_K1 16      // layer 1's K: the features, zero-padded
 
-// 64 activations of this thread's row -> A hi and A lo rows (16-byte stores)
+static_assert(SI_OFF_A % 1024 == 0 && SI_OFF_W1 % 16 == 0 && SI_OFF_W4 % 16 == 0, "operand alignment");
+static_assert(MLP_IN <= SI_K1, "layer 1 fits one K step");
+
+// NCH x 8 values of this thread's row -> A hi and A lo rows, chunks [0, NCH) (16-byte stores)
+template <int NCH>
 __device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned char* alo, int row, const float* v) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
+    for (int c = 0; c < NCH; ++c) {
         uint32_t h[4], l[4];
 #pragma unroll
         for (int w = 0; w < 4; ++w) {  // a pair: hi = bf16(v) (nearest), lo = bf16(v - hi), two values per conversion
@@ -652,15 +708,15 @@ __device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned ch
     }
 }
 
-// The network's small parameters, passed by value in the kernel's arguments (5,696 bytes of the constant bank):
-// every thread reads the same weight at the same time, so the FMAs take them as constant operands, no loads.
+// The network's biases, passed by value in the kernel's arguments (832 bytes of the constant bank): every thread
+// reads the same bias at the same time, so the adds take them as constant operands, no loads.
 struct SmallNet {
-    float w1[MLP_H * MLP_IN], b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_OUT * MLP_H], b4[MLP_OUT];
+    float b1[MLP_H], b2[MLP_H], b3[MLP_H], b4[MLP_OUT];
 };
 
 struct PulseMmaArgs {
-    PulseArgs p;            // (p.params unused: the small parameters are in net, W2 and W3 in wtiles)
-    const uint8_t* wtiles;  // [4][8192]: W2 hi, W2 lo, W3 hi, W3 lo in the operand layout (bp_mlp_wtiles)
+    PulseArgs p;            // (p.params unused: the biases are in net, the weights in wtiles)
+    const uint8_t* wtiles;  // SI_WT_BYTES: W2 hi, W2 lo, W3 hi, W3 lo, W1 hi, W1 lo, W4 hi, W4 lo (bp_mlp_wtiles)
     int* status;
     SmallNet net;
 };
@@ -676,7 +732,6 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
     unsigned char* alo = smb + SI_OFF_A + SI_A_BYTES;
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t sW = smem_u32(smb), sA = smem_u32(ahi);
-    const uint32_t idesc = umma_idesc_bf16_f32(128, MLP_H);
 
     const SmallNet& net = args.net;
     if (tid == 0) {
@@ -685,8 +740,8 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
         mbar_init(&bars[1], 1);
         fence_mbar_init();
         fence_proxy_async_smem();
-        mbar_expect_tx(&bars[0], 4 * SI_W_BYTES);
-        tma_load_1d(smb, args.wtiles, 4 * SI_W_BYTES, &bars[0]);
+        mbar_expect_tx(&bars[0], SI_WT_BYTES);
+        tma_load_1d(smb, args.wtiles, SI_WT_BYTES, &bars[0]);
     }
     if (warp == 0) tmem_alloc(tmem_slot, SI_COLS);
     tc_fence_before();
@@ -707,18 +762,20 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
         const float df = p.db0 + a.b0off;
         const float zr = (float)(((double)p.pz - a.z0) / a.thickness);
         const bool inside = active && fabsf(df) <= a.dom_df && fabsf(p.b1 - 1.0f) <= a.dom_b1 && fabsf(zr) <= a.dom_z;
-        float v[MLP_H];
-        {   // layer 1 (the inputs of rows outside the domain are clamped: their outputs are not used)
-            const float x0 = fminf(fmaxf(df / a.dom_df, -1.f), 1.f);
-            const float x1 = fminf(fmaxf((p.b1 - 1.0f) / a.dom_b1, -1.f), 1.f);
-            const float x2 = fminf(fmaxf(zr / a.dom_z, -1.f), 1.f);
+        float v[MLP_H], y[MLP_OUT];
+        {   // layer 1's input: the features, zero-padded to 16
+            float xin[MLP_X];
+            pulse_inputs(a, p, df, xin);
+            mlp_features(xin[0], xin[1], v);
 #pragma unroll
-            for (int k = 0; k < MLP_H; ++k)
-                v[k] = gelu_f(fmaf(net.w1[3 * k], x0, fmaf(net.w1[3 * k + 1], x1, fmaf(net.w1[3 * k + 2], x2, net.b1[k]))));
+            for (int i = MLP_IN; i < SI_K1; ++i) v[i] = 0.0f;
         }
 #pragma unroll
-        for (int layer = 0; layer < 2; ++layer) {  // unrolled: the biases are indexed by constants
-            store_row_bf16x2(ahi, alo, tid, v);
+        for (int layer = 0; layer < 4; ++layer) {  // unrolled: operands, shapes and biases are constants per layer
+            if (layer == 0)
+                store_row_bf16x2<SI_K1 / 8>(ahi, alo, tid, v);
+            else
+                store_row_bf16x2<MLP_H / 8>(ahi, alo, tid, v);
             fence_proxy_async_smem();
             tc_fence_before();
             if (__syncthreads_or(err)) {
@@ -730,14 +787,21 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
                 w_ready = true;
                 if (!err) {
                     tc_fence_after();
-                    const uint32_t wh = sW + (uint32_t)(2 * layer) * SI_W_BYTES, wl = wh + SI_W_BYTES;
+                    const uint32_t wh = layer == 0 ? sW + SI_OFF_W1
+                                      : layer == 3 ? sW + SI_OFF_W4
+                                                   : sW + (uint32_t)(2 * (layer - 1)) * SI_W_BYTES;
+                    const uint32_t wl = wh + (layer == 0 ? SI_W1_BYTES : layer == 3 ? SI_W4_BYTES : SI_W_BYTES);
+                    const uint32_t sbo_w = layer == 0 ? SI_SBO_W1 : SI_SBO;
+                    const uint32_t idesc = umma_idesc_bf16_f32(128, layer == 3 ? MLP_OUT : MLP_H);
+                    const uint32_t d = tmem + (layer == 3 ? SI_D4 : 0u);
                     uint64_t ah_d = umma_desc(sA, SI_LBO, SI_SBO), al_d = umma_desc(sA + SI_A_BYTES, SI_LBO, SI_SBO);
-                    uint64_t bh_d = umma_desc(wh, SI_LBO, SI_SBO), bl_d = umma_desc(wl, SI_LBO, SI_SBO);
+                    uint64_t bh_d = umma_desc(wh, SI_LBO, sbo_w), bl_d = umma_desc(wl, SI_LBO, sbo_w);
+                    const int k_steps = layer == 0 ? SI_K1 / 16 : MLP_H / 16;
 #pragma unroll
-                    for (int kk = 0; kk < MLP_H / 16; ++kk) {
-                        umma_bf16(tmem, ah_d, bh_d, idesc, kk > 0 ? 1u : 0u);
-                        umma_bf16(tmem, ah_d, bl_d, idesc, 1u);
-                        umma_bf16(tmem, al_d, bh_d, idesc, 1u);
+                    for (int kk = 0; kk < k_steps; ++kk) {
+                        umma_bf16(d, ah_d, bh_d, idesc, kk > 0 ? 1u : 0u);
+                        umma_bf16(d, ah_d, bl_d, idesc, 1u);
+                        umma_bf16(d, al_d, bh_d, idesc, 1u);
                         ah_d += 2 * SI_LBO / 16, al_d += 2 * SI_LBO / 16, bh_d += 2 * SI_LBO / 16, bl_d += 2 * SI_LBO / 16;
                     }
                     umma_commit(&bars[1]);
@@ -755,13 +819,22 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
                 break;
             }
             tc_fence_after();
+            if (layer < 3) {
 #pragma unroll
-            for (int c0 = 0; c0 < MLP_H; c0 += 16) {
+                for (int c0 = 0; c0 < MLP_H; c0 += 16) {
+                    float d[16];
+                    tmem_ld16(lane_addr + (uint32_t)c0, d);
+                    tmem_ld_wait();
+                    const float* b = layer == 0 ? net.b1 : layer == 1 ? net.b2 : net.b3;
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) v[c0 + i] = gelu_f(d[i] + b[c0 + i]);
+                }
+            } else {
                 float d[16];
-                tmem_ld16(lane_addr + (uint32_t)c0, d);
+                tmem_ld16(lane_addr + (uint32_t)SI_D4, d);
                 tmem_ld_wait();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) v[c0 + i] = gelu_f(d[i] + (layer == 0 ? net.b2[c0 + i] : net.b3[c0 + i]));
+                for (int o = 0; o < MLP_OUT; ++o) y[o] = d[o] + net.b4[o];
             }
             tc_fence_before();
         }
@@ -769,14 +842,6 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
         if (inside) {
             float mx = a.state[j], my = a.state[a.n + j], mz = a.state[2 * a.n + j];
             float lx = a.state[3 * a.n + j], ly = a.state[4 * a.n + j], lz = a.state[5 * a.n + j];
-            float y[MLP_OUT];
-#pragma unroll
-            for (int o = 0; o < MLP_OUT; ++o) {
-                float s = net.b4[o];
-#pragma unroll
-                for (int i = 0; i < MLP_H; ++i) s = fmaf(net.w4[MLP_H * o + i], v[i], s);
-                y[o] = s;
-            }
             apply_pulse_map(y, a, p, df, mx, my, mz, lx, ly, lz);
             a.state[j] = mx, a.state[a.n + j] = my, a.state[2 * a.n + j] = mz;
             a.state[3 * a.n + j] = lx, a.state[4 * a.n + j] = ly, a.state[5 * a.n + j] = lz;
@@ -817,25 +882,44 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
     }
 }
 
-// W2 and W3 -> four 8192-byte bfloat16 tiles (W2 hi, W2 lo, W3 hi, W3 lo) in the operand layout: row n (output
-// unit) and column k (input unit) at element (n / 8) 512 + (k / 8) 64 + (n % 8) 8 + k % 8.
+// The weights -> bfloat16 high / low tiles in the operand layout, row n (output unit), column k (input unit):
+//   W2, W3 (64 x 64): element (n / 8) 512 + (k / 8) 64 + (n % 8) 8 + k % 8 of tiles 0-1 (W2 hi, lo) and 2-3 (W3);
+//   W1 (64 x 16, columns 14 and 15 zero): element (n / 8) 128 + (k / 8) 64 + (n % 8) 8 + k % 8 of tiles 4-5;
+//   W4 (16 x 64): as W2, of tiles 6-7.
+#define WT_N23 (2 * MLP_H * MLP_H)
+#define WT_N1 (MLP_H * SI_K1)
+#define WT_N4 (MLP_OUT * MLP_H)
 __global__ void bp_mlp_wtiles_kernel(const float* __restrict__ params, uint16_t* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 2 * MLP_H * MLP_H) return;
-    const int l = i / (MLP_H * MLP_H), r = i % (MLP_H * MLP_H), n = r / MLP_H, k = r % MLP_H;
+    if (i >= WT_N23 + WT_N1 + WT_N4) return;
     uint16_t h, lo;
-    split_bf16(params[(l ? P_W3 : P_W2) + r], h, lo);
-    const int e = (n >> 3) * 512 + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
-    out[(2 * l) * (SI_W_BYTES / 2) + e] = h;
-    out[(2 * l + 1) * (SI_W_BYTES / 2) + e] = lo;
+    int base, half, e;
+    if (i < WT_N23) {
+        const int l = i / (MLP_H * MLP_H), r = i % (MLP_H * MLP_H), n = r / MLP_H, k = r % MLP_H;
+        split_bf16(params[(l ? P_W3 : P_W2) + r], h, lo);
+        base = 2 * l * (SI_W_BYTES / 2), half = SI_W_BYTES / 2;
+        e = (n >> 3) * 512 + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
+    } else if (i < WT_N23 + WT_N1) {
+        const int r = i - WT_N23, n = r / SI_K1, k = r % SI_K1;
+        split_bf16(k < MLP_IN ? params[P_W1 + MLP_IN * n + k] : 0.0f, h, lo);
+        base = SI_OFF_W1 / 2, half = SI_W1_BYTES / 2;
+        e = (n >> 3) * 128 + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
+    } else {
+        const int r = i - WT_N23 - WT_N1, n = r / MLP_H, k = r % MLP_H;
+        split_bf16(params[P_W4 + r], h, lo);
+        base = SI_OFF_W4 / 2, half = SI_W4_BYTES / 2;
+        e = (n >> 3) * 512 + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
+    }
+    out[base + e] = h;
+    out[base + half + e] = lo;
 }
 
-extern "C" int bp_mlp_wtiles_bytes(void) { return 4 * SI_W_BYTES; }
+extern "C" int bp_mlp_wtiles_bytes(void) { return SI_WT_BYTES; }
 
 extern "C" int bp_mlp_wtiles(const float* params, void* tiles, void* stream) {
     if (!params || !tiles) return BP_E_ARG;
     if ((reinterpret_cast<uintptr_t>(tiles) & 15) != 0) return BP_E_ALIGN;
-    bp_mlp_wtiles_kernel<<<(2 * MLP_H * MLP_H + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    bp_mlp_wtiles_kernel<<<(WT_N23 + WT_N1 + WT_N4 + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         params, static_cast<uint16_t*>(tiles));
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
@@ -897,13 +981,11 @@ extern "C" int bp_surrogate_pulse_mma(const float* spins, float* state, int n, c
     const int code = pulse_mma_grid(n, max_ctas, &grid);
     if (code != BP_OK) return code;
     PulseMmaArgs a{{spins, state, nullptr, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0,
-                    phi0, b0off, counts, dom_df, dom_b1, dom_z},
+                    phi0, b0off, counts, dom_df, dom_b1, dom_z, dom_df + fabs(gz) * dom_z * thickness},
                    static_cast<const uint8_t*>(wtiles), status, {}};
-    std::memcpy(a.net.w1, params_host + P_W1, sizeof(a.net.w1));
     std::memcpy(a.net.b1, params_host + P_B1, sizeof(a.net.b1));
     std::memcpy(a.net.b2, params_host + P_B2, sizeof(a.net.b2));
     std::memcpy(a.net.b3, params_host + P_B3, sizeof(a.net.b3));
-    std::memcpy(a.net.w4, params_host + P_W4, sizeof(a.net.w4));
     std::memcpy(a.net.b4, params_host + P_B4, sizeof(a.net.b4));
     bp_surrogate_pulse_mma_kernel<<<grid, 128, SI_SMEM, static_cast<cudaStream_t>(stream)>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;

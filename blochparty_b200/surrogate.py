@@ -3,17 +3,19 @@ sub-stepped integration (``simulate(..., pulses="surrogate", surrogate=[...])``)
 
 The reference has no learned part; its nearest mechanism is the exact per-spin map of a reused pulse
 (blochparty ``engines/gpu/driver.py:112-164``, ``engines/gpu/cuda/pulse.cu.in:3-32``). Here each distinct pulse
-waveform (dt, slice gradient G along z, RF samples) gets a 3 -> 64 -> 64 -> 64 -> 4 GELU network mapping
-(off-resonance df, B1 scale, slice position z_rel = (z - z0) / thickness) to the unit quaternion (the Cayley-Klein
-pair) of the pulse's rotation reduced by its free precession, R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T.
-The targets come from the plain integrator (``bp_pulse_quats``: the per-step rotations composed in float64); the
-network is trained by the hand-written kernels ``bp_mlp_grad`` / ``bp_mlp_reduce`` / ``bp_adam``.
+waveform (dt, slice gradient G along z, RF samples) gets a 14 -> 64 -> 64 -> 64 -> 16 GELU network. Its inputs are
+the spin's off-resonance in the slice gradient f = df + G (z - z0) and its B1 scale (the pulse depends on nothing
+else), seen by the first layer with Fourier features of f. Its outputs are the unit quaternion (the Cayley-Klein
+pair) of the pulse's rotation reduced by its free precession, R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T,
+and the pulse's first-order relaxation terms beyond the relax / rotate / relax splitting. The targets come from the
+plain integrator (``bp_pulse_targets``: the per-step maps composed in float64); the network is trained by the
+hand-written kernels ``bp_mlp_grad`` / ``bp_mlp_reduce`` / ``bp_adam``.
 
 In a simulation, every occurrence of a trained pulse (the same dt and gradient, RF = trained waveform x exp(i phi0),
 uniform b0_offset, no sample or spoil inside) is applied by ``bp_surrogate_pulse``: spins inside the training
 domain (by default |df| <= 200 Hz, |b1 - 1| <= 0.3, |z_rel| <= 2; a network's own ``domain`` otherwise) take the
-network's rotation between two half-pulse relaxations; the others take the plain sub-stepped segments (the fallback,
-which is also the judge: the plain simulation is the same call without the surrogate).
+network's rotation between two half-pulse relaxations, with its first-order relaxation terms; the others take the
+plain sub-stepped segments (the fallback; the plain simulation is the same call without the surrogate).
 """
 
 from __future__ import annotations
@@ -36,7 +38,7 @@ def _fan_in_init(seed: int) -> torch.Tensor:
     """Flat initial parameters: weights N(0, 1/fan_in), biases 0 (seeded)."""
     g = torch.Generator().manual_seed(seed)
     parts = []
-    for shape in ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (16, 64), (16,)):
+    for shape in ((64, 14), (64,), (64, 64), (64,), (64, 64), (64,), (16, 64), (16,)):
         if len(shape) == 2:
             parts.append(torch.randn(shape, generator=g, dtype=F64).reshape(-1) / math.sqrt(shape[1]))
         else:
@@ -112,9 +114,17 @@ class RFSurrogate:
         _lib.check(code, "bp_pulse_targets")
         return (tg, qfull) if full else tg
 
+    @property
+    def fmax(self) -> float:
+        """The largest |f| = |df + G (z - z0)| [Hz] of the training domain: the scale of the input f^."""
+        return self.domain[0] + abs(self.gz) * self.domain[2] * self.thickness
+
     def normalise(self, samples: torch.Tensor) -> torch.Tensor:
-        s, d = samples, self.domain
-        return torch.stack([s[:, 0] / d[0], (s[:, 1] - 1) / d[1], s[:, 2] / d[2]], -1).contiguous()
+        """The network's inputs (n, 2) of samples (df, b1, z_rel): f^ = (df + G z_rel thickness) / F and
+        b^ = (b1 - 1) / dom_b1 (float64 arithmetic, rounded once)."""
+        s, d = samples.to(F64), self.domain
+        f = (s[:, 0] + self.gz * self.thickness * s[:, 2]) / self.fmax
+        return torch.stack([f, (s[:, 1] - 1) / d[1]], -1).to(F32).contiguous()
 
     def gradient(self, x: torch.Tensor, target: torch.Tensor, vweight: float = 1.0, cweight: float = 1.0):
         """(mean loss, gradient) of the batch through the training kernels (x normalised; ``vweight`` weights the
@@ -131,9 +141,11 @@ class RFSurrogate:
         _lib.check(lib.bp_mlp_reduce(ptr(gpart), ptr(lpart), ctas, 1.0 / n, ptr(grad), ptr(loss), st), "bp_mlp_reduce")
         return loss, grad
 
-    def train(self, n_samples: int = 1 << 20, epochs: int = 400, batch: int = 16384, lr: float = 2e-3,
-              lr_min: float = 3e-5, seed: int | None = None) -> TrainLog:
-        """Adam with a cosine learning-rate decay over ``epochs`` passes of ``n_samples`` plain-integrator targets.
+    def train(self, n_samples: int = 1 << 20, epochs: int = 400, batch: int = 4096, lr: float = 4e-3,
+              lr_min: float = 1e-6, seed: int | None = None) -> TrainLog:
+        """Adam with a cosine learning-rate decay over ``epochs`` passes of ``n_samples`` plain-integrator targets
+        (the defaults: 102,400 steps of 4,096 samples, about 16 s on one B200; the decay down to 1e-6 matters,
+        since Adam's steps of about the learning rate per weight set the error floor).
         The loss weights the quaternion's vector part by 1 / s^2, s its largest magnitude among the targets (clipped
         to [1e-2, 1]): a small rotation (a 10-degree excitation) is then learned to a relative, not an absolute,
         precision."""

@@ -148,16 +148,19 @@ int bp_pulse_apply(const double* maps, int n, float* state, double phase, void* 
 
 /* ---- learned RF surrogate (no counterpart in the reference; its nearest part is the exact per-spin map of a
  * reused pulse, engines/gpu/cuda/pulse.cu.in:3-32) ----
- * A 3 -> 64 -> 64 -> 64 -> 16 GELU network per shaped pulse: inputs (df / dom_df, (b1 - 1) / dom_b1,
- * z_rel / dom_z) with z_rel = (z - z0) / slice thickness and the network's training domain (dom_df, dom_b1, dom_z)
- * (the host side's default: 200 Hz, 0.3, 2). Outputs:
+ * A 14 -> 64 -> 64 -> 64 -> 16 GELU network per shaped pulse. The training domain (dom_df, dom_b1, dom_z) bounds
+ * |df| [Hz], |b1 - 1| and |z_rel| = |z - z0| / slice thickness (the host side's default: 200 Hz, 0.3, 2). A pulse
+ * acts on a spin through f = df + G (z - z0) and b1 alone, so the inputs x are (f^, b^) = (f / F, (b1 - 1) / dom_b1),
+ * F = dom_df + |G| dom_z thickness; the 14 features of the first layer are f^, b^, sin(k pi f^), cos(k pi f^) for
+ * k = 1..6 (Fourier features). Outputs:
  *   [0, 4)   a unit quaternion (q0, q1, q2, q3), the Cayley-Klein pair alpha = q0 - i q3, beta = -i (q1 + i q2), of
  *            the pulse's rotation reduced by its free precession: R = Rz(wz/2) R~ Rz(wz/2), wz = -2 pi (G z + df) T;
  *   [4, 13)  dA~ / T (row-major), [13, 16) dC~ / T: the pulse's first-order relaxation terms beyond the relax (T/2)
  *            / rotate / relax (T/2) splitting, reduced like R (the pulse maps m to E (R - (r2 - r1) dA)(E m + c) +
  *            c + r1 pd dC, E and c the half-pulse relaxation and recovery).
- * Parameters: BP_MLP_PARAMS floats, W1 (64x3), b1, W2 (64x64), b2, W3 (64x64), b3, W4 (16x64), b4 (16). */
-#define BP_MLP_PARAMS 9616
+ * Parameters: BP_MLP_PARAMS floats, W1 (64x14), b1, W2 (64x64), b2, W3 (64x64), b3, W4 (16x64), b4 (16). */
+#define BP_MLP_PARAMS 10320
+#define BP_MLP_INPUTS 2
 #define BP_MLP_OUTPUTS 16
 
 /* Training targets from the plain integrator: samples [n][3] (df [Hz], b1, z_rel) -> targets [n][16] (the outputs
@@ -165,7 +168,7 @@ int bp_pulse_apply(const double* maps, int n, float* state, double phase, void* 
 int bp_pulse_targets(const double* rf, int k_steps, double dt, double gz, double thickness, double z0,
                      const float* samples, int n, float* targets, float* qfull, void* stream);
 
-/* One training step's gradient: x [n][3] normalised inputs, target [n][16]; loss (q0 - t0)^2 + vweight |q_vec -
+/* One training step's gradient: x [n][2] inputs (f^, b^), target [n][16]; loss (q0 - t0)^2 + vweight |q_vec -
  * t_vec|^2 + cweight |c - t_c|^2 per sample (q the normalised quaternion, c the 12 correction outputs; vweight > 0
  * weights the vector part: relative precision for small rotations); per-CTA partials gpart
  * [bp_mlp_grad_ctas(n)][BP_MLP_PARAMS] and loss sums lpart [bp_mlp_grad_ctas(n)] (scratch of the caller). */
@@ -178,7 +181,7 @@ int bp_mlp_reduce(const float* gpart, const float* lpart, int n_cta, float scale
 /* Adam step number `step` (1-based) on params with moments m, v. */
 int bp_adam(float* params, const float* grad, float* m, float* v, float lr, float beta1, float beta2, float eps,
             int step, void* stream);
-/* The network's outputs y [n][16] (the quaternion normalised) for normalised inputs x [n][3]. */
+/* The network's outputs y [n][16] (the quaternion normalised) for inputs x [n][2] (f^, b^). */
 int bp_mlp_eval(const float* params, const float* x, int n, float* y, void* stream);
 
 /* One pulse occurrence (segments [seg0, seg0 + k_steps) of `segs`, the trained waveform times exp(i phi0), slice

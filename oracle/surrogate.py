@@ -14,7 +14,9 @@ Conventions (shared with ``blochparty_b200/csrc/surrogate.cu``):
   beta = -i (q1 + i q2);
 * the pulse's whole precession without RF is the z rotation by wz = -2 pi (G z + df) T; the network learns
   the reduced rotation R~ with R = Rz(wz / 2) R~ Rz(wz / 2), smooth in z where R itself winds around z;
-* inputs normalised to [-1, 1]: (df / 200 Hz, (b1 - 1) / 0.3, z_rel / 2), z_rel = z / slice thickness;
+* the pulse acts on a spin through its off-resonance in the slice gradient f = df + G (z - z0) and its B1 scale
+  alone: the network's inputs are (f^, b^) = (f / F, (b1 - 1) / dom_b1) with F the largest |f| of the training
+  domain, and its first layer sees the 14 features f^, b^, sin(k pi f^), cos(k pi f^), k = 1..6;
 * relaxation during the pulse, to first order in the rates: the plain integrator's pulse is the affine map
   m -> M m + v with M = R - r2 A - r1 B + O(r^2), v = r1 pd C + O(r^2); A + B = T R, so the network learns what
   the relax (T/2) / rotate / relax (T/2) splitting misses, dA = A - (T/2)(P R + R P) (P = diag(1, 1, 0)) and
@@ -121,9 +123,10 @@ def gelu(x):
     return 0.5 * x * (1.0 + torch.tanh(math.sqrt(2.0 / math.pi) * (x + 0.044715 * x ** 3)))
 
 
-# parameter layout of the flat vector (as the kernels): W1 (64, 3), b1 (64), W2 (64, 64), b2, W3 (64, 64), b3,
-# W4 (16, 64), b4 (16): 9,616 floats
-SHAPES = ((64, 3), (64,), (64, 64), (64,), (64, 64), (64,), (16, 64), (16,))
+# parameter layout of the flat vector (as the kernels): W1 (64, 14), b1 (64), W2 (64, 64), b2, W3 (64, 64), b3,
+# W4 (16, 64), b4 (16): 10,320 floats
+SHAPES = ((64, 14), (64,), (64, 64), (64,), (64, 64), (64,), (16, 64), (16,))
+FOURIER_ORDERS = 6
 N_PARAMS = sum(math.prod(s) for s in SHAPES)
 
 
@@ -136,11 +139,21 @@ def unflatten(p):
     return out
 
 
+def features(x):
+    """The first layer's features (B, 14) of inputs x (B, 2) = (f^, b^): f^, b^, then sin(k pi f^), cos(k pi f^) for
+    k = 1..6 (the kernels' ``mlp_features``, which builds the higher orders by angle addition)."""
+    f = x[:, :1]
+    k = torch.arange(1, FOURIER_ORDERS + 1, dtype=x.dtype)
+    a = math.pi * f * k
+    sc = torch.stack([torch.sin(a), torch.cos(a)], -1).reshape(x.shape[0], 2 * FOURIER_ORDERS)
+    return torch.cat([x, sc], -1)
+
+
 def mlp(p, x):
-    """Network output (B, 16) for normalised inputs x (B, 3): the quaternion (normalised to unit length), then the
+    """Network output (B, 16) for inputs x (B, 2) = (f^, b^): the quaternion (normalised to unit length), then the
     12 correction outputs as they are."""
     w1, b1, w2, b2, w3, b3, w4, b4 = unflatten(p)
-    h = gelu(x @ w1.T + b1)
+    h = gelu(features(x) @ w1.T + b1)
     h = gelu(h @ w2.T + b2)
     h = gelu(h @ w3.T + b3)
     y = h @ w4.T + b4

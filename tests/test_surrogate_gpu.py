@@ -7,7 +7,8 @@ within 1e-4 (largest relative error) of float64 autograd; tensor-core inference 
 (magnetization, unit PD scale), the fallback spins bit-identical; the TSE and the 3D GRE through the surrogate
 within 1e-3 relative L2 of the float64 oracle (whole-pulse relax / rotate / relax splitting alone is 2.3e-2 off on
 the TSE's refocusing train; the networks' first-order relaxation terms bring the splitting to 1.0e-4, measured by a
-float64 CPU emulation with exact terms); and a measured speed-up over plain sub-stepping on the same GPU.
+float64 CPU emulation with exact terms, so the rest is the networks' own error: the refocusing pulses' rotations
+dominate it); and a measured speed-up over plain sub-stepping on the same GPU.
 """
 
 import math
@@ -90,8 +91,8 @@ def test_training_lowers_the_loss_and_the_error():
 
 @pytest.fixture(scope="module")
 def tse_surrogates():
-    """Networks for the six TSE pulses (3 slices x excitation / refocusing), trained on 2^20 samples each (400
-    epochs, ~6 s per pulse) over |z_rel| <= 2.5: the slices are contiguous, so every spin of the 3-slice stack lies
+    """Networks for the six TSE pulses (3 slices x excitation / refocusing), trained on 2^20 samples each (600
+    epochs of 4,096-sample steps, ~24 s per pulse) over |z_rel| <= 2.5: the slices are contiguous, so every spin of the 3-slice stack lies
     within 2.5 slice widths of every pulse's centre."""
     out, info = [], []
     for z0 in (-5e-3, 0.0, 5e-3):
@@ -99,7 +100,7 @@ def tse_surrogates():
             w, dt, gz, _ = _pulse(flip, z0, phase)
             sg = surrogate.RFSurrogate(w, dt, gz, 5e-3, domain=(200.0, 0.3, 2.5))
             t = time.perf_counter()
-            sg.train(n_samples=1 << 20, epochs=400, batch=16384)
+            sg.train(epochs=600)
             info.append((flip, z0, time.perf_counter() - t, sg.validate()))
             out.append(sg)
     for flip, z0, sec, (mx, rms, cmx, crms) in info:
@@ -190,16 +191,21 @@ def test_surrogate_gain_on_the_tse_workload(tse_surrogates):
 
 
 def test_weight_tiles_layout():
-    """bp_mlp_wtiles: every W2 / W3 entry is hi + lo at its operand-layout position, hi = bf16(w) (nearest)."""
+    """bp_mlp_wtiles: every weight is hi + lo at its operand-layout position, hi = bf16(w) (nearest); W1's two
+    padding columns are zero."""
     sg = surrogate.RFSurrogate(*_pulse()[:3], 5e-3, seed=21)
-    t = sg.wtiles().cpu().view(torch.int16).view(torch.bfloat16).float().reshape(4, 8, 8, 8, 8)
+    all_ = sg.wtiles().cpu().view(torch.int16).view(torch.bfloat16).float()
+    assert all_.numel() == 16384 + 2048 + 2048
     # element (n / 8) 512 + (k / 8) 64 + (n % 8) 8 + k % 8 -> [n // 8, k // 8, n % 8, k % 8]
-    t = t.permute(0, 1, 3, 2, 4).reshape(4, 64, 64)
-    _, _, w2, _, w3, _, _, _ = S.unflatten(sg.params.cpu())
-    assert torch.equal(t[0], w2.to(torch.bfloat16).float())
-    assert torch.equal(t[2], w3.to(torch.bfloat16).float())
-    assert float(((t[0] + t[1]) - w2).abs().max() / w2.abs().max()) < 2 ** -16
-    assert float(((t[2] + t[3]) - w3).abs().max() / w3.abs().max()) < 2 ** -16
+    t = all_[:16384].reshape(4, 8, 8, 8, 8).permute(0, 1, 3, 2, 4).reshape(4, 64, 64)
+    # W1 (64 x 16): (n / 8) 128 + (k / 8) 64 + (n % 8) 8 + k % 8; W4 (16 x 64) as W2
+    t1 = all_[16384:18432].reshape(2, 8, 2, 8, 8).permute(0, 1, 3, 2, 4).reshape(2, 64, 16)
+    t4 = all_[18432:].reshape(2, 2, 8, 8, 8).permute(0, 1, 3, 2, 4).reshape(2, 16, 64)
+    w1, _, w2, _, w3, _, w4, _ = S.unflatten(sg.params.cpu())
+    w1 = torch.cat([w1, torch.zeros(64, 2)], 1)
+    for hi, lo, w in ((t[0], t[1], w2), (t[2], t[3], w3), (t1[0], t1[1], w1), (t4[0], t4[1], w4)):
+        assert torch.equal(hi, w.to(torch.bfloat16).float())
+        assert float(((hi + lo) - w).abs().max() / w.abs().max()) < 2 ** -16
 
 
 @pytest.mark.parametrize("n,max_ctas", [(300, 0), (300, 1), (5000, 7)])

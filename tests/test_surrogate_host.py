@@ -46,11 +46,11 @@ def test_rf_phase_conjugates_the_reduced_rotation():
 def test_network_oracle_gradient_against_central_differences():
     g = torch.Generator().manual_seed(0)
     p = torch.randn(S.N_PARAMS, generator=g, dtype=F64) * 0.1
-    x = torch.rand(16, 3, generator=g, dtype=F64) * 2 - 1
+    x = torch.rand(16, 2, generator=g, dtype=F64) * 2 - 1
     t = torch.cat([torch.nn.functional.normalize(torch.randn(16, 4, generator=g, dtype=F64), dim=-1),
                    0.1 * torch.randn(16, 12, generator=g, dtype=F64)], -1)
     loss, grad = S.loss_and_grad(p, x, t, vweight=30.0, cweight=0.5)
-    for i in (0, 100, 300, 5000, 8600, 9610):
+    for i in (0, 100, 900, 5000, 9300, 10310):
         e = torch.zeros_like(p)
         e[i] = 1e-6
         fd = (S.loss_and_grad(p + e, x, t, 30.0, 0.5)[0] - S.loss_and_grad(p - e, x, t, 30.0, 0.5)[0]) / 2e-6
