@@ -193,11 +193,11 @@ int bp_surrogate_pulse(const float* spins, float* state, int n, const float* par
                        int k_steps, double T, double gz, double thickness, double z0, double phi0, float b0off,
                        float dom_df, float dom_b1, float dom_z, int32_t* counts, void* stream);
 
-/* The same occurrence with layers 2 and 3 of the network on the tensor cores (tcgen05, split bfloat16: hi x hi +
+/* The same occurrence with all four layers of the network on the tensor cores (tcgen05, split bfloat16: hi x hi +
  * hi x lo + lo x hi, float32 accumulation in tensor memory; 128 spins per tile, persistent CTAs, at most
- * `max_ctas` when > 0). `params_host` is the network in HOST memory (BP_MLP_PARAMS floats): W1, W4 and the biases
- * travel by value in the launch's arguments; `wtiles` (device, 16-byte aligned, bp_mlp_wtiles_bytes()) holds W2
- * and W3 split by bp_mlp_wtiles;
+ * `max_ctas` when > 0). `params_host` is the network in HOST memory (BP_MLP_PARAMS floats): the biases travel by
+ * value in the launch's arguments; `wtiles` (device, 16-byte aligned, bp_mlp_wtiles_bytes() = 40960 bytes) holds
+ * every weight split into bfloat16 high / low tiles by bp_mlp_wtiles (W1 zero-padded to 16 columns);
  * `status` |= 1 when a bounded wait on the weights' copy or an MMA ran out (the CTA then stops, its remaining
  * spins not written). Spins outside the domain are queued per CTA and stepped 128 at a time. bp_surrogate_pulse_mma_grid(n) returns the CTA count a launch for n spins uses (< 0: -error). */
 int bp_mlp_wtiles_bytes(void);
