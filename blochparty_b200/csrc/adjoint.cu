@@ -25,6 +25,13 @@
 #define ADJ_THREADS 128
 #define ADJ_WARPS (ADJ_THREADS / 32)
 #define ADJ_SLOTS (BP_ADJ_WIN + 1)
+// the sweep's own bits in a staged record's flags (above the record's): the segment before it (in the window)
+// spoils; the segment after it (in the window, swept just before) shares its RF relaxation, its RF off-resonance,
+// or its free factors, so the sweep keeps them
+#define A_PREV_SPOIL (1 << 8)
+#define A_KEEP_RELAX (1 << 9)
+#define A_KEEP_WZ (1 << 10)
+#define A_KEEP_FREE (1 << 11)
 
 // per-spin gradient rows of `gs`
 enum { G_PX, G_PY, G_PZ, G_DB0, G_PD, G_R1, G_R2, G_B1, N_GS };
@@ -50,20 +57,22 @@ struct AdjArgs {
     int seg_mask;         // which of the N_SG segment gradients are reduced (bit k: component k)
 };
 
-// Rodrigues rotation factors with the derivative factors f1 = (c - s1)/phi^2, f2 = (s1 - 2 s2)/phi^2 (the
-// derivatives of c, s1, s2 in phi, divided by phi). Below phi^2 = 1 all are Taylor series in phi^2:
-// f1 = sum_{k>=1} (-1)^k 2k phi^(2k-2) / (2k+1)!, f2 = sum_{k>=1} (-1)^k 2k phi^(2k-2) / (2k+2)!.
-__device__ __forceinline__ void rot_factors(float p2, float& c, float& s1, float& s2, float& f1, float& f2) {
+// Rodrigues factors of the rotation by |w| (p2 = |w|^2) with the third factor of its left Jacobian:
+// c = cos phi, s1 = sin(phi)/phi, s2 = (1 - cos phi)/phi^2, s3 = (phi - sin phi)/phi^3 = (1 - s1)/p2. Below
+// phi = 1 all are Taylor series in p2 (s3 = sum_k (-1)^k p2^k / (2k+3)!), truncated like rodrigues_coeffs (first
+// dropped terms below 4e-13 under phi = 1/4, below 2e-10 under phi = 1).
+__device__ __forceinline__ void rot_factors(float p2, float& c, float& s1, float& s2, float& s3) {
     rodrigues_coeffs(p2, s1, s2);
     c = fmaf(-s2, p2, 1.0f);
-    if (p2 < 1.0f) {
-        f1 = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -2.5052108385441720e-07f, 2.2045855379188713e-05f),
-                                     -1.1904761904761905e-03f), 3.3333333333333333e-02f), -3.3333333333333333e-01f);
-        f2 = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -2.0876756987868099e-08f, 2.2045855379188713e-06f),
-                                     -1.4880952380952381e-04f), 5.5555555555555556e-03f), -8.3333333333333333e-02f);
+    if (p2 < 0.0625f) {
+        s3 = fmaf(p2, fmaf(p2, fmaf(p2, -2.7557319223985893e-06f, 1.9841269841269841e-04f), -8.3333333333333333e-03f),
+                  1.6666666666666667e-01f);
+    } else if (p2 < 1.0f) {
+        s3 = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -1.6059043836821615e-10f, 2.5052108385441720e-08f),
+                                              -2.7557319223985893e-06f), 1.9841269841269841e-04f),
+                           -8.3333333333333333e-03f), 1.6666666666666667e-01f);
     } else {
-        f1 = (c - s1) / p2;
-        f2 = (s1 - 2.0f * s2) / p2;
+        s3 = (1.0f - s1) / p2;
     }
 }
 
@@ -84,35 +93,86 @@ __device__ __forceinline__ void offset_grads(float gcyc, const SegRec& q, const 
     sg.v[S_DT] += gcyc * p.db0;
 }
 
-// Reverse of an RF segment from its input state (x0, y0, z0): lambda in/out, gradients accumulated.
-__device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, float e1h, float e2h, float wz, float x0,
-                                           float y0, float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
-    const float h = 0.5f * q.dt;
-    const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;  // wz = rf_wz(q, p)
+// The half-step relaxation of an RF segment as the sweep uses it: e1h = expm1(-dt r1 / 2), a1 = 1 + e1h (and
+// e2h, a2 likewise), the inverses of a1 and a2, and whether they are safe to divide by (a >= 1/2: T1, T2 above
+// 0.72 dt; otherwise the rotated state is formed from the segment's input instead).
+struct RevRelax {
+    float e1h, e2h, a1, a2, ia1, ia2;
+    bool invert;
+};
+
+__device__ __forceinline__ RevRelax rev_relax(float dt, const Spin& p) {
+    RevRelax r;
+    r.e1h = expm1f(-0.5f * dt * p.r1);
+    r.e2h = expm1f(-0.5f * dt * p.r2);
+    r.a1 = 1.0f + r.e1h;
+    r.a2 = 1.0f + r.e2h;
+    r.invert = r.a1 >= 0.5f && r.a2 >= 0.5f;
+    r.ia1 = r.invert ? 1.0f / r.a1 : 0.0f;
+    r.ia2 = r.invert ? 1.0f / r.a2 : 0.0f;
+    return r;
+}
+
+// An RF segment of the recompute in plain float32 (the states only feed the gradients, which need no
+// compensated sums): m1 = E m + c, n = R m1 = c m1 + s1 (w x m1) + s2 w (w . m1), m = E n + c.
+__device__ __forceinline__ void rf_step_plain(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float& mx,
+                                              float& my, float& mz) {
+    const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
+    const float m1x = mx * r.a2, m1y = my * r.a2, m1z = fmaf(mz - p.pd, r.e1h, mz);
     const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
-    float c, s1, s2, f1, f2;
-    rot_factors(p2, c, s1, s2, f1, f2);
-    const float a2 = 1.0f + e2h, a1 = 1.0f + e1h;
-    const float m1x = x0 * a2, m1y = y0 * a2, m1z = fmaf(z0 - p.pd, e1h, z0);
-    const float dot = fmaf(wx, m1x, fmaf(wy, m1y, wz * m1z));
-    const float cx = wy * m1z - wz * m1y, cy = wz * m1x - wx * m1z, cz = wx * m1y - wy * m1x;  // w x m1
-    const float nx = fmaf(c, m1x, fmaf(s1, cx, s2 * wx * dot));
-    const float ny = fmaf(c, m1y, fmaf(s1, cy, s2 * wy * dot));
-    const float nz = fmaf(c, m1z, fmaf(s1, cz, s2 * wz * dot));
+    float s1, s2;
+    rodrigues_coeffs(p2, s1, s2);
+    const float c = fmaf(-s2, p2, 1.0f);
+    const float k = s2 * fmaf(wx, m1x, fmaf(wy, m1y, wz * m1z));
+    const float nx = fmaf(c, m1x, fmaf(s1, wy * m1z - wz * m1y, k * wx));
+    const float ny = fmaf(c, m1y, fmaf(s1, wz * m1x - wx * m1z, k * wy));
+    const float nz = fmaf(c, m1z, fmaf(s1, wx * m1y - wy * m1x, k * wz));
+    mx = nx * r.a2, my = ny * r.a2, mz = fmaf(nz - p.pd, r.e1h, nz);
+}
+
+// A free segment of the recompute in plain float32: rotation about z by the factors' (float32) phase, relaxation.
+__device__ __forceinline__ void free_step_plain(const FreeFactors& f, const Spin& p, float& mx, float& my, float& mz) {
+    const float x = fmaf(f.ch, mx, -f.sh * my), y = fmaf(f.sh, mx, f.ch * my);
+    mx = fmaf(x, f.e2, x), my = fmaf(y, f.e2, y), mz = fmaf(mz - p.pd, f.e1, mz);
+}
+
+// Reverse of an RF segment from its input state (x0, y0, z0) and output state (ox, oy, oz): lambda in/out,
+// gradients accumulated. The rotated state n = R m1 comes from the output, m2 = E n + c, by E's inverse (or, with
+// strong relaxation, from the input). dL/dw = J^T (n x a), a = dL/dn and J the rotation's left Jacobian
+// (R(w + d) = exp([J d]x) R(w)): J^T u = s1 u - s2 (w x u) + s3 (w . u) w.
+__device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float x0,
+                                           float y0, float z0, float ox, float oy, float oz, float& lx, float& ly,
+                                           float& lz, float* g, SegGrad& sg) {
+    const float h = 0.5f * q.dt;
+    const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
+    const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
+    float c, s1, s2, s3;
+    rot_factors(p2, c, s1, s2, s3);
+    const float a2 = r.a2, a1 = r.a1, e1h = r.e1h;
+    float nx, ny, nz;
+    if (r.invert) {
+        nx = ox * r.ia2, ny = oy * r.ia2, nz = fmaf(p.pd, e1h, oz) * r.ia1;
+    } else {
+        const float m1x = x0 * a2, m1y = y0 * a2, m1z = fmaf(z0 - p.pd, e1h, z0);
+        const float k = s2 * fmaf(wx, m1x, fmaf(wy, m1y, wz * m1z));
+        nx = fmaf(c, m1x, fmaf(s1, wy * m1z - wz * m1y, k * wx));
+        ny = fmaf(c, m1y, fmaf(s1, wz * m1x - wx * m1z, k * wy));
+        nz = fmaf(c, m1z, fmaf(s1, wx * m1y - wy * m1x, k * wz));
+    }
     // second half relaxation: m2 = (n a2, n a2, nz + (nz - pd) e1h)
     float gd2 = fmaf(lx, nx, ly * ny), gd1 = lz * (nz - p.pd), gpd = -lz * e1h;
     const float ax = lx * a2, ay = ly * a2, az = lz * a1;  // dL/dn
-    // rotation: b = R^T a, gw = dL/dw
-    const float wa = fmaf(wx, ax, fmaf(wy, ay, wz * az));
-    const float bx = fmaf(c, ax, fmaf(-s1, wy * az - wz * ay, s2 * wx * wa));
-    const float by = fmaf(c, ay, fmaf(-s1, wz * ax - wx * az, s2 * wy * wa));
-    const float bz = fmaf(c, az, fmaf(-s1, wx * ay - wy * ax, s2 * wz * wa));
-    const float am = fmaf(ax, m1x, fmaf(ay, m1y, az * m1z));
-    const float awm = fmaf(ax, cx, fmaf(ay, cy, az * cz));
-    const float k = fmaf(-s1, am, fmaf(f1, awm, f2 * wa * dot));
-    const float gwx = fmaf(k, wx, fmaf(s1, m1y * az - m1z * ay, s2 * fmaf(wa, m1x, dot * ax)));
-    const float gwy = fmaf(k, wy, fmaf(s1, m1z * ax - m1x * az, s2 * fmaf(wa, m1y, dot * ay)));
-    const float gwz = fmaf(k, wz, fmaf(s1, m1x * ay - m1y * ax, s2 * fmaf(wa, m1z, dot * az)));
+    // rotation: b = R^T a = c a - s1 (w x a) + s2 w (w . a)
+    const float k2 = s2 * fmaf(wx, ax, fmaf(wy, ay, wz * az));
+    const float bx = fmaf(c, ax, fmaf(-s1, wy * az - wz * ay, k2 * wx));
+    const float by = fmaf(c, ay, fmaf(-s1, wz * ax - wx * az, k2 * wy));
+    const float bz = fmaf(c, az, fmaf(-s1, wx * ay - wy * ax, k2 * wz));
+    // gw = J^T u, u = n x a
+    const float ux = ny * az - nz * ay, uy = nz * ax - nx * az, uz = nx * ay - ny * ax;
+    const float k3 = s3 * fmaf(wx, ux, fmaf(wy, uy, wz * uz));
+    const float gwx = fmaf(s1, ux, fmaf(-s2, wy * uz - wz * uy, k3 * wx));
+    const float gwy = fmaf(s1, uy, fmaf(-s2, wz * ux - wx * uz, k3 * wy));
+    const float gwz = fmaf(s1, uz, fmaf(-s2, wx * uy - wy * ux, k3 * wz));
     // first half relaxation
     gd2 = fmaf(bx, x0, fmaf(by, y0, gd2));
     gd1 = fmaf(bz, z0 - p.pd, gd1);
@@ -147,7 +207,13 @@ __device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, con
     offset_grads(-BP_TWO_PI_F * gphi, q, p, g, sg);
 }
 
-template <int NCG>
+template <int K>
+struct KindTag {
+    static constexpr int value = K;
+};
+
+// NCG: groups of 8 coils; CG: whether the coil gradients are wanted (a.gc not null).
+template <int NCG, bool CG>
 __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kernel(AdjArgs a) {
     extern __shared__ __align__(16) float sm[];
     float* slots = sm;                                     // [ADJ_SLOTS][3][ADJ_THREADS]
@@ -176,12 +242,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
         float g[N_GS];
 #pragma unroll
         for (int k = 0; k < N_GS; ++k) g[k] = active ? a.gs[k * n + j] : 0.0f;
-        const bool want_gc = a.gc != nullptr && active;
-        float gcr[8 * NCG], gci[8 * NCG], sr[8 * NCG], si[8 * NCG];
+        const bool want_gc = CG && active;
+        float gcr[CG ? 8 * NCG : 1], gci[CG ? 8 * NCG : 1], sr[8 * NCG], si[8 * NCG];
 #pragma unroll
         for (int c = 0; c < 8 * NCG; ++c) {
-            gcr[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c) * n + j] : 0.0f;
-            gci[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c + 1) * n + j] : 0.0f;
+            if (CG) {
+                gcr[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c) * n + j] : 0.0f;
+                gci[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c + 1) * n + j] : 0.0f;
+            }
             sr[c] = active ? a.sens[(2 * c) * n + j] : 0.0f;
             si[c] = active ? a.sens[(2 * c + 1) * n + j] : 0.0f;
         }
@@ -190,102 +258,135 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
             const int nseg = win.y - win.x;
             if (nseg < 0 || nseg > BP_ADJ_WIN) continue;  // not an adjoint window (uniform): never index past the slots
             // the window's records into shared memory (every warp of the CTA sweeps the same window); the barrier
-            // at the end of the previous window ended its reads
+            // at the end of the previous window ended its reads. The flags word of record s is written by thread s
+            // alone, with the sweep's own bits added (from the global records, so no thread reads a word another
+            // writes)
+            const SegRec* gw = a.segs + win.x;
             for (int i = tid; i < nseg * 8; i += ADJ_THREADS)
-                reinterpret_cast<float*>(wrec)[i] = reinterpret_cast<const float*>(a.segs + win.x)[i];
+                if ((i & 7) != 7) reinterpret_cast<float*>(wrec)[i] = reinterpret_cast<const float*>(gw)[i];
+            for (int i = tid; i < nseg; i += ADJ_THREADS) {
+                const int f = gw[i].flags, fn = i + 1 < nseg ? gw[i + 1].flags : 0;
+                int x = f;
+                if (i > 0 && (gw[i - 1].flags & BP_SPOIL)) x |= A_PREV_SPOIL;
+                if ((f & BP_RF) && (fn & BP_RF) && (fn & BP_SAME_RFDT)) x |= A_KEEP_RELAX;
+                if ((f & BP_RF) && (fn & BP_RF) && (fn & BP_SAME_OFF)) x |= A_KEEP_WZ;
+                if (!(f & BP_RF) && i + 1 < nseg && !(fn & BP_RF) && (fn & BP_SAME_FREE)) x |= A_KEEP_FREE;
+                wrec[i].flags = x;
+            }
             for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
                 reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
-            __syncthreads();
-            // recompute the window: slot k = state after segment k-1 (before its spoil), slot 0 = window start
-            const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
-            float mx = 0.f, my = 0.f, mz = 0.f, llx = 0.f, lly = 0.f, llz = 0.f;
-            if (active) {
-                mx = ws[j], my = ws[n + j], mz = ws[2 * n + j];
-                llx = ws[3 * n + j], lly = ws[4 * n + j], llz = ws[5 * n + j];
+            // the window's kind (the same for the whole CTA): every segment RF with the dt and offset of the first,
+            // no sample and no spoil (the steps of an RF pulse); or every segment free with the factors of the
+            // first and no spoil (a readout's samples). Their sweeps skip the per-segment tests.
+            bool rf_ok = true, free_ok = true;
+            if (tid < nseg) {
+                const int f = gw[tid].flags;
+                rf_ok = (f & BP_RF) && !(f & (BP_ADC | BP_SPOIL)) && (tid == 0 || (f & BP_SAME_OFF));
+                free_ok = !(f & BP_RF) && !(f & BP_SPOIL) && (tid == 0 || (f & BP_SAME_FREE));
             }
-            slots[tid] = mx + llx, slots[ADJ_THREADS + tid] = my + lly, slots[2 * ADJ_THREADS + tid] = mz + llz;
-            FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
-            float e1h = 0.f, e2h = 0.f, wz = 0.f;
-            for (int s = 0; s < nseg; ++s) {
-                const SegRec q = wrec[s];
-                if (q.flags & BP_RF) {
-                    if (s == 0 || !(q.flags & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
-                    if (s == 0 || !(q.flags & BP_SAME_OFF)) wz = rf_wz(q, p);
-                    rf_step_wz(q, p, rr, wz, mx, my, mz, llx, lly, llz);
-                } else {
-                    if (s == 0 || !(q.flags & BP_SAME_FREE)) ff = free_factors(q, wk64[s], p);
-                    free_step(ff, p, mx, my, mz, llx, lly, llz);
+            const bool all_rf = __syncthreads_and(rf_ok), all_free = __syncthreads_and(free_ok);
+            auto sweep = [&](auto kind_tag) {
+                constexpr int KIND = decltype(kind_tag)::value;  // 0: any segments, 1: uniform RF, 2: uniform free
+                // recompute the window in plain float32 from its (compensated) start state: slot k = state after
+                // segment k-1 (before its spoil), slot 0 = window start
+                const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
+                float mx = 0.f, my = 0.f, mz = 0.f;
+                if (active)
+                    mx = ws[j] + ws[3 * n + j], my = ws[n + j] + ws[4 * n + j], mz = ws[2 * n + j] + ws[5 * n + j];
+                slots[tid] = mx, slots[ADJ_THREADS + tid] = my, slots[2 * ADJ_THREADS + tid] = mz;
+                FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                RevRelax rr{0.f, 0.f, 1.f, 1.f, 1.f, 1.f, true};
+                float wz = 0.f;
+                if (KIND == 1) rr = rev_relax(wrec[0].dt, p), wz = rf_wz(wrec[0], p);
+                if (KIND == 2) ff = free_factors(wrec[0], wk64[0], p);
+                for (int s = 0; s < nseg; ++s) {
+                    const SegRec q = wrec[s];
+                    if (KIND == 1 || (KIND == 0 && (q.flags & BP_RF))) {
+                        if (KIND == 0) {
+                            if (s == 0 || !(q.flags & BP_SAME_RFDT)) rr = rev_relax(q.dt, p);
+                            if (s == 0 || !(q.flags & BP_SAME_OFF)) wz = rf_wz(q, p);
+                        }
+                        rf_step_plain(q, p, rr, wz, mx, my, mz);
+                    } else {
+                        if (KIND == 0 && (s == 0 || !(q.flags & BP_SAME_FREE))) ff = free_factors(q, wk64[s], p);
+                        free_step_plain(ff, p, mx, my, mz);
+                    }
+                    float* sl = slots + (s + 1) * 3 * ADJ_THREADS;
+                    sl[tid] = mx, sl[ADJ_THREADS + tid] = my, sl[2 * ADJ_THREADS + tid] = mz;
+                    if (KIND == 0 && (q.flags & BP_SPOIL)) mx = my = 0.0f;
                 }
-                float* sl = slots + (s + 1) * 3 * ADJ_THREADS;
-                sl[tid] = mx + llx, sl[ADJ_THREADS + tid] = my + lly, sl[2 * ADJ_THREADS + tid] = mz + llz;
-                if (q.flags & BP_SPOIL) mx = my = llx = lly = 0.0f;
-            }
-            // sweep back
-            int row = win.z + win.w;
-            int cached_free = -1, cached_rf = -1;
-            for (int s = nseg - 1; s >= 0; --s) {
-                const SegRec q = wrec[s];
-                const int f = q.flags;
-                if (f & BP_SPOIL) lx = ly = 0.0f;
-                if ((f & BP_ADC) && a.h != nullptr) {
-                    --row;
-                    const float* hr = a.h + (size_t)row * nv;
+                // sweep back
+                int row = win.z + win.w;
+                for (int s = nseg - 1; s >= 0; --s) {
+                    const SegRec q = wrec[s];
+                    const int f = q.flags;
+                    if (KIND == 0 && (f & BP_SPOIL)) lx = ly = 0.0f;
+                    // the segment's output state: slot s + 1
                     const float* out = slots + (s + 1) * 3 * ADJ_THREADS;
                     const float ox = out[tid], oy = out[ADJ_THREADS + tid];
-                    float dx = 0.0f, dy = 0.0f;
+                    if (KIND != 1 && (f & BP_ADC) && a.h != nullptr) {
+                        --row;
+                        const float* hr = a.h + (size_t)row * nv;
+                        float dx = 0.0f, dy = 0.0f;
 #pragma unroll
-                    for (int c = 0; c < 8 * NCG; ++c) {
-                        if (c < a.n_coils) {
-                            const float h0 = hr[2 * c], h1 = hr[2 * c + 1];
-                            dx = fmaf(h0, sr[c], fmaf(h1, si[c], dx));
-                            dy = fmaf(-h0, si[c], fmaf(h1, sr[c], dy));
-                            gcr[c] = fmaf(h0, ox, fmaf(h1, oy, gcr[c]));
-                            gci[c] = fmaf(-h0, oy, fmaf(h1, ox, gci[c]));
+                        for (int c = 0; c < 8 * NCG; ++c) {
+                            if (c < a.n_coils) {
+                                const float h0 = hr[2 * c], h1 = hr[2 * c + 1];
+                                dx = fmaf(h0, sr[c], fmaf(h1, si[c], dx));
+                                dy = fmaf(-h0, si[c], fmaf(h1, sr[c], dy));
+                                if (CG) {
+                                    gcr[c] = fmaf(h0, ox, fmaf(h1, oy, gcr[c]));
+                                    gci[c] = fmaf(-h0, oy, fmaf(h1, ox, gci[c]));
+                                }
+                            }
                         }
+                        lx += dx, ly += dy;
                     }
-                    lx += dx, ly += dy;
-                }
-                // the segment's input state: slot s, spoiled by segment s-1 if it spoils
-                const float* in = slots + s * 3 * ADJ_THREADS;
-                float x0 = in[tid], y0 = in[ADJ_THREADS + tid];
-                const float z0 = in[2 * ADJ_THREADS + tid];
-                if (s > 0 && (wrec[s - 1].flags & BP_SPOIL)) x0 = y0 = 0.0f;
-                SegGrad sg;
+                    // the segment's input state: slot s, spoiled by segment s-1 if it spoils
+                    const float* in = slots + s * 3 * ADJ_THREADS;
+                    float x0 = in[tid], y0 = in[ADJ_THREADS + tid];
+                    const float z0 = in[2 * ADJ_THREADS + tid];
+                    if (KIND == 0 && (f & A_PREV_SPOIL)) x0 = y0 = 0.0f;
+                    SegGrad sg;
 #pragma unroll
-                for (int k = 0; k < N_SG; ++k) sg.v[k] = 0.0f;
-                if (f & BP_RF) {
-                    // the factors of the segment after this one (swept just before) when they are the same
-                    if (cached_rf != s + 1 || !(wrec[s + 1].flags & BP_SAME_RFDT)) {
-                        e1h = expm1f(-0.5f * q.dt * p.r1);
-                        e2h = expm1f(-0.5f * q.dt * p.r2);
+                    for (int k = 0; k < N_SG; ++k) sg.v[k] = 0.0f;
+                    if (KIND == 1 || (KIND == 0 && (f & BP_RF))) {
+                        // the factors of the segment after this one (swept just before) when they are the same
+                        if (KIND == 0) {
+                            if (!(f & A_KEEP_RELAX)) rr = rev_relax(q.dt, p);
+                            if (!(f & A_KEEP_WZ)) wz = rf_wz(q, p);
+                        }
+                        rf_reverse(q, p, rr, wz, x0, y0, z0, ox, oy, out[2 * ADJ_THREADS + tid], lx, ly, lz, g, sg);
+                    } else {
+                        if (KIND == 0 && !(f & A_KEEP_FREE)) ff = free_factors(q, wk64[s], p);
+                        free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
                     }
-                    if (cached_rf != s + 1 || !(wrec[s + 1].flags & BP_SAME_OFF)) wz = rf_wz(q, p);
-                    cached_rf = s;
-                    rf_reverse(q, p, e1h, e2h, wz, x0, y0, z0, lx, ly, lz, g, sg);
-                } else {
-                    if (cached_free != s + 1 || !(wrec[s + 1].flags & BP_SAME_FREE))
-                        ff = free_factors(q, wk64[s], p);
-                    cached_free = s;
-                    free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
-                }
-                if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0 and 16 hold them)
-                    const bool up = lane & 16;
-                    const float v0 = active ? sg.v[S_WX] : 0.0f, v1 = active ? sg.v[S_WY] : 0.0f;
-                    float t = (up ? v1 : v0) + __shfl_xor_sync(0xffffffffu, up ? v0 : v1, 16);
+                    if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0, 16 hold them)
+                        if (KIND != 2) {  // (a free segment's are 0: a uniform free window writes and adds none)
+                            const bool up = lane & 16;
+                            const float v0 = sg.v[S_WX], v1 = sg.v[S_WY];  // (0 for a padding row: its lambda is 0)
+                            float t = (up ? v1 : v0) + __shfl_xor_sync(0xffffffffu, up ? v0 : v1, 16);
 #pragma unroll
-                    for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-                    if ((lane & 15) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + (up ? S_WY : S_WX)] = t;
-                } else if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
-                    float v[N_SG];
+                            for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                            if ((lane & 15) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + (up ? S_WY : S_WX)] = t;
+                        }
+                    } else if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
+                        float v[N_SG];
 #pragma unroll
-                    for (int k = 0; k < N_SG; ++k) v[k] = active ? sg.v[k] : 0.0f;
-                    const float t = warp_reduce_scatter8(v, lane);
-                    if ((lane & 3) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + ((lane >> 2) & 7)] = t;
+                        for (int k = 0; k < N_SG; ++k) v[k] = sg.v[k];
+                        const float t = warp_reduce_scatter8(v, lane);
+                        if ((lane & 3) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + ((lane >> 2) & 7)] = t;
+                    }
                 }
-            }
+            };
+            if (all_rf)
+                sweep(KindTag<1>{});
+            else if (all_free)
+                sweep(KindTag<2>{});
+            else
+                sweep(KindTag<0>{});
             __syncthreads();  // segacc complete; every thread is done reading this window's slots
-            if (need_seg) {
+            if (need_seg && !(rf_only && all_free)) {
                 float* dst = a.gseg + ((size_t)blockIdx.x * a.seg_len + (win.x - a.seg0)) * N_SG;
                 for (int i = tid; i < nseg * N_SG; i += ADJ_THREADS) {
                     float t = 0.0f;
@@ -300,7 +401,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
             a.lam[j] = lx, a.lam[n + j] = ly, a.lam[2 * n + j] = lz;
 #pragma unroll
             for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] = g[k];
-            if (want_gc) {
+            if (CG) {
 #pragma unroll
                 for (int c = 0; c < 8 * NCG; ++c) {
                     if (c < a.n_coils) {
@@ -323,31 +424,49 @@ __global__ void bp_seg_reduce_kernel(const float* __restrict__ gseg, int n_cta, 
     seg[(size_t)seg0 * N_SG + i] += t;
 }
 
-template <int NCG>
 static size_t adj_smem() {
     return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) +
            (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4));
 }
 
-template <int NCG>
-static int adj_grid(int n) {
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+// One variant's shared-memory size, set once per device: 0, or -1 on failure.
+template <int NCG, bool CG>
+static int adj_configure() {
     static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)adj_smem<NCG>()) != cudaSuccess ||
-            cudaFuncSetAttribute(bp_adjoint_kernel<NCG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)adj_smem()) != cudaSuccess ||
+            cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return -1;
         configured[dev] = true;
     }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG>, ADJ_THREADS, adj_smem<NCG>()) !=
-        cudaSuccess)
+    return 0;
+}
+
+// CTAs per SM of one variant, or -1
+template <int NCG, bool CG>
+static int adj_per_sm() {
+    int per_sm = 0;
+    if (adj_configure<NCG, CG>() < 0 ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG>, ADJ_THREADS,
+                                                      adj_smem()) != cudaSuccess)
         return -1;
+    return per_sm > 0 ? per_sm : 1;
+}
+
+// one grid for both variants (with and without coil gradients): the smaller residency of the two
+template <int NCG>
+static int adj_grid(int n) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int with_cg = adj_per_sm<NCG, true>(), without = adj_per_sm<NCG, false>();
+    if (with_cg < 0 || without < 0) return -1;
     const int n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
-    int grid = sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = sms * (with_cg < without ? with_cg : without);
     return grid < n_tiles ? grid : n_tiles;
 }
 
@@ -363,7 +482,13 @@ extern "C" int bp_adjoint_grid(int n, int n_coils) {
 
 template <int NCG>
 static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
-    bp_adjoint_kernel<NCG><<<grid, ADJ_THREADS, adj_smem<NCG>(), st>>>(a);
+    if (a.gc) {
+        if (adj_configure<NCG, true>() < 0) return BP_E_LAUNCH;
+        bp_adjoint_kernel<NCG, true><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
+    } else {
+        if (adj_configure<NCG, false>() < 0) return BP_E_LAUNCH;
+        bp_adjoint_kernel<NCG, false><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
+    }
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
