@@ -61,10 +61,15 @@ struct AdjArgs {
 // c = cos phi, s1 = sin(phi)/phi, s2 = (1 - cos phi)/phi^2, s3 = (phi - sin phi)/phi^3 = (1 - s1)/p2. Below
 // phi = 1 all are Taylor series in p2 (s3 = sum_k (-1)^k p2^k / (2k+3)!), truncated like rodrigues_coeffs (first
 // dropped terms below 4e-13 under phi = 1/4, below 2e-10 under phi = 1).
+// SMALL: the caller knows p2 < 1/16 (the first tier, no tests).
+template <bool SMALL>
 __device__ __forceinline__ void rot_factors(float p2, float& c, float& s1, float& s2, float& s3) {
-    rodrigues_coeffs(p2, s1, s2);
+    if (SMALL)
+        rodrigues_small(p2, s1, s2);
+    else
+        rodrigues_coeffs(p2, s1, s2);
     c = fmaf(-s2, p2, 1.0f);
-    if (p2 < 0.0625f) {
+    if (SMALL || p2 < 0.0625f) {
         s3 = fmaf(p2, fmaf(p2, fmaf(p2, -2.7557319223985893e-06f, 1.9841269841269841e-04f), -8.3333333333333333e-03f),
                   1.6666666666666667e-01f);
     } else if (p2 < 1.0f) {
@@ -115,13 +120,17 @@ __device__ __forceinline__ RevRelax rev_relax(float dt, const Spin& p) {
 
 // An RF segment of the recompute in plain float32 (the states only feed the gradients, which need no
 // compensated sums): m1 = E m + c, n = R m1 = c m1 + s1 (w x m1) + s2 w (w . m1), m = E n + c.
+template <bool SMALL>
 __device__ __forceinline__ void rf_step_plain(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float& mx,
                                               float& my, float& mz) {
     const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
     const float m1x = mx * r.a2, m1y = my * r.a2, m1z = fmaf(mz - p.pd, r.e1h, mz);
     const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
     float s1, s2;
-    rodrigues_coeffs(p2, s1, s2);
+    if (SMALL)
+        rodrigues_small(p2, s1, s2);
+    else
+        rodrigues_coeffs(p2, s1, s2);
     const float c = fmaf(-s2, p2, 1.0f);
     const float k = s2 * fmaf(wx, m1x, fmaf(wy, m1y, wz * m1z));
     const float nx = fmaf(c, m1x, fmaf(s1, wy * m1z - wz * m1y, k * wx));
@@ -140,6 +149,7 @@ __device__ __forceinline__ void free_step_plain(const FreeFactors& f, const Spin
 // gradients accumulated. The rotated state n = R m1 comes from the output, m2 = E n + c, by E's inverse (or, with
 // strong relaxation, from the input). dL/dw = J^T (n x a), a = dL/dn and J the rotation's left Jacobian
 // (R(w + d) = exp([J d]x) R(w)): J^T u = s1 u - s2 (w x u) + s3 (w . u) w.
+template <bool SMALL>
 __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float x0,
                                            float y0, float z0, float ox, float oy, float oz, float& lx, float& ly,
                                            float& lz, float* g, SegGrad& sg) {
@@ -147,7 +157,7 @@ __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const
     const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
     const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
     float c, s1, s2, s3;
-    rot_factors(p2, c, s1, s2, s3);
+    rot_factors<SMALL>(p2, c, s1, s2, s3);
     const float a2 = r.a2, a1 = r.a1, e1h = r.e1h;
     float nx, ny, nz;
     if (r.invert) {
@@ -220,6 +230,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
     float* segacc = slots + ADJ_SLOTS * 3 * ADJ_THREADS;  // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
     SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * N_SG);  // [BP_ADJ_WIN] the window's
     double4* wk64 = reinterpret_cast<double4*>(wrec + BP_ADJ_WIN);                     // records and moments
+    __shared__ float wmax[1];  // the window's largest wx0^2 + wy0^2
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
     const int nv = 2 * a.n_coils;
@@ -284,9 +295,16 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 rf_ok = (f & BP_RF) && !(f & (BP_ADC | BP_SPOIL)) && (tid == 0 || (f & BP_SAME_OFF));
                 free_ok = !(f & BP_RF) && !(f & BP_SPOIL) && (tid == 0 || (f & BP_SAME_FREE));
             }
+            if (warp == 0) {  // the window's largest wx0^2 + wy0^2 (non-negative floats order as their bits)
+                const float v = lane < nseg ? fmaf(gw[lane].wx0, gw[lane].wx0, gw[lane].wy0 * gw[lane].wy0) : 0.0f;
+                const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(v));
+                if (lane == 0) *wmax = __uint_as_float(m);
+            }
             const bool all_rf = __syncthreads_and(rf_ok), all_free = __syncthreads_and(free_ok);
             auto sweep = [&](auto kind_tag) {
-                constexpr int KIND = decltype(kind_tag)::value;  // 0: any segments, 1: uniform RF, 2: uniform free
+                // 0: any segments, 1: uniform RF, 2: uniform free, 3: uniform RF with every |w| < 1/4 in the warp
+                constexpr int KIND = decltype(kind_tag)::value;
+                constexpr bool URF = KIND == 1 || KIND == 3;
                 // recompute the window in plain float32 from its (compensated) start state: slot k = state after
                 // segment k-1 (before its spoil), slot 0 = window start
                 const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
@@ -297,16 +315,16 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 RevRelax rr{0.f, 0.f, 1.f, 1.f, 1.f, 1.f, true};
                 float wz = 0.f;
-                if (KIND == 1) rr = rev_relax(wrec[0].dt, p), wz = rf_wz(wrec[0], p);
+                if (URF) rr = rev_relax(wrec[0].dt, p), wz = rf_wz(wrec[0], p);
                 if (KIND == 2) ff = free_factors(wrec[0], wk64[0], p);
                 for (int s = 0; s < nseg; ++s) {
                     const SegRec q = wrec[s];
-                    if (KIND == 1 || (KIND == 0 && (q.flags & BP_RF))) {
+                    if (URF || (KIND == 0 && (q.flags & BP_RF))) {
                         if (KIND == 0) {
                             if (s == 0 || !(q.flags & BP_SAME_RFDT)) rr = rev_relax(q.dt, p);
                             if (s == 0 || !(q.flags & BP_SAME_OFF)) wz = rf_wz(q, p);
                         }
-                        rf_step_plain(q, p, rr, wz, mx, my, mz);
+                        rf_step_plain<KIND == 3>(q, p, rr, wz, mx, my, mz);
                     } else {
                         if (KIND == 0 && (s == 0 || !(q.flags & BP_SAME_FREE))) ff = free_factors(q, wk64[s], p);
                         free_step_plain(ff, p, mx, my, mz);
@@ -324,7 +342,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     // the segment's output state: slot s + 1
                     const float* out = slots + (s + 1) * 3 * ADJ_THREADS;
                     const float ox = out[tid], oy = out[ADJ_THREADS + tid];
-                    if (KIND != 1 && (f & BP_ADC) && a.h != nullptr) {
+                    if (!URF && (f & BP_ADC) && a.h != nullptr) {
                         --row;
                         const float* hr = a.h + (size_t)row * nv;
                         float dx = 0.0f, dy = 0.0f;
@@ -350,13 +368,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     SegGrad sg;
 #pragma unroll
                     for (int k = 0; k < N_SG; ++k) sg.v[k] = 0.0f;
-                    if (KIND == 1 || (KIND == 0 && (f & BP_RF))) {
+                    if (URF || (KIND == 0 && (f & BP_RF))) {
                         // the factors of the segment after this one (swept just before) when they are the same
                         if (KIND == 0) {
                             if (!(f & A_KEEP_RELAX)) rr = rev_relax(q.dt, p);
                             if (!(f & A_KEEP_WZ)) wz = rf_wz(q, p);
                         }
-                        rf_reverse(q, p, rr, wz, x0, y0, z0, ox, oy, out[2 * ADJ_THREADS + tid], lx, ly, lz, g, sg);
+                        rf_reverse<KIND == 3>(q, p, rr, wz, x0, y0, z0, ox, oy, out[2 * ADJ_THREADS + tid], lx, ly, lz, g, sg);
                     } else {
                         if (KIND == 0 && !(f & A_KEEP_FREE)) ff = free_factors(q, wk64[s], p);
                         free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
@@ -379,12 +397,20 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     }
                 }
             };
-            if (all_rf)
-                sweep(KindTag<1>{});
-            else if (all_free)
+            if (all_rf) {
+                // every rotation of the window below |w| = 1/4 for every spin of the warp: |w|^2 <= b1^2 max(wx0^2 +
+                // wy0^2) + wz^2 (one offset for the window)
+                const float wz0 = rf_wz(wrec[0], p);
+                const bool small = fmaf(p.b1 * p.b1, *wmax, wz0 * wz0) < 0.0624f;
+                if (__all_sync(0xffffffffu, small))
+                    sweep(KindTag<3>{});
+                else
+                    sweep(KindTag<1>{});
+            } else if (all_free) {
                 sweep(KindTag<2>{});
-            else
+            } else {
                 sweep(KindTag<0>{});
+            }
             __syncthreads();  // segacc complete; every thread is done reading this window's slots
             if (need_seg && !(rf_only && all_free)) {
                 float* dst = a.gseg + ((size_t)blockIdx.x * a.seg_len + (win.x - a.seg0)) * N_SG;

@@ -80,12 +80,15 @@ __device__ __forceinline__ void quick_two_sum(float& hi, float& lo, float d) {
 // p2^3 below phi = 1/4 (the usual RF step; first dropped terms p2^4 / 9! < 4.3e-11) and after p2^5 below phi = 1
 // (first dropped terms below 2e-10), far under a float32 ulp, on the FMA pipe with no square root. Above, the
 // accurate sine of the angle and of its half.
+// The first tier alone (p2 < 1/16 known to the caller).
+__device__ __forceinline__ void rodrigues_small(float p2, float& s1, float& s2) {
+    s1 = fmaf(p2, fmaf(p2, fmaf(p2, -1.9841269841269841e-04f, 8.3333333333333333e-03f), -1.6666666666666667e-01f), 1.0f);
+    s2 = fmaf(p2, fmaf(p2, fmaf(p2, -2.4801587301587302e-05f, 1.3888888888888889e-03f), -4.1666666666666667e-02f), 0.5f);
+}
+
 __device__ __forceinline__ void rodrigues_coeffs(float p2, float& s1, float& s2) {
     if (p2 < 0.0625f) {
-        s1 = fmaf(p2, fmaf(p2, fmaf(p2, -1.9841269841269841e-04f, 8.3333333333333333e-03f), -1.6666666666666667e-01f),
-                  1.0f);
-        s2 = fmaf(p2, fmaf(p2, fmaf(p2, -2.4801587301587302e-05f, 1.3888888888888889e-03f), -4.1666666666666667e-02f),
-                  0.5f);
+        rodrigues_small(p2, s1, s2);
     } else if (p2 < 1.0f) {
         s1 = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -2.5052108385441720e-08f, 2.7557319223985893e-06f),
                                               -1.9841269841269841e-04f), 8.3333333333333333e-03f),
