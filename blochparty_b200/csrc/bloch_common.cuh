@@ -23,6 +23,8 @@
 #define BP_SAME_FREE 8   // free segment identical (dt, moment, offset) to the free segment just before it
 #define BP_SAME_RFDT 16  // RF segment with the dt of the RF segment just before it
 #define BP_SAME_OFF 32   // RF segment with the dt, moment and offset of the RF segment just before it (same G.r)
+#define BP_SMALL 64      // RF segment whose rotation stays below |w| = 1/4 for every spin (a bound from the spins'
+                         // extents, set by the host): the first tier of the Rodrigues factors without tests
 
 // status bits written by the kernels (read by the host after the launch)
 #define BP_ERR_TMA_TIMEOUT 1
@@ -145,13 +147,18 @@ __device__ __forceinline__ float rf_wz(const SegRec& q, const Spin& p) {
 // relax dt/2 (E n + c), composed into one increment of m: (E E - I) m + E (R - I) m1 + (E + I) c, with
 // (R - I) m1 = s1 (w x m1) + s2 w x (w x m1). The increment is small next to m and computed from m directly,
 // so one (fast) two-sum per component (instead of one per sub-step) keeps the float32 state compensated.
+// SMALL: the segment carries BP_SMALL (p2 < 1/16 for every spin).
+template <bool SMALL = false>
 __device__ __forceinline__ void rf_step_wz(const SegRec& q, const Spin& p, const RfRelax& r, float wz, float& mx,
                                            float& my, float& mz, float& lx, float& ly, float& lz) {
     const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
     const float m1x = mx * r.a2, m1y = my * r.a2, m1z = fmaf(-p.pd, r.e1h, mz * r.a1);
     const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
     float s1, s2;
-    rodrigues_coeffs(p2, s1, s2);
+    if (SMALL)
+        rodrigues_small(p2, s1, s2);
+    else
+        rodrigues_coeffs(p2, s1, s2);
     const float cx = wy * m1z - wz * m1y, cy = wz * m1x - wx * m1z, cz = wx * m1y - wy * m1x;
     const float dx = wy * cz - wz * cy, dy = wz * cx - wx * cz, dz = wx * cy - wy * cx;
     const float qx = fmaf(s1, cx, s2 * dx), qy = fmaf(s1, cy, s2 * dy), qz = fmaf(s1, cz, s2 * dz);

@@ -204,6 +204,15 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                     if (!(f & (BP_ADC | BP_SPOIL))) {
                         // the rest of a pulse with this dt and offset: only the RF changes from step to step
                         constexpr int kRun = BP_RF | BP_SAME_RFDT | BP_SAME_OFF;
+                        if (f & BP_SMALL) {  // (the run's small steps without the factors' tier tests)
+                            constexpr int kSmall = kRun | BP_SMALL;
+                            while (s + 1 < nseg) {
+                                const SegRec& qn = q0[s + 1];
+                                if ((qn.flags & (kSmall | BP_ADC | BP_SPOIL)) != kSmall) break;
+                                ++s;
+                                rf_step_wz<true>(qn, p, rr, wz, mx, my, mz, lx, ly, lz);
+                            }
+                        }
                         while (s + 1 < nseg) {
                             const SegRec& qn = q0[s + 1];
                             if ((qn.flags & (kRun | BP_ADC | BP_SPOIL)) != kRun) break;

@@ -213,6 +213,15 @@ __global__ void __launch_bounds__(MM_THREADS, 3) bp_forward_mma_kernel(MmaArgs a
                     rf_step_wz(q, p, rr, wz, mx, my, mz, lx, ly, lz);
                     if (!(f & (BP_ADC | BP_SPOIL))) {  // the rest of the pulse, as in bp_forward
                         constexpr int kRun = BP_RF | BP_SAME_RFDT | BP_SAME_OFF;
+                        if (f & BP_SMALL) {  // (the run's small steps without the factors' tier tests)
+                            constexpr int kSmall = kRun | BP_SMALL;
+                            while (s + 1 < nseg) {
+                                const SegRec& qn = q0[s + 1];
+                                if ((qn.flags & (kSmall | BP_ADC | BP_SPOIL)) != kSmall) break;
+                                ++s;
+                                rf_step_wz<true>(qn, p, rr, wz, mx, my, mz, lx, ly, lz);
+                            }
+                        }
                         while (s + 1 < nseg) {
                             const SegRec& qn = q0[s + 1];
                             if ((qn.flags & (kRun | BP_ADC | BP_SPOIL)) != kRun) break;

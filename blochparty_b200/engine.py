@@ -30,7 +30,7 @@ from ._lib import ptr
 TWO_PI = 2.0 * math.pi
 F32, F64 = torch.float32, torch.float64
 
-RF, ADC, SPOIL, SAME_FREE, SAME_RFDT, SAME_OFF = 1, 2, 4, 8, 16, 32
+RF, ADC, SPOIL, SAME_FREE, SAME_RFDT, SAME_OFF, SMALL = 1, 2, 4, 8, 16, 32, 64
 
 
 @dataclass
@@ -139,10 +139,29 @@ def final_m(state: torch.Tensor) -> torch.Tensor:
     return (s[0:3] + s[3:6]).to(F32).T.contiguous().cpu()
 
 
+def mark_small_rf(spins: torch.Tensor, segs: torch.Tensor, flags: np.ndarray) -> None:
+    """Set SMALL on the RF segments whose rotation |w|^2 = b1^2 (wx0^2 + wy0^2) + wz^2 stays below 0.0624 (under
+    the first tier's 1/16) for every spin, bounding |wz| = 2 pi |k.r + dt dB0 + beta| by the spins' extents (in the
+    device records and the host flags). The kernels then take the first-tier factors without tests: the same
+    arithmetic the tests would choose."""
+    if spins.shape[1] == 0 or segs.shape[0] == 0:
+        return
+    ext = spins.abs().amax(dim=1).to(F64)  # |x|, |y|, |z|, pd, r1, r2, |dB0|, |b1| maxima
+    rec = segs.to(F64)
+    wz = TWO_PI * (rec[:, 3].abs() * ext[0] + rec[:, 4].abs() * ext[1] + rec[:, 5].abs() * ext[2]
+                   + rec[:, 0].abs() * ext[6] + rec[:, 6].abs())
+    p2 = ext[7] ** 2 * (rec[:, 1] ** 2 + rec[:, 2] ** 2) + wz ** 2
+    bits = segs.view(torch.int32)[:, 7]
+    small = ((bits & RF) != 0) & (p2 < 0.0624)
+    bits |= small.to(torch.int32) * SMALL
+    flags |= small.cpu().numpy().astype(np.int32) * SMALL
+
+
 def pack(case, device) -> Packed:
     spins, sens = pack_spins(case.pos, case.pd, case.t1, case.t2, case.db0, case.b1, case.coils, device)
     segs, seg64, psi, flags, n_adc = pack_segments(case.dt, case.rf, case.grad, case.b0_offset, case.adc_phase,
                                                    case.is_rf, case.adc, case.spoil, device)
+    mark_small_rf(spins, segs, flags)
     return Packed(case.pd.shape[0], case.coils.shape[1], n_adc, spins, sens, segs, seg64, psi, flags, device)
 
 

@@ -78,6 +78,34 @@ def test_segment_records():
     assert rec.view(torch.int32)[:, 7].tolist() == flags.tolist()
 
 
+def test_small_rf_marks_follow_the_rotation_bound():
+    """SMALL goes on the RF segments whose |w|^2 is below 0.0624 for every spin (b1 and the positions' extents
+    bounding it), in the device records and the host flags alike; never on a free segment."""
+    b = sequences.SequenceBuilder().rf(1e-4, flip_deg=30.0, n_steps=10, grad=(0, 0, 100.0))
+    b.readout(4, 1e-5, grad=(1000.0, 0.0, 0.0))
+    seq = b.build()
+    rec, _, _, flags, _ = engine.pack_segments(seq.dt, seq.rf, seq.grad, None, seq.adc_phase, seq.is_rf, seq.adc,
+                                               seq.spoil, "cpu")
+
+    def marks(z_max, b1):
+        pos = torch.zeros(2, 3, dtype=F64)
+        pos[1, 2] = z_max
+        spins, _ = engine.pack_spins(pos, torch.ones(2, dtype=F64), torch.ones(2, dtype=F64),
+                                     torch.full((2,), 0.1, dtype=F64), torch.zeros(2, dtype=F64),
+                                     torch.full((2,), b1, dtype=F64), torch.ones(2, 1, dtype=torch.complex128), "cpu")
+        r, f = rec.clone(), flags.copy()
+        engine.mark_small_rf(spins, r, f)
+        assert r.view(torch.int32)[:, 7].tolist() == f.tolist()
+        return (f & engine.SMALL) != 0
+
+    rf = np.asarray(seq.is_rf)
+    # 30 degrees over 10 steps: 0.052 rad per step, and 2 pi 100 Hz/m 1e-5 s z: small up to z of a few metres
+    assert (marks(0.1, 1.0) == rf).all()
+    assert not marks(100.0, 1.0).any()     # the off-resonance of a spin far out in the slice gradient
+    assert not marks(0.1, 6.0).any()       # B1 scale 6: |w| = 0.31 > 1/4
+    assert not (marks(0.1, 1.0) & ~rf).any()
+
+
 def test_initial_state_split_is_exact():
     pd = torch.rand(100, dtype=F64)
     m = torch.rand(100, 3, dtype=F64)
