@@ -57,22 +57,27 @@ def flops_per_spin(flags: np.ndarray, n_coils: int) -> int:
             + (FLOP_ADC_PER_COIL * n_coils + FLOP_ADC) * n_adc)
 
 
-# the backward's work per spin and segment (counted from blochparty_b200/csrc/adjoint.cu; fixed): the interval
-# replay and the in-window recompute each repeat the forward's propagation (no coil contraction), then the
-# reverse sweep: RF segment 227 flops (rf_reverse with its rotation factors and offset gradients), free segment
-# 58 (free_reverse), ADC sample 16 per coil (signal and coil gradients) + 2.
-FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 227, 58, 16, 2
+# the backward's work per spin and segment (counted from blochparty_b200/csrc/adjoint.cu): the interval replay
+# repeats the forward's propagation (no coil contraction); the in-window recompute steps in plain float32: RF
+# segment 61 flops (rf_step_plain), free segment 13 (free_step_plain) + 18 when it recomputes its factors; the
+# reverse sweep: RF segment 163 (rf_reverse with its rotation factors and offset gradients), free segment 58
+# (free_reverse), ADC sample 8 per coil (the signal's cotangent; 16 with the coil gradients, which the measured
+# run does not request) + 2.
+FLOP_RF_RECOMP, FLOP_FREE_RECOMP, FLOP_FACTORS = 61, 13, 18
+FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 163, 58, 8, 2
 
 
 def grad_flops_per_spin(flags: np.ndarray, n_coils: int) -> tuple[int, int]:
-    """(forward, backward) algorithmic flops per spin of a simulation with gradients."""
+    """(forward, backward) algorithmic flops per spin of a simulation with gradients (no coil gradients)."""
     rf = (flags & 1) != 0
     n_rf, n_free = int(rf.sum()), int((~rf).sum())
+    n_free_miss = int((~rf & ((flags & 8) == 0)).sum())
     n_adc = int(((flags & 2) != 0).sum())
     fwd = flops_per_spin(flags, n_coils)
     prop = flops_per_spin(flags, 0) - FLOP_ADC * n_adc
+    recomp = FLOP_RF_RECOMP * n_rf + FLOP_FREE_RECOMP * n_free + FLOP_FACTORS * n_free_miss
     rev = FLOP_RF_REV * n_rf + FLOP_FREE_REV * n_free + (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc
-    return fwd, 2 * prop + rev
+    return fwd, prop + recomp + rev
 
 
 class Clocks:
