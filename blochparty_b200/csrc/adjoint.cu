@@ -32,6 +32,7 @@
 #define A_KEEP_RELAX (1 << 9)
 #define A_KEEP_WZ (1 << 10)
 #define A_KEEP_FREE (1 << 11)
+// (bits 0-6 are the record's own flags; BP_SMALL, bit 6, is not used by the sweep, which tests per warp)
 
 // per-spin gradient rows of `gs`
 enum { G_PX, G_PY, G_PZ, G_DB0, G_PD, G_R1, G_R2, G_B1, N_GS };
@@ -344,12 +345,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     const float ox = out[tid], oy = out[ADJ_THREADS + tid];
                     if (!URF && (f & BP_ADC) && a.h != nullptr) {
                         --row;
-                        const float* hr = a.h + (size_t)row * nv;
+                        // the row's (re, im) pairs: 8-byte aligned (rows of 2 C floats on a 256-byte aligned base)
+                        const float2* hr = reinterpret_cast<const float2*>(a.h + (size_t)row * nv);
                         float dx = 0.0f, dy = 0.0f;
 #pragma unroll
                         for (int c = 0; c < 8 * NCG; ++c) {
                             if (c < a.n_coils) {
-                                const float h0 = hr[2 * c], h1 = hr[2 * c + 1];
+                                const float2 hc = hr[c];
+                                const float h0 = hc.x, h1 = hc.y;
                                 dx = fmaf(h0, sr[c], fmaf(h1, si[c], dx));
                                 dy = fmaf(-h0, si[c], fmaf(h1, sr[c], dy));
                                 if (CG) {
@@ -525,6 +528,7 @@ extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_co
     if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg_len < 0 || grid < 1)
         return BP_E_ARG;
     if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs) return BP_E_ARG;
+    if ((reinterpret_cast<uintptr_t>(h) & 7) != 0) return BP_E_ALIGN;  // read as (re, im) pairs
     if (wb == wa) return BP_OK;
     AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
               reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, lam, gs, gc,

@@ -94,7 +94,8 @@ int bp_adjoint_grid(int n, int n_coils);
  * BP_ADJ_WIN segments, boundaries on multiples of BP_ADJ_WIN), [wa, wb) the interval's, covering segments
  * [seg0, seg0 + seg_len).
  *   wstates [wb - wa][6][n] the state at every window start (bp_forward replay of the interval, stride 1)
- *   h       [n_adc][2C] float32 dL/d(raw coil sums) = dL/dsignal rotated by exp(+i psi), or NULL
+ *   h       [n_adc][2C] float32 dL/d(raw coil sums) = dL/dsignal rotated by exp(+i psi), or NULL (8-byte
+ *           aligned: BP_E_ALIGN otherwise)
  *   lam     [3][n] in: dL/dm after the interval; out: dL/dm before it
  *   gs      [8][n] += dL/d(x, y, z, dB0, pd, r1, r2, b1)
  *   gc      [2C][n] += dL/d(coil c real, imaginary) at rows 2c, 2c+1, or NULL
