@@ -280,6 +280,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grad", action="store_true", help="forward + adjoint (gradients of T1 and the RF), one GPU")
     ap.add_argument("--surrogate-pieces", type=int, default=1, help="networks per slab pulse (--pulses surrogate)")
+    ap.add_argument("--surrogate-epochs", type=int, default=400,
+                    help="training epochs per network (--pulses surrogate; speed does not depend on them)")
     ap.add_argument("--workload", default="gre3d_64", choices=("gre3d_64", "gre3d_128_4echo"))
     ap.add_argument("--max-segments", type=int, default=0,
                     help="time the workload's first whole TRs only, up to this many segments (0: all)")
@@ -341,9 +343,9 @@ def main():
                                      float(seq.meta["slab_thickness"]), pieces=args.surrogate_pieces, device=dev)
         t0 = time.perf_counter()
         for sg in sgs:
-            sg.train()
-        sur_info = {"pieces": args.surrogate_pieces, "train_s": time.perf_counter() - t0,
-                    "network_error_max_rms": [sg.validate() for sg in sgs]}
+            sg.train(epochs=args.surrogate_epochs)
+        sur_info = {"pieces": args.surrogate_pieces, "epochs": args.surrogate_epochs,
+                    "train_s": time.perf_counter() - t0, "network_error_max_rms": [sg.validate() for sg in sgs]}
         sur = surrogate.SurrogateRun(inp, pk, sgs)
         windows, wdev = sur.plan[0], sur.plan[1]
     elif args.readout == "bf16x3":
