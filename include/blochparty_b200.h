@@ -48,7 +48,12 @@ int bp_forward_samp_max(int n_coils);
  * and the dispatch loop engines/gpu/driver.py:658-698).
  *   spins   [8][n] float32: x y z [m], pd, r1 = 1/T1, r2 = 1/T2 [1/s], dB0 [Hz], B1 scale
  *   sens    [16 ceil(C/8)][n] float32: coil c real part at row 2c, imaginary at 2c+1, zero padding rows
- *   segs    [S] 32-byte segment records (dt, -2 pi dt rf_x, -2 pi dt rf_y, g dt (3), b0_offset dt, flags)
+ *   segs    [S] 32-byte segment records (dt, -2 pi dt rf_x, -2 pi dt rf_y, g dt (3), b0_offset dt, flags);
+ *           flag bits: 1 RF, 2 ADC (sample after the segment), 4 spoil, 8 a free segment equal to the free segment
+ *           before it, 16 an RF segment with the dt of the RF segment before it, 32 the same with its moments and
+ *           offset too, 64 an RF segment whose rotation angle stays below 1/4 for every spin (optional: it only
+ *           spares the kernels' tests of the rotation factors' series; blochparty_b200.engine.mark_small_rf sets
+ *           it from a bound on the spins' extents)
  *   seg64   [S][4] float64: g dt (3), b0_offset dt (the free segments' phase, in float64)
  *   windows [n_windows][4] int32 from bp_plan_windows
  *   state   [6][n] float32 in/out: mx my mz and their compensation (low) parts
