@@ -210,7 +210,15 @@ def run_grad(args, dev):
     import blochparty_b200 as bpb
     from blochparty_b200 import adjoint, engine, workloads
 
-    ph, seq, coils = workloads.gre3d_64(args.n)
+    if args.workload == "gre3d_128_4echo":
+        ph, seq, coils = workloads.gre3d_128_4echo()
+        workload = WORKLOAD_128
+    else:
+        ph, seq, coils = workloads.gre3d_64(args.n)
+        workload = WORKLOAD if args.n == 64 else f"gre3d_{args.n}"
+    if args.max_segments:
+        seq = workloads.first_trs(seq, args.max_segments)
+        workload += f"; its first {len(seq)} segments (whole TRs)"
     n, S = len(ph.pd), len(seq)
     g = torch.Generator().manual_seed(7)
     n_adc = int(sum(seq.adc))
@@ -254,7 +262,7 @@ def run_grad(args, dev):
         "metric": "isochromat-steps/s (fwd+adjoint)", "value": n * S / (ms * 1e-3), "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD if args.n == 64 else f"gre3d_{args.n}", "spins": n, "segments": S,
+        "config": {"workload": workload, "spins": n, "segments": S,
                    "coils": coils.shape[1], "grad_wrt": ["t1", "rf"], "checkpoint_every": every,
                    "forward_ms": f_ms, "backward_ms": b_ms,
                    "l2": "inputs larger than L2; the forward starts from host tensors (packing and copies inside)"},

@@ -31,9 +31,11 @@ TWO_PI = 2.0 * math.pi
 
 
 def default_checkpoint_every(n_segments: int) -> int:
-    """About sqrt(segments), a multiple of the 32-segment adjoint window."""
+    """About sqrt(32 x segments), a multiple of the 32-segment adjoint window: the interval that minimises the
+    stored states, S / every checkpoints plus every / 32 window starts of one replayed interval (each segment is
+    replayed once whatever the interval)."""
     w = _lib.BP_ADJ_WIN
-    return w * max(1, math.ceil(math.sqrt(max(n_segments, 1)) / w))
+    return w * max(1, math.ceil(math.sqrt(w * max(n_segments, 1)) / w))
 
 
 class Plan:
