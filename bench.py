@@ -38,6 +38,10 @@ WORKLOAD = "gre3d_64: 3D spoiled GRE 64^3, 1,048,576 spins, 8 coils, 200-step si
 WORKLOAD_128 = ("gre3d_128_4echo: 4-echo 3D GRE 128^3 head phantom, 8,388,608 spins, 8 coils, 200-step sinc slab, "
                 "TR 20 ms")
 
+
+def head_workload(n: int) -> str:
+    return WORKLOAD_128 if n == 128 else f"gre3d_128_4echo at {n}^3 ({4 * n ** 3:,} spins, {n} samples per echo)"
+
 # algorithmic FP32 flops per spin and segment of the forward kernel (counted from its formulas in
 # blochparty_b200/csrc/bloch_common.cuh; kept fixed across versions): RF segment, free segment with cached
 # factors, free segment recomputing them, and an ADC sample per coil (complex multiply-add, 8 flops) + 2.
@@ -211,8 +215,8 @@ def run_grad(args, dev):
     from blochparty_b200 import adjoint, engine, workloads
 
     if args.workload == "gre3d_128_4echo":
-        ph, seq, coils = workloads.gre3d_128_4echo()
-        workload = WORKLOAD_128
+        ph, seq, coils = workloads.gre3d_128_4echo(args.head_n)
+        workload = head_workload(args.head_n)
     else:
         ph, seq, coils = workloads.gre3d_64(args.n)
         workload = WORKLOAD if args.n == 64 else f"gre3d_{args.n}"
@@ -291,6 +295,7 @@ def main():
     ap.add_argument("--surrogate-epochs", type=int, default=400,
                     help="training epochs per network (--pulses surrogate; speed does not depend on them)")
     ap.add_argument("--workload", default="gre3d_64", choices=("gre3d_64", "gre3d_128_4echo"))
+    ap.add_argument("--head-n", type=int, default=128, help="grid size of the 4-echo head workload (128: as named)")
     ap.add_argument("--max-segments", type=int, default=0,
                     help="time the workload's first whole TRs only, up to this many segments (0: all)")
     ap.add_argument("--pulses", default="step", choices=("step", "reuse", "surrogate"),
@@ -322,8 +327,8 @@ def main():
     from blochparty_b200 import _lib, engine, workloads
 
     if args.workload == "gre3d_128_4echo":
-        ph, seq, coils = workloads.gre3d_128_4echo()
-        workload = WORKLOAD_128
+        ph, seq, coils = workloads.gre3d_128_4echo(args.head_n)
+        workload = head_workload(args.head_n)
     else:
         ph, seq, coils = workloads.gre3d_64(args.n) if rank == 0 else _rank_workload(args.n, rank)
         workload = WORKLOAD if args.n == 64 else f"gre3d_{args.n}"
