@@ -336,6 +336,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 }
                 // sweep back
                 int row = win.z + win.w;
+                // the cotangent rows as (re, im) pairs: 8-byte aligned (rows of 2 C floats on an 8-byte aligned
+                // base, checked by bp_adjoint). A readout window loads each sample's row one sample ahead, so the
+                // loads' latency overlaps the sweep of the sample before (rows [win.z, win.z + win.w) only)
+                float2 hnext[8 * NCG];
+                if (KIND == 2 && a.h != nullptr && win.w > 0) {
+                    const float2* hr = reinterpret_cast<const float2*>(a.h + (size_t)(row - 1) * nv);
+#pragma unroll
+                    for (int c = 0; c < 8 * NCG; ++c) hnext[c] = c < a.n_coils ? hr[c] : make_float2(0.f, 0.f);
+                }
                 for (int s = nseg - 1; s >= 0; --s) {
                     const SegRec q = wrec[s];
                     const int f = q.flags;
@@ -345,13 +354,27 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     const float ox = out[tid], oy = out[ADJ_THREADS + tid];
                     if (!URF && (f & BP_ADC) && a.h != nullptr) {
                         --row;
-                        // the row's (re, im) pairs: 8-byte aligned (rows of 2 C floats on a 256-byte aligned base)
-                        const float2* hr = reinterpret_cast<const float2*>(a.h + (size_t)row * nv);
+                        float2 hrow[8 * NCG];
+                        if (KIND == 2) {
+#pragma unroll
+                            for (int c = 0; c < 8 * NCG; ++c) hrow[c] = hnext[c];
+                            if (row > win.z) {
+                                const float2* hr = reinterpret_cast<const float2*>(a.h + (size_t)(row - 1) * nv);
+#pragma unroll
+                                for (int c = 0; c < 8 * NCG; ++c)
+                                    if (c < a.n_coils) hnext[c] = hr[c];
+                            }
+                        } else {
+                            const float2* hr = reinterpret_cast<const float2*>(a.h + (size_t)row * nv);
+#pragma unroll
+                            for (int c = 0; c < 8 * NCG; ++c)
+                                if (c < a.n_coils) hrow[c] = hr[c];
+                        }
                         float dx = 0.0f, dy = 0.0f;
 #pragma unroll
                         for (int c = 0; c < 8 * NCG; ++c) {
                             if (c < a.n_coils) {
-                                const float2 hc = hr[c];
+                                const float2 hc = hrow[c];
                                 const float h0 = hc.x, h1 = hc.y;
                                 dx = fmaf(h0, sr[c], fmaf(h1, si[c], dx));
                                 dy = fmaf(-h0, si[c], fmaf(h1, sr[c], dy));
