@@ -345,13 +345,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
 #pragma unroll
                     for (int c = 0; c < 8 * NCG; ++c) hnext[c] = c < a.n_coils ? hr[c] : make_float2(0.f, 0.f);
                 }
+                // the state after the segment being swept (its output, before its spoil): slot s + 1, which the
+                // previous iteration read as its input
+                float outx = slots[nseg * 3 * ADJ_THREADS + tid], outy = slots[(nseg * 3 + 1) * ADJ_THREADS + tid];
+                float outz = slots[(nseg * 3 + 2) * ADJ_THREADS + tid];
                 for (int s = nseg - 1; s >= 0; --s) {
                     const SegRec q = wrec[s];
                     const int f = q.flags;
                     if (KIND == 0 && (f & BP_SPOIL)) lx = ly = 0.0f;
-                    // the segment's output state: slot s + 1
-                    const float* out = slots + (s + 1) * 3 * ADJ_THREADS;
-                    const float ox = out[tid], oy = out[ADJ_THREADS + tid];
+                    const float ox = outx, oy = outy, oz = outz;
                     if (!URF && (f & BP_ADC) && a.h != nullptr) {
                         --row;
                         float2 hrow[8 * NCG];
@@ -390,6 +392,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     const float* in = slots + s * 3 * ADJ_THREADS;
                     float x0 = in[tid], y0 = in[ADJ_THREADS + tid];
                     const float z0 = in[2 * ADJ_THREADS + tid];
+                    outx = x0, outy = y0, outz = z0;
                     if (KIND == 0 && (f & A_PREV_SPOIL)) x0 = y0 = 0.0f;
                     SegGrad sg;
 #pragma unroll
@@ -400,7 +403,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                             if (!(f & A_KEEP_RELAX)) rr = rev_relax(q.dt, p);
                             if (!(f & A_KEEP_WZ)) wz = rf_wz(q, p);
                         }
-                        rf_reverse<KIND == 3>(q, p, rr, wz, x0, y0, z0, ox, oy, out[2 * ADJ_THREADS + tid], lx, ly, lz, g, sg);
+                        rf_reverse<KIND == 3>(q, p, rr, wz, x0, y0, z0, ox, oy, oz, lx, ly, lz, g, sg);
                     } else {
                         if (KIND == 0 && !(f & A_KEEP_FREE)) ff = free_factors(q, wk64[s], p);
                         free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
