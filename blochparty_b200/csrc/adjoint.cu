@@ -273,6 +273,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
             // at the end of the previous window ended its reads. The flags word of record s is written by thread s
             // alone, with the sweep's own bits added (from the global records, so no thread reads a word another
             // writes)
+            // the window's start state (from the replay, in DRAM for long intervals): loaded first, so that its
+            // latency overlaps the staging below and its barrier
+            float m0x = 0.f, m0y = 0.f, m0z = 0.f;
+            if (active) {
+                const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
+                m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j], m0z = ws[2 * n + j] + ws[5 * n + j];
+            }
             const SegRec* gw = a.segs + win.x;
             for (int i = tid; i < nseg * 8; i += ADJ_THREADS)
                 if ((i & 7) != 7) reinterpret_cast<float*>(wrec)[i] = reinterpret_cast<const float*>(gw)[i];
@@ -308,10 +315,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 constexpr bool URF = KIND == 1 || KIND == 3;
                 // recompute the window in plain float32 from its (compensated) start state: slot k = state after
                 // segment k-1 (before its spoil), slot 0 = window start
-                const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
-                float mx = 0.f, my = 0.f, mz = 0.f;
-                if (active)
-                    mx = ws[j] + ws[3 * n + j], my = ws[n + j] + ws[4 * n + j], mz = ws[2 * n + j] + ws[5 * n + j];
+                float mx = m0x, my = m0y, mz = m0z;
                 slots[tid] = mx, slots[ADJ_THREADS + tid] = my, slots[2 * ADJ_THREADS + tid] = mz;
                 FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 RevRelax rr{0.f, 0.f, 1.f, 1.f, 1.f, 1.f, true};
