@@ -687,9 +687,10 @@ extern "C" int bp_surrogate_pulse(const float* spins, float* state, int n, const
 static_assert(SI_OFF_A % 1024 == 0 && SI_OFF_W1 % 16 == 0 && SI_OFF_W4 % 16 == 0, "operand alignment");
 static_assert(MLP_IN <= SI_K1, "layer 1 fits one K step");
 
-// NCH x 8 values of this thread's row -> A hi and A lo rows, chunks [0, NCH) (16-byte stores)
+// NCH x 8 values of this thread's row -> A hi and A lo rows, chunks [chunk0, chunk0 + NCH) (16-byte stores)
 template <int NCH>
-__device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned char* alo, int row, const float* v) {
+__device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned char* alo, int row, const float* v,
+                                                 int chunk0) {
 #pragma unroll
     for (int c = 0; c < NCH; ++c) {
         uint32_t h[4], l[4];
@@ -702,16 +703,16 @@ __device__ __forceinline__ void store_row_bf16x2(unsigned char* ahi, unsigned ch
             h[w] = *reinterpret_cast<const uint32_t*>(&hp);
             l[w] = *reinterpret_cast<const uint32_t*>(&lp);
         }
-        const uint32_t off = (uint32_t)((row >> 3) * SI_SBO + c * SI_LBO + (row & 7) * 16);
+        const uint32_t off = (uint32_t)((row >> 3) * SI_SBO + (chunk0 + c) * SI_LBO + (row & 7) * 16);
         *reinterpret_cast<uint4*>(ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
         *reinterpret_cast<uint4*>(alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
     }
 }
 
-// The network's biases, passed by value in the kernel's arguments (832 bytes of the constant bank): every thread
-// reads the same bias at the same time, so the adds take them as constant operands, no loads.
+// The network's biases, passed by value in the kernel's arguments (832 bytes of the constant bank; every thread
+// reads the same bias at the same time): b1, b2, b3 (64 each), then b4 (16).
 struct SmallNet {
-    float b1[MLP_H], b2[MLP_H], b3[MLP_H], b4[MLP_OUT];
+    float bias[3 * MLP_H + MLP_OUT];
 };
 
 struct PulseMmaArgs {
@@ -721,7 +722,8 @@ struct PulseMmaArgs {
     SmallNet net;
 };
 
-__global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMmaArgs args) {
+// (__grid_constant__: the biases are indexed in place in the parameter space, not copied to the stack)
+__global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(const __grid_constant__ PulseMmaArgs args) {
     extern __shared__ __align__(1024) unsigned char smb[];
     const PulseArgs& a = args.p;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smb + SI_OFF_BAR);  // [0] weights, [1] MMA
@@ -733,7 +735,7 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t sW = smem_u32(smb), sA = smem_u32(ahi);
 
-    const SmallNet& net = args.net;
+    const float* bias = args.net.bias;
     if (tid == 0) {
         *queued = 0;
         mbar_init(&bars[0], 1);
@@ -762,20 +764,17 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
         const float df = p.db0 + a.b0off;
         const float zr = (float)(((double)p.pz - a.z0) / a.thickness);
         const bool inside = active && fabsf(df) <= a.dom_df && fabsf(p.b1 - 1.0f) <= a.dom_b1 && fabsf(zr) <= a.dom_z;
-        float v[MLP_H], y[MLP_OUT];
-        {   // layer 1's input: the features, zero-padded to 16
-            float xin[MLP_X];
+        float y[MLP_OUT];
+        {   // layer 1's input: the features, zero-padded to 16, as the A operand's first two chunks
+            float xin[MLP_X], g[SI_K1];
             pulse_inputs(a, p, df, xin);
-            mlp_features(xin[0], xin[1], v);
+            mlp_features(xin[0], xin[1], g);
 #pragma unroll
-            for (int i = MLP_IN; i < SI_K1; ++i) v[i] = 0.0f;
+            for (int i = MLP_IN; i < SI_K1; ++i) g[i] = 0.0f;
+            store_row_bf16x2<SI_K1 / 8>(ahi, alo, tid, g, 0);
         }
-#pragma unroll
-        for (int layer = 0; layer < 4; ++layer) {  // unrolled: operands, shapes and biases are constants per layer
-            if (layer == 0)
-                store_row_bf16x2<SI_K1 / 8>(ahi, alo, tid, v);
-            else
-                store_row_bf16x2<MLP_H / 8>(ahi, alo, tid, v);
+#pragma unroll 1
+        for (int layer = 0; layer < 4; ++layer) {  // a real loop: one copy of the code serves the four layers
             fence_proxy_async_smem();
             tc_fence_before();
             if (__syncthreads_or(err)) {
@@ -797,7 +796,6 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
                     uint64_t ah_d = umma_desc(sA, SI_LBO, SI_SBO), al_d = umma_desc(sA + SI_A_BYTES, SI_LBO, SI_SBO);
                     uint64_t bh_d = umma_desc(wh, SI_LBO, sbo_w), bl_d = umma_desc(wl, SI_LBO, sbo_w);
                     const int k_steps = layer == 0 ? SI_K1 / 16 : MLP_H / 16;
-#pragma unroll
                     for (int kk = 0; kk < k_steps; ++kk) {
                         umma_bf16(d, ah_d, bh_d, idesc, kk > 0 ? 1u : 0u);
                         umma_bf16(d, ah_d, bl_d, idesc, 1u);
@@ -820,21 +818,24 @@ __global__ void __launch_bounds__(128, 3) bp_surrogate_pulse_mma_kernel(PulseMma
             }
             tc_fence_after();
             if (layer < 3) {
-#pragma unroll
+                // the layer's output 16 columns at a time: bias and GELU, split straight into the next A operand
+                // (the MMA that read the A operand has completed)
+                const float* b = bias + layer * MLP_H;
+#pragma unroll 1
                 for (int c0 = 0; c0 < MLP_H; c0 += 16) {
                     float d[16];
                     tmem_ld16(lane_addr + (uint32_t)c0, d);
                     tmem_ld_wait();
-                    const float* b = layer == 0 ? net.b1 : layer == 1 ? net.b2 : net.b3;
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) v[c0 + i] = gelu_f(d[i] + b[c0 + i]);
+                    for (int i = 0; i < 16; ++i) d[i] = gelu_f(d[i] + b[c0 + i]);
+                    store_row_bf16x2<2>(ahi, alo, tid, d, c0 / 8);
                 }
             } else {
                 float d[16];
                 tmem_ld16(lane_addr + (uint32_t)SI_D4, d);
                 tmem_ld_wait();
 #pragma unroll
-                for (int o = 0; o < MLP_OUT; ++o) y[o] = d[o] + net.b4[o];
+                for (int o = 0; o < MLP_OUT; ++o) y[o] = d[o] + bias[3 * MLP_H + o];
             }
             tc_fence_before();
         }
@@ -983,10 +984,10 @@ extern "C" int bp_surrogate_pulse_mma(const float* spins, float* state, int n, c
     PulseMmaArgs a{{spins, state, nullptr, static_cast<const SegRec*>(segs), seg0, k_steps, n, T, gz, thickness, z0,
                     phi0, b0off, counts, dom_df, dom_b1, dom_z, dom_df + fabs(gz) * dom_z * thickness},
                    static_cast<const uint8_t*>(wtiles), status, {}};
-    std::memcpy(a.net.b1, params_host + P_B1, sizeof(a.net.b1));
-    std::memcpy(a.net.b2, params_host + P_B2, sizeof(a.net.b2));
-    std::memcpy(a.net.b3, params_host + P_B3, sizeof(a.net.b3));
-    std::memcpy(a.net.b4, params_host + P_B4, sizeof(a.net.b4));
+    std::memcpy(a.net.bias, params_host + P_B1, MLP_H * sizeof(float));
+    std::memcpy(a.net.bias + MLP_H, params_host + P_B2, MLP_H * sizeof(float));
+    std::memcpy(a.net.bias + 2 * MLP_H, params_host + P_B3, MLP_H * sizeof(float));
+    std::memcpy(a.net.bias + 3 * MLP_H, params_host + P_B4, MLP_OUT * sizeof(float));
     bp_surrogate_pulse_mma_kernel<<<grid, 128, SI_SMEM, static_cast<cudaStream_t>(stream)>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
