@@ -38,6 +38,29 @@ def default_checkpoint_every(n_segments: int) -> int:
     return w * max(1, math.ceil(math.sqrt(w * max(n_segments, 1)) / w))
 
 
+def run_breaks(flags: np.ndarray) -> np.ndarray:
+    """Window breaks for the adjoint at the start of every run of like segments: where RF and free segments
+    alternate, where an RF segment changes dt or offset, where a free segment changes its factors, and after every
+    spoiling segment, and at every multiple of 32 segments. The sweep runs a window whose segments are all one RF
+    run, or all one free run (spoiling at most in its last segment), without per-segment tests. The windows are
+    the 32-segment blocks cut at these breaks: the checkpoint intervals (multiples of 32) add no cut, so every
+    window, its recompute and the gradients keep the same bits for every interval. No break falls inside a
+    readout run of the forward kernel (samples with one segment's factors, the last of which may spoil, cut at
+    32-segment blocks), whose arithmetic would change with a cut: the replayed states keep their bits too."""
+    S = flags.shape[0]
+    out = np.zeros(S, dtype=np.uint8)
+    if S < 2:
+        return out
+    rf = (flags & engine.RF) != 0
+    spoil = (flags & engine.SPOIL) != 0
+    same_off = (flags & engine.SAME_OFF) != 0
+    same_free = (flags & engine.SAME_FREE) != 0
+    cut = (rf[1:] != rf[:-1]) | (rf[1:] & ~same_off[1:]) | (~rf[1:] & ~same_free[1:]) | spoil[:-1]
+    out[1:] = cut
+    out[::_lib.BP_ADJ_WIN] = 1
+    return out
+
+
 class Plan:
     """Windows and intervals of one gradient-carrying simulation."""
 
@@ -50,7 +73,7 @@ class Plan:
         samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
         self.fwin = engine.plan_windows(pk.flags, samp, breaks=breaks)
         w = _lib.BP_ADJ_WIN
-        self.awin = engine.plan_windows(pk.flags, w, seg_max=w, breaks=breaks)
+        self.awin = engine.plan_windows(pk.flags, w, seg_max=w, breaks=breaks | run_breaks(pk.flags))
         self.fwin_dev = torch.from_numpy(self.fwin).to(device)
         self.awin_dev = torch.from_numpy(self.awin).to(device)
         # window ranges of every interval

@@ -295,13 +295,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
             for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
                 reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
             // the window's kind (the same for the whole CTA): every segment RF with the dt and offset of the first,
-            // no sample and no spoil (the steps of an RF pulse); or every segment free with the factors of the
-            // first and no spoil (a readout's samples). Their sweeps skip the per-segment tests.
+            // no sample (the steps of an RF pulse); or every segment free with the factors of the first (a
+            // readout's samples); in either, a spoil at most after the last segment. Their sweeps skip the
+            // per-segment tests.
             bool rf_ok = true, free_ok = true;
             if (tid < nseg) {
                 const int f = gw[tid].flags;
-                rf_ok = (f & BP_RF) && !(f & (BP_ADC | BP_SPOIL)) && (tid == 0 || (f & BP_SAME_OFF));
-                free_ok = !(f & BP_RF) && !(f & BP_SPOIL) && (tid == 0 || (f & BP_SAME_FREE));
+                const bool spoil_ok = !(f & BP_SPOIL) || tid == nseg - 1;
+                rf_ok = (f & BP_RF) && !(f & BP_ADC) && spoil_ok && (tid == 0 || (f & BP_SAME_OFF));
+                free_ok = !(f & BP_RF) && spoil_ok && (tid == 0 || (f & BP_SAME_FREE));
             }
             if (warp == 0) {  // the window's largest wx0^2 + wy0^2 (non-negative floats order as their bits)
                 const float v = lane < nseg ? fmaf(gw[lane].wx0, gw[lane].wx0, gw[lane].wy0 * gw[lane].wy0) : 0.0f;
@@ -340,6 +342,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 }
                 // sweep back
                 int row = win.z + win.w;
+                // (a uniform window spoils at most after its last segment, where the sweep starts)
+                if (KIND != 0 && (wrec[nseg - 1].flags & BP_SPOIL)) lx = ly = 0.0f;
                 // the cotangent rows as (re, im) pairs: 8-byte aligned (rows of 2 C floats on an 8-byte aligned
                 // base, checked by bp_adjoint). A readout window loads each sample's row one sample ahead, so the
                 // loads' latency overlaps the sweep of the sample before (rows [win.z, win.z + win.w) only)
