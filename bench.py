@@ -64,11 +64,11 @@ def flops_per_spin(flags: np.ndarray, n_coils: int) -> int:
 # the backward's work per spin and segment (counted from blochparty_b200/csrc/adjoint.cu): the interval replay
 # repeats the forward's propagation (no coil contraction); the in-window recompute steps in plain float32: RF
 # segment 61 flops (rf_step_plain), free segment 13 (free_step_plain) + 18 when it recomputes its factors; the
-# reverse sweep: RF segment 163 (rf_reverse with its rotation factors and offset gradients), free segment 58
-# (free_reverse), ADC sample 8 per coil (the signal's cotangent; 16 with the coil gradients, which the measured
-# run does not request) + 2.
+# reverse sweep as the measured run (gradients of T1 and the RF) takes it, without the offsets' gradients: RF
+# segment 130 (rf_reverse with its rotation factors; 163 with the offsets'), free segment 30 (free_reverse; 58),
+# ADC sample 8 per coil (the signal's cotangent; 16 with the coil gradients) + 2.
 FLOP_RF_RECOMP, FLOP_FREE_RECOMP, FLOP_FACTORS = 61, 13, 18
-FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 163, 58, 8, 2
+FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 130, 30, 8, 2
 
 
 def grad_flops_per_spin(flags: np.ndarray, n_coils: int) -> tuple[int, int]:

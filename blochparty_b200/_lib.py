@@ -38,6 +38,7 @@ BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 BP_PULSE_MAP_BYTES = 96
 BP_SEG_DT, BP_SEG_WX, BP_SEG_WY, BP_SEG_KX, BP_SEG_KY, BP_SEG_KZ, BP_SEG_BETA = (1 << k for k in range(7))
 BP_SEG_ALL = 0x7F
+BP_SPIN_NO_OFFSETS = 0x80  # with seg_mask: the position and dB0 rows of the spin gradients are not wanted
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",

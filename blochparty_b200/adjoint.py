@@ -145,7 +145,7 @@ class _Simulate(torch.autograd.Function):
         # with dt), the RF its two components, the gradient the moments, b0_offset its phase
         seg_mask = (_lib.BP_SEG_ALL if need[8] else 0) | ((_lib.BP_SEG_WX | _lib.BP_SEG_WY) if need[9] else 0) | (
             (_lib.BP_SEG_KX | _lib.BP_SEG_KY | _lib.BP_SEG_KZ) if need[10] else 0) | (
-            _lib.BP_SEG_BETA if need[12] else 0)
+            _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5]) else _lib.BP_SPIN_NO_OFFSETS)
         grid = _lib.lib().bp_adjoint_grid(n, C)
         if grid < 1:
             raise RuntimeError("bp_adjoint_grid failed")

@@ -150,7 +150,7 @@ __device__ __forceinline__ void free_step_plain(const FreeFactors& f, const Spin
 // gradients accumulated. The rotated state n = R m1 comes from the output, m2 = E n + c, by E's inverse (or, with
 // strong relaxation, from the input). dL/dw = J^T (n x a), a = dL/dn and J the rotation's left Jacobian
 // (R(w + d) = exp([J d]x) R(w)): J^T u = s1 u - s2 (w x u) + s3 (w . u) w.
-template <bool SMALL>
+template <bool SMALL, bool OG>
 __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float x0,
                                            float y0, float z0, float ox, float oy, float oz, float& lx, float& ly,
                                            float& lz, float* g, SegGrad& sg) {
@@ -183,7 +183,7 @@ __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const
     const float k3 = s3 * fmaf(wx, ux, fmaf(wy, uy, wz * uz));
     const float gwx = fmaf(s1, ux, fmaf(-s2, wy * uz - wz * uy, k3 * wx));
     const float gwy = fmaf(s1, uy, fmaf(-s2, wz * ux - wx * uz, k3 * wy));
-    const float gwz = fmaf(s1, uz, fmaf(-s2, wx * uy - wy * ux, k3 * wz));
+    const float gwz = OG ? fmaf(s1, uz, fmaf(-s2, wx * uy - wy * ux, k3 * wz)) : 0.0f;
     // first half relaxation
     gd2 = fmaf(bx, x0, fmaf(by, y0, gd2));
     gd1 = fmaf(bz, z0 - p.pd, gd1);
@@ -193,20 +193,24 @@ __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const
     g[G_R1] = fmaf(-gd1 * h, a1, g[G_R1]);
     g[G_R2] = fmaf(-gd2 * h, a2, g[G_R2]);
     g[G_PD] += gpd;
-    sg.v[S_DT] -= 0.5f * (gd1 * p.r1 * a1 + gd2 * p.r2 * a2);
     g[G_B1] = fmaf(gwx, q.wx0, fmaf(gwy, q.wy0, g[G_B1]));
     sg.v[S_WX] += gwx * p.b1;
     sg.v[S_WY] += gwy * p.b1;
-    offset_grads(-BP_TWO_PI_F * gwz, q, p, g, sg);
+    if (OG) {  // the offset's and dt's gradients (position, dB0, segment dt, moments, b0_offset)
+        sg.v[S_DT] -= 0.5f * (gd1 * p.r1 * a1 + gd2 * p.r2 * a2);
+        offset_grads(-BP_TWO_PI_F * gwz, q, p, g, sg);
+    }
 }
 
-// Reverse of a free segment (rotation about z by phi = -2 pi cyc, then exact relaxation).
+// Reverse of a free segment (rotation about z by phi = -2 pi cyc, then exact relaxation). OG: the offset's and dt's
+// gradients are wanted.
+template <bool OG>
 __device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, const FreeFactors& f, float x0, float y0,
                                              float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
     const float c = f.ch, s = f.sh, a2 = 1.0f + f.e2, a1 = 1.0f + f.e1;
     const float ux = fmaf(c, x0, -s * y0), uy = fmaf(s, x0, c * y0);
     const float gd2 = fmaf(lx, ux, ly * uy);
-    const float gphi = a2 * fmaf(ly, ux, -lx * uy);
+    const float gphi = OG ? a2 * fmaf(ly, ux, -lx * uy) : 0.0f;
     const float nlx = a2 * fmaf(c, lx, s * ly), nly = a2 * fmaf(-s, lx, c * ly);
     const float gd1 = lz * (z0 - p.pd);
     g[G_PD] = fmaf(-lz, f.e1, g[G_PD]);
@@ -214,8 +218,10 @@ __device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, con
     lx = nlx, ly = nly;
     g[G_R2] = fmaf(-gd2 * q.dt, a2, g[G_R2]);
     g[G_R1] = fmaf(-gd1 * q.dt, a1, g[G_R1]);
-    sg.v[S_DT] -= gd2 * p.r2 * a2 + gd1 * p.r1 * a1;
-    offset_grads(-BP_TWO_PI_F * gphi, q, p, g, sg);
+    if (OG) {
+        sg.v[S_DT] -= gd2 * p.r2 * a2 + gd1 * p.r1 * a1;
+        offset_grads(-BP_TWO_PI_F * gphi, q, p, g, sg);
+    }
 }
 
 template <int K>
@@ -223,8 +229,10 @@ struct KindTag {
     static constexpr int value = K;
 };
 
-// NCG: groups of 8 coils; CG: whether the coil gradients are wanted (a.gc not null).
-template <int NCG, bool CG>
+// NCG: groups of 8 coils; CG: whether the coil gradients are wanted (a.gc not null); OG: whether the gradients
+// of the spins' offsets (position, dB0) or of the segments' dt, moments or b0_offset are wanted (otherwise their
+// rows of gs and columns of gseg are left as they were).
+template <int NCG, bool CG, bool OG>
 __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kernel(AdjArgs a) {
     extern __shared__ __align__(16) float sm[];
     float* slots = sm;                                     // [ADJ_SLOTS][3][ADJ_THREADS]
@@ -236,7 +244,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
     const int nv = 2 * a.n_coils;
     const bool need_seg = a.gseg != nullptr;
-    const bool rf_only = need_seg && (a.seg_mask & ~((1 << S_WX) | (1 << S_WY))) == 0;
+    const bool rf_only = need_seg && (a.seg_mask & BP_SEG_ALL & ~((1 << S_WX) | (1 << S_WY))) == 0;
     for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) segacc[i] = 0.0f;
     if (need_seg)
         for (int i = tid; i < a.seg_len * N_SG; i += ADJ_THREADS) a.gseg[(size_t)blockIdx.x * a.seg_len * N_SG + i] = 0.0f;
@@ -411,10 +419,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                             if (!(f & A_KEEP_RELAX)) rr = rev_relax(q.dt, p);
                             if (!(f & A_KEEP_WZ)) wz = rf_wz(q, p);
                         }
-                        rf_reverse<KIND == 3>(q, p, rr, wz, x0, y0, z0, ox, oy, oz, lx, ly, lz, g, sg);
+                        rf_reverse<KIND == 3, OG>(q, p, rr, wz, x0, y0, z0, ox, oy, oz, lx, ly, lz, g, sg);
                     } else {
                         if (KIND == 0 && !(f & A_KEEP_FREE)) ff = free_factors(q, wk64[s], p);
-                        free_reverse(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
+                        free_reverse<OG>(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
                     }
                     if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0, 16 hold them)
                         if (KIND != 2) {  // (a free segment's are 0: a uniform free window writes and adds none)
@@ -493,15 +501,15 @@ static size_t adj_smem() {
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.
-template <int NCG, bool CG>
+template <int NCG, bool CG, bool OG>
 static int adj_configure() {
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)adj_smem()) != cudaSuccess ||
-            cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return -1;
         configured[dev] = true;
@@ -510,11 +518,11 @@ static int adj_configure() {
 }
 
 // CTAs per SM of one variant, or -1
-template <int NCG, bool CG>
+template <int NCG, bool CG, bool OG>
 static int adj_per_sm() {
     int per_sm = 0;
-    if (adj_configure<NCG, CG>() < 0 ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG>, ADJ_THREADS,
+    if (adj_configure<NCG, CG, OG>() < 0 ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG, OG>, ADJ_THREADS,
                                                       adj_smem()) != cudaSuccess)
         return -1;
     return per_sm > 0 ? per_sm : 1;
@@ -526,10 +534,13 @@ static int adj_grid(int n) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int with_cg = adj_per_sm<NCG, true>(), without = adj_per_sm<NCG, false>();
-    if (with_cg < 0 || without < 0) return -1;
+    const int with_cg = adj_per_sm<NCG, true, true>(), without = adj_per_sm<NCG, false, true>();
+    const int lean = adj_per_sm<NCG, false, false>();
+    if (with_cg < 0 || without < 0 || lean < 0) return -1;
     const int n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
-    const int grid = sms * (with_cg < without ? with_cg : without);
+    int per_sm = with_cg < without ? with_cg : without;
+    if (lean < per_sm) per_sm = lean;
+    const int grid = sms * per_sm;
     return grid < n_tiles ? grid : n_tiles;
 }
 
@@ -545,12 +556,18 @@ extern "C" int bp_adjoint_grid(int n, int n_coils) {
 
 template <int NCG>
 static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
+    // the offsets' gradients: wanted unless the caller marks the spins' ones unwanted and wants no segment
+    // gradient that uses them (with coil gradients, always computed)
+    const bool og = !(a.seg_mask & BP_SPIN_NO_OFFSETS) || (a.seg_mask & (BP_SEG_ALL & ~(BP_SEG_WX | BP_SEG_WY)));
     if (a.gc) {
-        if (adj_configure<NCG, true>() < 0) return BP_E_LAUNCH;
-        bp_adjoint_kernel<NCG, true><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
+        if (adj_configure<NCG, true, true>() < 0) return BP_E_LAUNCH;
+        bp_adjoint_kernel<NCG, true, true><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
+    } else if (og) {
+        if (adj_configure<NCG, false, true>() < 0) return BP_E_LAUNCH;
+        bp_adjoint_kernel<NCG, false, true><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
     } else {
-        if (adj_configure<NCG, false>() < 0) return BP_E_LAUNCH;
-        bp_adjoint_kernel<NCG, false><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
+        if (adj_configure<NCG, false, false>() < 0) return BP_E_LAUNCH;
+        bp_adjoint_kernel<NCG, false, false><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
     }
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }

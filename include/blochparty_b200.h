@@ -107,7 +107,9 @@ int bp_adjoint_grid(int n, int n_coils);
  *   gseg    [grid][seg_len][8] scratch: per-CTA segment gradients (w.r.t. the record's dt, -2 pi dt rf_x,
  *           -2 pi dt rf_y, g dt (3), b0_offset dt), or NULL when no segment gradient is wanted
  *   seg_mask  the segment gradients wanted (BP_SEG_* bits; the others in gseg are left 0 or unreduced): only
- *           BP_SEG_WX | BP_SEG_WY (the RF alone) takes a cheaper reduction
+ *           BP_SEG_WX | BP_SEG_WY (the RF alone) takes a cheaper reduction; plus BP_SPIN_NO_OFFSETS when the
+ *           rows x, y, z and dB0 of gs are not wanted (left as they were): without coil gradients and without
+ *           BP_SEG_DT, KX, KY, KZ, BETA, the sweep then skips the offsets' gradients altogether
  *   grid    bp_adjoint_grid(n, n_coils) */
 #define BP_SEG_DT 1
 #define BP_SEG_WX 2
@@ -117,6 +119,7 @@ int bp_adjoint_grid(int n, int n_coils);
 #define BP_SEG_KZ 32
 #define BP_SEG_BETA 64
 #define BP_SEG_ALL 127
+#define BP_SPIN_NO_OFFSETS 128
 int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
                const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates, const float* h,
                float* lam, float* gs, float* gc, float* gseg, int seg_mask, int grid, void* stream);

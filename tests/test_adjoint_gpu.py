@@ -158,6 +158,19 @@ def test_gradients_do_not_depend_on_checkpoint_interval():
         assert torch.equal(b[k], c[k]), k
 
 
+def test_sweep_without_offset_gradients_matches_the_full_sweep():
+    """Asking for T1, T2, PD and the RF alone takes the sweep variant that skips the offsets' gradients (position,
+    dB0, segment dt, moments, b0_offset): its gradients are the full sweep's, bit for bit."""
+    ph, seq, coils, flips, t1_target = _adjoint_case(16)
+    target = _target(ph, seq, coils, t1_target)
+    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum() + m.double().sum()
+    lean = ("pd", "t1", "t2", "rf")
+    _, a = gpu_gradients(ph, seq, coils, None, loss, lean)
+    _, b = gpu_gradients(ph, seq, coils, None, loss, lean + ("pos", "db0"))
+    for k in lean:
+        assert torch.equal(a[k], b[k]), k
+
+
 def test_checkpoint_every_must_be_window_multiple():
     ph, seq, coils, _, _ = _adjoint_case(8)
     with pytest.raises(ValueError, match="multiple of 32"):
