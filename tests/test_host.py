@@ -106,6 +106,42 @@ def test_small_rf_marks_follow_the_rotation_bound():
     assert not (marks(0.1, 1.0) & ~rf).any()
 
 
+@pytest.mark.parametrize("workload", ["gre3d_16", "head_16"])
+def test_adjoint_windows_follow_runs_and_not_intervals(workload):
+    """The adjoint's windows (32-segment blocks cut again at every run start): the same for every checkpoint
+    interval (a multiple of 32), every window one RF run or one free run (spoiling at most last), and no cut inside
+    a readout run of the forward kernel (whose merged arithmetic a cut would change)."""
+    from blochparty_b200 import adjoint, workloads
+
+    if workload == "gre3d_16":
+        _, seq, _ = workloads.gre3d_64(16)
+    else:
+        _, seq, _ = workloads.gre3d_128_4echo(16)
+    flags = engine.pack_segments(seq.dt, seq.rf, seq.grad, None, seq.adc_phase, list(seq.is_rf), list(seq.adc),
+                                 list(seq.spoil), "cpu")[3]
+    S, w = len(flags), _lib.BP_ADJ_WIN
+    rb = adjoint.run_breaks(flags)
+    plans = []
+    for every in (w * 2, w * 37, w * 1000):
+        br = np.zeros(S, dtype=np.uint8)
+        br[::every] = 1
+        plans.append(engine.plan_windows(flags, w, seg_max=w, breaks=br | rb))
+    assert all(np.array_equal(plans[0], p) for p in plans[1:])
+    win = plans[0]
+    for s0, s1, _, _ in win.tolist():
+        f = flags[s0:s1]
+        rf = (f & engine.RF) != 0
+        assert rf.all() or (~rf).all(), (s0, s1)
+        assert not (f[:-1] & engine.SPOIL).any(), (s0, s1)
+        same = engine.SAME_OFF if rf[0] else engine.SAME_FREE
+        assert ((f[1:] & same) != 0).all(), (s0, s1)
+        if s0 % w and s0 > 0:  # a cut the 32-segment blocks do not make: not inside a readout run
+            prev, cur = int(flags[s0 - 1]), int(flags[s0])
+            inside = ((cur & ~engine.SPOIL) & 0x3F) == (engine.ADC | engine.SAME_FREE) and (prev & engine.ADC) \
+                and not (prev & (engine.SPOIL | engine.RF))
+            assert not inside, s0
+
+
 def test_initial_state_split_is_exact():
     pd = torch.rand(100, dtype=F64)
     m = torch.rand(100, 3, dtype=F64)
