@@ -231,9 +231,18 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                         // recurrence; the state after the run is this one advanced by the merged factors (exact
                         // phase in float64), as if stepped one by one.
                         const int block_end = min(nseg, (win.x + s) / BP_ADJ_WIN * BP_ADJ_WIN + BP_ADJ_WIN - win.x);
-                        int e = s + 1;  // the run's end: one scan of the flags, then a tight loop over its samples
-                        while (e < block_end && (q0[e].flags & ~BP_SPOIL) == (BP_ADC | BP_SAME_FREE))
-                            if (q0[e++].flags & BP_SPOIL) break;
+                        // the run's end, from one flag per lane (the candidates s + 1 + lane, at most 31 before the
+                        // block's end): the samples that continue the run, up to the first that does not, or
+                        // through the first that spoils. Then a tight loop over its samples.
+                        const int ec = s + 1 + lane;
+                        const int fc = ec < block_end ? q0[ec].flags : 0;
+                        const unsigned cont = __ballot_sync(0xffffffffu, ec < block_end &&
+                                                                          (fc & ~BP_SPOIL) == (BP_ADC | BP_SAME_FREE));
+                        const unsigned spoils = cont & __ballot_sync(0xffffffffu, (fc & BP_SPOIL) != 0);
+                        int len = __ffs(~cont) - 1;  // leading continuing samples (cont != ~0: lane 31 is past the block)
+                        const unsigned sp = spoils & ((1u << len) - 1u);
+                        if (sp) len = __ffs(sp);     // through the first spoiling one
+                        const int e = s + 1 + len;
                         if (readout) {
                             float zr = mx + lx, zi = my + ly;
                             stage(zr, zi);
