@@ -49,6 +49,19 @@ class Packed:
     device: torch.device
 
 
+def _bools(flags, n: int) -> np.ndarray:
+    """A sequence of n truth values (Python bools or ints, as blochparty's Sequence holds them) as a bool array:
+    through bytes() when every item is a small int (four times faster on a million items), else item by item."""
+    if isinstance(flags, (list, tuple)):
+        try:
+            out = np.frombuffer(bytes(flags), dtype=np.uint8).astype(bool)
+            if out.shape[0] == n:
+                return out
+        except (TypeError, ValueError):
+            pass
+    return np.fromiter((bool(x) for x in flags), dtype=bool, count=n)
+
+
 def _np64(t) -> np.ndarray:
     return t.detach().to(F64).cpu().numpy()
 
@@ -68,35 +81,40 @@ def pack_spins(pos, pd, t1, t2, db0, b1, coils, device):
 
 
 def pack_segments(dt, rf, grad, b0_offset, adc_phase, is_rf, adc, spoil, device):
-    """Segment records (float64 arithmetic, one rounding to float32), the float64 moments, flags and psi."""
+    """Segment records (float64 arithmetic, one rounding to float32), the float64 moments, flags and psi. The
+    fields are filled and compared as contiguous rows of a field-major array, then transposed once into records."""
     dt, rf, grad = _np64(dt), _np64(rf), _np64(grad)
     S = dt.shape[0]
     b0 = np.zeros(S) if b0_offset is None else _np64(b0_offset)
     w = -TWO_PI * dt
-    k = grad * dt[:, None]
+    k = grad.T * dt  # (3, S)
     beta = b0 * dt
-    rec = np.empty((S, 8), dtype=np.float32)
-    rec[:, 0] = dt
-    rec[:, 1] = w * rf[:, 0]
-    rec[:, 2] = w * rf[:, 1]
-    rec[:, 3:6] = k
-    rec[:, 6] = beta
-    seg64 = np.empty((S, 4), dtype=np.float64)
-    seg64[:, 0:3] = k
-    seg64[:, 3] = beta
-    is_rf = np.asarray(is_rf, dtype=bool)
-    adc_b = np.asarray(adc, dtype=bool)
-    spoil_b = np.asarray(spoil, dtype=bool)
+    cols = np.empty((8, S), dtype=np.float32)  # the record's fields, one row each
+    cols[0] = dt
+    cols[1] = w * rf[:, 0]
+    cols[2] = w * rf[:, 1]
+    cols[3:6] = k
+    cols[6] = beta
+    k64 = np.empty((4, S), dtype=np.float64)
+    k64[0:3] = k
+    k64[3] = beta
+    is_rf, adc_b, spoil_b = (_bools(f, S) for f in (is_rf, adc, spoil))
     flags = is_rf.astype(np.int32) | (adc_b.astype(np.int32) << 1) | (spoil_b.astype(np.int32) << 2)
     if S > 1:
         free = ~is_rf
-        same_dt = rec[1:, 0] == rec[:-1, 0]
-        same_free = free[1:] & free[:-1] & same_dt & (seg64[1:] == seg64[:-1]).all(1)
+        same_dt = cols[0, 1:] == cols[0, :-1]
+        same_k = same_dt.copy()  # the moments and the offset phase
+        for c in range(4):
+            same_k &= k64[c, 1:] == k64[c, :-1]
+        same_free = free[1:] & free[:-1] & same_k
         same_rf = is_rf[1:] & is_rf[:-1] & same_dt
-        same_off = same_rf & (rec[1:, 3:7] == rec[:-1, 3:7]).all(1)  # the same G.r + dt dB0 + beta per spin
+        same_off = same_rf.copy()  # the same G.r + dt dB0 + beta per spin
+        for c in range(3, 7):
+            same_off &= cols[c, 1:] == cols[c, :-1]
         flags[1:] |= ((same_free.astype(np.int32) << 3) | (same_rf.astype(np.int32) << 4)
                       | (same_off.astype(np.int32) << 5))
-    rec.view(np.int32)[:, 7] = flags
+    cols.view(np.int32)[7] = flags
+    rec, seg64 = np.ascontiguousarray(cols.T), np.ascontiguousarray(k64.T)
     psi = np.remainder(_np64(adc_phase)[adc_b], TWO_PI)
     return (torch.from_numpy(rec).to(device).contiguous(), torch.from_numpy(seg64).to(device).contiguous(),
             torch.from_numpy(psi).to(device).contiguous(), flags, int(adc_b.sum()))
