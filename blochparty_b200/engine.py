@@ -161,7 +161,8 @@ def mark_small_rf(spins: torch.Tensor, segs: torch.Tensor, flags: np.ndarray) ->
     """Set SMALL on the RF segments whose rotation |w|^2 = b1^2 (wx0^2 + wy0^2) + wz^2 stays below 0.0624 (under
     the first tier's 1/16) for every spin, bounding |wz| = 2 pi |k.r + dt dB0 + beta| by the spins' extents (in the
     device records and the host flags). The kernels then take the first-tier factors without tests: the same
-    arithmetic the tests would choose."""
+    arithmetic the tests would choose. (The reference tests phi per spin and step, switching to its two-term
+    series below phi = 1e-3: blochparty ``engines/gpu/shaders/common.metal:57-72``.)"""
     if spins.shape[1] == 0 or segs.shape[0] == 0:
         return
     ext = spins.abs().amax(dim=1).to(F64)  # |x|, |y|, |z|, pd, r1, r2, |dB0|, |b1| maxima
