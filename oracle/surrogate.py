@@ -5,7 +5,8 @@ The reference (blochparty) has no learned surrogate: its closest parts are the e
 pulses (``engines/gpu/cuda/pulse.cu.in:3-32``, ``engines/gpu/driver.py:112-164``). What this oracle restates is
 the plain integrator's rotation part (blochparty ``engines/core.py:97-108``: a rotation by
 w = -2 pi dt (b1 rf_x, b1 rf_y, G z + df) per RF segment), composed over a pulse as unit quaternions, and the
-surrogate's network in float64 with autograd (to check the hand-written training kernels' gradients).
+surrogate's network in float64 with autograd (to check the hand-written training kernels' gradients), and the
+map the inference kernels apply to one pulse occurrence (``pulse_map``).
 
 Conventions (shared with ``blochparty_b200/csrc/surrogate.cu``):
 
@@ -168,3 +169,30 @@ def loss_and_grad(p, x, target, vweight: float = 1.0, cweight: float = 1.0):
     loss = (w * (mlp(p, x.to(F64)) - target.to(F64)) ** 2).sum(-1).mean()
     (g,) = torch.autograd.grad(loss, [p])
     return float(loss), g
+
+
+def _rz(a):
+    c, s = torch.cos(a), torch.sin(a)
+    z, o = torch.zeros_like(a), torch.ones_like(a)
+    return torch.stack([torch.stack([c, -s, z], -1), torch.stack([s, c, z], -1), torch.stack([z, z, o], -1)], -2)
+
+
+def pulse_map(t, T, half, phi0, r1, r2, pd, m, first_order=True):
+    """The surrogate's map of one pulse occurrence in float64, as the inference kernels apply it
+    (``apply_pulse_map`` in ``blochparty_b200/csrc/surrogate.cu``): targets (or network outputs) ``t`` (n, 16), the
+    pulse's duration ``T``, ``half`` (n,) = -pi (G z + df) T (half the whole-pulse precession), the occurrence's RF
+    phase ``phi0``, the spins' rates and PD, magnetisation ``m`` (n, 3) -> (n, 3). With a1 = half + phi0 and
+    a2 = half - phi0: R = Rz(a1) R~ Rz(a2), dA = Rz(a1) dA~ Rz(a2), dC = Rz(a1) dC~; relax T/2, apply
+    R - (r2 - r1) dA, relax T/2, add r1 pd dC (``first_order=False``: the splitting alone)."""
+    q = t[:, :4] / torch.linalg.vector_norm(t[:, :4], dim=-1, keepdim=True)
+    ra, rb = _rz(half + phi0), _rz(half - phi0)
+    M = ra @ rotmat(q) @ rb
+    if first_order:
+        dA = ra @ (T * t[:, 4:13].reshape(-1, 3, 3)) @ rb
+        M = M - ((r2 - r1) * 1.0)[:, None, None] * dA
+    e2, e1 = torch.exp(-0.5 * T * r2), torch.exp(-0.5 * T * r1)
+    E = lambda v: torch.stack([v[:, 0] * e2, v[:, 1] * e2, pd + (v[:, 2] - pd) * e1], -1)
+    out = E((M @ E(m)[..., None])[..., 0])
+    if first_order:
+        out = out + (r1 * pd * T)[:, None] * (ra @ t[:, 13:16, None])[..., 0]
+    return out

@@ -6,9 +6,9 @@ Bars: targets (float64 composition rounded to float32) within 1e-6 of the oracle
 within 1e-4 (largest relative error) of float64 autograd; tensor-core inference within 1e-4 of float32 inference
 (magnetization, unit PD scale), the fallback spins bit-identical; the TSE and the 3D GRE through the surrogate
 within 1e-3 relative L2 of the float64 oracle (whole-pulse relax / rotate / relax splitting alone is 2.3e-2 off on
-the TSE's refocusing train; the networks' first-order relaxation terms bring the splitting to 1.0e-4, measured by a
-float64 CPU emulation with exact terms, so the rest is the networks' own error: the refocusing pulses' rotations
-dominate it); and a measured speed-up over plain sub-stepping on the same GPU.
+the TSE's refocusing train; the networks' first-order relaxation terms bring the splitting to 1.0e-4 with exact
+terms, `test_surrogate_host.py::test_first_order_pulse_map_reaches_the_stepped_signal`, so the rest is the
+networks' own error: the refocusing pulses' rotations dominate it); and a measured speed-up over plain sub-stepping on the same GPU.
 """
 
 import math
@@ -117,7 +117,7 @@ def test_tse_through_the_surrogate_against_the_float64_oracle(tse_surrogates):
     l2 = lambda a: float(torch.linalg.vector_norm(a.to(sig64.dtype) - sig64) / torch.linalg.vector_norm(sig64))
     e_sur, e_plain = l2(sur.signal), l2(plain.signal)
     print(f"\nTSE 16^2 x 3 slices: surrogate rel L2 {e_sur:.2e}, plain sub-stepping {e_plain:.2e} (vs float64)")
-    # splitting alone is 2.3e-2 off here; with exact first-order terms 1.0e-4 (float64 CPU emulation)
+    # splitting alone is 2.3e-2 off here; with exact first-order terms 1.0e-4 (the host test of pulse_map)
     assert e_plain < 2e-5
     assert e_sur < 1e-3
 
