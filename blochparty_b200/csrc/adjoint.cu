@@ -5,16 +5,19 @@
 //
 // Checkpointing has three levels. The forward stores the state at the start of every checkpoint interval. The
 // backward replays one interval at a time with the forward kernel (no readout), storing the state at the start
-// of every adjoint window (<= BP_ADJ_WIN segments). This kernel then sweeps the interval's windows in reverse:
-// per window it recomputes the window forward from its start state, keeping the state after every segment in
-// shared memory (one slot per segment and spin), and runs the segments backward from them.
+// of every adjoint window (<= BP_ADJ_WIN segments, also cut at every run of like segments). This kernel then
+// sweeps the interval's windows in reverse: per window it recomputes the window forward from its start state in
+// plain float32, keeping the state after every segment in shared memory (one slot per segment and spin), and runs
+// the segments backward from them. A window that is one RF run or one readout run takes a sweep without
+// per-segment tests.
 //
 // Segment s maps the magnetization affinely, m_s = A_s m_{s-1} + b_s. With lambda = dL/dm after segment s
 // (after its spoil), the sweep is lambda_{s-1} = A_s^T (P_s lambda + dL/dm of the sample), P_s the spoil
-// projection; the parameter gradients of segment s follow from lambda and m_{s-1}. Per-spin gradients stay in
-// registers over a window and are added to global memory at its end; per-segment gradients are reduced over the warp by shuffles, over the CTA's
-// warps in fixed order in shared memory, and written as one float32 partial per CTA and segment; bp_seg_reduce
-// adds the CTAs' partials in fixed order in float64. No atomics: every run gives the same bits.
+// projection; the parameter gradients of segment s follow from lambda and m_{s-1} (for an RF segment's rotation,
+// through the rotation's left Jacobian). Per-spin gradients are running totals in registers through the interval;
+// per-segment gradients are reduced over the warp by shuffles, over the CTA's warps in fixed order in shared
+// memory, and written as one float32 partial per CTA and segment; bp_seg_reduce adds the CTAs' partials in fixed
+// order in float64. No atomics: every run gives the same bits.
 #include <cuda_runtime.h>
 
 #include <cstdint>
