@@ -6,10 +6,11 @@ identical ``types``) and runs them on hand-written sm_100a CUDA kernels through 
 """
 
 from .api import simulate
+from .pulseq import read_pulseq
 from .phantoms import birdcage_sensitivities, ellipse_phantom_2d, ellipsoid_phantom_3d, grid_positions, head_phantom_3d
 from .sequences import SequenceBuilder, gre, sinc_pulse, tse_2d
 from .types import Phantom, Sequence, SimResult
 
 __all__ = ["simulate", "Phantom", "Sequence", "SimResult", "SequenceBuilder", "gre", "tse_2d", "sinc_pulse",
            "birdcage_sensitivities", "ellipse_phantom_2d", "ellipsoid_phantom_3d", "head_phantom_3d",
-           "grid_positions"]
+           "grid_positions", "read_pulseq"]
