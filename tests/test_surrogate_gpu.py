@@ -8,7 +8,8 @@ within 1e-4 (largest relative error) of float64 autograd; tensor-core inference 
 within 1e-3 relative L2 of the float64 oracle (whole-pulse relax / rotate / relax splitting alone is 2.3e-2 off on
 the TSE's refocusing train; the networks' first-order relaxation terms bring the splitting to 1.0e-4 with exact
 terms, `test_surrogate_host.py::test_first_order_pulse_map_reaches_the_stepped_signal`, so the rest is the
-networks' own error: the refocusing pulses' rotations dominate it); and a measured speed-up over plain sub-stepping on the same GPU.
+networks' own error: the refocusing pulses' rotations dominate it); and a measured speed-up over plain
+sub-stepping on the same GPU.
 """
 
 import math
@@ -92,8 +93,8 @@ def test_training_lowers_the_loss_and_the_error():
 @pytest.fixture(scope="module")
 def tse_surrogates():
     """Networks for the six TSE pulses (3 slices x excitation / refocusing), trained on 2^20 samples each (600
-    epochs of 4,096-sample steps, ~24 s per pulse) over |z_rel| <= 2.5: the slices are contiguous, so every spin of the 3-slice stack lies
-    within 2.5 slice widths of every pulse's centre."""
+    epochs of 4,096-sample steps, ~24 s per pulse) over |z_rel| <= 2.5: the slices are contiguous, so every spin
+    of the 3-slice stack lies within 2.5 slice widths of every pulse's centre."""
     out, info = [], []
     for z0 in (-5e-3, 0.0, 5e-3):
         for flip, phase in ((90.0, 0.0), (180.0, 0.5 * math.pi)):
