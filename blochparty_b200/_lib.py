@@ -25,6 +25,21 @@ class BpSpan(ctypes.Structure):
                 ("wtiles", c_void_p), ("T", c_double), ("gz", c_double), ("thickness", c_double), ("z0", c_double),
                 ("dom_df", c_float), ("dom_b1", c_float), ("dom_z", c_float), ("counts", c_void_p)]
 
+
+
+class BpForwardWorkspace(ctypes.Structure):
+    """``BpForwardWorkspace`` of the C ABI: the forward's device buffer sizes in bytes."""
+
+    _fields_ = [(f, c_int64) for f in ("state", "raw", "psi", "signal", "status", "total")]
+
+
+class BpAdjointWorkspace(ctypes.Structure):
+    """``BpAdjointWorkspace`` of the C ABI: the checkpointed adjoint's device buffer sizes in bytes."""
+
+    _fields_ = [(f, c_int64) for f in ("checkpoints", "wstates", "replay_state", "gseg", "seg", "lam", "gs", "gc",
+                                        "h", "total")]
+
+
 BP_OK, BP_E_ARG, BP_E_ALIGN, BP_E_LAUNCH, BP_E_SIZE = 0, 1, 2, 3, 4
 BP_MAX_COILS = 32
 BP_SEG_MAX = 160
@@ -42,7 +57,7 @@ BP_SPIN_NO_OFFSETS = 0x80  # with seg_mask: the position and dB0 rows of the spi
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",
-               2: "a window record was invalid"}
+               2: "a window record was invalid (outside the sequence, the interval or the samples)"}
 
 _P = c_void_p
 # (restype, argtypes) of every exported entry point, as declared in include/blochparty_b200.h
@@ -59,8 +74,8 @@ SIGNATURES = {
     "bp_mma_atiles": (c_int, [_P, c_int, c_int, _P, _P]),
     "bp_forward_mma": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P]),
     "bp_adjoint_grid": (c_int, [c_int, c_int]),
-    "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P,
-                           c_int, c_int, _P]),
+    "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, c_int, _P, _P, _P,
+                           _P, c_int, c_int, _P, _P]),
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
     "bp_pulse_targets": (c_int, [_P, c_int, c_double, c_double, c_double, c_double, _P, c_int, _P, _P, _P]),
     "bp_mlp_grad_ctas": (c_int, [c_int]),
@@ -77,8 +92,10 @@ SIGNATURES = {
     "bp_surrogate_pulse_mma_grid": (c_int, [c_int]),
     "bp_surrogate_pulse_mma": (c_int, [_P, _P, c_int, _P, _P, _P, c_int, c_int, c_double, c_double, c_double,
                                        c_double, c_double, c_float, c_float, c_float, c_float, _P, _P, c_int, _P]),
-    "bp_adjoint_noalloc": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P,
-                                   _P, _P]),
+    "bp_adjoint_noalloc": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, c_int, _P,
+                                   _P, _P, _P, _P, _P]),
+    "bp_forward_workspace_bytes": (c_int, [c_int, c_int64, c_int, _P]),
+    "bp_adjoint_workspace_bytes": (c_int, [c_int, c_int64, c_int64, c_int, c_int, c_int, c_int, _P]),
 }
 
 _lib = None
@@ -121,3 +138,19 @@ def ptr(t: torch.Tensor | None) -> int | None:
 
 def stream_ptr() -> int:
     return torch.cuda.current_stream().cuda_stream
+
+
+def forward_workspace(n: int, n_adc: int, n_coils: int) -> BpForwardWorkspace:
+    """The forward's buffer sizes (``bp_forward_workspace_bytes``; host arithmetic, no GPU)."""
+    out = BpForwardWorkspace()
+    check(lib().bp_forward_workspace_bytes(n, n_adc, n_coils, ctypes.byref(out)), "bp_forward_workspace_bytes")
+    return out
+
+
+def adjoint_workspace(n: int, n_segments: int, n_adc: int, n_coils: int, every: int, max_interval_windows: int,
+                      grid: int) -> BpAdjointWorkspace:
+    """The checkpointed adjoint's buffer sizes (``bp_adjoint_workspace_bytes``; host arithmetic, no GPU)."""
+    out = BpAdjointWorkspace()
+    check(lib().bp_adjoint_workspace_bytes(n, n_segments, n_adc, n_coils, every, max_interval_windows, grid,
+                                           ctypes.byref(out)), "bp_adjoint_workspace_bytes")
+    return out

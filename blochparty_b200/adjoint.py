@@ -30,6 +30,15 @@ F32, F64 = torch.float32, torch.float64
 TWO_PI = 2.0 * math.pi
 
 
+def sized(nbytes: int, shape, dtype, device, zero: bool = False) -> torch.Tensor:
+    """A device buffer of ``shape`` whose size is the C ABI's workspace figure ``nbytes`` (checked)."""
+    t = (torch.zeros if zero else torch.empty)(*shape, dtype=dtype, device=device)
+    if t.numel() * t.element_size() != nbytes:
+        raise RuntimeError(f"buffer {tuple(shape)} {dtype}: {t.numel() * t.element_size()} bytes, the workspace "
+                           f"query says {nbytes}")
+    return t
+
+
 def default_checkpoint_every(n_segments: int) -> int:
     """About sqrt(32 x segments), a multiple of the 32-segment adjoint window: the interval that minimises the
     stored states, S / every checkpoints plus every / 32 window starts of one replayed interval (each segment is
@@ -103,8 +112,10 @@ class _Simulate(torch.autograd.Function):
         pk = engine.pack(inp, dev)
         plan = Plan(pk, every, dev)
         state = engine.initial_state(inp.pd, inp.m_init, dev)
-        ckpts = torch.empty(len(plan.starts), 6, pk.n, dtype=F32, device=dev)
-        raw = torch.zeros(max(pk.n_adc, 1), 2 * pk.n_coils, dtype=F64, device=dev)
+        fws = _lib.forward_workspace(pk.n, pk.n_adc, pk.n_coils)
+        aws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, every, plan.max_aw, 1)
+        ckpts = sized(aws.checkpoints, (len(plan.starts), 6, pk.n), F32, dev)
+        raw = sized(fws.raw, (max(pk.n_adc, 1), 2 * pk.n_coils), F64, dev, zero=True)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         for k, (fa, fb) in enumerate(plan.franges):
             ckpts[k].copy_(state)
@@ -130,29 +141,31 @@ class _Simulate(torch.autograd.Function):
         if g_sig is None and g_m is None:
             return (None,) * 14
         n, C, A, S = pk.n, pk.n_coils, pk.n_adc, len(dt)
+        grid = _lib.lib().bp_adjoint_grid(n, C)
+        if grid < 1:
+            raise RuntimeError("bp_adjoint_grid failed")
+        ws = _lib.adjoint_workspace(n, S, A, C, plan.every, plan.max_aw, grid)
         h = None
         if g_sig is not None and A:
             g = torch.complex(g_sig[..., 0].to(F64), g_sig[..., 1].to(F64)).to(dev)  # (C, A)
             hr = g * torch.exp(1j * pk.psi)[None, :]  # dL/draw = dL/dsignal e^{+i psi}
-            h = torch.view_as_real(hr.T.contiguous()).reshape(A, 2 * C).to(F32).contiguous()
-        lam = torch.zeros(3, n, dtype=F32, device=dev)
+            h = sized(ws.h, (A, 2 * C), F32, dev)
+            h.copy_(torch.view_as_real(hr.T.contiguous()).reshape(A, 2 * C))
+        lam = sized(ws.lam, (3, n), F32, dev, zero=True)
         if g_m is not None:
             lam.copy_(g_m.T.to(F32))
-        gs = torch.zeros(8, n, dtype=F32, device=dev)
-        gc = torch.zeros(2 * C, n, dtype=F32, device=dev) if (need[7] and h is not None) else None
+        gs = sized(ws.gs, (8, n), F32, dev, zero=True)
+        gc = sized(ws.gc, (2 * C, n), F32, dev, zero=True) if (need[7] and h is not None) else None
         need_seg = any(need[i] for i in (8, 9, 10, 12))
         # the segment gradients the chain rules below use: dt needs all of them (the record's every field scales
         # with dt), the RF its two components, the gradient the moments, b0_offset its phase
         seg_mask = (_lib.BP_SEG_ALL if need[8] else 0) | ((_lib.BP_SEG_WX | _lib.BP_SEG_WY) if need[9] else 0) | (
             (_lib.BP_SEG_KX | _lib.BP_SEG_KY | _lib.BP_SEG_KZ) if need[10] else 0) | (
             _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5]) else _lib.BP_SPIN_NO_OFFSETS)
-        grid = _lib.lib().bp_adjoint_grid(n, C)
-        if grid < 1:
-            raise RuntimeError("bp_adjoint_grid failed")
-        gseg = torch.empty(grid, plan.max_len, 8, dtype=F32, device=dev) if need_seg else None
-        seg = torch.zeros(S, 8, dtype=F64, device=dev)
-        wstates = torch.empty(plan.max_aw, 6, n, dtype=F32, device=dev)
-        state = torch.empty(6, n, dtype=F32, device=dev)
+        gseg = sized(ws.gseg, (grid, plan.max_len, 8), F32, dev) if need_seg else None
+        seg = sized(ws.seg, (S, 8), F64, dev, zero=True)
+        wstates = sized(ws.wstates, (plan.max_aw, 6, n), F32, dev)
+        state = sized(ws.replay_state, (6, n), F32, dev)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         lib, stream = _lib.lib(), _lib.stream_ptr()
         for k in reversed(range(len(plan.starts))):
@@ -161,13 +174,13 @@ class _Simulate(torch.autograd.Function):
             state.copy_(ctx.ckpts[k])
             engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, status, wstates=wstates, wstate_stride=1)
             code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
-                                  aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
-                                  seg_mask, grid, stream)
+                                  aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
+                                  seg_mask, grid, ptr(status), stream)
             _lib.check(code, "bp_adjoint")
             if need_seg:
                 _lib.check(lib.bp_seg_reduce(ptr(gseg), grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
         torch.cuda.synchronize(dev)
-        _lib.check_status(status, "bp_forward (replay)")
+        _lib.check_status(status, "bp_forward (replay) / bp_adjoint")
         gs64, lam64 = gs.to(F64).cpu(), lam.to(F64).cpu()
         out = [None] * 13
         if need[1]:

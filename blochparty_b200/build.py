@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -43,9 +44,9 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     nvcc = _nvcc()
     objdir = ROOT / "_build"
     objdir.mkdir(exist_ok=True)
-    objs = []
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Wno-deprecated-gpu-targets", f"-I{ROOT / 'include'}"]
-    for src in sources():
+
+    def compile_one(src: Path) -> str:
         obj = objdir / (src.stem + ".o")
         if src.suffix == ".cu":
             cmd = [nvcc, *ARCH, "-lineinfo", *common, "-c", str(src), "-o", str(obj)]
@@ -58,7 +59,11 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             raise RuntimeError(f"nvcc failed on {src.name}:\n{r.stdout}\n{r.stderr}")
         if verbose and r.stderr:
             print(r.stderr, file=sys.stderr)
-        objs.append(str(obj))
+        return str(obj)
+
+    # one nvcc per source, in parallel (the sources are independent translation units)
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
+        objs = list(pool.map(compile_one, sources()))
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

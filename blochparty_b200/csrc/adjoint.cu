@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "bloch_common.cuh"
 #include "../../include/blochparty_b200.h"
@@ -54,11 +55,13 @@ struct AdjArgs {
     int seg0, seg_len;    // first segment of the interval, segments in it
     const float* wstates; // [wb - wa][6][n] state at every window start (replay)
     const float* h;       // [n_adc][2C] dL/d(raw coil sums), or null
+    int n_adc;            // rows of h
     float* lam;           // [3][n] in: dL/dm at the interval's end; out: at its start
     float* gs;            // [N_GS][n] += per-spin gradients
     float* gc;            // [2C][n] += coil gradients (rows 2c real, 2c+1 imaginary), or null
     float* gseg;          // [gridDim.x][seg_len][N_SG] per-CTA segment gradients, or null
     int seg_mask;         // which of the N_SG segment gradients are reduced (bit k: component k)
+    int* status;          // |= BP_ERR_BAD_WINDOW for a window outside the interval (skipped)
 };
 
 // Rodrigues factors of the rotation by |w| (p2 = |w|^2) with the third factor of its left Jacobian:
@@ -279,7 +282,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
         for (int w = a.wb - 1; w >= a.wa; --w) {
             const int4 win = a.windows[w];
             const int nseg = win.y - win.x;
-            if (nseg < 0 || nseg > BP_ADJ_WIN) continue;  // not an adjoint window (uniform): never index past the slots
+            // a window the sweep can run: at most BP_ADJ_WIN segments (the slots), inside the interval (the rows of
+            // gseg), its samples inside h. Anything else is skipped (the same for the whole CTA) and reported.
+            if (nseg < 0 || nseg > BP_ADJ_WIN || win.x < a.seg0 || win.y > a.seg0 + a.seg_len || win.z < 0 ||
+                win.w < 0 || (a.h != nullptr && win.z + win.w > a.n_adc)) {
+                if (tid == 0) atomicOr(a.status, BP_ERR_BAD_WINDOW);
+                continue;
+            }
             // the window's records into shared memory (every warp of the CTA sweeps the same window); the barrier
             // at the end of the previous window ended its reads. The flags word of record s is written by thread s
             // alone, with the sweep's own bits added (from the global records, so no thread reads a word another
@@ -577,16 +586,17 @@ static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
 
 extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs,
                           const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
-                          const float* wstates, const float* h, float* lam, float* gs, float* gc, float* gseg,
-                          int seg_mask, int grid, void* stream) {
-    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg_len < 0 || grid < 1)
+                          const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc,
+                          float* gseg, int seg_mask, int grid, int32_t* status, void* stream) {
+    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg0 < 0 || seg_len < 0 || grid < 1 ||
+        n_adc < 0)
         return BP_E_ARG;
-    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs) return BP_E_ARG;
+    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs || !status) return BP_E_ARG;
     if ((reinterpret_cast<uintptr_t>(h) & 7) != 0) return BP_E_ALIGN;  // read as (re, im) pairs
     if (wb == wa) return BP_OK;
     AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
-              reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, lam, gs, gc,
-              gseg, seg_mask};
+              reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, n_adc, lam, gs,
+              gc, gseg, seg_mask, status};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch ((n_coils + 7) / 8) {
         case 1: return launch_adj<1>(a, grid, st);
@@ -618,29 +628,38 @@ extern "C" int bp_seg_reduce(const float* gseg, int n_cta, int seg_len, int seg0
 
 static __device__ __align__(256) float bp_noalloc_scratch[BP_NOALLOC_SCRATCH_FLOATS];
 
-// Device address of the array per device, looked up once with that device current (in host code the array's
-// name is only a host-side stand-in, not a device address).
+// Device address of the array per device, looked up once per device with that device current (in host code the
+// array's name is only a host-side stand-in, not a device address). std::call_once makes the lookup safe from
+// several host threads. A cudaDeviceReset unloads the module, which leaves the stored address stale: callers of
+// this entry point must not reset the device between calls.
+static std::once_flag g_noalloc_once[64];
 static float* g_noalloc_ptr[64];
+static int g_noalloc_code[64];
 
 static int noalloc_scratch(float** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BP_E_LAUNCH;
-    if (!g_noalloc_ptr[dev]) {
+    std::call_once(g_noalloc_once[dev], [dev] {
         void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, bp_noalloc_scratch) != cudaSuccess || p == nullptr) return BP_E_LAUNCH;
+        if (cudaGetSymbolAddress(&p, bp_noalloc_scratch) != cudaSuccess || p == nullptr) {
+            g_noalloc_code[dev] = BP_E_LAUNCH;
+            return;
+        }
         g_noalloc_ptr[dev] = static_cast<float*>(p);
-    }
+        g_noalloc_code[dev] = BP_OK;
+    });
+    if (g_noalloc_code[dev] != BP_OK) return g_noalloc_code[dev];
     *out = g_noalloc_ptr[dev];
     return BP_OK;
 }
 
 extern "C" int bp_adjoint_noalloc(const float* spins, const float* sens, int n, int n_coils, const void* segs,
                                   const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
-                                  const float* wstates, const float* h, float* lam, float* gs, float* gc, double* seg,
-                                  void* stream) {
-    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg_len < 0 || seg0 < 0)
+                                  const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc,
+                                  double* seg, int32_t* status, void* stream) {
+    if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg_len < 0 || seg0 < 0 || n_adc < 0)
         return BP_E_ARG;
-    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs) return BP_E_ARG;
+    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs || !status) return BP_E_ARG;
     // one CTA needs seg_len * N_SG floats of the array; more CTAs share it up to its size
     const long long per_cta = (long long)seg_len * N_SG;
     if (seg && per_cta > BP_NOALLOC_SCRATCH_FLOATS) return BP_E_SIZE;
@@ -653,8 +672,8 @@ extern "C" int bp_adjoint_noalloc(const float* spins, const float* sens, int n, 
     if (seg && per_cta > 0 && (long long)grid * per_cta > BP_NOALLOC_SCRATCH_FLOATS)
         grid = (int)(BP_NOALLOC_SCRATCH_FLOATS / per_cta);
     // the kernel clears each CTA's rows of the scratch before accumulating into them
-    code = bp_adjoint(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, lam, gs, gc,
-                      seg ? scratch : nullptr, BP_SEG_ALL, grid, stream);
+    code = bp_adjoint(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, n_adc, lam, gs,
+                      gc, seg ? scratch : nullptr, BP_SEG_ALL, grid, status, stream);
     if (code != BP_OK || !seg) return code;
     return bp_seg_reduce(scratch, grid, seg_len, seg0, seg, stream);
 }

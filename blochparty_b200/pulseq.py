@@ -199,7 +199,8 @@ class _Reader:
             w = amp * self.shape(sid)
             if tid == 0:  # samples at the raster cells' centres; edges from continuity and the cells' means
                 edges = np.empty(w.shape[0] + 1)
-                edges[0] = self.last[axis]
+                # a delayed waveform starts from the zero gradient of its delay, else from the previous block's end
+                edges[0] = 0.0 if delay > 0 else self.last[axis]
                 for i in range(w.shape[0]):
                     edges[i + 1] = 2.0 * w[i] - edges[i]
                 t = np.concatenate([[0.0], (np.arange(w.shape[0]) + 0.5) * self.grad_raster,

@@ -41,6 +41,26 @@ extern "C" {
 int bp_plan_windows(const int32_t* flags, int64_t n_segments, int seg_max, int samp_max, const uint8_t* breaks,
                     int32_t* windows, int64_t max_windows, int64_t* n_windows);
 
+/* Device buffer sizes (bytes) of one simulation, host arithmetic only (no GPU): what blochparty's driver sizes in
+ * Python (engines/gpu/driver.py:109, engines/gpu/adjoint.py:146), for callers that allocate the buffers
+ * themselves. bp_forward_workspace_bytes: the forward's state, raw coil sums, receiver phases, demodulated signal
+ * and status word for n spins, n_adc samples and n_coils coils (`raw` and `signal` keep one row when n_adc = 0).
+ * bp_adjoint_workspace_bytes: what the checkpointed adjoint adds for a sequence of n_segments segments: the
+ * checkpoints (one [6][n] state per interval of checkpoint_every segments, a multiple of BP_ADJ_WIN), the window
+ * states of one replayed interval (max_interval_windows: the most adjoint windows in one interval, from the
+ * caller's bp_plan_windows plan), the replayed state, the per-CTA segment gradients (`grid` = bp_adjoint_grid,
+ * times the longest interval), the float64 segment gradients, lambda, the per-spin gradients, the coil gradients
+ * and the signal's cotangent h. Return BP_OK, or BP_E_ARG. */
+typedef struct {
+    int64_t state, raw, psi, signal, status, total;
+} BpForwardWorkspace;
+typedef struct {
+    int64_t checkpoints, wstates, replay_state, gseg, seg, lam, gs, gc, h, total;
+} BpAdjointWorkspace;
+int bp_forward_workspace_bytes(int n, int64_t n_adc, int n_coils, BpForwardWorkspace* out);
+int bp_adjoint_workspace_bytes(int n, int64_t n_segments, int64_t n_adc, int n_coils, int checkpoint_every,
+                               int max_interval_windows, int grid, BpAdjointWorkspace* out);
+
 /* ADC samples per window that bp_forward's float32 readout accumulates for `n_coils` coils (0 if unsupported). */
 int bp_forward_samp_max(int n_coils);
 
@@ -100,7 +120,7 @@ int bp_adjoint_grid(int n, int n_coils);
  * [seg0, seg0 + seg_len).
  *   wstates [wb - wa][6][n] the state at every window start (bp_forward replay of the interval, stride 1)
  *   h       [n_adc][2C] float32 dL/d(raw coil sums) = dL/dsignal rotated by exp(+i psi), or NULL (8-byte
- *           aligned: BP_E_ALIGN otherwise)
+ *           aligned: BP_E_ALIGN otherwise); n_adc its rows
  *   lam     [3][n] in: dL/dm after the interval; out: dL/dm before it
  *   gs      [8][n] += dL/d(x, y, z, dB0, pd, r1, r2, b1)
  *   gc      [2C][n] += dL/d(coil c real, imaginary) at rows 2c, 2c+1, or NULL
@@ -110,7 +130,9 @@ int bp_adjoint_grid(int n, int n_coils);
  *           BP_SEG_WX | BP_SEG_WY (the RF alone) takes a cheaper reduction; plus BP_SPIN_NO_OFFSETS when the
  *           rows x, y, z and dB0 of gs are not wanted (left as they were): without coil gradients and without
  *           BP_SEG_DT, KX, KY, KZ, BETA, the sweep then skips the offsets' gradients altogether
- *   grid    bp_adjoint_grid(n, n_coils) */
+ *   grid    bp_adjoint_grid(n, n_coils)
+ *   status  |= 2 (a malformed window) for every window the sweep skips: more than BP_ADJ_WIN segments, segments
+ *           outside [seg0, seg0 + seg_len), or samples outside h's n_adc rows */
 #define BP_SEG_DT 1
 #define BP_SEG_WX 2
 #define BP_SEG_WY 4
@@ -122,7 +144,8 @@ int bp_adjoint_grid(int n, int n_coils);
 #define BP_SPIN_NO_OFFSETS 128
 int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
                const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates, const float* h,
-               float* lam, float* gs, float* gc, float* gseg, int seg_mask, int grid, void* stream);
+               int n_adc, float* lam, float* gs, float* gc, float* gseg, int seg_mask, int grid, int32_t* status,
+               void* stream);
 
 /* seg[seg0 + s][k] += sum over the `n_cta` CTAs, in CTA order, of gseg[cta][s][k], in float64 (replaces
  * seg_reduce, engines/gpu/cuda/seg_reduce.cu:3-11). `seg` is [S][8] float64. */
@@ -135,14 +158,15 @@ int bp_seg_reduce(const float* gseg, int n_cta, int seg_len, int seg0, double* s
  * loading the library holds until exit; the call allocates nothing. Returns BP_E_SIZE when one CTA's share,
  * seg_len * 8 floats, exceeds the array; the grid is capped so that all CTAs fit. `seg` ([S][8] float64, +=) may
  * be NULL (no segment gradients). The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current: make it before any stream capture. Every call uses the same
+ * (cudaGetSymbolAddress) with that device current, once per device: make it before any stream capture, and do
+ * not reset the device (cudaDeviceReset) between calls. `n_adc` and `status` as in bp_adjoint. Every call uses the same
  * array: calls that overlap on the GPU (other streams, other host threads) race on it. Results equal bp_adjoint's
  * for lam, gs, gc, and seg up to the order of the float64 sum over CTAs. */
 #define BP_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
 int bp_adjoint_noalloc(const float* spins, const float* sens, int n, int n_coils, const void* segs,
                        const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
-                       const float* wstates, const float* h, float* lam, float* gs, float* gc, double* seg,
-                       void* stream);
+                       const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc, double* seg,
+                       int32_t* status, void* stream);
 
 /* ---- reused pulses (replace the pulse maps of engines/gpu/cuda/pulse.cu.in:3-32 and the reuse branch of
  * engines/gpu/cuda/kernels.cu.in:141-165) ----

@@ -1,8 +1,8 @@
 """Writes the golden fixtures ``tests/golden/*.npz`` by running blochparty's own core engine in float64.
 
-Run once, in a container where the reference source tree is present:
+Run once, with the reference source tree (its ``src`` directory) on PYTHONPATH:
 
-    PYTHONPATH=/root/reference/src python tests/golden/make_golden.py
+    PYTHONPATH=<reference>/src python tests/golden/make_golden.py
 
 Each case's inputs are built here with this package's builders and phantoms (seeded), converted to the
 reference's ``Phantom`` / ``Sequence`` classes, and simulated by ``blochparty.simulate(..., engine="core")``

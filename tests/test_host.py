@@ -212,3 +212,52 @@ def test_span_descriptor_layout_matches_the_header(tmp_path):
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [getattr(_lib.BpSpan, f).offset for f in fields] + [ctypes.sizeof(_lib.BpSpan)]
     assert got == want
+
+
+def test_workspace_query_matches_the_host_allocations():
+    """``bp_forward_workspace_bytes`` / ``bp_adjoint_workspace_bytes`` give the sizes of the buffers the host side
+    allocates (``adjoint.sized`` checks every allocation against them); here the same shapes, from a plan of the
+    4-echo head workload at 16^3 with a 37-window checkpoint interval, against the query."""
+    from blochparty_b200 import adjoint, workloads
+
+    ph, seq, coils = workloads.gre3d_128_4echo(16)
+    inp = bpb.api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad,
+                         seq.adc_phase, None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
+    pk = engine.pack(inp, "cpu")
+    every = 37 * _lib.BP_ADJ_WIN
+    plan = adjoint.Plan(pk, every, "cpu")
+    n, S, A, C, grid = pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, 592
+    f = _lib.forward_workspace(n, A, C)
+    assert (f.state, f.raw, f.psi, f.signal) == (6 * n * 4, A * 2 * C * 8, pk.psi.numel() * 8, C * A * 8)
+    w = _lib.adjoint_workspace(n, S, A, C, every, plan.max_aw, grid)
+    assert w.checkpoints == len(plan.starts) * 6 * n * 4
+    assert w.wstates == plan.max_aw * 6 * n * 4
+    assert w.gseg == grid * plan.max_len * 8 * 4
+    assert (w.seg, w.lam, w.gs, w.gc, w.h) == (S * 64, 3 * n * 4, 8 * n * 4, 2 * C * n * 4, A * 2 * C * 4)
+    assert w.total == sum(getattr(w, k) for k in ("checkpoints", "wstates", "replay_state", "gseg", "seg", "lam",
+                                                   "gs", "gc", "h"))
+    lib = _lib.lib()
+    assert lib.bp_adjoint_workspace_bytes(n, S, A, C, every + 1, plan.max_aw, grid, None) == _lib.BP_E_ARG
+    assert lib.bp_forward_workspace_bytes(n, A, 33, None) == _lib.BP_E_ARG
+
+
+def test_workspace_structs_match_the_header(tmp_path):
+    """The ctypes workspace structs have the C structs' sizes and field offsets (compiled with gcc)."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    inc = Path(__file__).resolve().parents[1] / "include"
+    for struct in (_lib.BpForwardWorkspace, _lib.BpAdjointWorkspace):
+        name = struct.__name__
+        fields = [f for f, _ in struct._fields_]
+        src = tmp_path / f"{name}.c"
+        src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "blochparty_b200.h"\nint main(void) {\n'
+                       + "".join(f'  printf("%zu\\n", offsetof({name}, {f}));\n' for f in fields)
+                       + f'  printf("%zu\\n", sizeof({name}));\n  return 0;\n}}\n')
+        exe = tmp_path / name
+        subprocess.run(["gcc", f"-I{inc}", str(src), "-o", str(exe)], check=True)
+        got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+        assert got == [getattr(struct, f).offset for f in fields] + [ctypes.sizeof(struct)]

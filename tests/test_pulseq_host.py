@@ -140,6 +140,20 @@ def test_arbitrary_gradient_on_the_raster_is_continuous_with_the_block_before():
     assert np.allclose(g[c:d], 200.0, rtol=0, atol=1e-9)
 
 
+def test_delayed_arbitrary_gradient_starts_from_zero():
+    """A raster-sampled gradient with a delay, after a block whose gradient ends at 200: the axis is at zero during
+    the delay, so the waveform's first edge is 0 (not the previous block's 200). Samples (100, 200) then give the
+    edges 0, 200, 200 and the points (0, 0), (5 us, 100), (15 us, 200), (20 us, 200) after the 10 us delay: 250 +
+    1500 + 1000 Hz/m us (from the previous block's 200, the edges 200, 0, 400 would give 3750)."""
+    text = seq_text([[1, 2, 0, 1, 0, 0, 0, 0], [2, 3, 0, 2, 0, 0, 0, 0]],
+                    grads=[[1, 200.0, 1, 0, 0], [2, 200.0, 2, 0, 10]], shapes=[(1, 2, [0.5, 1.0]), (2, 2, [0.5, 1.0])])
+    seq = pulseq.read_pulseq(text)
+    g, dt = seq.grad[:, 0].numpy(), seq.dt.numpy()
+    (a, b), (c, d) = seq.meta["block_segments"]
+    assert abs(float(np.sum(g[c:d] * dt[c:d])) - 2750e-6) < 1e-12
+    assert np.allclose(g[c:d][np.cumsum(dt[c:d]) <= 10e-6 + 1e-12], 0.0, atol=1e-9)
+
+
 def test_shape_compression():
     assert np.array_equal(pulseq.decompress_shape([1.0, 0.0, 0.0, 97.0], 100), np.ones(100))
     assert np.array_equal(pulseq.decompress_shape([0.5, 0.25, 0.25], 3), np.array([0.5, 0.25, 0.25]))

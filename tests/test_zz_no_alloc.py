@@ -67,9 +67,11 @@ def test_noalloc_adjoint_matches_the_allocating_entry_point():
     gseg = torch.empty(grid, s1 - s0, 8, device=pk.device)
     lam_ref = lam0.clone()
     gs_ref, gc_ref, seg_ref = _outputs(pk, S)
+    status = torch.zeros(1, dtype=torch.int32, device=pk.device)
     _lib.check(lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
-                              ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), ptr(lam_ref),
-                              ptr(gs_ref), ptr(gc_ref), ptr(gseg), _lib.BP_SEG_ALL, grid, stream), "bp_adjoint")
+                              ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), pk.n_adc, ptr(lam_ref),
+                              ptr(gs_ref), ptr(gc_ref), ptr(gseg), _lib.BP_SEG_ALL, grid, ptr(status), stream),
+               "bp_adjoint")
     _lib.check(lib.bp_seg_reduce(ptr(gseg), grid, s1 - s0, s0, ptr(seg_ref), stream), "bp_seg_reduce")
     torch.cuda.synchronize()
     assert seg_ref.abs().max() > 0 and gs_ref.abs().max() > 0
@@ -78,10 +80,11 @@ def test_noalloc_adjoint_matches_the_allocating_entry_point():
         lam = lam0.clone()
         gs, gc, seg = _outputs(pk, S)
         code = lib.bp_adjoint_noalloc(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
-                                      ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), ptr(lam),
-                                      ptr(gs), ptr(gc), ptr(seg), stream)
+                                      ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), pk.n_adc,
+                                      ptr(lam), ptr(gs), ptr(gc), ptr(seg), ptr(status), stream)
         _lib.check(code, "bp_adjoint_noalloc")
         torch.cuda.synchronize()
+        assert int(status.item()) == 0
         errors = {"lam": rel(lam, lam_ref), "gs": rel(gs, gs_ref), "gc": rel(gc, gc_ref),
                   "seg": rel(seg[s0:s1], seg_ref[s0:s1])}
         assert max(errors.values()) < TOL, (call, errors)
@@ -95,7 +98,30 @@ def test_noalloc_adjoint_rejects_an_interval_beyond_its_scratch():
     aa, ab = plan.aranges[k]
     gs, gc, seg = _outputs(pk, pk.flags.shape[0])
     too_long = _lib.BP_NOALLOC_SCRATCH_BYTES // 4 // 8 + 1  # segments: one CTA's share exceeds the array
+    status = torch.zeros(1, dtype=torch.int32, device=pk.device)
     code = lib.bp_adjoint_noalloc(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
-                                  ptr(plan.awin_dev), aa, ab, 0, too_long, ptr(wstates), ptr(h), ptr(lam0), ptr(gs),
-                                  ptr(gc), ptr(seg), _lib.stream_ptr())
+                                  ptr(plan.awin_dev), aa, ab, 0, too_long, ptr(wstates), ptr(h), pk.n_adc, ptr(lam0),
+                                  ptr(gs), ptr(gc), ptr(seg), ptr(status), _lib.stream_ptr())
     assert code == _lib.BP_E_SIZE
+
+
+def test_noalloc_adjoint_skips_windows_outside_the_interval():
+    """An interval start that does not match the windows (seg0 one window late): the sweep skips the window that
+    begins before seg0 instead of writing before its rows of the shared scratch, and reports it in the status
+    word; the segment gradients stay inside [seg0, seg0 + seg_len)."""
+    lib = _lib.lib()
+    pk, plan, k, wstates, h, lam0 = _interval_inputs()
+    aa, ab = plan.aranges[k]
+    s0, s1 = plan.seg_ranges[k]
+    S = pk.flags.shape[0]
+    assert s1 + _lib.BP_ADJ_WIN <= S
+    gs, gc, seg = _outputs(pk, S)
+    status = torch.zeros(1, dtype=torch.int32, device=pk.device)
+    seg0 = s0 + _lib.BP_ADJ_WIN
+    code = lib.bp_adjoint_noalloc(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
+                                  ptr(plan.awin_dev), aa, ab, seg0, s1 - s0, ptr(wstates), ptr(h), pk.n_adc,
+                                  ptr(lam0.clone()), ptr(gs), ptr(gc), ptr(seg), ptr(status), _lib.stream_ptr())
+    _lib.check(code, "bp_adjoint_noalloc")
+    torch.cuda.synchronize()
+    assert int(status.item()) & 2
+    assert float(seg[:seg0].abs().max()) == 0.0 and float(seg[seg0 + s1 - s0:].abs().max()) == 0.0
