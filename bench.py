@@ -207,6 +207,87 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+REF_CASES = {"3d-32": 32, "3d-48": 48, "3d-64": 64, "3d-96": 96, "gre3d-128": 128}
+
+
+def run_reference_gpu(args):
+    """The reference's own CUDA engine (``engine="cuda"``: NVRTC-compiled SIMT kernels, blochparty
+    ``engines/gpu/cuda/__init__.py:93-132``) on this GPU, installed unmodified in ``baseline/_ref``, against this
+    engine on the same inputs: the reference's benchmark cases (``benchmarks/bench.py:36-95``: Shepp-Logan,
+    Cartesian spoiled GRE, 8 birdcage coils, 200 dummy TRs, float32) and its 128^3 example
+    (``examples/gre3d_128.py:15-27``), built with the reference's own builders. Both through their public
+    ``simulate`` from CPU tensors (packing, copies and read-back inside the timing), one untimed warm-up each
+    (NVRTC compile), then the fastest of ``--repeat`` runs, wall clock around a synchronising call. ``--grad``: forward
+    + backward of sum |signal|^2 with respect to the flip angle, the T1 map and the coil maps (the reference's
+    ``run_grad_case``). One JSON line per case."""
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "blochparty").is_dir():
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "the reference is not installed in baseline/_ref"}))
+        return
+    sys.path.insert(0, str(ref))
+    import blochparty as bp
+
+    import blochparty_b200 as bpb
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    f32 = torch.float32
+
+    def case(name, grad):
+        n = REF_CASES[name]
+        if grad:
+            maps = bp.shepp_logan_maps(n, ndim=3, dtype=f32)
+            t1 = maps["t1"].clone().requires_grad_()
+            ph = bp.phantom_from_maps(maps["pd"], t1, maps["t2"], 0.22)
+            coils = bp.birdcage_sensitivities(ph.pos, n_coils=8).detach().requires_grad_()
+            flip = torch.tensor(15.0, dtype=f32, requires_grad=True)
+            seq = bp.gre_cartesian((n,) * 3, flip_deg=flip, n_dummy=200, dtype=f32)
+            return ph, seq, coils, (flip, t1, coils)
+        ph = bp.shepp_logan(n, ndim=3, dtype=torch.float64).to(dtype=f32)
+        coils = bp.birdcage_sensitivities(ph.pos, n_coils=8)
+        if name == "gre3d-128":
+            seq = bp.gre_3d(n, flip_deg=15.0, tr=10e-3, n_dummy=200, dtype=f32)
+        else:
+            seq = bp.gre_cartesian((n,) * 3, n_dummy=200, dtype=f32)
+        return ph, seq, coils, ()
+
+    def timed(fn, grad_of):
+        best, out = float("inf"), None
+        for i in range(1 + args.repeat):
+            for t in grad_of:
+                t.grad = None
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sig = fn()
+            if grad_of:
+                (sig.abs() ** 2).sum().backward()
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            if i > 0:
+                best = min(best, dt)
+            out = (sig.detach().clone(), [t.grad.clone() for t in grad_of])
+        return best, out
+
+    for name in args.cases.split(","):
+        ph, seq, coils, grad_of = case(name, args.grad)
+        ctx = torch.enable_grad() if args.grad else torch.no_grad()
+        with ctx:
+            t_ref, (s_ref, g_ref) = timed(lambda: bp.simulate(ph, seq, coils, engine="cuda").signal, grad_of)
+            t_b2, (s_b2, g_b2) = timed(lambda: bpb.simulate(ph, seq, coils).signal, grad_of)
+        n, S = len(ph.pd), len(seq)
+        rel = lambda a, b: float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double()))
+        line = {"impl": "reference_gpu", "case": name, "grad": args.grad, "spins": n, "segments": S,
+                "adc": int(sum(seq.adc)), "gpu": torch.cuda.get_device_name(dev),
+                "reference_cuda_s": t_ref, "b200_s": t_b2, "speedup": t_ref / t_b2,
+                "reference_cuda_isochromat_steps_per_s": n * S / t_ref, "b200_isochromat_steps_per_s": n * S / t_b2,
+                "signal_rel_l2_b200_vs_reference_cuda": rel(s_b2, s_ref),
+                "timing": f"fastest of {args.repeat} after one warm-up, public simulate() from CPU tensors"}
+        if args.grad:
+            line["grad_rel_l2_b200_vs_reference_cuda"] = {k: rel(a, b) for k, a, b in
+                                                          zip(("flip", "t1", "coils"), g_b2, g_ref)}
+        print(json.dumps(line), flush=True)
+
+
 def run_grad(args, dev):
     """Forward + adjoint through the public API (gradients w.r.t. T1 and the RF waveform of a seeded linear loss
     of the signal), one GPU: isochromat-steps/s of the pair, timed by CUDA events around the forward call and the
@@ -285,7 +366,11 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference", "reference_gpu"),
+                    help="reference: the reference algorithm on the host CPU; reference_gpu: the reference's own CUDA "
+                         "engine (baseline/_ref) against this engine on the reference's benchmark cases")
+    ap.add_argument("--cases", default="3d-32,3d-48,3d-64,3d-96,gre3d-128", help="--impl reference_gpu: cases")
+    ap.add_argument("--repeat", type=int, default=2, help="--impl reference_gpu: timed runs per case (fastest kept)")
     ap.add_argument("--readout", default="fp32", choices=("fp32", "bf16x3"))
     ap.add_argument("--n", type=int, default=64, help="grid size of the 3D GRE (64: the measured workload)")
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -308,6 +393,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.impl == "reference_gpu":
+        if rank == 0:
+            run_reference_gpu(args)
         return
 
     import torch.distributed as dist
