@@ -231,7 +231,7 @@ def run_reference_gpu(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    f32 = torch.float32
+    f32, F64 = torch.float32, torch.float64
 
     def case(name, grad):
         n = REF_CASES[name]
@@ -251,33 +251,31 @@ def run_reference_gpu(args):
             seq = bp.gre_cartesian((n,) * 3, n_dummy=200, dtype=f32)
         return ph, seq, coils, ()
 
-    def timed(fn, grad_of):
+    def timed(simulate, name):
         best, out = float("inf"), None
         for i in range(1 + args.repeat):
-            for t in grad_of:
-                t.grad = None
+            ph, seq, coils, grad_of = case(name, args.grad)  # (built outside the timing, as the reference's bench)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            sig = fn()
+            sig = simulate(ph, seq, coils).signal
             if grad_of:
                 (sig.abs() ** 2).sum().backward()
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
             if i > 0:
                 best = min(best, dt)
-            out = (sig.detach().clone(), [t.grad.clone() for t in grad_of])
+            out = (sig.detach().clone(), [t.grad.clone() for t in grad_of], len(ph.pd), len(seq), int(sum(seq.adc)))
         return best, out
 
     for name in args.cases.split(","):
-        ph, seq, coils, grad_of = case(name, args.grad)
         ctx = torch.enable_grad() if args.grad else torch.no_grad()
         with ctx:
-            t_ref, (s_ref, g_ref) = timed(lambda: bp.simulate(ph, seq, coils, engine="cuda").signal, grad_of)
-            t_b2, (s_b2, g_b2) = timed(lambda: bpb.simulate(ph, seq, coils).signal, grad_of)
-        n, S = len(ph.pd), len(seq)
-        rel = lambda a, b: float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double()))
+            t_ref, (s_ref, g_ref, n, S, n_adc) = timed(lambda p, s, c: bp.simulate(p, s, c, engine="cuda"), name)
+            t_b2, (s_b2, g_b2, _, _, _) = timed(bpb.simulate, name)
+        rel = lambda a, b: float(torch.linalg.vector_norm((a - b).to(torch.complex128 if b.is_complex() else F64))
+                                 / torch.linalg.vector_norm(b.to(torch.complex128 if b.is_complex() else F64)))
         line = {"impl": "reference_gpu", "case": name, "grad": args.grad, "spins": n, "segments": S,
-                "adc": int(sum(seq.adc)), "gpu": torch.cuda.get_device_name(dev),
+                "adc": n_adc, "gpu": torch.cuda.get_device_name(dev),
                 "reference_cuda_s": t_ref, "b200_s": t_b2, "speedup": t_ref / t_b2,
                 "reference_cuda_isochromat_steps_per_s": n * S / t_ref, "b200_isochromat_steps_per_s": n * S / t_b2,
                 "signal_rel_l2_b200_vs_reference_cuda": rel(s_b2, s_ref),

@@ -44,13 +44,18 @@ def gre3d_64(n=64):
     return ph, seq, phantoms.birdcage_sensitivities(ph.pos, 8)
 
 
+def adjoint_2d_128_sequence(flips, n=128):
+    """The 2D GRE of ``adjoint_2d_128`` with the per-TR flip train ``flips`` [deg] (n values)."""
+    return sequences.gre((n, n), 0.25, flip_deg=np.asarray(flips, dtype=np.float64), tr=10e-3, te=5e-3, dwell=10e-6,
+                         rf_duration=20e-6, rf_steps=1, spoiling="rf")
+
+
 def adjoint_2d_128(n=128):
     ph = phantoms.ellipse_phantom_2d(n, 0.25, n_ellipses=10, seed=0)
     ph.b1 = phantoms.radial_b1(ph.pos, 0.8, 1.2)
     g = torch.Generator().manual_seed(3)
     flips = 5.0 + 25.0 * torch.rand(n, generator=g, dtype=F64)
-    seq = sequences.gre((n, n), 0.25, flip_deg=flips.numpy(), tr=10e-3, te=5e-3, dwell=10e-6, rf_duration=20e-6,
-                        rf_steps=1, spoiling="rf")
+    seq = adjoint_2d_128_sequence(flips.numpy(), n)
     g4 = torch.Generator().manual_seed(4)
     t1_target = ph.t1 * (1.0 + 0.05 * torch.randn(ph.t1.shape, generator=g4, dtype=F64))
     return ph, seq, phantoms.birdcage_sensitivities(ph.pos, 8), flips, t1_target

@@ -142,8 +142,58 @@ def busy_case(seed=3, n=40, n_coils=4):
     return ph, seq, coils, m_init
 
 
+def adjoint128():
+    """The 128^2 flip-train case at its own size (16,384 spins, 128 TRs, 8 coils): the reference's float64 core
+    and its autograd. Loss = sum |s(T1) - s_t|^2, s_t the signal of the perturbed T1 map. Stored: the target
+    signal (complex64), the loss, the gradients with respect to T1, T2, PD, dB0, B1 (float32), the coil
+    sensitivities of every 8th spin (complex64) and the flip train (through the RF waveform: every TR's hard
+    pulse is flip / 360 / duration times its spoiling phase), and float64 sums of the inputs, so a test can check
+    that this package's builders still make the same case."""
+    from blochparty_b200 import workloads
+
+    ph, seq, coils, flips, t1_target = workloads.adjoint_2d_128()
+    rph, rseq = ref_objects(ph, seq)
+    rph_t = bp.Phantom(ph.pos, ph.pd, t1_target, ph.t2, ph.db0, b1=ph.b1)
+    s_t = bp.simulate(rph_t, rseq, coils, engine="core").signal.detach()
+    leaves = {k: v.detach().clone().requires_grad_() for k, v in
+              (("t1", ph.t1), ("t2", ph.t2), ("pd", ph.pd), ("db0", ph.db0), ("b1", ph.b1), ("coils", coils),
+               ("rf", seq.rf))}
+    gph = bp.Phantom(ph.pos, leaves["pd"], leaves["t1"], leaves["t2"], leaves["db0"], b1=leaves["b1"])
+    gseq = bp.Sequence(seq.dt, leaves["rf"], seq.grad, seq.adc_phase, list(seq.is_rf), list(seq.adc),
+                       list(seq.spoil), {}, seq.b0_offset)
+    r = bp.simulate(gph, gseq, leaves["coils"], engine="core")
+    loss = ((r.signal - s_t).abs() ** 2).sum()
+    g = dict(zip(leaves, torch.autograd.grad(loss, list(leaves.values()))))
+    # d rf / d flip_i on TR i's pulse segments: rf = flip / 360 / duration (cos phi, sin phi)
+    is_rf = np.asarray(seq.is_rf, dtype=bool)
+    starts = np.flatnonzero(is_rf & ~np.concatenate([[False], is_rf[:-1]]))
+    gflip = np.zeros(len(flips))
+    rf = seq.rf.numpy()
+    for i, a in enumerate(starts[-len(flips):] if len(starts) >= len(flips) else starts):
+        e = a
+        while e < len(is_rf) and is_rf[e]:
+            e += 1
+        amp = np.hypot(rf[a:e, 0], rf[a:e, 1])
+        unit = rf[a:e] / amp[:, None]
+        gflip[i] = float((g["rf"].numpy()[a:e] * unit).sum(1) @ (amp / flips[i].item()))
+    sums = {k: float(v.double().sum()) for k, v in (("pos", ph.pos), ("pd", ph.pd), ("t1", ph.t1), ("t2", ph.t2),
+                                                     ("db0", ph.db0), ("b1", ph.b1), ("dt", seq.dt),
+                                                     ("rf", seq.rf), ("grad", seq.grad), ("t1_target", t1_target),
+                                                     ("coils_abs", coils.abs()))}
+    out = dict(s_t_re=s_t.real.float().numpy(), s_t_im=s_t.imag.float().numpy(), loss=np.array(float(loss.detach())),
+               flips=flips.numpy(), grad_flips=gflip,
+               **{f"grad_{k}": g[k].float().numpy() for k in ("t1", "t2", "pd", "db0", "b1")},
+               grad_coils8_re=g["coils"][::8].real.float().numpy(), grad_coils8_im=g["coils"][::8].imag.float().numpy(),
+               **{f"sum_{k}": np.array(v) for k, v in sums.items()})
+    np.savez_compressed(HERE / "adjoint128.npz", **out)
+    print("adjoint128", float(loss), {k: v.shape for k, v in out.items() if k.startswith("grad")})
+
+
 def main():
     torch.set_default_dtype(F64)
+    if "adjoint128" in sys.argv[1:]:
+        adjoint128()
+        return
     for seed in (0, 1):
         ph, seq, coils = rand_case(seed)
         run(f"rand{seed}", ph, seq, coils)
@@ -169,3 +219,5 @@ def main():
 
 if __name__ == "__main__":
     main()
+    if not sys.argv[1:]:
+        adjoint128()

@@ -32,3 +32,17 @@ def objects(case):
     seq = Sequence(case.dt, case.rf, case.grad, case.adc_phase, list(case.is_rf), list(case.adc), list(case.spoil),
                    b0_offset=case.b0_offset)
     return ph, seq, case.coils, case.m_init
+
+
+def load_adjoint128():
+    """The 128^2 flip-train golden (``make_golden.py adjoint128``): this package's builders make the case
+    (``workloads.adjoint_2d_128``); the fixture holds the reference's target signal, loss and gradients, and float64
+    sums of the inputs it was made from."""
+    from blochparty_b200 import workloads
+
+    z = np.load(GOLDEN / "adjoint128.npz")
+    ph, seq, coils, flips, t1_target = workloads.adjoint_2d_128()
+    sums = {"pos": ph.pos, "pd": ph.pd, "t1": ph.t1, "t2": ph.t2, "db0": ph.db0, "b1": ph.b1, "dt": seq.dt,
+            "rf": seq.rf, "grad": seq.grad, "t1_target": t1_target, "coils_abs": coils.abs()}
+    same = {k: float(v.double().sum()) == float(z[f"sum_{k}"]) for k, v in sums.items()}
+    return z, (ph, seq, coils, flips, t1_target), same

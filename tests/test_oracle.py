@@ -110,3 +110,49 @@ def test_spoiled_gre_steady_state():
     a, e1 = math.radians(deg), math.exp(-tr / t1)
     ernst = math.sin(a) * (1 - e1) / (1 - math.cos(a) * e1)
     assert abs(abs(complex(sig[0, -1])) - ernst) < 1e-4
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_c_oracle_matches_reference_core(name):
+    """The C restatement (``oracle/bloch_c.c``, for the workloads' long sequences) against the reference's float64
+    outputs, with one thread and with chunks of 3 samples (every chunk boundary case), and against the Python
+    restatement."""
+    from oracle import fast
+
+    case, sig, m, _ = load(name)
+    ref_s, ref_m = bloch.simulate(case)
+    for threads, chunk in ((0, 0), (1, 3)):
+        s, mm = fast.simulate(case, threads=threads, chunk=chunk)
+        assert s.shape == sig.shape
+        assert rel(s, sig) < 1e-11 and rel(mm, m) < 1e-11
+        assert rel(s, ref_s) < 1e-11 and rel(mm, ref_m) < 1e-11
+
+
+def test_c_oracle_matches_python_oracle_on_a_2d_gre():
+    """Both restatements on a 16^2 GRE with 20 dummy TRs and radial B1 (many runs and samples), 3-sample chunks."""
+    from blochparty_b200 import phantoms, sequences
+    from oracle import fast
+
+    ph = phantoms.ellipse_phantom_2d(16, 0.25, seed=2)
+    ph.b1 = phantoms.radial_b1(ph.pos)
+    seq = sequences.gre((16, 16), 0.25, flip_deg=25.0, tr=6e-3, te=3e-3, n_dummy=20, dwell=20e-6)
+    case = bloch.case_from(ph, seq, phantoms.birdcage_sensitivities(ph.pos, 3))
+    s0, m0 = bloch.simulate(case)
+    s1, m1 = fast.simulate(case, chunk=3)
+    assert rel(s1, s0) < 1e-11 and rel(m1, m0) < 1e-11
+
+
+def test_adjoint128_golden_is_this_packages_case_and_the_oracle_follows_it():
+    """The 128^2 flip-train golden (the reference's float64 core and autograd at the case's own size): this
+    package's builders still make the inputs it was written from, and the oracle's loss and gradients follow it."""
+    from golden_cases import load_adjoint128
+
+    z, (ph, seq, coils, flips, t1_target), same = load_adjoint128()
+    assert all(same.values()), same
+    s_t = torch.complex(torch.from_numpy(z["s_t_re"]).to(F64), torch.from_numpy(z["s_t_im"]).to(F64))
+    case = bloch.case_from(ph, seq, coils)
+    loss, g = bloch.gradients(case, lambda s, m: ((s - s_t).abs() ** 2).sum(), names=("t1", "t2", "pd", "db0", "b1"))
+    assert abs(loss - float(z["loss"])) < 1e-5 * float(z["loss"])
+    for k in ("t1", "t2", "pd", "db0", "b1"):
+        ref = torch.from_numpy(z[f"grad_{k}"]).to(F64)
+        assert rel(g[k], ref) < 1e-5, k

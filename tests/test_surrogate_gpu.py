@@ -90,26 +90,6 @@ def test_training_lowers_the_loss_and_the_error():
     assert after[1] < 0.1 * before[1]
 
 
-@pytest.fixture(scope="module")
-def tse_surrogates():
-    """Networks for the six TSE pulses (3 slices x excitation / refocusing), trained on 2^20 samples each (600
-    epochs of 4,096-sample steps, ~24 s per pulse) over |z_rel| <= 2.5: the slices are contiguous, so every spin
-    of the 3-slice stack lies within 2.5 slice widths of every pulse's centre."""
-    out, info = [], []
-    for z0 in (-5e-3, 0.0, 5e-3):
-        for flip, phase in ((90.0, 0.0), (180.0, 0.5 * math.pi)):
-            w, dt, gz, _ = _pulse(flip, z0, phase)
-            sg = surrogate.RFSurrogate(w, dt, gz, 5e-3, domain=(200.0, 0.3, 2.5))
-            t = time.perf_counter()
-            sg.train(epochs=600)
-            info.append((flip, z0, time.perf_counter() - t, sg.validate()))
-            out.append(sg)
-    for flip, z0, sec, (mx, rms, cmx, crms) in info:
-        print(f"\nsurrogate {flip:.0f} deg at {z0 * 1e3:+.0f} mm: trained in {sec:.1f} s, rotation max {mx:.1e} "
-              f"rms {rms:.1e}, first-order terms max {cmx:.1e} rms {crms:.1e}")
-    return out
-
-
 def test_tse_through_the_surrogate_against_the_float64_oracle(tse_surrogates):
     ph, seq, coils = workloads.tse_3slice_128(16)
     sig64, m64 = bloch.simulate(bloch.case_from(ph, seq, coils))
