@@ -1,16 +1,25 @@
-"""Benchmark: isochromat-steps/s (spins x segments / s, blochparty's spin-segments/s, benchmarks/bench.py:64)
-of the forward simulation on the 3D GRE 64^3 workload (1,048,576 spins x 1,097,728 segments, 8 coils; see
-``blochparty_b200/workloads.py``) on N GPUs of one node, one process per GPU.
+"""Benchmark: isochromat-steps/s (spins x segments / s, blochparty's spin-segments/s, benchmarks/bench.py:64) of
+the forward simulation and of the forward + adjoint, on N GPUs of one node, one process per GPU.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--readout fp32|bf16x3]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference|reference_gpu]
+                    [--workload gre3d_128_4echo|gre3d_64] [--trs T] [--readout fp32|bf16x3]
+                    [--pulses step|reuse|surrogate] [--no-grad]
 
-Prints ONE JSON line on rank 0. ``value``: the whole job's isochromat-steps/s with the inputs resident in HBM,
-timed with CUDA events (max over ranks). ``e2e``: the same metric through the public ``simulate`` call with host
-inputs, packing and host<->device copies inside the timed region (wall clock around a synchronising call).
-Multi-GPU: weak scaling; every rank simulates its own 1,048,576-spin phantom (the same workload with its own
-sub-voxel offsets), and the float64 raw signal is summed onto rank 0 with one NCCL reduce per step (the spin
-sum is the path's only exchange). ``--impl reference``: the reference algorithm on the host CPU (the float64
-oracle restating blochparty's core engine), on a bounded sample of the workload; rank 0 only.
+Default workload: the 4-echo 3D GRE on the 128^3 head phantom (8,388,608 spins, 8 coils, 200-step sinc slab
+pulses, TR 20 ms; ``blochparty_b200/workloads.py``), its first ``--trs`` TRs (64 of 16,384: the sequence is
+TR-periodic, so a whole-TR prefix has the full sequence's work per segment). ``--workload gre3d_64``: the 3D GRE
+64^3 (1,048,576 spins), all of its 1,097,728 segments by default.
+
+Prints ONE JSON line on rank 0. ``value``: the whole job's forward isochromat-steps/s with the inputs resident in
+HBM, timed with CUDA events (max over ranks). ``fwd_adjoint`` (one GPU): the same for the checkpointed forward +
+the hand-written adjoint (gradient of a seeded linear loss of the signal with respect to the RF waveform, the flip
+train), with its own roofline. ``e2e``: the forward through the public ``simulate`` call with host inputs, packing
+and host<->device copies inside the timed region (wall clock around a synchronising call). Multi-GPU: weak
+scaling; every rank simulates its own phantom (the workload with its own sub-voxel offsets), and the float64 raw
+signal is summed onto rank 0 with one NCCL reduce per step (the spin sum is the path's only exchange).
+``--impl reference``: the reference algorithm on the host CPU (the float64 oracle restating blochparty's core
+engine), on a bounded sample of the same workload; rank 0 only. ``--impl reference_gpu``: the reference's own CUDA
+engine (installed in ``baseline/_ref``) against this engine on the reference's benchmark cases.
 """
 
 from __future__ import annotations
@@ -34,13 +43,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "isochromat-steps/s (fwd)"
 UNIT = "isochromat-steps/s"
-WORKLOAD = "gre3d_64: 3D spoiled GRE 64^3, 1,048,576 spins, 8 coils, 200-step sinc slab, TR 8 ms"
-WORKLOAD_128 = ("gre3d_128_4echo: 4-echo 3D GRE 128^3 head phantom, 8,388,608 spins, 8 coils, 200-step sinc slab, "
-                "TR 20 ms")
-
-
-def head_workload(n: int) -> str:
-    return WORKLOAD_128 if n == 128 else f"gre3d_128_4echo at {n}^3 ({4 * n ** 3:,} spins, {n} samples per echo)"
+DEFAULT_TRS = {"gre3d_128_4echo": 64, "gre3d_64": 0}
 
 # algorithmic FP32 flops per spin and segment of the forward kernel (counted from its formulas in
 # blochparty_b200/csrc/bloch_common.cuh; kept fixed across versions): RF segment, free segment with cached
@@ -64,9 +67,9 @@ def flops_per_spin(flags: np.ndarray, n_coils: int) -> int:
 # the backward's work per spin and segment (counted from blochparty_b200/csrc/adjoint.cu): the interval replay
 # repeats the forward's propagation (no coil contraction); the in-window recompute steps in plain float32: RF
 # segment 61 flops (rf_step_plain), free segment 13 (free_step_plain) + 18 when it recomputes its factors; the
-# reverse sweep as the measured run (gradients of T1 and the RF) takes it, without the offsets' gradients: RF
-# segment 130 (rf_reverse with its rotation factors; 163 with the offsets'), free segment 30 (free_reverse; 58),
-# ADC sample 8 per coil (the signal's cotangent; 16 with the coil gradients) + 2.
+# reverse sweep without the offsets' gradients (the RF waveform's gradient needs none): RF segment 130 (rf_reverse
+# with its rotation factors; 163 with the offsets'), free segment 30 (free_reverse; 58), ADC sample 8 per coil (the
+# signal's cotangent; 16 with the coil gradients) + 2.
 FLOP_RF_RECOMP, FLOP_FREE_RECOMP, FLOP_FACTORS = 61, 13, 18
 FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 130, 30, 8, 2
 
@@ -152,23 +155,50 @@ def ffma_peak_tflops(dev) -> float:
     return best
 
 
-def cpu_sample(workload_fn, n_spins=4096, n_tr=32, seed=0):
-    """A bounded sample of the workload for the CPU oracle: ``n_spins`` spins drawn with a seeded generator and
-    the segments of the first ``n_tr`` TRs (TR boundaries at the spoiler-fill segments)."""
-    from oracle import bloch
+def build_workload(args, rank: int = 0):
+    """(phantom, sequence, coils, description) of the measured workload: rank r > 0 gets the same workload with
+    its own sub-voxel offsets (seed 1 + r), for weak scaling."""
+    from blochparty_b200 import phantoms, workloads
 
-    ph, seq, coils = workload_fn()
-    g = torch.Generator().manual_seed(seed)
-    idx = torch.randperm(len(ph.pd), generator=g)[:n_spins]
-    end = min(len(seq), n_tr * (len(seq) // seq.meta["n_tr"]))
-    c = bloch.case_from(ph, seq, coils)
+    if args.workload == "gre3d_128_4echo":
+        ph, seq, coils = workloads.gre3d_128_4echo(args.head_n)
+        if rank:
+            ph = phantoms.head_phantom_3d(args.head_n, 0.25, spins_per_voxel=4, subvoxel_seed=1 + rank, b0_max=150.0)
+            coils = phantoms.birdcage_sensitivities(ph.pos, 8)
+        desc = (f"gre3d_128_4echo: 4-echo 3D GRE {args.head_n}^3 head phantom, {len(ph.pd):,} spins, 8 coils, "
+                f"200-step sinc slab, TR 20 ms, {args.head_n} samples per echo")
+    else:
+        ph, seq, coils = workloads.gre3d_64(args.n)
+        if rank:
+            ph = phantoms.ellipsoid_phantom_3d(args.n, 0.25, n_ellipsoids=10, spins_per_voxel=4, seed=0,
+                                               subvoxel_seed=1 + rank, b0_seed=2, b0_max=100.0, sigma_vox=4.0)
+            coils = phantoms.birdcage_sensitivities(ph.pos, 8)
+        desc = (f"gre3d_64: 3D spoiled GRE {args.n}^3, {len(ph.pd):,} spins, 8 coils, 200-step sinc slab, "
+                f"TR 8 ms")
+    n_tr_all = seq.meta["n_tr"]
+    trs = DEFAULT_TRS[args.workload] if args.trs is None else args.trs
+    if trs and trs < n_tr_all:
+        seq = workloads.first_n_trs(seq, trs)
+        desc += f"; its first {trs} TRs ({len(seq):,} segments) of {n_tr_all:,}"
+    else:
+        desc += f"; all {n_tr_all:,} TRs ({len(seq):,} segments)"
+    return ph, seq, coils, desc
+
+
+def cpu_sample(ph, seq, coils, n_spins=4096, n_tr=32, seed=0):
+    """A bounded sample of the workload for the CPU oracle: ``n_spins`` spins drawn with a seeded generator and
+    the segments of the first ``n_tr`` TRs."""
     from dataclasses import replace
 
-    c = replace(c, pos=c.pos[idx], pd=c.pd[idx], t1=c.t1[idx], t2=c.t2[idx], db0=c.db0[idx], coils=c.coils[idx],
-                dt=c.dt[:end], rf=c.rf[:end], grad=c.grad[:end], adc_phase=c.adc_phase[:end],
-                b0_offset=None if c.b0_offset is None else c.b0_offset[:end], is_rf=c.is_rf[:end],
-                adc=c.adc[:end], spoil=c.spoil[:end])
-    return c, f"{n_spins} seeded spins x the first {end} segments ({n_tr} TRs) of {workload_fn.__name__}"
+    from blochparty_b200 import workloads
+    from oracle import bloch
+
+    g = torch.Generator().manual_seed(seed)
+    idx = torch.randperm(len(ph.pd), generator=g)[:n_spins]
+    sub = workloads.first_n_trs(seq, min(n_tr, seq.meta.get("n_tr", n_tr)))
+    c = bloch.case_from(ph, sub, coils)
+    c = replace(c, pos=c.pos[idx], pd=c.pd[idx], t1=c.t1[idx], t2=c.t2[idx], db0=c.db0[idx], coils=c.coils[idx])
+    return c, f"{len(idx)} seeded spins x the first {len(sub)} segments ({n_tr} TRs) of the workload"
 
 
 def time_cpu(case, reps=1):
@@ -186,11 +216,10 @@ def time_cpu(case, reps=1):
 
 
 def run_reference(args, rank):
-    from blochparty_b200 import workloads
-
     if rank != 0:
         return
-    case, sample = cpu_sample(workloads.gre3d_64)
+    ph, seq, coils, desc = build_workload(args)
+    case, sample = cpu_sample(ph, seq, coils)
     rates = []
     for i in range(args.warmup + args.steps):
         v, cores = time_cpu(case)
@@ -201,7 +230,7 @@ def run_reference(args, rank):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": n * s / value * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": sample, "readout": "float64 CPU"},
+            "config": {"workload": desc, "sample": sample, "readout": "float64 CPU"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -286,77 +315,83 @@ def run_reference_gpu(args):
         print(json.dumps(line), flush=True)
 
 
-def run_grad(args, dev):
-    """Forward + adjoint through the public API (gradients w.r.t. T1 and the RF waveform of a seeded linear loss
-    of the signal), one GPU: isochromat-steps/s of the pair, timed by CUDA events around the forward call and the
-    backward call."""
-    import blochparty_b200 as bpb
-    from blochparty_b200 import adjoint, engine, workloads
+def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
+    """Forward + adjoint on the resident inputs: the checkpointed forward and the backward (replay, reverse sweep,
+    segment-gradient reduction) of a seeded linear loss of the signal, gradient with respect to the RF waveform
+    (the flip train), K timed steps with CUDA events around each half. Returns the ``fwd_adjoint`` object."""
+    from blochparty_b200 import _lib, adjoint
 
-    if args.workload == "gre3d_128_4echo":
-        ph, seq, coils = workloads.gre3d_128_4echo(args.head_n)
-        workload = head_workload(args.head_n)
-    else:
-        ph, seq, coils = workloads.gre3d_64(args.n)
-        workload = WORKLOAD if args.n == 64 else f"gre3d_{args.n}"
-    if args.max_segments:
-        seq = workloads.first_trs(seq, args.max_segments)
-        workload += f"; its first {len(seq)} segments (whole TRs)"
-    n, S = len(ph.pd), len(seq)
+    every = adjoint.default_checkpoint_every(S)
+    run = adjoint.Checkpointed(pk, every, dev)
     g = torch.Generator().manual_seed(7)
-    n_adc = int(sum(seq.adc))
-    wr, wi = torch.randn(coils.shape[1], n_adc, generator=g), torch.randn(coils.shape[1], n_adc, generator=g)
-    t1 = ph.t1.clone().requires_grad_()
-    rf = seq.rf.clone().requires_grad_()
-    phg = bpb.Phantom(ph.pos, ph.pd, t1, ph.t2, ph.db0)
-    seqg = bpb.Sequence(seq.dt, rf, seq.grad, seq.adc_phase, list(seq.is_rf), list(seq.adc), list(seq.spoil))
+    w = torch.complex(torch.randn(pk.n_coils, pk.n_adc, generator=g, dtype=torch.float64),
+                      torch.randn(pk.n_coils, pk.n_adc, generator=g, dtype=torch.float64))
+    h = run.cotangent(w)  # loss = sum(Re s Re w + Im s Im w): dL/ds = w
+    lam = torch.zeros(3, pk.n, dtype=torch.float32, device=dev)
+    mask = _lib.BP_SEG_WX | _lib.BP_SEG_WY | _lib.BP_SPIN_NO_OFFSETS
+    state = torch.empty_like(state0)
 
-    def step():
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        t1.grad = rf.grad = None
-        torch.cuda.synchronize()
-        e0.record()
-        r = bpb.simulate(phg, seqg, coils)
-        e1.record()
-        loss = (r.signal.real * wr).sum() + (r.signal.imag * wi).sum()
-        loss.backward()
-        e2.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1), e1.elapsed_time(e2)
+    def step(times=None):
+        state.copy_(state0)
+        lam.zero_()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        run.forward(state)
+        e[1].record()
+        run.backward(h, lam, mask, False, True)
+        e[2].record()
+        if times is not None:
+            times.append(e)
 
     for _ in range(args.warmup):
         step()
-    clocks = Clocks(dev.index or 0)
+    run.check()
     times = []
+    clocks = Clocks(dev.index or 0)
     with clocks:
         for _ in range(args.steps):
-            times.append(step())
-    f_ms = statistics.mean(t[0] for t in times)
-    b_ms = statistics.mean(t[1] for t in times)
+            flush.zero_()
+            torch.cuda.synchronize()
+            step(times)
+            torch.cuda.synchronize()
+    run.check()
+    f_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in times)
+    b_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in times)
     ms = f_ms + b_ms
-    flags = engine.pack_segments(seq.dt, seq.rf, seq.grad, None, seq.adc_phase, list(seq.is_rf), list(seq.adc),
-                                 list(seq.spoil), "cpu")[3]
-    fwd, bwd = grad_flops_per_spin(flags, coils.shape[1])
-    every = adjoint.default_checkpoint_every(S)
-    intervals = math.ceil(S / every)
+    fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils)
     peak = ffma_peak_tflops(dev)
     achieved = n * (fwd + bwd) / (ms * 1e-3) / 1e12
-    line = {
-        "metric": "isochromat-steps/s (fwd+adjoint)", "value": n * S / (ms * 1e-3), "unit": UNIT, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload, "spins": n, "segments": S,
-                   "coils": coils.shape[1], "grad_wrt": ["t1", "rf"], "checkpoint_every": every,
-                   "forward_ms": f_ms, "backward_ms": b_ms,
-                   "l2": "inputs larger than L2; the forward starts from host tensors (packing and copies inside)"},
+    lf, lb = run.launches(True)
+    return {
+        "metric": "isochromat-steps/s (fwd+adjoint)", "value": n * S / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+        "forward_ms": f_ms, "backward_ms": b_ms, "steps": args.steps, "warmup": args.warmup,
+        "grad_wrt": "the RF waveform (flip train), seeded linear loss of the signal",
+        "checkpoint_every": every, "intervals": len(run.plan.starts),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": None, "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU",
-                     "kernel": "bp_forward_kernel (forward, replay) + bp_adjoint_kernel",
+                     "kernel": "bp_forward_kernel (forward, replay) + bp_adjoint_kernel + bp_seg_reduce_kernel",
                      "flops_per_spin": {"forward": fwd, "backward": bwd}},
-        "gpu_launches": intervals * 4 + 1,
-        "clocks": clocks.summary(),
+        "gpu_launches": args.steps * (lf + lb), "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+
+
+def e2e_fwd_adjoint(ph, seq, coils):
+    """The forward + adjoint through the public API from host tensors (one run after the timed steps): simulate
+    with the RF waveform requiring grad, the seeded linear loss, backward; wall clock (ms), bytes in and out."""
+    import blochparty_b200 as bpb
+
+    g = torch.Generator().manual_seed(7)
+    n_adc = int(sum(seq.adc))
+    wr = torch.randn(coils.shape[1], n_adc, generator=g, dtype=torch.float64)
+    wi = torch.randn(coils.shape[1], n_adc, generator=g, dtype=torch.float64)
+    rf = seq.rf.clone().requires_grad_()
+    seqg = bpb.Sequence(seq.dt, rf, seq.grad, seq.adc_phase, list(seq.is_rf), list(seq.adc), list(seq.spoil))
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r = bpb.simulate(ph, seqg, coils)
+    ((r.signal.real.double() * wr).sum() + (r.signal.imag.double() * wi).sum()).backward()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t) * 1e3, rf.grad.numel() * rf.grad.element_size()
 
 
 def main():
@@ -369,21 +404,22 @@ def main():
                          "engine (baseline/_ref) against this engine on the reference's benchmark cases")
     ap.add_argument("--cases", default="3d-32,3d-48,3d-64,3d-96,gre3d-128", help="--impl reference_gpu: cases")
     ap.add_argument("--repeat", type=int, default=2, help="--impl reference_gpu: timed runs per case (fastest kept)")
-    ap.add_argument("--readout", default="fp32", choices=("fp32", "bf16x3"))
-    ap.add_argument("--n", type=int, default=64, help="grid size of the 3D GRE (64: the measured workload)")
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--grad", action="store_true", help="forward + adjoint (gradients of T1 and the RF), one GPU")
-    ap.add_argument("--surrogate-pieces", type=int, default=1, help="networks per slab pulse (--pulses surrogate)")
-    ap.add_argument("--surrogate-epochs", type=int, default=400,
-                    help="training epochs per network (--pulses surrogate; speed does not depend on them)")
-    ap.add_argument("--workload", default="gre3d_64", choices=("gre3d_64", "gre3d_128_4echo"))
+    ap.add_argument("--grad", action="store_true", help="--impl reference_gpu: forward + backward")
+    ap.add_argument("--workload", default="gre3d_128_4echo", choices=("gre3d_128_4echo", "gre3d_64"))
+    ap.add_argument("--trs", type=int, default=None,
+                    help="time the workload's first TRs only (default: 64 for gre3d_128_4echo, all for gre3d_64)")
     ap.add_argument("--head-n", type=int, default=128, help="grid size of the 4-echo head workload (128: as named)")
-    ap.add_argument("--max-segments", type=int, default=0,
-                    help="time the workload's first whole TRs only, up to this many segments (0: all)")
+    ap.add_argument("--n", type=int, default=64, help="grid size of the gre3d_64 workload")
+    ap.add_argument("--readout", default="fp32", choices=("fp32", "bf16x3"))
     ap.add_argument("--pulses", default="step", choices=("step", "reuse", "surrogate"),
                     help="reuse: recurring pulses through their exact per-spin maps (composed inside every step); "
                          "surrogate: the slab pulse through a network trained before the timed region")
+    ap.add_argument("--surrogate-pieces", type=int, default=1, help="networks per slab pulse (--pulses surrogate)")
+    ap.add_argument("--surrogate-epochs", type=int, default=400,
+                    help="training epochs per network (--pulses surrogate; speed does not depend on them)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-grad", action="store_true", help="skip the forward + adjoint measurement")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -402,26 +438,13 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if args.grad:
-        if world > 1:
-            raise SystemExit("--grad measures one GPU")
-        run_grad(args, dev)
-        return
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     import blochparty_b200 as bpb
-    from blochparty_b200 import _lib, engine, workloads
+    from blochparty_b200 import _lib, engine
 
-    if args.workload == "gre3d_128_4echo":
-        ph, seq, coils = workloads.gre3d_128_4echo(args.head_n)
-        workload = head_workload(args.head_n)
-    else:
-        ph, seq, coils = workloads.gre3d_64(args.n) if rank == 0 else _rank_workload(args.n, rank)
-        workload = WORKLOAD if args.n == 64 else f"gre3d_{args.n}"
-    if args.max_segments:
-        seq = workloads.first_trs(seq, args.max_segments)
-        workload += f"; its first {len(seq)} segments (whole TRs)"
+    ph, seq, coils, workload = build_workload(args, rank)
     inp = bpb.api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad,
                          seq.adc_phase, None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
     pk = engine.pack(inp, dev)
@@ -533,6 +556,13 @@ def main():
     _lib.check_status(status, "forward")
     d2h = pk.n_coils * pk.n_adc * 8 + state.numel() * 4
 
+    grad_line = None
+    if world == 1 and not args.no_grad and replaced is None and mma is None:
+        grad_line = measure_fwd_adjoint(args, dev, pk, state0, flush, n, S)
+        g_ms, g_d2h = e2e_fwd_adjoint(ph, seq, coils)
+        grad_line["e2e"] = {"value": n * S / (g_ms * 1e-3), "unit": UNIT, "ms_per_step": g_ms, "h2d_bytes_per_step": h2d,
+                            "d2h_bytes_per_step": d2h + g_d2h, "runs": 1}
+
     if rank != 0:
         dist.destroy_process_group() if world > 1 else None
         return
@@ -563,8 +593,9 @@ def main():
                    "coils": pk.n_coils, "readout": args.readout, "pulses": args.pulses, **({"surrogate": sur_info}
                                                                                                if sur_info else {}),
                    "ctas": (_lib.lib().bp_forward_mma_grid(n) if mma is not None
-                            else _lib.lib().bp_forward_grid(n, pk.n_coils)), "l2": "inputs larger than L2 (state, spins, coils, "
-                   "segments ~220 MB per GPU) and a 256 MB L2 flush between timed steps"},
+                            else _lib.lib().bp_forward_grid(n, pk.n_coils)),
+                   "l2": "inputs larger than L2 (state, spins, coils, segments: hundreds of MB per GPU) and a 256 MB L2 "
+                         "flush between timed steps"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU; MEASURED_PEAKS.json has no FP32",
@@ -578,24 +609,16 @@ def main():
                                        + len(fwd_events) + 1)),
         "clocks": clocks.summary(),
     }
+    if grad_line is not None:
+        line["fwd_adjoint"] = grad_line
+        line["gpu_launches"] += grad_line["gpu_launches"]
     if world == 1 and not args.no_cpu_baseline:
-        case, sample = cpu_sample(workloads.gre3d_128_4echo if args.workload == "gre3d_128_4echo"
-                                  else workloads.gre3d_64)
+        case, sample = cpu_sample(ph, seq, coils)
         v, cores = time_cpu(case)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
-
-
-def _rank_workload(n, rank):
-    """Rank r's own phantom for weak scaling: the workload with sub-voxel offsets seeded by 1 + r."""
-    from blochparty_b200 import phantoms, workloads
-
-    ph0, seq, coils = workloads.gre3d_64(n)
-    ph = phantoms.ellipsoid_phantom_3d(n, 0.25, n_ellipsoids=10, spins_per_voxel=4, seed=0, subvoxel_seed=1 + rank,
-                                       b0_seed=2, b0_max=100.0, sigma_vox=4.0)
-    return ph, seq, phantoms.birdcage_sensitivities(ph.pos, 8)
 
 
 if __name__ == "__main__":

@@ -99,6 +99,103 @@ class Plan:
         self.max_len = max(b - a for a, b in self.seg_ranges)
 
 
+class Checkpointed:
+    """The device side of a simulation with gradients on a packed case: the forward that stores the state at every
+    interval start, and the backward (per interval in reverse: replay, reverse sweep, segment-gradient reduction).
+    Every buffer is sized by the C ABI's workspace query (``bp_forward_workspace_bytes``,
+    ``bp_adjoint_workspace_bytes``); the backward's buffers are allocated on its first call and reused."""
+
+    def __init__(self, pk: engine.Packed, every: int, device):
+        self.pk, self.dev = pk, device
+        self.plan = plan = Plan(pk, every, device)
+        fws = _lib.forward_workspace(pk.n, pk.n_adc, pk.n_coils)
+        self.grid = _lib.lib().bp_adjoint_grid(pk.n, pk.n_coils)
+        if self.grid < 1:
+            raise RuntimeError("bp_adjoint_grid failed")
+        self.ws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, every, plan.max_aw, self.grid)
+        self.ckpts = sized(self.ws.checkpoints, (len(plan.starts), 6, pk.n), F32, device)
+        self.raw = sized(fws.raw, (max(pk.n_adc, 1), 2 * pk.n_coils), F64, device, zero=True)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self._bufs = None
+
+    def forward(self, state: torch.Tensor) -> None:
+        """All intervals from ``state`` ([6][n], advanced in place), the raw coil sums into ``raw`` (zeroed first),
+        the state at every interval start into the checkpoints."""
+        pk, plan = self.pk, self.plan
+        self.raw.zero_()
+        for k, (fa, fb) in enumerate(plan.franges):
+            self.ckpts[k].copy_(state)
+            engine.run_forward(pk, state, plan.fwin_dev, fa, fb, self.raw if pk.n_adc else None, self.status)
+
+    def buffers(self, need_seg: bool, want_gc: bool):
+        pk, plan, ws, dev = self.pk, self.plan, self.ws, self.dev
+        if self._bufs is None:
+            self._bufs = {"gs": sized(ws.gs, (8, pk.n), F32, dev), "seg": sized(ws.seg, (pk.flags.shape[0], 8), F64, dev),
+                          "wstates": sized(ws.wstates, (plan.max_aw, 6, pk.n), F32, dev),
+                          "state": sized(ws.replay_state, (6, pk.n), F32, dev)}
+        b = self._bufs
+        if need_seg and "gseg" not in b:
+            b["gseg"] = sized(ws.gseg, (self.grid, plan.max_len, 8), F32, dev)
+        if want_gc and "gc" not in b:
+            b["gc"] = sized(ws.gc, (2 * pk.n_coils, pk.n), F32, dev)
+        return b
+
+    def backward(self, h: torch.Tensor | None, lam: torch.Tensor, seg_mask: int, want_gc: bool, need_seg: bool):
+        """dL/d(per-spin inputs) ``gs`` [8][n], dL/d(coils) ``gc`` [2C][n] (or None) and the segment gradients
+        ``seg`` [S][8] (float64), from the cotangent ``h`` of the raw coil sums ([A][2C] float32, or None) and
+        ``lam`` = dL/dm at the end ([3][n], turned into dL/dm at the start in place). Asynchronous: the status word
+        is checked by ``check``."""
+        pk, plan = self.pk, self.plan
+        b = self.buffers(need_seg, want_gc)
+        gs, seg, wstates, state = b["gs"], b["seg"], b["wstates"], b["state"]
+        gc, gseg = (b["gc"] if want_gc else None), (b["gseg"] if need_seg else None)
+        gs.zero_()
+        seg.zero_()
+        if gc is not None:
+            gc.zero_()
+        lib, stream, n, C, A = _lib.lib(), _lib.stream_ptr(), pk.n, pk.n_coils, pk.n_adc
+        for k in reversed(range(len(plan.starts))):
+            aa, ab = plan.aranges[k]
+            s0, s1 = plan.seg_ranges[k]
+            state.copy_(self.ckpts[k])
+            engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, self.status, wstates=wstates, wstate_stride=1)
+            code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
+                                  aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
+                                  seg_mask, self.grid, ptr(self.status), stream)
+            _lib.check(code, "bp_adjoint")
+            if need_seg:
+                _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
+        return gs, gc, seg
+
+    def launches(self, need_seg: bool) -> tuple[int, int]:
+        """(forward, backward) kernel launches of one call each."""
+        k = len(self.plan.starts)
+        return k, k * (3 if need_seg else 2)
+
+    def check(self, what: str = "bp_forward / bp_adjoint") -> None:
+        torch.cuda.synchronize(self.dev)
+        _lib.check_status(self.status, what)
+
+    def cotangent(self, g_sig: torch.Tensor) -> torch.Tensor:
+        """h = dL/d(raw coil sums) [A][2C] float32 on the device from dL/dsignal (C, A) (complex, or (C, A, 2)
+        real pairs): dL/draw = dL/dsignal e^{+i psi}."""
+        pk = self.pk
+        g = g_sig if g_sig.is_complex() else torch.complex(g_sig[..., 0].to(F64), g_sig[..., 1].to(F64))
+        hr = g.to(torch.complex128).to(self.dev) * torch.exp(1j * pk.psi)[None, :]
+        h = sized(self.ws.h, (pk.n_adc, 2 * pk.n_coils), F32, self.dev)
+        h.copy_(torch.view_as_real(hr.T.contiguous()).reshape(pk.n_adc, 2 * pk.n_coils))
+        return h
+
+
+def seg_mask_for(need) -> int:
+    """The segment gradients the chain rules use (``need``: ``_Simulate``'s needs_input_grad): dt needs all of
+    them (the record's every field scales with dt), the RF its two components, the gradient the moments,
+    b0_offset its phase; and ``BP_SPIN_NO_OFFSETS`` unless the positions' or dB0's gradients are wanted."""
+    return (_lib.BP_SEG_ALL if need[8] else 0) | ((_lib.BP_SEG_WX | _lib.BP_SEG_WY) if need[9] else 0) | (
+        (_lib.BP_SEG_KX | _lib.BP_SEG_KY | _lib.BP_SEG_KZ) if need[10] else 0) | (
+        _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5]) else _lib.BP_SPIN_NO_OFFSETS)
+
+
 class _Simulate(torch.autograd.Function):
     @staticmethod
     def forward(ctx, opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0):
@@ -110,20 +207,12 @@ class _Simulate(torch.autograd.Function):
         inp = Inputs(d(pos), d(pd), d(t1), d(t2), d(db0), d(b1), coils, d(dt), d(rf), d(grad), d(adc_phase),
                      d(b0_offset), *flags_in, d(m0))
         pk = engine.pack(inp, dev)
-        plan = Plan(pk, every, dev)
+        run = Checkpointed(pk, every, dev)
         state = engine.initial_state(inp.pd, inp.m_init, dev)
-        fws = _lib.forward_workspace(pk.n, pk.n_adc, pk.n_coils)
-        aws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, every, plan.max_aw, 1)
-        ckpts = sized(aws.checkpoints, (len(plan.starts), 6, pk.n), F32, dev)
-        raw = sized(fws.raw, (max(pk.n_adc, 1), 2 * pk.n_coils), F64, dev, zero=True)
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
-        for k, (fa, fb) in enumerate(plan.franges):
-            ckpts[k].copy_(state)
-            engine.run_forward(pk, state, plan.fwin_dev, fa, fb, raw if pk.n_adc else None, status)
-        sig = engine.finish_signal(pk, raw)
-        torch.cuda.synchronize(dev)
-        _lib.check_status(status, "bp_forward")
-        ctx.pk, ctx.plan, ctx.ckpts, ctx.dev = pk, plan, ckpts, dev
+        run.forward(state)
+        sig = engine.finish_signal(pk, run.raw)
+        run.check("bp_forward")
+        ctx.run, ctx.dev = run, dev
         ctx.like = [None if t is None else (t.dtype, t.device) for t in
                     (pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0)]
         sig_ri = torch.view_as_real(sig).cpu().contiguous()  # (C, A, 2)
@@ -135,52 +224,20 @@ class _Simulate(torch.autograd.Function):
     @once_differentiable
     def backward(ctx, g_sig, g_m):
         t1, t2, dt, rf, grad, b0_offset, adc_phase, sig_ri = ctx.saved_tensors
-        pk, plan, dev = ctx.pk, ctx.plan, ctx.dev
+        run, dev = ctx.run, ctx.dev
+        pk = run.pk
         # inputs: opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0
         need = ctx.needs_input_grad
         if g_sig is None and g_m is None:
             return (None,) * 14
         n, C, A, S = pk.n, pk.n_coils, pk.n_adc, len(dt)
-        grid = _lib.lib().bp_adjoint_grid(n, C)
-        if grid < 1:
-            raise RuntimeError("bp_adjoint_grid failed")
-        ws = _lib.adjoint_workspace(n, S, A, C, plan.every, plan.max_aw, grid)
-        h = None
-        if g_sig is not None and A:
-            g = torch.complex(g_sig[..., 0].to(F64), g_sig[..., 1].to(F64)).to(dev)  # (C, A)
-            hr = g * torch.exp(1j * pk.psi)[None, :]  # dL/draw = dL/dsignal e^{+i psi}
-            h = sized(ws.h, (A, 2 * C), F32, dev)
-            h.copy_(torch.view_as_real(hr.T.contiguous()).reshape(A, 2 * C))
-        lam = sized(ws.lam, (3, n), F32, dev, zero=True)
+        h = run.cotangent(g_sig) if (g_sig is not None and A) else None
+        lam = sized(run.ws.lam, (3, n), F32, dev, zero=True)
         if g_m is not None:
             lam.copy_(g_m.T.to(F32))
-        gs = sized(ws.gs, (8, n), F32, dev, zero=True)
-        gc = sized(ws.gc, (2 * C, n), F32, dev, zero=True) if (need[7] and h is not None) else None
         need_seg = any(need[i] for i in (8, 9, 10, 12))
-        # the segment gradients the chain rules below use: dt needs all of them (the record's every field scales
-        # with dt), the RF its two components, the gradient the moments, b0_offset its phase
-        seg_mask = (_lib.BP_SEG_ALL if need[8] else 0) | ((_lib.BP_SEG_WX | _lib.BP_SEG_WY) if need[9] else 0) | (
-            (_lib.BP_SEG_KX | _lib.BP_SEG_KY | _lib.BP_SEG_KZ) if need[10] else 0) | (
-            _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5]) else _lib.BP_SPIN_NO_OFFSETS)
-        gseg = sized(ws.gseg, (grid, plan.max_len, 8), F32, dev) if need_seg else None
-        seg = sized(ws.seg, (S, 8), F64, dev, zero=True)
-        wstates = sized(ws.wstates, (plan.max_aw, 6, n), F32, dev)
-        state = sized(ws.replay_state, (6, n), F32, dev)
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
-        lib, stream = _lib.lib(), _lib.stream_ptr()
-        for k in reversed(range(len(plan.starts))):
-            aa, ab = plan.aranges[k]
-            s0, s1 = plan.seg_ranges[k]
-            state.copy_(ctx.ckpts[k])
-            engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, status, wstates=wstates, wstate_stride=1)
-            code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
-                                  aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
-                                  seg_mask, grid, ptr(status), stream)
-            _lib.check(code, "bp_adjoint")
-            if need_seg:
-                _lib.check(lib.bp_seg_reduce(ptr(gseg), grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
-        torch.cuda.synchronize(dev)
-        _lib.check_status(status, "bp_forward (replay) / bp_adjoint")
+        gs, gc, seg = run.backward(h, lam, seg_mask_for(need), need[7] and h is not None, need_seg)
+        run.check("bp_forward (replay) / bp_adjoint")
         gs64, lam64 = gs.to(F64).cpu(), lam.to(F64).cpu()
         out = [None] * 13
         if need[1]:

@@ -96,3 +96,17 @@ def first_trs(seq, max_segments: int):
     return Sequence(seq.dt[sl], seq.rf[sl], seq.grad[sl], seq.adc_phase[sl], list(seq.is_rf[:cut]),
                     list(seq.adc[:cut]), list(seq.spoil[:cut]), dict(seq.meta, first_segments=cut),
                     None if seq.b0_offset is None else seq.b0_offset[sl])
+
+
+def first_n_trs(seq, n_tr: int):
+    """The sequence's first ``n_tr`` TRs (cut at the start of the pulse that begins TR ``n_tr``; the whole sequence
+    if it has no more TRs): a bounded sample of a TR-periodic workload with the same work per segment."""
+    is_rf = np.asarray(seq.is_rf, dtype=bool)
+    starts = np.flatnonzero(is_rf & ~np.concatenate([[False], is_rf[:-1]]))
+    if n_tr >= len(starts) or n_tr < 1:
+        return seq
+    cut = int(starts[n_tr])
+    sl = slice(0, cut)
+    return Sequence(seq.dt[sl], seq.rf[sl], seq.grad[sl], seq.adc_phase[sl], list(seq.is_rf[:cut]),
+                    list(seq.adc[:cut]), list(seq.spoil[:cut]), dict(seq.meta, n_tr=n_tr, first_segments=cut),
+                    None if seq.b0_offset is None else seq.b0_offset[sl])
