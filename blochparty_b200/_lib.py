@@ -70,6 +70,7 @@ SIGNATURES = {
     "bp_forward_spans": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, _P, c_int, _P, _P, _P, c_int, _P, _P]),
     "bp_signal_finish": (c_int, [_P, _P, c_int, c_int, _P, _P]),
     "bp_ffma_peak": (c_int, [_P, c_int, _P, _P]),
+    "bp_ffma2_peak": (c_int, [_P, c_int, _P, _P]),
     "bp_mma_atiles_bytes": (c_int64, [c_int]),
     "bp_mma_atiles": (c_int, [_P, c_int, c_int, _P, _P]),
     "bp_forward_mma": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P]),

@@ -215,9 +215,13 @@ class _Simulate(torch.autograd.Function):
         ctx.run, ctx.dev = run, dev
         ctx.like = [None if t is None else (t.dtype, t.device) for t in
                     (pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0)]
+        ctx.raw_mode = bool(opts.get("raw"))
+        ctx.set_materialize_grads(False)
+        if ctx.raw_mode:  # the float64 raw coil sums on the device, not demodulated (the caller demodulates)
+            ctx.save_for_backward(t1, t2, dt, rf, grad, b0_offset, adc_phase, None)
+            return run.raw[: pk.n_adc].clone(), engine.final_m(state)
         sig_ri = torch.view_as_real(sig).cpu().contiguous()  # (C, A, 2)
         ctx.save_for_backward(t1, t2, dt, rf, grad, b0_offset, adc_phase, sig_ri)
-        ctx.set_materialize_grads(False)
         return sig_ri, engine.final_m(state)
 
     @staticmethod
@@ -231,7 +235,10 @@ class _Simulate(torch.autograd.Function):
         if g_sig is None and g_m is None:
             return (None,) * 14
         n, C, A, S = pk.n, pk.n_coils, pk.n_adc, len(dt)
-        h = run.cotangent(g_sig) if (g_sig is not None and A) else None
+        if ctx.raw_mode:  # dL/d(raw coil sums) directly
+            h = sized(run.ws.h, (A, 2 * C), F32, dev).copy_(g_sig) if (g_sig is not None and A) else None
+        else:
+            h = run.cotangent(g_sig) if (g_sig is not None and A) else None
         lam = sized(run.ws.lam, (3, n), F32, dev, zero=True)
         if g_m is not None:
             lam.copy_(g_m.T.to(F32))
@@ -269,7 +276,7 @@ class _Simulate(torch.autograd.Function):
                 out[9] = sg[:, 3:6] * dt64[:, None]
             if need[12]:
                 out[11] = sg[:, 6] * dt64
-        if need[11] and g_sig is not None and A:
+        if need[11] and g_sig is not None and A and not ctx.raw_mode:
             adc_idx = torch.tensor(np.flatnonzero(pk.flags & engine.ADC))
             sr, si_ = sig_ri[..., 0].to(F64), sig_ri[..., 1].to(F64)
             gr, gi = g_sig[..., 0].to(F64), g_sig[..., 1].to(F64)
@@ -282,8 +289,7 @@ class _Simulate(torch.autograd.Function):
                         for i, v in enumerate(out)])
 
 
-def simulate_grad(inp, dev, checkpoint_every, options) -> SimResult:
-    """``simulate`` with gradients: the inputs as tensors of ``_Simulate``."""
+def _check_grad_options(options):
     if options.get("readout", "fp32") != "fp32":
         raise NotImplementedError("b200 engine: gradients through readout='bf16x3' are not implemented; use the "
                                   "default float32 readout (or torch.no_grad())")
@@ -292,6 +298,9 @@ def simulate_grad(inp, dev, checkpoint_every, options) -> SimResult:
     if options.get("pulses", "step") != "step":
         raise NotImplementedError("b200 engine: gradients through pulses='surrogate' are not implemented; use "
                                   "pulses='step' (or torch.no_grad())")
+
+
+def _apply(inp, dev, checkpoint_every, raw: bool):
     S = len(inp.dt)
     every = checkpoint_every or default_checkpoint_every(S)
     if every % _lib.BP_ADJ_WIN:
@@ -302,8 +311,30 @@ def simulate_grad(inp, dev, checkpoint_every, options) -> SimResult:
         z = torch.zeros_like(inp.pd)
         m0 = torch.stack([z, z, inp.pd], -1)
     coils_ri = torch.view_as_real(inp.coils if inp.coils.is_complex() else inp.coils.to(torch.complex64))
-    opts = {"device": dev, "every": every, "flags": (inp.is_rf, inp.adc, inp.spoil)}
-    sig_ri, m = _Simulate.apply(opts, inp.pos, inp.pd, inp.t1, inp.t2, inp.db0, inp.b1, coils_ri, inp.dt, inp.rf,
-                                inp.grad, inp.adc_phase, inp.b0_offset, m0)
-    signal = torch.view_as_complex(sig_ri.contiguous())
-    return SimResult(signal, m)
+    opts = {"device": dev, "every": every, "flags": (inp.is_rf, inp.adc, inp.spoil), "raw": raw}
+    return _Simulate.apply(opts, inp.pos, inp.pd, inp.t1, inp.t2, inp.db0, inp.b1, coils_ri, inp.dt, inp.rf, inp.grad,
+                           inp.adc_phase, inp.b0_offset, m0)
+
+
+def simulate_grad(inp, dev, checkpoint_every, options) -> SimResult:
+    """``simulate`` with gradients: the inputs as tensors of ``_Simulate``."""
+    _check_grad_options(options)
+    sig_ri, m = _apply(inp, dev, checkpoint_every, raw=False)
+    return SimResult(torch.view_as_complex(sig_ri.contiguous()), m)
+
+
+def simulate_raw(inp, dev, checkpoint_every=None):
+    """The differentiable float64 raw coil sums (A, 2 C) on the device (coil c's real part in column 2 c, its
+    imaginary part in 2 c + 1; not demodulated) and m (N, 3) float32 on the CPU, gradients by the adjoint: the
+    per-rank part of a sharded simulation, whose ranks sum their raw sums before demodulating
+    (``parallel.simulate``)."""
+    return _apply(inp, dev, checkpoint_every, raw=True)
+
+
+def demodulate(total: torch.Tensor, adc_phase: torch.Tensor, adc) -> torch.Tensor:
+    """The (C, A) complex signal from raw coil sums (A, 2 C): coil c is (total[:, 2c] + i total[:, 2c + 1])
+    exp(-i adc_phase) at the ADC segments (differentiable in both, float64)."""
+    idx = torch.tensor(np.flatnonzero(np.asarray([bool(x) for x in adc])), dtype=torch.long)
+    psi = adc_phase.to(F64)[idx.to(adc_phase.device)].to(total.device)
+    z = torch.complex(total[:, 0::2].to(F64), total[:, 1::2].to(F64))
+    return (z * torch.exp(-1j * psi)[:, None]).T

@@ -273,6 +273,8 @@ int bp_forward_spans(const float* spins, const float* sens, int n, int n_coils, 
  * independent FFMAs; `*flops` receives the flop count of the launch, which the caller divides by the launch's
  * CUDA-event duration. `out` needs 4 * SMs * 256 floats (never written in practice). */
 int bp_ffma_peak(float* out, int iters, int64_t* flops, void* stream);
+/* The same with paired FMAs (two per instruction on float pairs, 8 independent FMAs per thread per step). */
+int bp_ffma2_peak(float* out, int iters, int64_t* flops, void* stream);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,46 @@ def _oracle_forward(inp):
     return raw, finish, m.to(torch.float32)
 
 
+def _oracle_grad_forward(inp):
+    """One rank's differentiable part through the oracle (autograd through its float64 arithmetic): the demodulated
+    signal as (A, 2 C) sums; ``finish`` turns the summed sums back into the (C, A) signal."""
+    case = bloch.Case(*[getattr(inp, f) for f in bloch.Case.__dataclass_fields__])
+    sig, m = bloch.simulate(case)
+    raw = torch.view_as_real(sig.T.contiguous()).reshape(sig.shape[1], -1)
+    finish = lambda total, adc_phase: torch.view_as_complex(total.reshape(total.shape[0], -1, 2).contiguous()).T
+    return raw, finish, m
+
+
+class _FailInBackward(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x):
+        return x.clone()
+
+    @staticmethod
+    def backward(ctx, g):
+        raise ValueError("rank 1's backward failed")
+
+
+def _failing_grad_forward(inp):
+    raw, finish, m = _oracle_grad_forward(inp)
+    return (_FailInBackward.apply(raw) if dist.get_rank() == 1 else raw), finish, m
+
+
+GRAD_NAMES = ("t1", "pd", "db0", "coils", "rf", "dt", "adc_phase", "m_init")
+
+
+def _grad_leaves(case):
+    """The golden case's inputs, the ones in GRAD_NAMES as leaves requiring grad."""
+    from dataclasses import replace
+
+    return replace(case, **{k: getattr(case, k).detach().clone().requires_grad_() for k in GRAD_NAMES})
+
+
+def _grad_loss(sig, m, z):
+    wr, wi, wm = (torch.from_numpy(z[k]).to(F64) for k in ("w_re", "w_im", "w_m"))
+    return (sig.real * wr).sum() + (sig.imag * wi).sum() + (m.to(F64) * wm).sum()
+
+
 def _failing_forward(inp):
     if dist.get_rank() == 1:
         raise ValueError("rank 1's forward failed")
@@ -61,6 +101,17 @@ def _worker(rank, world, port, mode, out):
             mine, c, m0 = parallel.shard_phantom(ph, coils, m_init, lo, hi)
             r = parallel.simulate(mine, seq, c, m_init=m0, sharded=False, local_forward=_oracle_forward)
             out.put((rank, "ok", r.signal, r.m))
+        elif mode in ("grad", "grad_fail"):
+            case, _, _, z = golden_cases.load("grad_busy")
+            c = _grad_leaves(case)
+            ph, seq, coils, m_init = golden_cases.objects(c)
+            fwd = _oracle_grad_forward if mode == "grad" else _failing_grad_forward
+            try:
+                r = parallel.simulate(ph, seq, coils, m_init=m_init, local_forward=fwd)
+                _grad_loss(r.signal, r.m, z).backward()
+                out.put((rank, "ok", {k: getattr(c, k).grad.detach().clone() for k in GRAD_NAMES}, r.signal.detach()))
+            except Exception as e:
+                out.put((rank, type(e).__name__, str(e), None))
         else:
             try:
                 parallel.simulate(ph, seq, coils, m_init=m_init, local_forward=_failing_forward)
@@ -104,4 +155,35 @@ def test_two_ranks_equal_one_process(mode):
 def test_a_failed_rank_fails_every_rank():
     res = _run("fail")
     assert res[0][1] == "RuntimeError" and "1 rank(s) failed" in res[0][2]
+    assert res[1][1] == "ValueError" and "rank 1" in res[1][2]
+
+
+SEQ = ("rf", "dt", "adc_phase")
+
+
+def test_two_ranks_gradients_equal_one_process():
+    """The sharded simulation with gradients (world size 2, each rank's part through the oracle's autograd): the
+    sequence tensors' gradients (all-reduced) are the single process's on every rank; the per-spin gradients are
+    local, and their sum over the ranks is the single process's."""
+    case, _, _, z = golden_cases.load("grad_busy")
+    c = _grad_leaves(case)
+    sig, m = bloch.simulate(c)
+    _grad_loss(sig, m, z).backward()
+    ref = {k: getattr(c, k).grad for k in GRAD_NAMES}
+    res = _run("grad")
+    assert all(r[1] == "ok" for r in res), res
+    for k in GRAD_NAMES:
+        if k in SEQ:
+            for r in res:
+                assert float((r[2][k] - ref[k]).abs().max() / ref[k].abs().max()) < 1e-12, k
+        else:
+            tot = res[0][2][k] + res[1][2][k]
+            assert float((tot - ref[k]).abs().max() / ref[k].abs().max()) < 1e-12, (k, float((tot - ref[k]).abs().max() / ref[k].abs().max()))
+            lo, hi = parallel.shard_range(len(case.pd), 2, 1)
+            assert float(res[0][2][k][lo:hi].abs().max()) == 0.0  # rank 0 holds only its own rows
+
+
+def test_a_failed_backward_fails_every_rank():
+    res = _run("grad_fail")
+    assert res[0][1] == "RuntimeError" and "failed in their local backward" in res[0][2]
     assert res[1][1] == "ValueError" and "rank 1" in res[1][2]
