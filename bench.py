@@ -71,7 +71,23 @@ def flops_per_spin(flags: np.ndarray, n_coils: int) -> int:
 # with its rotation factors; 163 with the offsets'), free segment 30 (free_reverse; 58), ADC sample 8 per coil (the
 # signal's cotangent; 16 with the coil gradients) + 2.
 FLOP_RF_RECOMP, FLOP_FREE_RECOMP, FLOP_FACTORS = 61, 13, 18
+# the NUFFT readout's work per spin and run (readout="nufft", counted from bp_forward_kernel's NUFFT path): the
+# factors and first sample (34 + 8), the centring shift (6), per grid cell the kernel weight (8) and per (cell,
+# term) the weight product (6) and the coil contraction (8 per coil)
+FLOP_NUF_RUN, FLOP_NUF_CELL, FLOP_NUF_TERM, FLOP_NUF_TERM_PER_COIL = 48, 8, 6, 8
 FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 130, 30, 8, 2
+
+
+def nufft_flops_per_spin(flags: np.ndarray, n_coils: int, plan) -> int:
+    """The forward's algorithmic flops per spin with the NUFFT readout runs: the plain model for every segment
+    outside the runs, the NUFFT path's for every run (W + 1 cells per warp on average: a tile's spread), and the
+    grid's float64 DFT counted in the finish kernel, not here."""
+    keep = np.ones(flags.shape[0], dtype=bool)
+    for a, k in plan.runs:
+        keep[a:a + k] = False
+    cells = plan.W + 1
+    per_run = FLOP_NUF_RUN + cells * (FLOP_NUF_CELL + plan.M * (FLOP_NUF_TERM + FLOP_NUF_TERM_PER_COIL * n_coils))
+    return flops_per_spin(flags[keep], n_coils) + len(plan.runs) * per_run
 
 
 def grad_flops_per_spin(flags: np.ndarray, n_coils: int) -> tuple[int, int]:
@@ -410,7 +426,7 @@ def main():
                     help="time the workload's first TRs only (default: 64 for gre3d_128_4echo, all for gre3d_64)")
     ap.add_argument("--head-n", type=int, default=128, help="grid size of the 4-echo head workload (128: as named)")
     ap.add_argument("--n", type=int, default=64, help="grid size of the gre3d_64 workload")
-    ap.add_argument("--readout", default="fp32", choices=("fp32", "bf16x3"))
+    ap.add_argument("--readout", default="fp32", choices=("fp32", "bf16x3", "nufft"))
     ap.add_argument("--pulses", default="step", choices=("step", "reuse", "surrogate"),
                     help="reuse: recurring pulses through their exact per-spin maps (composed inside every step); "
                          "surrogate: the slab pulse through a network trained before the timed region")
@@ -447,9 +463,15 @@ def main():
     ph, seq, coils, workload = build_workload(args, rank)
     inp = bpb.api.Inputs(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, None, coils, seq.dt, seq.rf, seq.grad,
                          seq.adc_phase, None, list(seq.is_rf), list(seq.adc), list(seq.spoil), None)
-    pk = engine.pack(inp, dev)
-    mma = reuse = sur = None
+    mma = reuse = sur = nr = None
     sur_info = {}
+    if args.readout == "nufft":  # the spins sorted by the readout runs' phase, the run tables
+        from blochparty_b200 import nufft
+
+        pk, nr, order = nufft.prepare(inp, dev)
+        inp = nufft.sorted_inputs(inp, order)
+    else:
+        pk = engine.pack(inp, dev)
     if args.pulses == "reuse":
         from blochparty_b200.pulses import Reuse
 
@@ -471,6 +493,8 @@ def main():
                     "train_s": time.perf_counter() - t0, "network_error_max_rms": [sg.validate() for sg in sgs]}
         sur = surrogate.SurrogateRun(inp, pk, sgs)
         windows, wdev = sur.plan[0], sur.plan[1]
+    elif nr is not None:
+        windows, wdev = nr.windows, nr.wdev
     elif args.readout == "bf16x3":
         from blochparty_b200.readout_mma import MmaBuffers, run_forward_mma
 
@@ -503,6 +527,8 @@ def main():
             sur.run(pk, state, raw, status, events=ev)
         elif mma is not None:
             run_forward_mma(pk, mma, state, raw, status)
+        elif nr is not None:
+            nr.run(state, raw, status)
         else:
             engine.run_forward(pk, state, wdev, 0, windows.shape[0], raw, status)
         if i is not None:
@@ -557,7 +583,7 @@ def main():
     d2h = pk.n_coils * pk.n_adc * 8 + state.numel() * 4
 
     grad_line = None
-    if world == 1 and not args.no_grad and replaced is None and mma is None:
+    if world == 1 and not args.no_grad and replaced is None and mma is None and nr is None:
         grad_line = measure_fwd_adjoint(args, dev, pk, state0, flush, n, S)
         g_ms, g_d2h = e2e_fwd_adjoint(ph, seq, coils)
         grad_line["e2e"] = {"value": n * S / (g_ms * 1e-3), "unit": UNIT, "ms_per_step": g_ms, "h2d_bytes_per_step": h2d,
@@ -583,7 +609,8 @@ def main():
         torch.cuda.synchronize()
         sur_info["signal_rel_l2_vs_stepping"] = float(torch.linalg.vector_norm(sig_sur - sig_plain)
                                                       / torch.linalg.vector_norm(sig_plain))
-    flops = n * flops_per_spin(stepped, pk.n_coils)
+    flops = n * (flops_per_spin(stepped, pk.n_coils) if nr is None else nufft_flops_per_spin(pk.flags, pk.n_coils,
+                                                                                            nr.plan))
     achieved = flops / (kernel_ms * 1e-3) / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -592,6 +619,8 @@ def main():
         "config": {"workload": workload, "spins_per_gpu": n, "segments": S, "adc_samples": pk.n_adc,
                    "coils": pk.n_coils, "readout": args.readout, "pulses": args.pulses, **({"surrogate": sur_info}
                                                                                                if sur_info else {}),
+                   **({"nufft": {"runs": len(nr.plan.runs), "run_samples": nr.plan.L, "grid": nr.plan.G,
+                                 "kernel_width": nr.plan.W, "decay_terms": nr.plan.M}} if nr is not None else {}),
                    "ctas": (_lib.lib().bp_forward_mma_grid(n) if mma is not None
                             else _lib.lib().bp_forward_grid(n, pk.n_coils)),
                    "l2": "inputs larger than L2 (state, spins, coils, segments: hundreds of MB per GPU) and a 256 MB L2 "
@@ -599,12 +628,14 @@ def main():
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU; MEASURED_PEAKS.json has no FP32",
-                     "kernel": "bp_forward_mma_kernel" if mma is not None else "bp_forward_kernel",
+                     "kernel": ("bp_forward_mma_kernel" if mma is not None else
+                                "bp_forward_kernel (NUFFT runs) + bp_nufft_finish_kernel" if nr is not None
+                                else "bp_forward_kernel"),
                      "kernel_ms": kernel_ms,
                      "flops_per_launch": flops},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": statistics.median(e2e_ms) if e2e_ms else None},
-        "gpu_launches": (2 * args.steps if replaced is None else
+        "gpu_launches": ((3 if nr is not None else 2) * args.steps if replaced is None else
                          args.steps * ((len(reuse.pulses) if reuse is not None else 0) + len(replaced.spans)
                                        + len(fwd_events) + 1)),
         "clocks": clocks.summary(),

@@ -27,6 +27,14 @@ class BpSpan(ctypes.Structure):
 
 
 
+class BpNufft(ctypes.Structure):
+    """``BpNufft`` of the C ABI: the NUFFT readout runs of ``bp_forward_nufft``."""
+
+    _fields_ = [("run_of", c_void_p), ("base", c_void_p), ("frac", c_void_p), ("shift", c_void_p),
+                ("decay", c_void_p), ("tile_cells", c_void_p), ("grid", c_void_p), ("G", c_int), ("W", c_int),
+                ("M", c_int), ("beta", c_float)]
+
+
 class BpForwardWorkspace(ctypes.Structure):
     """``BpForwardWorkspace`` of the C ABI: the forward's device buffer sizes in bytes."""
 
@@ -51,6 +59,7 @@ BP_MLP_OUTPUTS = 16
 BP_MMA_SAMPLES = 64
 BP_NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 BP_PULSE_MAP_BYTES = 96
+BP_NUF_MAX_TERMS = 6
 BP_SEG_DT, BP_SEG_WX, BP_SEG_WY, BP_SEG_KX, BP_SEG_KY, BP_SEG_KZ, BP_SEG_BETA = (1 << k for k in range(7))
 BP_SEG_ALL = 0x7F
 BP_SPIN_NO_OFFSETS = 0x80  # with seg_mask: the position and dB0 rows of the spin gradients are not wanted
@@ -96,6 +105,8 @@ SIGNATURES = {
     "bp_adjoint_noalloc": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, c_int, _P,
                                    _P, _P, _P, _P, _P]),
     "bp_forward_workspace_bytes": (c_int, [c_int, c_int64, c_int, _P]),
+    "bp_forward_nufft": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P, _P]),
+    "bp_nufft_finish": (c_int, [_P, _P, c_int, c_int, c_int, c_int, c_int, _P, _P, _P]),
     "bp_adjoint_workspace_bytes": (c_int, [c_int, c_int64, c_int64, c_int, c_int, c_int, c_int, _P]),
 }
 

@@ -291,8 +291,8 @@ class _Simulate(torch.autograd.Function):
 
 def _check_grad_options(options):
     if options.get("readout", "fp32") != "fp32":
-        raise NotImplementedError("b200 engine: gradients through readout='bf16x3' are not implemented; use the "
-                                  "default float32 readout (or torch.no_grad())")
+        raise NotImplementedError(f"b200 engine: gradients through readout={options['readout']!r} are not "
+                                  "implemented; use the default float32 readout (or torch.no_grad())")
     if options.get("pulses", "step") == "reuse":
         raise ValueError("pulses='reuse' is forward only")
     if options.get("pulses", "step") != "step":

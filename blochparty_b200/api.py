@@ -24,7 +24,7 @@ ENGINES = ("b200", "gpu", "cuda")  # "gpu" and "cuda" name this engine too, so a
 OPTIONS = ("readout", "pulses", "surrogate", "surrogate_inference", "max_ctas")
 PULSES = ("step", "reuse", "surrogate")
 REFERENCE_GPU_OPTIONS = ("chunk", "group", "mma", "readouts", "nufft_width", "nufft_terms")
-READOUTS = ("fp32", "bf16x3")
+READOUTS = ("fp32", "bf16x3", "nufft")
 
 
 @dataclass
@@ -79,8 +79,9 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
     m_init: (N, 3) starting magnetization (default: equilibrium, Mz = PD).
     checkpoint_every: with gradients, the adjoint stores the state every this many segments (rounded to window
         boundaries); default about sqrt(segments).
-    options: ``readout`` "fp32" (default: float32 coil products reduced by warp shuffles) or "bf16x3" (the coil
-        contraction on the tensor cores in split bfloat16 with float32 accumulation); ``pulses`` "step"
+    options: ``readout`` "fp32" (default: float32 coil products reduced by warp shuffles), "bf16x3" (the coil
+        contraction on the tensor cores in split bfloat16 with float32 accumulation) or "nufft" (readout runs
+        through a nonuniform FFT: forward only, at least a few thousand spins); ``pulses`` "step"
         (default), "reuse" (every recurring pulse through its exact per-spin map, forward only) or "surrogate"
         (shaped pulses through a trained ``surrogate``), whose ``surrogate_inference`` is "mma" (default: the
         hidden 64 x 64 layers on the tensor cores) or "fp32"; ``max_ctas`` caps the grid.
@@ -100,6 +101,8 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
         raise ValueError(f"pulses must be one of {PULSES}, not {pulses!r}")
     if pulses == "reuse" and readout != "fp32":
         raise ValueError("pulses='reuse' takes the float32 readout (readout='fp32')")
+    if pulses == "surrogate" and readout == "nufft":
+        raise ValueError("pulses='surrogate' takes readout='fp32' or 'bf16x3'")
     n = len(phantom.pd)
     if coils is not None and (coils.dim() != 2 or coils.shape[0] != n):
         raise ValueError(f"coils must be (N, C) = ({n}, C), got {tuple(coils.shape)}")
@@ -137,4 +140,8 @@ def _forward(inp: Inputs, dev, options):
         from .readout_mma import forward_bf16x3
 
         return forward_bf16x3(inp, dev, options.get("max_ctas", 0))
+    if options.get("readout", "fp32") == "nufft":
+        from .nufft import forward_nufft
+
+        return forward_nufft(inp, dev, options.get("max_ctas", 0))
     return engine.forward(inp, dev, options.get("max_ctas", 0))

@@ -7,8 +7,7 @@
 // Work decomposition (persistent, window-major):
 //  * The sequence is cut on the host into windows of consecutive segments (at most BP_SEG_MAX segments and
 //    samp_max(NCG) ADC samples each).
-//  * A CTA of 128 threads owns the spin tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (128 spins each, one
-//    spin per thread). For every window it stages the window's segment records into shared memory with one
+//  * A CTA of 128 threads owns one contiguous block of spin tiles (128 spins each, one spin per thread). For every window it stages the window's segment records into shared memory with one
 //    TMA bulk copy (double-buffered: window w+1 is in flight while window w runs), then runs each of its tiles
 //    through the window: the tile's state is loaded from HBM, propagated in registers, and stored back.
 //  * ADC samples: each warp stages the (mx, my) of its 32 spins for 16 samples in shared memory, then contracts
@@ -35,6 +34,24 @@
 #define BP_STAGE 8         // samples staged per warp before they are contracted
 #define BP_MB_STRIDE 33    // float2 per staged sample row (32 spins + 1: conflict-free column reads)
 
+// A readout run through the nonuniform FFT (bp_forward_nufft): per spin, the run's samples are z1 q^p (p < L,
+// z1 the first sample, q the segment's complex factor), a sum over spins of exp(-2 pi i x p) times a decay; the
+// spins spread their weight onto an oversampled grid of G cells (kernel of W cells, exp(beta (sqrt(1 - z^2) - 1)))
+// once per term m of the decay's time segmentation (exp(-p dt r2) ~ sum_m a_m(p) exp(-tau_m r2)), and
+// bp_nufft_finish turns the grid into the samples. The spins are sorted by x on the host, so a CTA's tiles cover
+// a few neighbouring cells.
+struct NufArgs {
+    const int* run_of;       // [n_windows]: the run a window holds, or -1 (a window of the plain readout)
+    const int* base;         // [n]: the spin's first grid cell (floor(x G) - W/2 + 1; may be below 0)
+    const float* frac;       // [n]: x G - floor(x G)
+    const float2* shift;     // [n]: exp(-2 pi i x floor(L / 2)) (the centred modes' phase)
+    const float* decay;      // [M][n]: exp(-tau_m r2)
+    const int2* tile_cells;  // [n_tiles]: the cells [lo, hi) the tile's spins reach
+    double* grid;            // [runs][G][M][2C] float64, accumulated
+    int G, W, M;
+    float beta;
+};
+
 struct FwdArgs {
     const float* spins;   // [8][n]: px py pz pd r1 r2 db0 b1
     const float* sens;    // [16 ncg][n]: coil c real at row 2c, imaginary at 2c + 1, zero rows to pad
@@ -48,6 +65,7 @@ struct FwdArgs {
     float* wstates;       // null, or [(w_end - w_begin) / stride rounded up][6][n]: state at window starts
     int wstate_stride;
     int* status;
+    NufArgs nu;           // NUFFT readout runs (bp_forward_nufft only)
 };
 
 template <int NCG>
@@ -87,6 +105,27 @@ __device__ __forceinline__ void warp_contract(const float2* mb, const float* st,
     }
 }
 
+// The CTA's NUFFT accumulator rows [0, nrows) (row = (cell - cbase) M + term), summed over the warps' slices in
+// fixed order and added to run `run`'s grid with one float64 atomic per value (cells taken modulo G); slots are
+// cleared as read. Called by every thread of the CTA between barriers.
+template <int NCG>
+__device__ __forceinline__ void nuf_flush(const FwdArgs& a, float* acc, int run, int cbase, int nrows, int tid) {
+    constexpr int VG = 16 * NCG;
+    const int nv = 2 * a.n_coils, M = a.nu.M, G = a.nu.G;
+    for (int k = tid; k < nrows * nv; k += BP_THREADS) {
+        const int r = k / nv, v = k % nv;
+        const int slot = r * VG + v;
+        float t = 0.0f;
+#pragma unroll
+        for (int ww = 0; ww < BP_WARPS; ++ww) {
+            t += acc[ww * samp_max<NCG>() * VG + slot];
+            acc[ww * samp_max<NCG>() * VG + slot] = 0.0f;
+        }
+        const int cell = ((cbase + r / M) % G + G) % G, m = r % M;
+        atomicAdd(a.nu.grid + (((size_t)run * G + cell) * M + m) * nv + v, (double)t);
+    }
+}
+
 template <int NCG>
 __host__ __device__ constexpr size_t fwd_smem_bytes_t() {
     return 2 * BP_SEG_MAX * sizeof(SegRec)                                   // segment blocks
@@ -96,7 +135,7 @@ __host__ __device__ constexpr size_t fwd_smem_bytes_t() {
            + 2 * sizeof(uint64_t);
 }
 
-template <int NCG>
+template <int NCG, bool NUF>
 __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kernel(FwdArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int VG = 16 * NCG;  // accumulator values per sample (coil groups of 8, padded)
@@ -148,10 +187,28 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
         if (tid == 0 && w + 1 < a.w_end) issue(w + 1, buf ^ 1);  // after the check: nothing left in flight
         const SegRec* q0 = segbuf + buf * BP_SEG_MAX;
         const int nseg = win.y - win.x;
-        const bool readout = a.raw != nullptr && win.w > 0;
+        const int nrun = NUF ? a.nu.run_of[w] : -1;  // a NUFFT readout run (the same for the whole CTA)
+        const bool readout = a.raw != nullptr && (win.w > 0 || nrun >= 0);
         const bool save = a.wstates != nullptr && (i % a.wstate_stride) == 0;
+        // the CTA's tiles: one contiguous block (the NUFFT runs' spins are sorted, so the block covers few cells)
+        const int tpc = (n_tiles + gridDim.x - 1) / gridDim.x;
+        const int t_end = min(n_tiles, (blockIdx.x + 1) * tpc);
+        int cbase = 0, chi = 0;  // NUFFT: the cells the accumulator holds, [cbase, chi) so far
+        if (NUF && nrun >= 0 && blockIdx.x * tpc < t_end) cbase = chi = a.nu.tile_cells[blockIdx.x * tpc].x;
 
-        for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        for (int tile = blockIdx.x * tpc; tile < t_end; ++tile) {
+            if (NUF && nrun >= 0) {
+                // the tile's cells must fit the accumulator's rows from cbase: if not, add what it holds to the
+                // grid and restart it at this tile (uniform: every warp of the CTA runs the same tiles)
+                const int2 tc = a.nu.tile_cells[tile];
+                if ((tc.y - cbase) * a.nu.M > samp_max<NCG>()) {
+                    __syncthreads();
+                    nuf_flush<NCG>(a, acc, nrun, cbase, (chi - cbase) * a.nu.M, tid);
+                    __syncthreads();
+                    cbase = tc.x;
+                }
+                chi = max(chi, tc.y);
+            }
             const int j0 = tile * BP_THREADS + tid;
             const bool active = j0 < n;
             const int j = active ? j0 : 0;
@@ -194,7 +251,47 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                     slot = 0;
                 }
             };
-            for (int s = 0; s < nseg; ++s) {
+            if (NUF && nrun >= 0) {
+                // the run's first sample z1 = z q, centred by the shift, spread onto the warp's cells for every
+                // decay term: the accumulator rows are (cell - cbase) M + m, one staged column per (cell, term),
+                // zero where this spin's kernel does not reach
+                const SegRec q = q0[0];
+                const double4 k64 = a.seg64[win.x];
+                ff = free_factors(q, k64, p);
+                float zr = mx + lx, zi = my + ly;
+                readout_advance(ff, zr, zi);
+                const float2 sh = active ? a.nu.shift[j] : make_float2(0.f, 0.f);
+                const float w0r = zr * sh.x - zi * sh.y, w0i = zr * sh.y + zi * sh.x;
+                const int b = active ? a.nu.base[j] : 0;
+                const float fr = active ? a.nu.frac[j] : 0.f;
+                const int M = a.nu.M, W = a.nu.W;
+                float dec[BP_NUF_MAX_TERMS];
+#pragma unroll
+                for (int m = 0; m < BP_NUF_MAX_TERMS; ++m) dec[m] = (active && m < M) ? a.nu.decay[(size_t)m * n + j] : 0.f;
+                const int wlo = __reduce_min_sync(0xffffffffu, active ? b : 0x7fffffff);
+                const int whi = __reduce_max_sync(0xffffffffu, active ? b : -0x7fffffff);
+                if (wlo <= whi) {  // (uniform in the warp) some lane is a spin
+                    row0 = (wlo - cbase) * M;
+                    const float zs = 2.0f / (float)W, half = (float)(W / 2 - 1);
+                    for (int c = 0; c < whi - wlo + W; ++c) {
+                        const int wi = wlo + c - b;
+                        float psi = 0.0f;
+                        if (active && wi >= 0 && wi < W) {
+                            const float z = zs * ((float)wi - half - fr);
+                            psi = expf(a.nu.beta * (sqrtf(fmaxf(0.0f, fmaf(-z, z, 1.0f))) - 1.0f));
+                        }
+                        const float vr = w0r * psi, vi = w0i * psi;
+#pragma unroll
+                        for (int m = 0; m < BP_NUF_MAX_TERMS; ++m)
+                            if (m < M) stage(vr * dec[m], vi * dec[m]);
+                    }
+                }
+                // the state after the run: the segment's factors merged over its nseg copies (exact phase)
+                const FreeFactors fm = free_factors_merged(q, k64, p, nseg);
+                free_step(fm, p, mx, my, mz, lx, ly, lz);
+                if (q0[nseg - 1].flags & BP_SPOIL) mx = my = lx = ly = 0.0f;
+            }
+            for (int s = 0; s < ((NUF && nrun >= 0) ? 0 : nseg); ++s) {
                 const SegRec q = q0[s];
                 const int f = q.flags;
                 if (f & BP_RF) {
@@ -280,7 +377,10 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
             }
         }
         __syncthreads();
-        if (readout) {
+        if (NUF && nrun >= 0 && readout) {
+            nuf_flush<NCG>(a, acc, nrun, cbase, (chi - cbase) * a.nu.M, tid);
+            __syncthreads();
+        } else if (readout) {
             // the warps' slices in fixed order (the CTA's sum does not depend on timing), then one float64 atomic
             // per value; slots are cleared as read
             for (int k = tid; k < win.w * nv; k += BP_THREADS) {
@@ -325,22 +425,22 @@ static int num_sms(int dev) {
     return g_num_sms[dev];
 }
 
-template <int NCG>
+template <int NCG, bool NUF>
 static int forward_grid(int n, int max_ctas, int* grid_out) {
     const size_t smem = fwd_smem_bytes<NCG>();
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        if (cudaFuncSetAttribute(bp_forward_kernel<NCG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                cudaSuccess ||
-            cudaFuncSetAttribute(bp_forward_kernel<NCG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        if (cudaFuncSetAttribute(bp_forward_kernel<NCG, NUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(bp_forward_kernel<NCG, NUF>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return BP_E_LAUNCH;
         configured[dev] = true;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_forward_kernel<NCG>, BP_THREADS, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_forward_kernel<NCG, NUF>, BP_THREADS, smem) !=
         cudaSuccess)
         return BP_E_LAUNCH;
     if (per_sm < 1) per_sm = 1;
@@ -353,12 +453,12 @@ static int forward_grid(int n, int max_ctas, int* grid_out) {
     return BP_OK;
 }
 
-template <int NCG>
+template <int NCG, bool NUF>
 static int launch_forward(const FwdArgs& a, int max_ctas, cudaStream_t stream) {
     int grid = 0;
-    const int code = forward_grid<NCG>(a.n, max_ctas, &grid);
+    const int code = forward_grid<NCG, NUF>(a.n, max_ctas, &grid);
     if (code != BP_OK) return code;
-    bp_forward_kernel<NCG><<<grid, BP_THREADS, fwd_smem_bytes<NCG>(), stream>>>(a);
+    bp_forward_kernel<NCG, NUF><<<grid, BP_THREADS, fwd_smem_bytes<NCG>(), stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
@@ -366,10 +466,10 @@ extern "C" int bp_forward_grid(int n, int n_coils) {
     if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS) return -BP_E_ARG;
     int grid = 0, code = BP_OK;
     switch ((n_coils + 7) / 8) {
-        case 1: code = forward_grid<1>(n, 0, &grid); break;
-        case 2: code = forward_grid<2>(n, 0, &grid); break;
-        case 3: code = forward_grid<3>(n, 0, &grid); break;
-        default: code = forward_grid<4>(n, 0, &grid); break;
+        case 1: code = forward_grid<1, false>(n, 0, &grid); break;
+        case 2: code = forward_grid<2, false>(n, 0, &grid); break;
+        case 3: code = forward_grid<3, false>(n, 0, &grid); break;
+        default: code = forward_grid<4, false>(n, 0, &grid); break;
     }
     return code == BP_OK ? grid : -code;
 }
@@ -385,16 +485,15 @@ extern "C" int bp_forward_samp_max(int n_coils) {
     }
 }
 
-extern "C" int bp_forward(const float* spins, const float* sens, int n, int n_coils, const void* segs,
-                          const double* seg64, const int* windows, int w_begin, int w_end, float* state, double* raw,
-                          float* wstates, int wstate_stride, int max_ctas, int* status, void* stream) {
+static int fill_args(FwdArgs& a, const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                     const double* seg64, const int* windows, int w_begin, int w_end, float* state, double* raw,
+                     float* wstates, int wstate_stride, int* status) {
     if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || w_begin < 0 || w_end < w_begin) return BP_E_ARG;
     if (!spins || !segs || !seg64 || !windows || !state || !status) return BP_E_ARG;
     if (raw && !sens) return BP_E_ARG;
     if (wstates && wstate_stride < 1) return BP_E_ARG;
     if ((reinterpret_cast<uintptr_t>(segs) & 15) != 0) return BP_E_ALIGN;
-    if (w_end == w_begin) return BP_OK;
-    FwdArgs a;
+    a = FwdArgs{};
     a.spins = spins;
     a.sens = sens;
     a.segs = static_cast<const SegRec*>(segs);
@@ -409,13 +508,121 @@ extern "C" int bp_forward(const float* spins, const float* sens, int n, int n_co
     a.wstates = wstates;
     a.wstate_stride = wstate_stride > 0 ? wstate_stride : 1;
     a.status = status;
+    return BP_OK;
+}
+
+extern "C" int bp_forward(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                          const double* seg64, const int* windows, int w_begin, int w_end, float* state, double* raw,
+                          float* wstates, int wstate_stride, int max_ctas, int* status, void* stream) {
+    FwdArgs a;
+    const int code = fill_args(a, spins, sens, n, n_coils, segs, seg64, windows, w_begin, w_end, state, raw, wstates,
+                               wstate_stride, status);
+    if (code != BP_OK || w_end == w_begin) return code;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch ((n_coils + 7) / 8) {
-        case 1: return launch_forward<1>(a, max_ctas, st);
-        case 2: return launch_forward<2>(a, max_ctas, st);
-        case 3: return launch_forward<3>(a, max_ctas, st);
-        default: return launch_forward<4>(a, max_ctas, st);
+        case 1: return launch_forward<1, false>(a, max_ctas, st);
+        case 2: return launch_forward<2, false>(a, max_ctas, st);
+        case 3: return launch_forward<3, false>(a, max_ctas, st);
+        default: return launch_forward<4, false>(a, max_ctas, st);
     }
+}
+
+extern "C" int bp_forward_nufft(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                                const double* seg64, const int* windows, int w_begin, int w_end, float* state,
+                                double* raw, int max_ctas, const BpNufft* nu, int* status, void* stream) {
+    FwdArgs a;
+    const int code = fill_args(a, spins, sens, n, n_coils, segs, seg64, windows, w_begin, w_end, state, raw, nullptr,
+                               1, status);
+    if (code != BP_OK) return code;
+    if (!nu || !raw || !nu->run_of || !nu->base || !nu->frac || !nu->shift || !nu->decay || !nu->tile_cells ||
+        !nu->grid || nu->G < 2 || nu->W < 2 || nu->W > nu->G || nu->M < 1 || nu->M > BP_NUF_MAX_TERMS ||
+        (reinterpret_cast<uintptr_t>(nu->shift) & 7) != 0 || (reinterpret_cast<uintptr_t>(nu->tile_cells) & 7) != 0)
+        return BP_E_ARG;
+    const int ncg = (n_coils + 7) / 8;
+    // a tile's cells (its spins' kernels: at most W + 1 cells for sorted spins, checked on the host) x terms must
+    // fit the accumulator
+    if (ncg > 2 || (nu->W + 1) * nu->M > BP_ACC_SAMPLES / ncg) return BP_E_SIZE;
+    if (w_end == w_begin) return BP_OK;
+    a.nu.run_of = nu->run_of;
+    a.nu.base = nu->base;
+    a.nu.frac = nu->frac;
+    a.nu.shift = static_cast<const float2*>(nu->shift);
+    a.nu.decay = nu->decay;
+    a.nu.tile_cells = reinterpret_cast<const int2*>(nu->tile_cells);
+    a.nu.grid = nu->grid;
+    a.nu.G = nu->G, a.nu.W = nu->W, a.nu.M = nu->M;
+    a.nu.beta = nu->beta;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return ncg == 1 ? launch_forward<1, true>(a, max_ctas, st) : launch_forward<2, true>(a, max_ctas, st);
+}
+
+// ---- NUFFT readout runs: grid -> samples (float64) ----
+// Block (run r, coil c): the run's grid [G][M] (coil c, re/im) and the twiddles exp(-2 pi i t / G) in shared memory;
+// thread p (< L) forms sum_m w[m][p] sum_g grid[g][m] exp(-2 pi i (p - L/2) g / G) and adds it to raw row
+// rows[r] + p (rows only these runs own: no other launch writes them).
+__global__ void bp_nufft_finish_kernel(const double* __restrict__ grid, const int* __restrict__ rows, int G, int M,
+                                       int L, int n_coils, const double* __restrict__ w, double* __restrict__ raw) {
+    extern __shared__ double smd[];
+    double2* tw = reinterpret_cast<double2*>(smd);  // [G]
+    double2* gm = tw + G;                            // [M][G]
+    const int r = blockIdx.x, c = blockIdx.y, nv = 2 * n_coils, h = L / 2;
+    for (int t = threadIdx.x; t < G; t += blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * (double)t / (double)G, &sn, &cs);
+        tw[t] = make_double2(cs, -sn);
+    }
+    for (int k = threadIdx.x; k < G * M; k += blockDim.x) {
+        const int g = k / M, m = k % M;
+        const double* src = grid + (((size_t)r * G + g) * M + m) * nv + 2 * c;
+        gm[m * G + g] = make_double2(src[0], src[1]);
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < L; p += blockDim.x) {
+        const int kap = p - h;
+        const int step = ((kap % G) + G) % G;
+        double orr = 0.0, oi = 0.0;
+        for (int m = 0; m < M; ++m) {
+            double sr = 0.0, si = 0.0;
+            int t = 0;
+            for (int g = 0; g < G; ++g) {
+                const double2 z = gm[m * G + g], e = tw[t];
+                sr = fma(z.x, e.x, fma(-z.y, e.y, sr));
+                si = fma(z.x, e.y, fma(z.y, e.x, si));
+                t += step;
+                if (t >= G) t -= G;
+            }
+            const double wm = w[(size_t)m * L + p];
+            orr = fma(wm, sr, orr);
+            oi = fma(wm, si, oi);
+        }
+        double* dst = raw + (size_t)(rows[r] + p) * nv + 2 * c;
+        dst[0] += orr;
+        dst[1] += oi;
+    }
+}
+
+extern "C" int bp_nufft_finish(const double* grid, const int* run_rows, int n_runs, int G, int M, int L,
+                               int n_coils, const double* weights, double* raw, void* stream) {
+    if (n_runs < 0 || G < 2 || M < 1 || M > BP_NUF_MAX_TERMS || L < 1 || n_coils < 1 || n_coils > BP_MAX_COILS)
+        return BP_E_ARG;
+    if (n_runs == 0) return BP_OK;
+    if (!grid || !run_rows || !weights || !raw) return BP_E_ARG;
+    const size_t smem = (size_t)G * (M + 1) * sizeof(double2);
+    if (smem > 200 * 1024) return BP_E_SIZE;
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        if (cudaFuncSetAttribute(bp_nufft_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+            cudaSuccess)
+            return BP_E_LAUNCH;
+        configured[dev] = true;
+    }
+    const dim3 blocks((unsigned)n_runs, (unsigned)n_coils);
+    const int threads = L < 128 ? 128 : 256;
+    bp_nufft_finish_kernel<<<blocks, threads, smem, static_cast<cudaStream_t>(stream)>>>(grid, run_rows, G, M, L,
+                                                                                        n_coils, weights, raw);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
 extern "C" int bp_signal_finish(const double* raw, const double* psi, int n_adc, int n_coils, void* out,

@@ -84,6 +84,45 @@ int bp_forward(const float* spins, const float* sens, int n, int n_coils, const 
                const int32_t* windows, int w_begin, int w_end, float* state, double* raw, float* wstates,
                int wstate_stride, int max_ctas, int32_t* status, void* stream);
 
+/* Readout runs through a nonuniform FFT (simulate(..., readout="nufft"); replaces the NUFFT readouts of
+ * engines/gpu/cuda/kernels.cu.in:91-140 with engines/gpu/driver.py:236-266). A run is L consecutive samples with
+ * one free segment's factors (dt, moments, offset), so spin j's samples are z1 q^p, p < L, q = e^(-dt r2)
+ * e^(-2 pi i x), x the segment's phase in cycles mod 1. With the spins sorted by x (the run's class, host side),
+ * bp_forward_nufft steps every window as bp_forward does, except a window that holds one run (run_of[w] = r >= 0):
+ * there every spin adds its first sample, times exp(-2 pi i x floor(L/2)) and times exp(-tau_m r2) for each of the
+ * M terms of the decay's time segmentation, onto an oversampled grid of G cells with the kernel
+ * exp(beta (sqrt(1 - z^2) - 1)) over W cells (z = 2 (cell - x G) / W), coil by coil, and jumps over the run in one
+ * free step. bp_nufft_finish then forms every run's samples, raw[rows[r] + p] += sum_m weights[m][p]
+ * sum_g grid[r][g][m] exp(-2 pi i (p - floor(L/2)) g / G) in float64 (weights: the time-segmentation coefficient
+ * of term m at sample p over G times the kernel's Fourier transform at p - floor(L/2)).
+ *   run_of      [n_windows] int32: the run a window holds, or -1 (a run's window holds it alone, and its samples
+ *               field is 0: the run's raw rows are filled by bp_nufft_finish)
+ *   base        [n] int32: floor(x G) - W/2 + 1, the spin's first cell (taken modulo G)
+ *   frac        [n] float32: x G - floor(x G)
+ *   shift       [n] (float32, float32): exp(-2 pi i x floor(L/2)) (8-byte aligned)
+ *   decay       [M][n] float32: exp(-tau_m r2)
+ *   tile_cells  [ceil(n / 128)] (int32, int32): the cells [lo, hi) a tile of 128 spins reaches (at most W + 1 apart
+ *               for the sorted spins; 8-byte aligned)
+ *   grid        [runs][G][M][2C] float64, accumulated (+=)
+ * At most 16 coils and (W + 1) M <= 64 / ceil(C / 8) (BP_E_SIZE otherwise); M <= BP_NUF_MAX_TERMS. */
+#define BP_NUF_MAX_TERMS 6
+typedef struct {
+    const int32_t* run_of;
+    const int32_t* base;
+    const float* frac;
+    const void* shift;
+    const float* decay;
+    const int32_t* tile_cells;
+    double* grid;
+    int G, W, M;
+    float beta;
+} BpNufft;
+int bp_forward_nufft(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
+                     const int32_t* windows, int w_begin, int w_end, float* state, double* raw, int max_ctas,
+                     const BpNufft* nu, int32_t* status, void* stream);
+int bp_nufft_finish(const double* grid, const int32_t* run_rows, int n_runs, int G, int M, int L, int n_coils,
+                    const double* weights, double* raw, void* stream);
+
 /* Persistent grid (CTAs) that bp_forward launches for n spins and n_coils coils; negative on error. */
 int bp_forward_grid(int n, int n_coils);
 
