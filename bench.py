@@ -76,6 +76,9 @@ FLOP_RF_RECOMP, FLOP_FREE_RECOMP, FLOP_FACTORS = 61, 13, 18
 # term) the weight product (6) and the coil contraction (8 per coil)
 FLOP_NUF_RUN, FLOP_NUF_CELL, FLOP_NUF_TERM, FLOP_NUF_TERM_PER_COIL = 48, 8, 6, 8
 FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 130, 30, 8, 2
+# a free segment of a window that carries lambda alone (no per-spin gradient and no gradient of free segments
+# wanted, every segment of the window free with one factor set): lambda turned and relaxed, 9 flops, no recompute
+FLOP_FREE_LAMBDA = 9
 
 
 def nufft_flops_per_spin(flags: np.ndarray, n_coils: int, plan) -> int:
@@ -90,16 +93,32 @@ def nufft_flops_per_spin(flags: np.ndarray, n_coils: int, plan) -> int:
     return flops_per_spin(flags[keep], n_coils) + len(plan.runs) * per_run
 
 
-def grad_flops_per_spin(flags: np.ndarray, n_coils: int) -> tuple[int, int]:
-    """(forward, backward) algorithmic flops per spin of a simulation with gradients (no coil gradients)."""
+def lambda_only_segments(flags: np.ndarray, windows: np.ndarray) -> np.ndarray:
+    """(S,) bool: the segments of the adjoint windows that are uniform runs of free segments (every segment free,
+    the later ones with the first one's factors, a spoil at most on the last): the windows a sweep without
+    per-spin gradients carries lambda through without recomputing states (bp_adjoint_kernel's uniform free kind)."""
+    out = np.zeros(flags.shape[0], dtype=bool)
+    for s0, s1, _, _ in windows.tolist():
+        f = flags[s0:s1]
+        if ((f & 1) == 0).all() and ((f[1:] & 8) != 0).all() and not (f[:-1] & 4).any():
+            out[s0:s1] = True
+    return out
+
+
+def grad_flops_per_spin(flags: np.ndarray, n_coils: int, lam_only: np.ndarray | None = None) -> tuple[int, int]:
+    """(forward, backward) algorithmic flops per spin of a simulation with gradients (no coil gradients);
+    ``lam_only``: the segments a sweep without per-spin gradients carries lambda through alone."""
     rf = (flags & 1) != 0
-    n_rf, n_free = int(rf.sum()), int((~rf).sum())
-    n_free_miss = int((~rf & ((flags & 8) == 0)).sum())
+    lam = np.zeros_like(rf) if lam_only is None else lam_only
+    n_rf, n_free = int(rf.sum()), int((~rf & ~lam).sum())
+    n_free_miss = int((~rf & ~lam & ((flags & 8) == 0)).sum())
+    n_lam = int(lam.sum())
     n_adc = int(((flags & 2) != 0).sum())
     fwd = flops_per_spin(flags, n_coils)
     prop = flops_per_spin(flags, 0) - FLOP_ADC * n_adc
     recomp = FLOP_RF_RECOMP * n_rf + FLOP_FREE_RECOMP * n_free + FLOP_FACTORS * n_free_miss
-    rev = FLOP_RF_REV * n_rf + FLOP_FREE_REV * n_free + (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc
+    rev = (FLOP_RF_REV * n_rf + FLOP_FREE_REV * n_free + FLOP_FREE_LAMBDA * n_lam
+           + (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc)
     return fwd, prop + recomp + rev
 
 
@@ -344,7 +363,7 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
                       torch.randn(pk.n_coils, pk.n_adc, generator=g, dtype=torch.float64))
     h = run.cotangent(w)  # loss = sum(Re s Re w + Im s Im w): dL/ds = w
     lam = torch.zeros(3, pk.n, dtype=torch.float32, device=dev)
-    mask = _lib.BP_SEG_WX | _lib.BP_SEG_WY | _lib.BP_SPIN_NO_OFFSETS
+    mask = _lib.BP_SEG_WX | _lib.BP_SEG_WY | _lib.BP_SPIN_NO_OFFSETS | _lib.BP_SPIN_NONE
     state = torch.empty_like(state0)
 
     def step(times=None):
@@ -374,7 +393,7 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
     f_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in times)
     b_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in times)
     ms = f_ms + b_ms
-    fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils)
+    fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils, lambda_only_segments(pk.flags, run.plan.awin))
     peak = ffma_peak_tflops(dev)
     achieved = n * (fwd + bwd) / (ms * 1e-3) / 1e12
     lf, lb = run.launches(True)

@@ -63,6 +63,7 @@ BP_NUF_MAX_TERMS = 6
 BP_SEG_DT, BP_SEG_WX, BP_SEG_WY, BP_SEG_KX, BP_SEG_KY, BP_SEG_KZ, BP_SEG_BETA = (1 << k for k in range(7))
 BP_SEG_ALL = 0x7F
 BP_SPIN_NO_OFFSETS = 0x80  # with seg_mask: the position and dB0 rows of the spin gradients are not wanted
+BP_SPIN_NONE = 0x100  # with seg_mask: no row of the spin gradients is wanted
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",

@@ -190,10 +190,13 @@ class Checkpointed:
 def seg_mask_for(need) -> int:
     """The segment gradients the chain rules use (``need``: ``_Simulate``'s needs_input_grad): dt needs all of
     them (the record's every field scales with dt), the RF its two components, the gradient the moments,
-    b0_offset its phase; and ``BP_SPIN_NO_OFFSETS`` unless the positions' or dB0's gradients are wanted."""
+    b0_offset its phase; ``BP_SPIN_NO_OFFSETS`` unless the positions' or dB0's gradients are wanted, and
+    ``BP_SPIN_NONE`` when no per-spin input (position, PD, T1, T2, dB0, B1, coils) needs one."""
+    spin_none = not any(need[i] for i in range(1, 8))
     return (_lib.BP_SEG_ALL if need[8] else 0) | ((_lib.BP_SEG_WX | _lib.BP_SEG_WY) if need[9] else 0) | (
         (_lib.BP_SEG_KX | _lib.BP_SEG_KY | _lib.BP_SEG_KZ) if need[10] else 0) | (
-        _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5]) else _lib.BP_SPIN_NO_OFFSETS)
+        _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5]) else _lib.BP_SPIN_NO_OFFSETS) | (
+        _lib.BP_SPIN_NONE if spin_none else 0)
 
 
 class _Simulate(torch.autograd.Function):

@@ -156,7 +156,7 @@ __device__ __forceinline__ void free_step_plain(const FreeFactors& f, const Spin
 // gradients accumulated. The rotated state n = R m1 comes from the output, m2 = E n + c, by E's inverse (or, with
 // strong relaxation, from the input). dL/dw = J^T (n x a), a = dL/dn and J the rotation's left Jacobian
 // (R(w + d) = exp([J d]x) R(w)): J^T u = s1 u - s2 (w x u) + s3 (w . u) w.
-template <bool SMALL, bool OG>
+template <bool SMALL, bool OG, bool SG = true>
 __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float x0,
                                            float y0, float z0, float ox, float oy, float oz, float& lx, float& ly,
                                            float& lz, float* g, SegGrad& sg) {
@@ -196,10 +196,12 @@ __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const
     gpd = fmaf(-bz, e1h, gpd);
     lx = bx * a2, ly = by * a2, lz = bz * a1;
     // e1h = expm1(-h r1): d/dr1 = -h (1 + e1h), d/d(dt) = -(r1 / 2)(1 + e1h)
-    g[G_R1] = fmaf(-gd1 * h, a1, g[G_R1]);
-    g[G_R2] = fmaf(-gd2 * h, a2, g[G_R2]);
-    g[G_PD] += gpd;
-    g[G_B1] = fmaf(gwx, q.wx0, fmaf(gwy, q.wy0, g[G_B1]));
+    if (SG) {
+        g[G_R1] = fmaf(-gd1 * h, a1, g[G_R1]);
+        g[G_R2] = fmaf(-gd2 * h, a2, g[G_R2]);
+        g[G_PD] += gpd;
+        g[G_B1] = fmaf(gwx, q.wx0, fmaf(gwy, q.wy0, g[G_B1]));
+    }
     sg.v[S_WX] += gwx * p.b1;
     sg.v[S_WY] += gwy * p.b1;
     if (OG) {  // the offset's and dt's gradients (position, dB0, segment dt, moments, b0_offset)
@@ -210,10 +212,15 @@ __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const
 
 // Reverse of a free segment (rotation about z by phi = -2 pi cyc, then exact relaxation). OG: the offset's and dt's
 // gradients are wanted.
-template <bool OG>
+template <bool OG, bool SG = true>
 __device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, const FreeFactors& f, float x0, float y0,
                                              float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
     const float c = f.ch, s = f.sh, a2 = 1.0f + f.e2, a1 = 1.0f + f.e1;
+    if (!SG && !OG) {  // lambda alone: no gradient of this segment is wanted (and the input state is not read)
+        const float nlx = a2 * fmaf(c, lx, s * ly), nly = a2 * fmaf(-s, lx, c * ly);
+        lx = nlx, ly = nly, lz *= a1;
+        return;
+    }
     const float ux = fmaf(c, x0, -s * y0), uy = fmaf(s, x0, c * y0);
     const float gd2 = fmaf(lx, ux, ly * uy);
     const float gphi = OG ? a2 * fmaf(ly, ux, -lx * uy) : 0.0f;
@@ -237,9 +244,12 @@ struct KindTag {
 
 // NCG: groups of 8 coils; CG: whether the coil gradients are wanted (a.gc not null); OG: whether the gradients
 // of the spins' offsets (position, dB0) or of the segments' dt, moments or b0_offset are wanted (otherwise their
-// rows of gs and columns of gseg are left as they were).
-template <int NCG, bool CG, bool OG>
+// rows of gs and columns of gseg are left as they were); SG: whether any per-spin gradient is wanted (without them,
+// and without CG and OG, gs is left as it was and a window of free segments only carries lambda back, with no
+// recompute: only the RF segments' gradients and lambda are formed).
+template <int NCG, bool CG, bool OG, bool SG>
 __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kernel(AdjArgs a) {
+    static_assert(SG || (!CG && !OG), "coil and offset gradients are per-spin gradients");
     extern __shared__ __align__(16) float sm[];
     float* slots = sm;                                     // [ADJ_SLOTS][3][ADJ_THREADS]
     float* segacc = slots + ADJ_SLOTS * 3 * ADJ_THREADS;  // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
@@ -267,7 +277,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
         // depend on where the checkpoint intervals fall
         float g[N_GS];
 #pragma unroll
-        for (int k = 0; k < N_GS; ++k) g[k] = active ? a.gs[k * n + j] : 0.0f;
+        for (int k = 0; k < N_GS; ++k) g[k] = (SG && active) ? a.gs[k * n + j] : 0.0f;
         const bool want_gc = CG && active;
         float gcr[CG ? 8 * NCG : 1], gci[CG ? 8 * NCG : 1], sr[8 * NCG], si[8 * NCG];
 #pragma unroll
@@ -335,16 +345,18 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 // 0: any segments, 1: uniform RF, 2: uniform free, 3: uniform RF with every |w| < 1/4 in the warp
                 constexpr int KIND = decltype(kind_tag)::value;
                 constexpr bool URF = KIND == 1 || KIND == 3;
+                // a uniform free window without gradients of its own carries lambda alone: no states needed
+                constexpr bool LAMBDA_ONLY = KIND == 2 && !SG && !OG;
                 // recompute the window in plain float32 from its (compensated) start state: slot k = state after
                 // segment k-1 (before its spoil), slot 0 = window start
                 float mx = m0x, my = m0y, mz = m0z;
-                slots[tid] = mx, slots[ADJ_THREADS + tid] = my, slots[2 * ADJ_THREADS + tid] = mz;
+                if (!LAMBDA_ONLY) slots[tid] = mx, slots[ADJ_THREADS + tid] = my, slots[2 * ADJ_THREADS + tid] = mz;
                 FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 RevRelax rr{0.f, 0.f, 1.f, 1.f, 1.f, 1.f, true};
                 float wz = 0.f;
                 if (URF) rr = rev_relax(wrec[0].dt, p), wz = rf_wz(wrec[0], p);
                 if (KIND == 2) ff = free_factors(wrec[0], wk64[0], p);
-                for (int s = 0; s < nseg; ++s) {
+                for (int s = 0; s < (LAMBDA_ONLY ? 0 : nseg); ++s) {
                     const SegRec q = wrec[s];
                     if (URF || (KIND == 0 && (q.flags & BP_RF))) {
                         if (KIND == 0) {
@@ -375,8 +387,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 }
                 // the state after the segment being swept (its output, before its spoil): slot s + 1, which the
                 // previous iteration read as its input
-                float outx = slots[nseg * 3 * ADJ_THREADS + tid], outy = slots[(nseg * 3 + 1) * ADJ_THREADS + tid];
-                float outz = slots[(nseg * 3 + 2) * ADJ_THREADS + tid];
+                float outx = 0.f, outy = 0.f, outz = 0.f;
+                if (!LAMBDA_ONLY) {
+                    outx = slots[nseg * 3 * ADJ_THREADS + tid], outy = slots[(nseg * 3 + 1) * ADJ_THREADS + tid];
+                    outz = slots[(nseg * 3 + 2) * ADJ_THREADS + tid];
+                }
                 for (int s = nseg - 1; s >= 0; --s) {
                     const SegRec q = wrec[s];
                     const int f = q.flags;
@@ -417,9 +432,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                         lx += dx, ly += dy;
                     }
                     // the segment's input state: slot s, spoiled by segment s-1 if it spoils
-                    const float* in = slots + s * 3 * ADJ_THREADS;
-                    float x0 = in[tid], y0 = in[ADJ_THREADS + tid];
-                    const float z0 = in[2 * ADJ_THREADS + tid];
+                    float x0 = 0.f, y0 = 0.f, z0 = 0.f;
+                    if (!LAMBDA_ONLY) {
+                        const float* in = slots + s * 3 * ADJ_THREADS;
+                        x0 = in[tid], y0 = in[ADJ_THREADS + tid], z0 = in[2 * ADJ_THREADS + tid];
+                    }
                     outx = x0, outy = y0, outz = z0;
                     if (KIND == 0 && (f & A_PREV_SPOIL)) x0 = y0 = 0.0f;
                     SegGrad sg;
@@ -431,10 +448,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                             if (!(f & A_KEEP_RELAX)) rr = rev_relax(q.dt, p);
                             if (!(f & A_KEEP_WZ)) wz = rf_wz(q, p);
                         }
-                        rf_reverse<KIND == 3, OG>(q, p, rr, wz, x0, y0, z0, ox, oy, oz, lx, ly, lz, g, sg);
+                        rf_reverse<KIND == 3, OG, SG>(q, p, rr, wz, x0, y0, z0, ox, oy, oz, lx, ly, lz, g, sg);
                     } else {
                         if (KIND == 0 && !(f & A_KEEP_FREE)) ff = free_factors(q, wk64[s], p);
-                        free_reverse<OG>(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
+                        free_reverse<OG, SG>(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
                     }
                     if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0, 16 hold them)
                         if (KIND != 2) {  // (a free segment's are 0: a uniform free window writes and adds none)
@@ -482,8 +499,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
         }
         if (active) {
             a.lam[j] = lx, a.lam[n + j] = ly, a.lam[2 * n + j] = lz;
+            if (SG) {
 #pragma unroll
-            for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] = g[k];
+                for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] = g[k];
+            }
             if (CG) {
 #pragma unroll
                 for (int c = 0; c < 8 * NCG; ++c) {
@@ -513,15 +532,15 @@ static size_t adj_smem() {
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.
-template <int NCG, bool CG, bool OG>
+template <int NCG, bool CG, bool OG, bool SG>
 static int adj_configure() {
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)adj_smem()) != cudaSuccess ||
-            cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return -1;
         configured[dev] = true;
@@ -530,28 +549,30 @@ static int adj_configure() {
 }
 
 // CTAs per SM of one variant, or -1
-template <int NCG, bool CG, bool OG>
+template <int NCG, bool CG, bool OG, bool SG>
 static int adj_per_sm() {
     int per_sm = 0;
-    if (adj_configure<NCG, CG, OG>() < 0 ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG, OG>, ADJ_THREADS,
+    if (adj_configure<NCG, CG, OG, SG>() < 0 ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG, OG, SG>, ADJ_THREADS,
                                                       adj_smem()) != cudaSuccess)
         return -1;
     return per_sm > 0 ? per_sm : 1;
 }
 
-// one grid for both variants (with and without coil gradients): the smaller residency of the two
+// one grid for every variant: the smallest residency of them
 template <int NCG>
 static int adj_grid(int n) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int with_cg = adj_per_sm<NCG, true, true>(), without = adj_per_sm<NCG, false, true>();
-    const int lean = adj_per_sm<NCG, false, false>();
-    if (with_cg < 0 || without < 0 || lean < 0) return -1;
+    const int v[4] = {adj_per_sm<NCG, true, true, true>(), adj_per_sm<NCG, false, true, true>(),
+                      adj_per_sm<NCG, false, false, true>(), adj_per_sm<NCG, false, false, false>()};
+    int per_sm = v[0];
+    for (int k = 0; k < 4; ++k) {
+        if (v[k] < 0) return -1;
+        per_sm = v[k] < per_sm ? v[k] : per_sm;
+    }
     const int n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
-    int per_sm = with_cg < without ? with_cg : without;
-    if (lean < per_sm) per_sm = lean;
     const int grid = sms * per_sm;
     return grid < n_tiles ? grid : n_tiles;
 }
@@ -566,22 +587,25 @@ extern "C" int bp_adjoint_grid(int n, int n_coils) {
     }
 }
 
+template <int NCG, bool CG, bool OG, bool SG>
+static int launch_variant(const AdjArgs& a, int grid, cudaStream_t st) {
+    if (adj_configure<NCG, CG, OG, SG>() < 0) return BP_E_LAUNCH;
+    bp_adjoint_kernel<NCG, CG, OG, SG><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+}
+
 template <int NCG>
 static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
     // the offsets' gradients: wanted unless the caller marks the spins' ones unwanted and wants no segment
-    // gradient that uses them (with coil gradients, always computed)
-    const bool og = !(a.seg_mask & BP_SPIN_NO_OFFSETS) || (a.seg_mask & (BP_SEG_ALL & ~(BP_SEG_WX | BP_SEG_WY)));
-    if (a.gc) {
-        if (adj_configure<NCG, true, true>() < 0) return BP_E_LAUNCH;
-        bp_adjoint_kernel<NCG, true, true><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
-    } else if (og) {
-        if (adj_configure<NCG, false, true>() < 0) return BP_E_LAUNCH;
-        bp_adjoint_kernel<NCG, false, true><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
-    } else {
-        if (adj_configure<NCG, false, false>() < 0) return BP_E_LAUNCH;
-        bp_adjoint_kernel<NCG, false, false><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
-    }
-    return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
+    // gradient that uses them (with coil gradients, always computed); the per-spin gradients: wanted unless marked
+    // unwanted (BP_SPIN_NONE, which implies no offsets' gradients of the spins)
+    const bool seg_offsets = (a.seg_mask & (BP_SEG_ALL & ~(BP_SEG_WX | BP_SEG_WY))) != 0;
+    const bool og = !(a.seg_mask & (BP_SPIN_NO_OFFSETS | BP_SPIN_NONE)) || seg_offsets;
+    const bool sg = !(a.seg_mask & BP_SPIN_NONE) || og;
+    if (a.gc) return launch_variant<NCG, true, true, true>(a, grid, st);
+    if (og) return launch_variant<NCG, false, true, true>(a, grid, st);
+    if (sg) return launch_variant<NCG, false, false, true>(a, grid, st);
+    return launch_variant<NCG, false, false, false>(a, grid, st);
 }
 
 extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs,

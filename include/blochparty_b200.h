@@ -168,7 +168,8 @@ int bp_adjoint_grid(int n, int n_coils);
  *   seg_mask  the segment gradients wanted (BP_SEG_* bits; the others in gseg are left 0 or unreduced): only
  *           BP_SEG_WX | BP_SEG_WY (the RF alone) takes a cheaper reduction; plus BP_SPIN_NO_OFFSETS when the
  *           rows x, y, z and dB0 of gs are not wanted (left as they were): without coil gradients and without
- *           BP_SEG_DT, KX, KY, KZ, BETA, the sweep then skips the offsets' gradients altogether
+ *           BP_SEG_DT, KX, KY, KZ, BETA, the sweep then skips the offsets' gradients altogether; or BP_SPIN_NONE
+ *           when no row of gs is wanted at all
  *   grid    bp_adjoint_grid(n, n_coils)
  *   status  |= 2 (a malformed window) for every window the sweep skips: more than BP_ADJ_WIN segments, segments
  *           outside [seg0, seg0 + seg_len), or samples outside h's n_adc rows */
@@ -181,6 +182,8 @@ int bp_adjoint_grid(int n, int n_coils);
 #define BP_SEG_BETA 64
 #define BP_SEG_ALL 127
 #define BP_SPIN_NO_OFFSETS 128
+#define BP_SPIN_NONE 256 /* no per-spin gradient wanted: gs is left as it was (with no coil gradients and no segment
+                          * gradient but the RF's, windows of free segments then only carry lambda back) */
 int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
                const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates, const float* h,
                int n_adc, float* lam, float* gs, float* gc, float* gseg, int seg_mask, int grid, int32_t* status,

@@ -171,6 +171,26 @@ def test_sweep_without_offset_gradients_matches_the_full_sweep():
         assert torch.equal(a[k], b[k]), k
 
 
+@pytest.mark.parametrize("case", ["adjoint", "head"])
+def test_sweep_without_spin_gradients_matches_the_full_sweep(case):
+    """Asking for the RF waveform alone takes the sweep variant without per-spin gradients, whose
+    windows of free segments carry lambda back without recomputing states: its RF gradients are the full
+    sweep's, bit for bit (the 2D flip-train case, and the 4-echo head workload at 16^3 with its readout runs)."""
+    if case == "adjoint":
+        ph, seq, coils, flips, t1_target = _adjoint_case(16)
+        target = _target(ph, seq, coils, t1_target)
+    else:
+        ph, seq, coils = workloads.gre3d_128_4echo(16)
+        seq = workloads.first_n_trs(seq, 12)
+        target = torch.zeros(coils.shape[1], int(sum(seq.adc)), dtype=torch.complex128)
+    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum() + m.double().sum()
+    lean = ("rf",)
+    _, a = gpu_gradients(ph, seq, coils, None, loss, lean)
+    _, b = gpu_gradients(ph, seq, coils, None, loss, lean + ("t1",))
+    for k in lean:
+        assert torch.equal(a[k], b[k]), k
+
+
 def test_checkpoint_every_must_be_window_multiple():
     ph, seq, coils, _, _ = _adjoint_case(8)
     with pytest.raises(ValueError, match="multiple of 32"):
