@@ -76,9 +76,12 @@ FLOP_RF_RECOMP, FLOP_FREE_RECOMP, FLOP_FACTORS = 61, 13, 18
 # term) the weight product (6) and the coil contraction (8 per coil)
 FLOP_NUF_RUN, FLOP_NUF_CELL, FLOP_NUF_TERM, FLOP_NUF_TERM_PER_COIL = 48, 8, 6, 8
 FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 130, 30, 8, 2
-# a free segment of a window that carries lambda alone (no per-spin gradient and no gradient of free segments
-# wanted, every segment of the window free with one factor set): lambda turned and relaxed, 9 flops, no recompute
-FLOP_FREE_LAMBDA = 9
+# the sweep without per-spin gradients (the RF waveform's gradient alone): an RF segment's reverse is 103 flops
+# (rf_reverse without the relaxation, PD and B1 terms: rotation factors 25, rotated state 5, R^T a 30, n x a 9, the
+# rotation's two gradient components 22, lambda 6, the segment's two partials 4, p2 2); a free segment of a window
+# that carries lambda alone (every segment free with one factor set): lambda turned and relaxed, 9 flops, no
+# recompute
+FLOP_RF_REV_NO_SPIN, FLOP_FREE_LAMBDA = 103, 9
 
 
 def nufft_flops_per_spin(flags: np.ndarray, n_coils: int, plan) -> int:
@@ -107,7 +110,7 @@ def lambda_only_segments(flags: np.ndarray, windows: np.ndarray) -> np.ndarray:
 
 def grad_flops_per_spin(flags: np.ndarray, n_coils: int, lam_only: np.ndarray | None = None) -> tuple[int, int]:
     """(forward, backward) algorithmic flops per spin of a simulation with gradients (no coil gradients);
-    ``lam_only``: the segments a sweep without per-spin gradients carries lambda through alone."""
+    ``lam_only``: given for the sweep without per-spin gradients, the segments it carries lambda through alone."""
     rf = (flags & 1) != 0
     lam = np.zeros_like(rf) if lam_only is None else lam_only
     n_rf, n_free = int(rf.sum()), int((~rf & ~lam).sum())
@@ -117,7 +120,8 @@ def grad_flops_per_spin(flags: np.ndarray, n_coils: int, lam_only: np.ndarray | 
     fwd = flops_per_spin(flags, n_coils)
     prop = flops_per_spin(flags, 0) - FLOP_ADC * n_adc
     recomp = FLOP_RF_RECOMP * n_rf + FLOP_FREE_RECOMP * n_free + FLOP_FACTORS * n_free_miss
-    rev = (FLOP_RF_REV * n_rf + FLOP_FREE_REV * n_free + FLOP_FREE_LAMBDA * n_lam
+    rev = ((FLOP_RF_REV if lam_only is None else FLOP_RF_REV_NO_SPIN) * n_rf + FLOP_FREE_REV * n_free
+           + FLOP_FREE_LAMBDA * n_lam
            + (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc)
     return fwd, prop + recomp + rev
 
