@@ -120,8 +120,9 @@ def grad_flops_per_spin(flags: np.ndarray, n_coils: int, lam_only: np.ndarray | 
     fwd = flops_per_spin(flags, n_coils)
     prop = flops_per_spin(flags, 0) - FLOP_ADC * n_adc
     recomp = FLOP_RF_RECOMP * n_rf + FLOP_FREE_RECOMP * n_free + FLOP_FACTORS * n_free_miss
-    rev = ((FLOP_RF_REV if lam_only is None else FLOP_RF_REV_NO_SPIN) * n_rf + FLOP_FREE_REV * n_free
-           + FLOP_FREE_LAMBDA * n_lam
+    no_spin = lam_only is not None  # every free segment's reverse is lambda's alone; the recompute skips lam_only
+    rev = ((FLOP_RF_REV_NO_SPIN if no_spin else FLOP_RF_REV) * n_rf
+           + (FLOP_FREE_LAMBDA if no_spin else FLOP_FREE_REV) * n_free + FLOP_FREE_LAMBDA * n_lam
            + (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc)
     return fwd, prop + recomp + rev
 
