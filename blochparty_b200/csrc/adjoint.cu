@@ -53,7 +53,7 @@ struct AdjArgs {
     int n, n_coils;
     int wa, wb;           // this interval's adjoint windows
     int seg0, seg_len;    // first segment of the interval, segments in it
-    const float* wstates; // [wb - wa][6][n] state at every window start (replay)
+    const float* wstates; // [wb - wa + 1][6][n] state at every window start, then after the last window (replay)
     const float* h;       // [n_adc][2C] dL/d(raw coil sums), or null
     int n_adc;            // rows of h
     float* lam;           // [3][n] in: dL/dm at the interval's end; out: at its start
@@ -210,6 +210,38 @@ __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const
     }
 }
 
+// Reverse of an RF segment without per-spin or offset gradients, from its output state alone (ox, oy, oz), which
+// it turns into the segment's input state: n = E^-1 (out - c) (the half-step relaxation undone), lambda and the
+// rotation's gradient as rf_reverse forms them, then m1 = R^T n and in = E^-1 (m1 - c). Needs the relaxation to be
+// invertible (r.invert). A window swept this way needs no recompute of its states: it integrates them backward
+// from the state after the window.
+template <bool SMALL>
+__device__ __forceinline__ void rf_back(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float& ox,
+                                        float& oy, float& oz, float& lx, float& ly, float& lz, SegGrad& sg) {
+    const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
+    const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
+    float c, s1, s2, s3;
+    rot_factors<SMALL>(p2, c, s1, s2, s3);
+    const float nx = ox * r.ia2, ny = oy * r.ia2, nz = fmaf(p.pd, r.e1h, oz) * r.ia1;
+    const float ax = lx * r.a2, ay = ly * r.a2, az = lz * r.a1;  // dL/dn
+    const float k2 = s2 * fmaf(wx, ax, fmaf(wy, ay, wz * az));
+    const float bx = fmaf(c, ax, fmaf(-s1, wy * az - wz * ay, k2 * wx));
+    const float by = fmaf(c, ay, fmaf(-s1, wz * ax - wx * az, k2 * wy));
+    const float bz = fmaf(c, az, fmaf(-s1, wx * ay - wy * ax, k2 * wz));
+    const float ux = ny * az - nz * ay, uy = nz * ax - nx * az, uz = nx * ay - ny * ax;
+    const float k3 = s3 * fmaf(wx, ux, fmaf(wy, uy, wz * uz));
+    const float gwx = fmaf(s1, ux, fmaf(-s2, wy * uz - wz * uy, k3 * wx));
+    const float gwy = fmaf(s1, uy, fmaf(-s2, wz * ux - wx * uz, k3 * wy));
+    lx = bx * r.a2, ly = by * r.a2, lz = bz * r.a1;
+    sg.v[S_WX] += gwx * p.b1;
+    sg.v[S_WY] += gwy * p.b1;
+    const float k4 = s2 * fmaf(wx, nx, fmaf(wy, ny, wz * nz));
+    const float m1x = fmaf(c, nx, fmaf(-s1, wy * nz - wz * ny, k4 * wx));
+    const float m1y = fmaf(c, ny, fmaf(-s1, wz * nx - wx * nz, k4 * wy));
+    const float m1z = fmaf(c, nz, fmaf(-s1, wx * ny - wy * nx, k4 * wz));
+    ox = m1x * r.ia2, oy = m1y * r.ia2, oz = fmaf(p.pd, r.e1h, m1z) * r.ia1;
+}
+
 // Reverse of a free segment (rotation about z by phi = -2 pi cyc, then exact relaxation). OG: the offset's and dt's
 // gradients are wanted.
 template <bool OG, bool SG = true>
@@ -305,10 +337,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
             // writes)
             // the window's start state (from the replay, in DRAM for long intervals): loaded first, so that its
             // latency overlaps the staging below and its barrier
-            float m0x = 0.f, m0y = 0.f, m0z = 0.f;
+            float m0x = 0.f, m0y = 0.f, m0z = 0.f, mex = 0.f, mey = 0.f, mez = 0.f;
             if (active) {
                 const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
                 m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j], m0z = ws[2 * n + j] + ws[5 * n + j];
+                if (!SG) {  // the state after the window (the next one's start, or the interval's end)
+                    const float* we = ws + 6 * (size_t)n;
+                    mex = we[j] + we[3 * n + j], mey = we[n + j] + we[4 * n + j], mez = we[2 * n + j] + we[5 * n + j];
+                }
             }
             const SegRec* gw = a.segs + win.x;
             for (int i = tid; i < nseg * 8; i += ADJ_THREADS)
@@ -341,12 +377,46 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 if (lane == 0) *wmax = __uint_as_float(m);
             }
             const bool all_rf = __syncthreads_and(rf_ok), all_free = __syncthreads_and(free_ok);
+            // the segment's partial gradients summed over the warp into its slice of segacc
+            auto reduce_seg = [&](int s, const SegGrad& sg) {
+                if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0, 16 hold them)
+                    const bool up = lane & 16;
+                    const float v0 = sg.v[S_WX], v1 = sg.v[S_WY];  // (0 for a padding row: its lambda is 0)
+                    float t = (up ? v1 : v0) + __shfl_xor_sync(0xffffffffu, up ? v0 : v1, 16);
+#pragma unroll
+                    for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                    if ((lane & 15) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + (up ? S_WY : S_WX)] = t;
+                } else if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
+                    float v[N_SG];
+#pragma unroll
+                    for (int k = 0; k < N_SG; ++k) v[k] = sg.v[k];
+                    const float t = warp_reduce_scatter8(v, lane);
+                    if ((lane & 3) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + ((lane >> 2) & 7)] = t;
+                }
+            };
             auto sweep = [&](auto kind_tag) {
                 // 0: any segments, 1: uniform RF, 2: uniform free, 3: uniform RF with every |w| < 1/4 in the warp
                 constexpr int KIND = decltype(kind_tag)::value;
                 constexpr bool URF = KIND == 1 || KIND == 3;
                 // a uniform free window without gradients of its own carries lambda alone: no states needed
                 constexpr bool LAMBDA_ONLY = KIND == 2 && !SG && !OG;
+                // a uniform RF window without per-spin gradients integrates its states backward from the state
+                // after it, when that state is unspoiled and every lane's relaxation is invertible
+                if constexpr (URF && !SG && !OG) {
+                    const RevRelax rb = rev_relax(wrec[0].dt, p);
+                    const float wzb = rf_wz(wrec[0], p);
+                    if (!(wrec[nseg - 1].flags & BP_SPOIL) && __all_sync(0xffffffffu, rb.invert)) {
+                        float ox = mex, oy = mey, oz = mez;
+                        for (int s = nseg - 1; s >= 0; --s) {
+                            SegGrad sg;
+#pragma unroll
+                            for (int k = 0; k < N_SG; ++k) sg.v[k] = 0.0f;
+                            rf_back<KIND == 3>(wrec[s], p, rb, wzb, ox, oy, oz, lx, ly, lz, sg);
+                            reduce_seg(s, sg);
+                        }
+                        return;
+                    }
+                }
                 // recompute the window in plain float32 from its (compensated) start state: slot k = state after
                 // segment k-1 (before its spoil), slot 0 = window start
                 float mx = m0x, my = m0y, mz = m0z;
@@ -453,22 +523,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                         if (KIND == 0 && !(f & A_KEEP_FREE)) ff = free_factors(q, wk64[s], p);
                         free_reverse<OG, SG>(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
                     }
-                    if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0, 16 hold them)
-                        if (KIND != 2) {  // (a free segment's are 0: a uniform free window writes and adds none)
-                            const bool up = lane & 16;
-                            const float v0 = sg.v[S_WX], v1 = sg.v[S_WY];  // (0 for a padding row: its lambda is 0)
-                            float t = (up ? v1 : v0) + __shfl_xor_sync(0xffffffffu, up ? v0 : v1, 16);
-#pragma unroll
-                            for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-                            if ((lane & 15) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + (up ? S_WY : S_WX)] = t;
-                        }
-                    } else if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
-                        float v[N_SG];
-#pragma unroll
-                        for (int k = 0; k < N_SG; ++k) v[k] = sg.v[k];
-                        const float t = warp_reduce_scatter8(v, lane);
-                        if ((lane & 3) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + ((lane >> 2) & 7)] = t;
-                    }
+                    if (!(rf_only && KIND == 2)) reduce_seg(s, sg);  // (a uniform free window's RF partials are 0)
                 }
             };
             if (all_rf) {

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                     __syncthreads();
                     nuf_flush<NCG>(a, acc, nrun, cbase, (chi - cbase) * a.nu.M, tid);
                     __syncthreads();
-                    cbase = tc.x;
+                    cbase = chi = tc.x;
                 }
                 chi = max(chi, tc.y);
             }
