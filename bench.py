@@ -78,10 +78,11 @@ FLOP_NUF_RUN, FLOP_NUF_CELL, FLOP_NUF_TERM, FLOP_NUF_TERM_PER_COIL = 48, 8, 6, 8
 FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 130, 30, 8, 2
 # the sweep without per-spin gradients (the RF waveform's gradient alone): an RF segment's reverse is 103 flops
 # (rf_reverse without the relaxation, PD and B1 terms: rotation factors 25, rotated state 5, R^T a 30, n x a 9, the
-# rotation's two gradient components 22, lambda 6, the segment's two partials 4, p2 2); a free segment of a window
-# that carries lambda alone (every segment free with one factor set): lambda turned and relaxed, 9 flops, no
-# recompute
-FLOP_RF_REV_NO_SPIN, FLOP_FREE_LAMBDA = 103, 9
+# rotation's two gradient components 22, lambda 6, the segment's two partials 4, p2 2); in a window of RF segments
+# integrated backward (rf_back) 138, with the input state from R^T n (30) and the relaxation undone (5), and no
+# recompute; a free segment's reverse is lambda's alone, 9 flops, and a window of free segments with one factor set
+# recomputes nothing
+FLOP_RF_REV_NO_SPIN, FLOP_RF_BACK, FLOP_FREE_LAMBDA = 103, 138, 9
 
 
 def nufft_flops_per_spin(flags: np.ndarray, n_coils: int, plan) -> int:
@@ -96,34 +97,43 @@ def nufft_flops_per_spin(flags: np.ndarray, n_coils: int, plan) -> int:
     return flops_per_spin(flags[keep], n_coils) + len(plan.runs) * per_run
 
 
-def lambda_only_segments(flags: np.ndarray, windows: np.ndarray) -> np.ndarray:
-    """(S,) bool: the segments of the adjoint windows that are uniform runs of free segments (every segment free,
-    the later ones with the first one's factors, a spoil at most on the last): the windows a sweep without
-    per-spin gradients carries lambda through without recomputing states (bp_adjoint_kernel's uniform free kind)."""
-    out = np.zeros(flags.shape[0], dtype=bool)
+def no_recompute_segments(flags: np.ndarray, windows: np.ndarray):
+    """((S,) bool, (S,) bool): the segments of the adjoint windows the sweep without per-spin gradients does not
+    recompute: uniform runs of free segments (every segment free, the later ones with the first one's factors, a
+    spoil at most on the last), which carry lambda alone, and uniform runs of RF segments (every segment RF with the
+    first one's dt and offset, no sample, no spoil), which it integrates backward (bp_adjoint_kernel's uniform
+    kinds)."""
+    free = np.zeros(flags.shape[0], dtype=bool)
+    rf = np.zeros(flags.shape[0], dtype=bool)
     for s0, s1, _, _ in windows.tolist():
         f = flags[s0:s1]
         if ((f & 1) == 0).all() and ((f[1:] & 8) != 0).all() and not (f[:-1] & 4).any():
-            out[s0:s1] = True
-    return out
+            free[s0:s1] = True
+        elif ((f & 1) != 0).all() and ((f[1:] & 32) != 0).all() and not (f & 6).any():
+            rf[s0:s1] = True
+    return free, rf
 
 
-def grad_flops_per_spin(flags: np.ndarray, n_coils: int, lam_only: np.ndarray | None = None) -> tuple[int, int]:
+def grad_flops_per_spin(flags: np.ndarray, n_coils: int, no_spin=None) -> tuple[int, int]:
     """(forward, backward) algorithmic flops per spin of a simulation with gradients (no coil gradients);
-    ``lam_only``: given for the sweep without per-spin gradients, the segments it carries lambda through alone."""
+    ``no_spin``: for the sweep without per-spin gradients, ``no_recompute_segments`` of its windows."""
     rf = (flags & 1) != 0
-    lam = np.zeros_like(rf) if lam_only is None else lam_only
-    n_rf, n_free = int(rf.sum()), int((~rf & ~lam).sum())
-    n_free_miss = int((~rf & ~lam & ((flags & 8) == 0)).sum())
-    n_lam = int(lam.sum())
     n_adc = int(((flags & 2) != 0).sum())
     fwd = flops_per_spin(flags, n_coils)
     prop = flops_per_spin(flags, 0) - FLOP_ADC * n_adc
+    adc = (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc
+    if no_spin is None:
+        n_rf, n_free = int(rf.sum()), int((~rf).sum())
+        n_free_miss = int((~rf & ((flags & 8) == 0)).sum())
+        recomp = FLOP_RF_RECOMP * n_rf + FLOP_FREE_RECOMP * n_free + FLOP_FACTORS * n_free_miss
+        rev = FLOP_RF_REV * n_rf + FLOP_FREE_REV * n_free + adc
+        return fwd, prop + recomp + rev
+    lam, back = no_spin
+    n_rf_back, n_rf = int(back.sum()), int((rf & ~back).sum())
+    n_free = int((~rf & ~lam).sum())
+    n_free_miss = int((~rf & ~lam & ((flags & 8) == 0)).sum())
     recomp = FLOP_RF_RECOMP * n_rf + FLOP_FREE_RECOMP * n_free + FLOP_FACTORS * n_free_miss
-    no_spin = lam_only is not None  # every free segment's reverse is lambda's alone; the recompute skips lam_only
-    rev = ((FLOP_RF_REV_NO_SPIN if no_spin else FLOP_RF_REV) * n_rf
-           + (FLOP_FREE_LAMBDA if no_spin else FLOP_FREE_REV) * n_free + FLOP_FREE_LAMBDA * n_lam
-           + (FLOP_ADC_REV_PER_COIL * n_coils + FLOP_ADC_REV) * n_adc)
+    rev = (FLOP_RF_BACK * n_rf_back + FLOP_RF_REV_NO_SPIN * n_rf + FLOP_FREE_LAMBDA * int((~rf).sum()) + adc)
     return fwd, prop + recomp + rev
 
 
@@ -398,7 +408,7 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
     f_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in times)
     b_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in times)
     ms = f_ms + b_ms
-    fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils, lambda_only_segments(pk.flags, run.plan.awin))
+    fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils, no_recompute_segments(pk.flags, run.plan.awin))
     peak = ffma_peak_tflops(dev)
     achieved = n * (fwd + bwd) / (ms * 1e-3) / 1e12
     lf, lb = run.launches(True)

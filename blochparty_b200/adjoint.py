@@ -131,7 +131,7 @@ class Checkpointed:
         pk, plan, ws, dev = self.pk, self.plan, self.ws, self.dev
         if self._bufs is None:
             self._bufs = {"gs": sized(ws.gs, (8, pk.n), F32, dev), "seg": sized(ws.seg, (pk.flags.shape[0], 8), F64, dev),
-                          "wstates": sized(ws.wstates, (plan.max_aw, 6, pk.n), F32, dev),
+                          "wstates": sized(ws.wstates, (plan.max_aw + 1, 6, pk.n), F32, dev),
                           "state": sized(ws.replay_state, (6, pk.n), F32, dev)}
         b = self._bufs
         if need_seg and "gseg" not in b:
@@ -159,6 +159,7 @@ class Checkpointed:
             s0, s1 = plan.seg_ranges[k]
             state.copy_(self.ckpts[k])
             engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, self.status, wstates=wstates, wstate_stride=1)
+            wstates[ab - aa].copy_(state)  # the state after the interval's last window
             code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
                                   aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
                                   seg_mask, self.grid, ptr(self.status), stream)

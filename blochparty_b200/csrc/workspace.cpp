@@ -25,7 +25,7 @@ extern "C" int bp_adjoint_workspace_bytes(int n, int64_t n_segments, int64_t n_a
     const int64_t intervals = n_segments > 0 ? (n_segments + every - 1) / every : 0;
     const int64_t longest = n_segments < every ? n_segments : every;  // segments of the longest interval
     out->checkpoints = intervals * 6 * nn * 4;
-    out->wstates = (int64_t)max_interval_windows * 6 * nn * 4;
+    out->wstates = ((int64_t)max_interval_windows + 1) * 6 * nn * 4;
     out->replay_state = 6 * nn * 4;
     out->gseg = (int64_t)grid * longest * 8 * 4;
     out->seg = n_segments * 8 * 8;

@@ -47,8 +47,8 @@ int bp_plan_windows(const int32_t* flags, int64_t n_segments, int seg_max, int s
  * and status word for n spins, n_adc samples and n_coils coils (`raw` and `signal` keep one row when n_adc = 0).
  * bp_adjoint_workspace_bytes: what the checkpointed adjoint adds for a sequence of n_segments segments: the
  * checkpoints (one [6][n] state per interval of checkpoint_every segments, a multiple of BP_ADJ_WIN), the window
- * states of one replayed interval (max_interval_windows: the most adjoint windows in one interval, from the
- * caller's bp_plan_windows plan), the replayed state, the per-CTA segment gradients (`grid` = bp_adjoint_grid,
+ * states of one replayed interval (max_interval_windows + 1: the most adjoint windows in one interval, from the
+ * caller's bp_plan_windows plan, and the state after them), the replayed state, the per-CTA segment gradients (`grid` = bp_adjoint_grid,
  * times the longest interval), the float64 segment gradients, lambda, the per-spin gradients, the coil gradients
  * and the signal's cotangent h. Return BP_OK, or BP_E_ARG. */
 typedef struct {
@@ -157,7 +157,9 @@ int bp_adjoint_grid(int n, int n_coils);
  * with the per-segment reverse of shaders/adjoint_common.metal:212-315). `windows` are adjoint windows (at most
  * BP_ADJ_WIN segments, boundaries on multiples of BP_ADJ_WIN), [wa, wb) the interval's, covering segments
  * [seg0, seg0 + seg_len).
- *   wstates [wb - wa][6][n] the state at every window start (bp_forward replay of the interval, stride 1)
+ *   wstates [wb - wa + 1][6][n] the state at every window start (bp_forward replay of the interval, stride 1),
+ *           then the state after the interval's last window (the replay's final state); the sweep without
+ *           per-spin gradients integrates a window of RF segments backward from the state after it
  *   h       [n_adc][2C] float32 dL/d(raw coil sums) = dL/dsignal rotated by exp(+i psi), or NULL (8-byte
  *           aligned: BP_E_ALIGN otherwise); n_adc its rows
  *   lam     [3][n] in: dL/dm after the interval; out: dL/dm before it

@@ -173,9 +173,12 @@ def test_sweep_without_offset_gradients_matches_the_full_sweep():
 
 @pytest.mark.parametrize("case", ["adjoint", "head"])
 def test_sweep_without_spin_gradients_matches_the_full_sweep(case):
-    """Asking for the RF waveform alone takes the sweep variant without per-spin gradients, whose
-    windows of free segments carry lambda back without recomputing states: its RF gradients are the full
-    sweep's, bit for bit (the 2D flip-train case, and the 4-echo head workload at 16^3 with its readout runs)."""
+    """Asking for the RF waveform alone takes the sweep variant without per-spin gradients: its windows of free
+    segments carry lambda back without recomputing states, and its windows of RF segments integrate the states
+    backward from the state after the window instead of recomputing them forward. Its RF gradients are the full
+    sweep's within 1e-5 (largest error over the largest value: the two sweeps' float32 states differ by their
+    roundings), on the 2D flip-train case and on the 4-echo head workload at 16^3 with its readout runs; and the
+    variant's own gradients are the same bits for every checkpoint interval."""
     if case == "adjoint":
         ph, seq, coils, flips, t1_target = _adjoint_case(16)
         target = _target(ph, seq, coils, t1_target)
@@ -185,10 +188,13 @@ def test_sweep_without_spin_gradients_matches_the_full_sweep(case):
         target = torch.zeros(coils.shape[1], int(sum(seq.adc)), dtype=torch.complex128)
     loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum() + m.double().sum()
     lean = ("rf",)
-    _, a = gpu_gradients(ph, seq, coils, None, loss, lean)
+    _, a = gpu_gradients(ph, seq, coils, None, loss, lean, checkpoint_every=64)
+    _, c = gpu_gradients(ph, seq, coils, None, loss, lean, checkpoint_every=32 * 40)
     _, b = gpu_gradients(ph, seq, coils, None, loss, lean + ("t1",))
-    for k in lean:
-        assert torch.equal(a[k], b[k]), k
+    assert torch.equal(a["rf"], c["rf"])
+    err = rel(a["rf"], b["rf"])
+    print(f"\n{case}: RF gradient without per-spin gradients against the full sweep {err:.1e}")
+    assert err < 1e-5, err
 
 
 def test_checkpoint_every_must_be_window_multiple():

@@ -231,7 +231,7 @@ def test_workspace_query_matches_the_host_allocations():
     assert (f.state, f.raw, f.psi, f.signal) == (6 * n * 4, A * 2 * C * 8, pk.psi.numel() * 8, C * A * 8)
     w = _lib.adjoint_workspace(n, S, A, C, every, plan.max_aw, grid)
     assert w.checkpoints == len(plan.starts) * 6 * n * 4
-    assert w.wstates == plan.max_aw * 6 * n * 4
+    assert w.wstates == (plan.max_aw + 1) * 6 * n * 4
     assert w.gseg == grid * plan.max_len * 8 * 4
     assert (w.seg, w.lam, w.gs, w.gc, w.h) == (S * 64, 3 * n * 4, 8 * n * 4, 2 * C * n * 4, A * 2 * C * 4)
     assert w.total == sum(getattr(w, k) for k in ("checkpoints", "wstates", "replay_state", "gseg", "seg", "lam",

@@ -38,8 +38,9 @@ def _interval_inputs():
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     engine.run_forward(pk, state, plan.fwin_dev, 0, plan.franges[k][0], None, status)
     aa, ab = plan.aranges[k]
-    wstates = torch.empty(ab - aa, 6, pk.n, dtype=torch.float32, device=dev)
+    wstates = torch.empty(ab - aa + 1, 6, pk.n, dtype=torch.float32, device=dev)
     engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, status, wstates=wstates, wstate_stride=1)
+    wstates[ab - aa].copy_(state)  # the state after the interval's last window
     g = torch.Generator(device="cpu").manual_seed(7)
     h = torch.randn(pk.n_adc, 2 * pk.n_coils, generator=g).to(dev).contiguous()
     lam0 = torch.randn(3, pk.n, generator=g).to(dev).contiguous()
