@@ -67,17 +67,28 @@ def _np64(t) -> np.ndarray:
 
 
 def pack_spins(pos, pd, t1, t2, db0, b1, coils, device):
+    """spins [8][N] and sens [16 ceil(C/8)][N] float32 on ``device``: every value rounded once to float32 from its
+    float64 value (the rates 1/T1, 1/T2 formed in float64), written row by row into the float32 buffers."""
     n = pd.shape[0]
-    b1 = torch.ones(n, dtype=F64) if b1 is None else b1.detach().to(F64).cpu()
-    rows = [pos[:, 0], pos[:, 1], pos[:, 2], pd, 1.0 / t1, 1.0 / t2, db0, b1]
-    spins = torch.stack([r.detach().to(F64).cpu() for r in rows]).to(F32)
+    d64 = lambda t: t.detach().cpu().to(F64)
+    spins = torch.empty(8, n, dtype=F32)
+    spins[0:3] = d64(pos).T
+    spins[3] = d64(pd)
+    spins[4] = 1.0 / d64(t1)
+    spins[5] = 1.0 / d64(t2)
+    spins[6] = d64(db0)
+    if b1 is None:
+        spins[7] = 1.0
+    else:
+        spins[7] = d64(b1)
     n_coils = coils.shape[1]
     ncg = (n_coils + 7) // 8
-    sens = torch.zeros(16 * ncg, n, dtype=F32)
-    c = coils.detach().to(torch.complex128).cpu()
-    sens[0:2 * n_coils:2] = c.real.T.to(F32)
-    sens[1:2 * n_coils:2] = c.imag.T.to(F32)
-    return spins.to(device).contiguous(), sens.to(device).contiguous()
+    # (N, 2C) float32 rounded on the host, moved as it lies, transposed on the device (a host-side transpose of the
+    # spin-major coil array costs more than the copy)
+    c = torch.view_as_real(coils.detach().cpu().to(torch.complex128).contiguous()).reshape(n, 2 * n_coils).to(F32)
+    sens = torch.zeros(16 * ncg, n, dtype=F32, device=device)
+    sens[0:2 * n_coils] = c.to(device).T
+    return spins.to(device).contiguous(), sens.contiguous()
 
 
 def pack_segments(dt, rf, grad, b0_offset, adc_phase, is_rf, adc, spoil, device):
@@ -143,13 +154,16 @@ def plan_windows(flags: np.ndarray, samp_max: int, seg_max: int = _lib.BP_SEG_MA
 def initial_state(pd, m_init, device):
     """[6][N] float32: m0 split exactly from float64 into a float32 high part and its float32 remainder."""
     n = pd.shape[0]
-    if m_init is None:
-        m64 = torch.stack([torch.zeros(n, dtype=F64), torch.zeros(n, dtype=F64), pd.detach().to(F64).cpu()])
+    out = torch.zeros(6, n, dtype=F32)
+    if m_init is None:  # (0, 0, pd): only the z rows are nonzero
+        z = pd.detach().cpu().to(F64)
+        out[2] = z
+        out[5] = z - out[2].to(F64)
     else:
-        m64 = m_init.detach().to(F64).cpu().T
-    hi = m64.to(F32)
-    lo = (m64 - hi.to(F64)).to(F32)
-    return torch.cat([hi, lo]).to(device).contiguous()
+        m64 = m_init.detach().cpu().to(F64).T
+        out[0:3] = m64
+        out[3:6] = m64 - out[0:3].to(F64)
+    return out.to(device).contiguous()
 
 
 def final_m(state: torch.Tensor) -> torch.Tensor:
