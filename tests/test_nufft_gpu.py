@@ -1,8 +1,10 @@
 """The NUFFT readout (``simulate(..., readout="nufft")``) on the GPU against the float64 oracle (its C restatement)
 fed the engine's float32 inputs, and against the plain float32 readout: a 3D GRE with two echoes per TR, and
-configuration 5's spins and sequence (4,096 seeded spins of the 128^3 head phantom, its first 256 TRs). Bar: 1e-6
-relative L2 on the signal (the spreading and the float32 tables; the float64 prototype of the same arithmetic is
-at 1.1e-7), 1e-5 on m (its state update is the plain path's closed form)."""
+configuration 5's spins and sequence (4,096 seeded spins of the 128^3 head phantom, its first 256 TRs). Bars: 1e-6
+relative L2 between the NUFFT and the plain readout (the spreading and the float32 tables; the float64 prototype of
+the same arithmetic is at 1.1e-7); against float64, 1e-6 or 1.5 times the plain readout's own error, whichever is
+larger (over 256 TRs the float32 state's rounding alone reaches 1.1e-6); 1e-5 on m (its state update is the plain
+path's closed form)."""
 
 import pytest
 import torch
@@ -25,7 +27,7 @@ def _check(ph, seq, coils, label):
          "m": rel(r.m, m32)}
     print(f"\n{label}: " + ", ".join(f"{k} {v:.2e}" for k, v in e.items()))
     assert r.signal.shape == plain.signal.shape and r.signal.dtype == torch.complex64
-    assert e["nufft"] < 1e-6 and e["m"] < 1e-5
+    assert e["nufft_vs_plain"] < 1e-6 and e["nufft"] < max(1e-6, 1.5 * e["plain"]) and e["m"] < 1e-5
     return e
 
 
