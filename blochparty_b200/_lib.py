@@ -15,6 +15,7 @@ import torch
 LIB_PATH = Path(__file__).resolve().parent / "libblochparty_b200.so"
 
 BP_SPAN_MAP, BP_SPAN_NET_MMA, BP_SPAN_NET_F32 = 0, 1, 2
+BP_BOUND_ONLY = 128  # segment flag: RF only the bound pool feels
 
 
 class BpSpan(ctypes.Structure):
@@ -33,6 +34,13 @@ class BpNufft(ctypes.Structure):
     _fields_ = [("run_of", c_void_p), ("base", c_void_p), ("frac", c_void_p), ("shift", c_void_p),
                 ("decay", c_void_p), ("tile_cells", c_void_p), ("grid", c_void_p), ("G", c_int), ("W", c_int),
                 ("M", c_int), ("beta", c_float)]
+
+
+class BpPhysics(ctypes.Structure):
+    """``BpPhysics`` of the C ABI: the bound pool and the field model of ``bp_forward_physics``."""
+
+    _fields_ = [("mt", c_int), ("conc_mode", c_int), ("pool", c_void_p), ("bstate", c_void_p), ("rf_freq", c_void_p),
+                ("line", c_void_p), ("conc", c_void_p), ("segq", c_void_p)]
 
 
 class BpForwardWorkspace(ctypes.Structure):
@@ -107,6 +115,7 @@ SIGNATURES = {
                                    _P, _P, _P, _P, _P]),
     "bp_forward_workspace_bytes": (c_int, [c_int, c_int64, c_int, _P]),
     "bp_forward_nufft": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P, _P]),
+    "bp_forward_physics": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P, _P]),
     "bp_nufft_finish": (c_int, [_P, _P, c_int, c_int, c_int, c_int, c_int, _P, _P, _P]),
     "bp_adjoint_workspace_bytes": (c_int, [c_int, c_int64, c_int64, c_int, c_int, c_int, c_int, _P]),
 }

@@ -106,8 +106,11 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
     n = len(phantom.pd)
     if coils is not None and (coils.dim() != 2 or coils.shape[0] != n):
         raise ValueError(f"coils must be (N, C) = ({n}, C), got {tuple(coils.shape)}")
-    if m_init is not None and tuple(m_init.shape) != (n, 3):
-        raise ValueError(f"m_init must be (N, 3) = ({n}, 3), got {tuple(m_init.shape)}")
+    bound = getattr(phantom, "bound", None)
+    if m_init is not None and tuple(m_init.shape) == (n, 4) and bound is None:
+        raise ValueError("m_init has a bound-pool column but the phantom has no bound pool")
+    if m_init is not None and tuple(m_init.shape) not in ((n, 3), (n, 4)):
+        raise ValueError(f"m_init must be (N, 3) = ({n}, 3) (or (N, 4) with a bound pool), got {tuple(m_init.shape)}")
     if checkpoint_every is not None and checkpoint_every < 1:
         raise ValueError(f"checkpoint_every must be positive, got {checkpoint_every}")
     grad = torch.is_grad_enabled() and requires_grad(phantom, seq, coils, m_init)
@@ -122,6 +125,17 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
         from .adjoint import simulate_grad
 
         return simulate_grad(inp, dev, checkpoint_every, options)
+    bound_only = getattr(seq, "bound_only", None)
+    if bound is not None or scanner is not None or (bound_only is not None and any(bound_only)):
+        if options.get("readout", "fp32") != "fp32" or options.get("pulses", "step") != "step":
+            raise ValueError("a bound pool, bound-only RF or a scanner field model takes readout='fp32' and "
+                             "pulses='step'")
+        from .physics import forward_physics
+
+        with torch.no_grad():
+            sig, m, m_bound = forward_physics(inp, dev, bound, scanner, bound_only, getattr(seq, "rf_freq", None),
+                                              options.get("max_ctas", 0))
+        return SimResult(sig, m, m_bound)
     with torch.no_grad():
         sig, m = _forward(inp, dev, options)
     return SimResult(sig, m)

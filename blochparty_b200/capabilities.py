@@ -2,7 +2,8 @@
 
 The feature names and the message follow blochparty ``engines/capabilities.py:12-91`` (``FEATURES``, ``features``,
 ``check``) so that a caller switching engines sees the same ``NotImplementedError`` text pattern. The b200 engine
-runs static spins with B1+ and an initial magnetization, forward and with gradients; every other feature of the
+runs static spins with B1+ and an initial magnetization, forward and with gradients, and forward also with the
+rate-model bound pool (magnetization transfer, bound-only RF) and the scanner field model; every other feature of the
 reference's engines is refused here.
 """
 
@@ -21,7 +22,7 @@ FEATURES = {
     "m_init": "an initial magnetization (m_init)",
 }
 SUPPORTED = {
-    "forward": frozenset({"b1", "m_init"}),
+    "forward": frozenset({"b1", "m_init", "bound", "scanner", "bound_only"}),
     "gradients": frozenset({"b1", "m_init"}),
 }
 

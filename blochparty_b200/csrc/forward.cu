@@ -26,6 +26,7 @@
 #include <cstdint>
 
 #include "bloch_common.cuh"
+#include "physics.cuh"
 #include "../../include/blochparty_b200.h"
 
 #define BP_THREADS 128
@@ -66,6 +67,7 @@ struct FwdArgs {
     int wstate_stride;
     int* status;
     NufArgs nu;           // NUFFT readout runs (bp_forward_nufft only)
+    PhysArgs ph;          // the bound pool and the field model (bp_forward_physics only)
 };
 
 template <int NCG>
@@ -135,7 +137,10 @@ __host__ __device__ constexpr size_t fwd_smem_bytes_t() {
            + 2 * sizeof(uint64_t);
 }
 
-template <int NCG, bool NUF>
+// PHYS: the physics variant (bp_forward_physics): every RF segment through the bound pool's step and/or with the
+// concomitant field in its offset, the free segments' phase with the concomitant phase and their longitudinal part
+// through the exchange step; the rest (windows, readout runs, the coil contraction) as the plain kernel.
+template <int NCG, bool NUF, bool PHYS = false>
 __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kernel(FwdArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int VG = 16 * NCG;  // accumulator values per sample (coil groups of 8, padded)
@@ -214,6 +219,18 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
             const int j = active ? j0 : 0;
             const Spin p = load_spin(a.spins, n, j, active);
             float mx = 0.f, my = 0.f, mz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+            // physics variant: the bound pool (inactive lanes read spin 0's, with pd 0: finite, never summed), its
+            // state, and the concomitant coefficients
+            Pool pb{0.f, 0.f, 1.f, 1.f, 0.f};
+            Conc ck{};
+            float zb = 0.f, zbl = 0.f, e2h = 0.f;  // the bound pool's Mz (hi, lo)
+            if constexpr (PHYS) {
+                if (a.ph.mt) {
+                    pb = load_pool(a.ph.pool, n, j);
+                    if (active) zb = a.ph.bstate[j], zbl = a.ph.bstate[n + j];
+                }
+                ck = load_conc(a.ph.conc, n, j, a.ph.conc_mode);
+            }
             if (active) {
                 mx = a.state[j];
                 my = a.state[n + j];
@@ -294,6 +311,24 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
             for (int s = 0; s < ((NUF && nrun >= 0) ? 0 : nseg); ++s) {
                 const SegRec q = q0[s];
                 const int f = q.flags;
+                if constexpr (PHYS) {
+                    if (f & BP_RF) {  // every RF segment alone: the bound pool's step, or the plain one
+                        if (s == 0 || !(f & BP_SAME_RFDT)) {
+                            rr = rf_relax(q.dt, p);
+                            e2h = expm1f(-0.5f * q.dt * p.r2);
+                        }
+                        if (s == 0 || !(f & BP_SAME_OFF))
+                            wz = phys_wz(q, p, a.ph.conc_mode, ck, a.ph.segq + 6 * (size_t)(win.x + s));
+                        if (a.ph.mt)
+                            rf_step_mt(q, p, pb, e2h, wz, a.ph.rf_freq[win.x + s], a.ph.line, mx, my, mz, lx, ly, lz,
+                                       zb, zbl);
+                        else
+                            rf_step_wz(q, p, rr, wz, mx, my, mz, lx, ly, lz);
+                        if ((f & BP_ADC) && readout) stage(mx + lx, my + ly);
+                        if (f & BP_SPOIL) mx = my = lx = ly = 0.0f;
+                        continue;
+                    }
+                }
                 if (f & BP_RF) {
                     if (s == 0 || !(f & BP_SAME_RFDT)) rr = rf_relax(q.dt, p);
                     if (s == 0 || !(f & BP_SAME_OFF)) wz = rf_wz(q, p);
@@ -319,8 +354,17 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                         continue;
                     }
                 } else {
-                    if (s == 0 || !(f & BP_SAME_FREE)) ff = free_factors(q, a.seg64[win.x + s], p);
-                    free_step(ff, p, mx, my, mz, lx, ly, lz);
+                    if (s == 0 || !(f & BP_SAME_FREE)) {
+                        if constexpr (PHYS)
+                            ff = free_factors_phys(q, a.seg64[win.x + s], p, 1, a.ph.conc_mode, ck,
+                                                   a.ph.segq + 6 * (size_t)(win.x + s));
+                        else
+                            ff = free_factors(q, a.seg64[win.x + s], p);
+                    }
+                    if (PHYS && a.ph.mt)
+                        free_step_mt(ff, zstep(q.dt, p, pb, 0.0f), mx, my, mz, lx, ly, lz, zb, zbl);
+                    else
+                        free_step(ff, p, mx, my, mz, lx, ly, lz);
                     if ((f & (BP_ADC | BP_SPOIL)) == BP_ADC) {
                         // a readout run: the following samples with this segment's factors (the last may spoil),
                         // within this window and this block of BP_ADJ_WIN segments (so that the runs are cut at
@@ -349,8 +393,19 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                             }
                         }
                         if (e > s + 1) {
-                            const FreeFactors fr = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
-                            free_step(fr, p, mx, my, mz, lx, ly, lz);
+                            if constexpr (PHYS) {
+                                const FreeFactors fr = free_factors_phys(q, a.seg64[win.x + s], p, e - s - 1,
+                                                                         a.ph.conc_mode, ck,
+                                                                         a.ph.segq + 6 * (size_t)(win.x + s));
+                                if (a.ph.mt)
+                                    free_step_mt(fr, zstep((float)((double)q.dt * (double)(e - s - 1)), p, pb, 0.0f),
+                                                 mx, my, mz, lx, ly, lz, zb, zbl);
+                                else
+                                    free_step(fr, p, mx, my, mz, lx, ly, lz);
+                            } else {
+                                const FreeFactors fr = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
+                                free_step(fr, p, mx, my, mz, lx, ly, lz);
+                            }
                             if (q0[e - 1].flags & BP_SPOIL) mx = my = lx = ly = 0.0f;
                         }
                         s = e - 1;
@@ -374,6 +429,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                 a.state[3 * n + j] = lx;
                 a.state[4 * n + j] = ly;
                 a.state[5 * n + j] = lz;
+                if (PHYS && a.ph.mt) a.ph.bstate[j] = zb, a.ph.bstate[n + j] = zbl;
             }
         }
         __syncthreads();
@@ -425,22 +481,22 @@ static int num_sms(int dev) {
     return g_num_sms[dev];
 }
 
-template <int NCG, bool NUF>
+template <int NCG, bool NUF, bool PHYS = false>
 static int forward_grid(int n, int max_ctas, int* grid_out) {
     const size_t smem = fwd_smem_bytes<NCG>();
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        if (cudaFuncSetAttribute(bp_forward_kernel<NCG, NUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(bp_forward_kernel<NCG, NUF, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess ||
-            cudaFuncSetAttribute(bp_forward_kernel<NCG, NUF>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            cudaFuncSetAttribute(bp_forward_kernel<NCG, NUF, PHYS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return BP_E_LAUNCH;
         configured[dev] = true;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_forward_kernel<NCG, NUF>, BP_THREADS, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_forward_kernel<NCG, NUF, PHYS>, BP_THREADS, smem) !=
         cudaSuccess)
         return BP_E_LAUNCH;
     if (per_sm < 1) per_sm = 1;
@@ -453,12 +509,12 @@ static int forward_grid(int n, int max_ctas, int* grid_out) {
     return BP_OK;
 }
 
-template <int NCG, bool NUF>
+template <int NCG, bool NUF, bool PHYS = false>
 static int launch_forward(const FwdArgs& a, int max_ctas, cudaStream_t stream) {
     int grid = 0;
-    const int code = forward_grid<NCG, NUF>(a.n, max_ctas, &grid);
+    const int code = forward_grid<NCG, NUF, PHYS>(a.n, max_ctas, &grid);
     if (code != BP_OK) return code;
-    bp_forward_kernel<NCG, NUF><<<grid, BP_THREADS, fwd_smem_bytes<NCG>(), stream>>>(a);
+    bp_forward_kernel<NCG, NUF, PHYS><<<grid, BP_THREADS, fwd_smem_bytes<NCG>(), stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
@@ -554,6 +610,35 @@ extern "C" int bp_forward_nufft(const float* spins, const float* sens, int n, in
     a.nu.beta = nu->beta;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return ncg == 1 ? launch_forward<1, true>(a, max_ctas, st) : launch_forward<2, true>(a, max_ctas, st);
+}
+
+extern "C" int bp_forward_physics(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                                  const double* seg64, const int* windows, int w_begin, int w_end, float* state,
+                                  double* raw, int max_ctas, const BpPhysics* ph, int* status, void* stream) {
+    FwdArgs a;
+    const int code = fill_args(a, spins, sens, n, n_coils, segs, seg64, windows, w_begin, w_end, state, raw, nullptr,
+                               1, status);
+    if (code != BP_OK) return code;
+    if (!ph || ph->conc_mode < 0 || ph->conc_mode > 2) return BP_E_ARG;
+    if (ph->mt && (!ph->pool || !ph->bstate || !ph->rf_freq || !ph->line)) return BP_E_ARG;
+    if (ph->conc_mode && !ph->conc) return BP_E_ARG;
+    if (ph->conc_mode == 1 && !ph->segq) return BP_E_ARG;
+    if (w_end == w_begin) return BP_OK;
+    a.ph.mt = ph->mt != 0;
+    a.ph.conc_mode = ph->conc_mode;
+    a.ph.pool = ph->pool;
+    a.ph.bstate = ph->bstate;
+    a.ph.rf_freq = ph->rf_freq;
+    a.ph.line = ph->line;
+    a.ph.conc = ph->conc;
+    a.ph.segq = ph->segq;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch ((n_coils + 7) / 8) {
+        case 1: return launch_forward<1, false, true>(a, max_ctas, st);
+        case 2: return launch_forward<2, false, true>(a, max_ctas, st);
+        case 3: return launch_forward<3, false, true>(a, max_ctas, st);
+        default: return launch_forward<4, false, true>(a, max_ctas, st);
+    }
 }
 
 // ---- NUFFT readout runs: grid -> samples (float64) ----

@@ -123,6 +123,40 @@ int bp_forward_nufft(const float* spins, const float* sens, int n, int n_coils, 
 int bp_nufft_finish(const double* grid, const int32_t* run_rows, int n_runs, int G, int M, int L, int n_coils,
                     const double* weights, double* raw, void* stream);
 
+/* The bound pool (magnetization transfer, rate model) and the scanner field model's concomitant fields, forward
+ * (replaces the V=1 kernels of engines/gpu/cuda/kernels.cu.in:2-185 with the steps of
+ * engines/gpu/shaders/common.metal:40-50 and :145-208, fed by engines/gpu/driver.py:377-440). bp_forward's
+ * arguments and layouts, and:
+ *   mt         nonzero: a bound pool. Its Mz exchanges with the water's (exact 2x2 step per segment), RF saturates
+ *              it at W = w1^2 G(rf_freq - bz - dw); flag bit 128 (BP_BOUND_ONLY) marks an RF segment that only the
+ *              pool feels (the water precesses about z alone)
+ *   pool       [5][n] float32: f (pool size / free pool), k [1/s] (exchange rate from the bound pool), r1b = 1/T1b
+ *              [1/s], T2b [s], dw [Hz] (the pool's resonance shift)
+ *   bstate     [2][n] float32 in/out: the bound pool's Mz and its low part
+ *   rf_freq    [S] float32: the RF's frequency per segment [Hz]
+ *   line       float32: kind (1 Lorentzian, 2 super-Lorentzian), cutoff [Hz], ln x0, step, x_min, size, then `size`
+ *              values ln F(x) at ln x = ln x0 + i step (the super-Lorentzian's integral; unused for kind 1)
+ *   conc_mode  0 none, 1 leading-order concomitant field, 2 exact |B|
+ *   conc       [7][n] float32: mode 1 the quadratic form's coefficients c (6; f_c = c . (gx^2, gy^2, gz^2, gx gy,
+ *              gx gz, gy gz)); mode 2 the transverse field's rows ax (3), ay (3) and f0 [Hz]
+ *   segq       [S][6] float64, mode 1: dt (gx^2, gy^2, gz^2, gx gy, gx gz, gy gz)
+ * Positions in `spins` are the encoding positions (gradient nonlinearity applied on the host); the concomitant
+ * coefficients come from the true ones. No NUFFT runs, no window states. */
+#define BP_BOUND_ONLY 128
+typedef struct {
+    int mt;
+    int conc_mode;
+    const float* pool;
+    float* bstate;
+    const float* rf_freq;
+    const float* line;
+    const float* conc;
+    const double* segq;
+} BpPhysics;
+int bp_forward_physics(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                       const double* seg64, const int32_t* windows, int w_begin, int w_end, float* state, double* raw,
+                       int max_ctas, const BpPhysics* ph, int32_t* status, void* stream);
+
 /* Persistent grid (CTAs) that bp_forward launches for n spins and n_coils coils; negative on error. */
 int bp_forward_grid(int n, int n_coils);
 

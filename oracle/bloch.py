@@ -19,6 +19,15 @@ What it restates (blochparty ``engines/core.py``), for static spins with PD, T1,
 * a sample (``core.py:182-187``) is sum_spins (Mx + i My) * coil, demodulated by exp(-i adc_phase), taken at the
   end of its segment and before that segment's spoil (``core.py:391-392``), which zeroes Mx and My.
 
+With a bound pool (rate model) and the scanner field model (``oracle.physics``), as the core does them:
+
+* RF segments (``core.py:124-150``): the concomitant field added to bz (``core.py:115-121``); the bound pool's Mz
+  exchanging with the water's Mz over each half step, saturated at W = w1^2 G(f_rf - bz - dw); a bound-only
+  segment rotates the water about z alone;
+* free runs (``core.py:268-319``): the concomitant phase (``core.py:190-218``: the cumulative dt-weighted gradient
+  monomials at leading order, the per-segment |B| excess in exact mode) added to the phase, and the exact
+  exchange step over the run instead of Mz's relaxation.
+
 Everything is plain torch arithmetic on float64 CPU tensors, so ``torch.autograd`` through it is the gradient
 oracle (the reference's own gradients are its core's autograd, blochparty ``tests/helpers.py:95-119``).
 """
@@ -54,18 +63,35 @@ class Case:
     is_rf: list
     adc: list
     spoil: list
-    m_init: torch.Tensor | None = None  # (N, 3)
+    m_init: torch.Tensor | None = None  # (N, 3), or (N, 4) with the bound pool's Mz
+    bound: object | None = None  # physics.PoolCase
+    f_rf: torch.Tensor | None = None  # (S,) the RF's frequency [Hz] (with a bound pool)
+    bound_only: list | None = None
+    conc: torch.Tensor | None = None  # (N, 6) or (N, 7) concomitant coefficients
+    mode: int = 0  # 0 none, 1 leading order, 2 exact
 
 
-def case_from(phantom, seq, coils=None, m_init=None) -> Case:
-    """A ``Case`` from phantom / sequence objects of either package (read by attribute), cast to float64 CPU."""
+def case_from(phantom, seq, coils=None, m_init=None, scanner=None) -> Case:
+    """A ``Case`` from phantom / sequence objects of either package (read by attribute), cast to float64 CPU; with
+    a bound pool (``phantom.bound``), bound-only RF and ``scanner`` (the field model) as the core derives them."""
+    from . import physics
+
     d = lambda t: None if t is None else t.to(F64).cpu()
     n = phantom.pd.shape[0]
     c = torch.ones(n, 1, dtype=torch.complex128) if coils is None else coils.to(torch.complex128).cpu()
-    return Case(d(phantom.pos), d(phantom.pd), d(phantom.t1), d(phantom.t2), d(phantom.db0),
+    pos, conc, mode = physics.spin_fields(scanner, phantom.pos)
+    case = Case(pos, d(phantom.pd), d(phantom.t1), d(phantom.t2), d(phantom.db0),
                 d(getattr(phantom, "b1", None)), c, d(seq.dt), d(seq.rf), d(seq.grad), d(seq.adc_phase),
                 d(getattr(seq, "b0_offset", None)), [bool(x) for x in seq.is_rf], [bool(x) for x in seq.adc],
-                [bool(x) for x in seq.spoil], d(m_init))
+                [bool(x) for x in seq.spoil], d(m_init), conc=conc, mode=mode)
+    bound = getattr(phantom, "bound", None)
+    bo = getattr(seq, "bound_only", None)
+    case.bound_only = None if bo is None else [bool(x) for x in bo]
+    if bound is not None:
+        case.bound = physics.pool_case(bound, n)
+        rf_freq = getattr(seq, "rf_freq", None)
+        case.f_rf = d(rf_freq) if rf_freq is not None else physics.rf_frequency(case.dt, case.rf, case.is_rf)
+    return case
 
 
 def _steps(is_rf, spoil, merge):
@@ -106,27 +132,68 @@ def _sample(mx, my, psi, c):
     return raw * torch.exp(-1j * psi)
 
 
-def _rf_step(mx, my, mz, s, c, off):
+def _relax_bound(mx, my, mz, mb, t, c, w=None):
+    from .physics import z_exchange
+
+    e2 = torch.exp(-t / c.t2)
+    mz, mb = z_exchange(mz, mb, t, c.pd, 1.0 / c.t1, c.bound, w)
+    return mx * e2, my * e2, mz, mb
+
+
+def _rf_step(mx, my, mz, s, c, off, mb=None):
+    from . import physics
+
     g = c.grad[s]
     bz = c.pos @ g + c.db0 + (off[s] if off is not None else 0.0)
+    if c.mode:
+        bz = bz + physics.concomitant(bz, g, c.conc, c.mode)
     half = 0.5 * c.dt[s]
-    mx, my, mz = _relax(mx, my, mz, half, c)
-    w = -TWO_PI * c.dt[s]
-    wx, wy = w * c.rf[s, 0], w * c.rf[s, 1]
-    if c.b1 is not None:
-        wx, wy = wx * c.b1, wy * c.b1
+    bound_only = c.bound_only is not None and c.bound_only[s]
+    if c.bound is not None:
+        sat = physics.saturation(c.bound, c.rf[s], c.b1, c.f_rf[s] - bz - c.bound.dw)
+        mx, my, mz, mb = _relax_bound(mx, my, mz, mb, half, c, sat)
     else:
-        wx, wy = wx * torch.ones_like(bz), wy * torch.ones_like(bz)
+        mx, my, mz = _relax(mx, my, mz, half, c)
+    w = -TWO_PI * c.dt[s]
+    if bound_only:
+        wx, wy = torch.zeros_like(bz), torch.zeros_like(bz)
+    else:
+        wx, wy = w * c.rf[s, 0], w * c.rf[s, 1]
+        if c.b1 is not None:
+            wx, wy = wx * c.b1, wy * c.b1
+        else:
+            wx, wy = wx * torch.ones_like(bz), wy * torch.ones_like(bz)
     mx, my, mz = _rotate(mx, my, mz, wx, wy, w * bz)
-    return _relax(mx, my, mz, half, c)
+    if c.bound is not None:
+        return _relax_bound(mx, my, mz, mb, half, c, sat)
+    return (*_relax(mx, my, mz, half, c), mb)
 
 
-def _free_run(mx, my, mz, a, b, c, off):
+def _extra_phase(a, b, c, off):
+    """(N, n) or (n,) cumulative phase [cycles] of the uniform offset and the concomitant field over [a, b)."""
+    from . import physics
+
+    dt, g = c.dt[a:b], c.grad[a:b]
+    extra = torch.cumsum(off[a:b] * dt, 0) if off is not None else torch.zeros_like(dt)
+    if c.mode == 1:
+        gx, gy, gz = g.unbind(-1)
+        q = torch.cumsum(torch.stack([gx * gx, gy * gy, gz * gz, gx * gy, gx * gz, gy * gz], -1) * dt[:, None], 0)
+        extra = extra + c.conc @ q.T
+    elif c.mode == 2:
+        lin = c.pos @ g.T + c.db0[:, None] + (off[a:b] if off is not None else 0.0)  # (N, n)
+        exc = torch.stack([physics.concomitant(lin[:, i], g[i], c.conc, 2) for i in range(b - a)], 1)
+        extra = extra + torch.cumsum(exc * dt, 1)
+    return extra
+
+
+def _free_run(mx, my, mz, a, b, c, off, mb=None):
     """Closed-form run of RF-free segments [a, b): samples at its ADC segments, state at its end."""
     dt = c.dt[a:b]
     t = torch.cumsum(dt, 0)
     k = torch.cumsum(c.grad[a:b] * dt[:, None], 0)
-    extra = torch.cumsum(off[a:b] * dt, 0) if off is not None else torch.zeros_like(t)
+    extra = _extra_phase(a, b, c, off)
+    if extra.dim() == 1:
+        extra = extra.expand(mx.shape[0], -1)
     samples = []
     idx = [i for i in range(b - a) if c.adc[a + i]]
     if idx:
@@ -136,39 +203,56 @@ def _free_run(mx, my, mz, a, b, c, off):
         block = max(1, _BLOCK // max(n, 1))
         for j in range(0, len(idx), block):
             sel = ii[j:j + block]
-            cyc = c.pos @ k[sel].T + c.db0[:, None] * t[sel] + extra[sel]  # (N, n) cycles
+            cyc = c.pos @ k[sel].T + c.db0[:, None] * t[sel] + extra[:, sel]  # (N, n) cycles
             e = torch.exp(-t[sel][None, :] / c.t2[:, None] - 1j * TWO_PI * cyc)
             raw = v.T @ e  # (C, n)
             samples.append(raw * torch.exp(-1j * c.adc_phase[a + sel])[None, :])
-    cyc = c.pos @ k[-1] + c.db0 * t[-1] + extra[-1]
+    cyc = c.pos @ k[-1] + c.db0 * t[-1] + extra[:, -1]
     cs, sn = torch.cos(-TWO_PI * cyc), torch.sin(-TWO_PI * cyc)
     mx, my = cs * mx - sn * my, sn * mx + cs * my
-    mx, my, mz = _relax(mx, my, mz, t[-1], c)
-    return mx, my, mz, samples
+    if c.bound is not None:
+        mx, my, mz, mb = _relax_bound(mx, my, mz, mb, t[-1], c)
+    else:
+        mx, my, mz = _relax(mx, my, mz, t[-1], c)
+    return mx, my, mz, mb, samples
 
 
-def simulate(c: Case, merge: bool = True):
-    """(signal (C, n_adc) complex128, m (N, 3) float64) of case ``c`` (module docstring)."""
+def simulate_with_pool(c: Case, merge: bool = True):
+    """(signal (C, n_adc) complex128, m (N, 3) float64, the bound pool's Mz (N,) or None) of case ``c``."""
     n = c.pd.shape[0]
+    mb = None
     if c.m_init is None:
         mx, my, mz = torch.zeros(n, dtype=F64), torch.zeros(n, dtype=F64), c.pd
+    elif c.m_init.shape[-1] == 4:
+        mx, my, mz, mb = c.m_init.unbind(-1)
     else:
         mx, my, mz = c.m_init.unbind(-1)
+    if c.bound is not None and mb is None:
+        mb = c.bound.f * c.pd
+    is_rf = list(c.is_rf)
+    if c.bound is None and c.bound_only is not None:  # RF only a bound pool would feel: free for the water
+        is_rf = [r and not bo for r, bo in zip(is_rf, c.bound_only)]
     off = c.b0_offset
     cols = []
-    for a, b in _steps(c.is_rf, c.spoil, merge):
-        if c.is_rf[a]:
-            mx, my, mz = _rf_step(mx, my, mz, a, c, off)
+    for a, b in _steps(is_rf, c.spoil, merge):
+        if is_rf[a]:
+            mx, my, mz, mb = _rf_step(mx, my, mz, a, c, off, mb)
             if c.adc[a]:
                 cols.append(_sample(mx, my, c.adc_phase[a], c)[:, None])
         else:
-            mx, my, mz, samples = _free_run(mx, my, mz, a, b, c, off)
+            mx, my, mz, mb, samples = _free_run(mx, my, mz, a, b, c, off, mb)
             cols += samples
         if c.spoil[b - 1]:
             mx, my = torch.zeros_like(mx), torch.zeros_like(my)
     n_coils = c.coils.shape[1]
     sig = torch.cat(cols, 1) if cols else torch.zeros(n_coils, 0, dtype=torch.complex128)
-    return sig, torch.stack([mx, my, mz], -1)
+    return sig, torch.stack([mx, my, mz], -1), mb
+
+
+def simulate(c: Case, merge: bool = True):
+    """(signal (C, n_adc) complex128, m (N, 3) float64) of case ``c`` (module docstring)."""
+    sig, m, _ = simulate_with_pool(c, merge)
+    return sig, m
 
 
 GRAD_INPUTS = ("pos", "pd", "t1", "t2", "db0", "b1", "coils", "dt", "rf", "grad", "adc_phase", "b0_offset", "m_init")

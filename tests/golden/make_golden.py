@@ -2,7 +2,8 @@
 
 Run once, with the reference source tree (its ``src`` directory) on PYTHONPATH:
 
-    PYTHONPATH=<reference>/src python tests/golden/make_golden.py
+    PYTHONPATH=<reference>/src python tests/golden/make_golden.py            # the plain cases and adjoint128
+    PYTHONPATH=<reference>/src python tests/golden/make_golden.py physics    # bound pool and field model
 
 Each case's inputs are built here with this package's builders and phantoms (seeded), converted to the
 reference's ``Phantom`` / ``Sequence`` classes, and simulated by ``blochparty.simulate(..., engine="core")``
@@ -25,6 +26,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 
 import blochparty as bp  # noqa: E402  (the reference, from PYTHONPATH)
+from blochparty.exchange import BoundPool  # noqa: E402
 
 from blochparty_b200 import phantoms, sequences  # noqa: E402
 
@@ -189,10 +191,131 @@ def adjoint128():
     print("adjoint128", float(loss), {k: v.shape for k, v in out.items() if k.startswith("grad")})
 
 
+def nonlinearity():
+    """x and y coils with third- and fifth-order terms and a z-coil term (r0 = 0.25 m): a few pixels of distortion
+    at the edge of a 0.25 m field of view."""
+    alpha, beta = torch.zeros(3, 6, 6, dtype=F64), torch.zeros(3, 6, 6, dtype=F64)
+    alpha[0, 3, 1], alpha[0, 5, 1], alpha[0, 3, 3] = -0.9, 0.35, 0.2
+    beta[1, 3, 1], beta[1, 5, 1], beta[1, 3, 3] = -0.8, 0.3, -0.15
+    alpha[2, 3, 0], alpha[2, 2, 1] = -0.4, 0.1
+    return alpha, beta, 0.25
+
+
+def mt_case(seed, shape, n=48, n_coils=4):
+    """Spins with a bound pool, three off-resonant shaped saturation pulses (phase ramps) with gradients between
+    delays, a hard pulse and a readout, a spoil, an 8-step pulse and a second readout."""
+    g = torch.Generator().manual_seed(seed)
+    rnd = lambda *s: torch.rand(*s, generator=g, dtype=F64)
+    pool = dict(f=0.08 + 0.12 * rnd(n), k=15 + 45 * rnd(n), t1=0.8 + 0.4 * rnd(n), t2=(8 + 6 * rnd(n)) * 1e-6,
+                dw=(rnd(n) - 0.5) * 600)
+    ph = bp.Phantom(pos=(rnd(n, 3) - 0.5) * 0.2, pd=0.5 + rnd(n), t1=0.4 + rnd(n), t2=0.02 + 0.08 * rnd(n),
+                    db0=(rnd(n) - 0.5) * 200, b1=0.8 + 0.4 * rnd(n),
+                    bound=BoundPool(**pool, lineshape=shape))
+    b = sequences.SequenceBuilder()
+    for _ in range(3):
+        k, dt = 48, 10e-6
+        t = (torch.arange(k, dtype=F64) + 0.5) * dt
+        f_off = float(rnd(()) - 0.5) * 8000
+        amp = 200 + 1600 * rnd(k)
+        wave = torch.stack([amp * torch.cos(-2 * math.pi * f_off * t), amp * torch.sin(-2 * math.pi * f_off * t)], -1)
+        b.rf_waveform(wave.numpy(), dt, grad=((rnd(3) - 0.5) * 2000).numpy())
+        b.delay(0.2e-3 + float(rnd(())) * 2e-3, grad=((rnd(3) - 0.5) * 4000).numpy())
+    b.rf(100e-6, flip_deg=30.0)
+    b.readout(16, 10e-6, grad=(800.0, -300.0, 150.0), phase=0.7)
+    b.delay(1e-3).spoil()
+    b.rf(200e-6, flip_deg=60.0, n_steps=8)
+    b.readout(12, 20e-6, grad=(-500.0, 200.0, 0.0), phase=0.3)
+    seq = b.build()
+    seq.b0_offset = (rnd(len(seq)) - 0.5) * 20
+    coils = torch.complex(rnd(n, n_coils) - 0.5, rnd(n, n_coils) - 0.5)
+    return ph, seq, coils, pool
+
+
+def run_physics(name, ph, seq, coils, pool=None, shape=None, bound_only=None, m_init=None, scanner=None,
+                scanner_args=None):
+    """The reference's core in float64 on a case with a bound pool and / or a field model; stores the inputs (the
+    pool's parameters, bound-only flags, the scanner's), the signal, m and the bound pool's Mz, and what the
+    reference derives on the way (its RF frequency per segment, encoding positions and concomitant
+    coefficients)."""
+    from blochparty.exchange import rf_frequency
+    from blochparty.fields import spin_fields
+
+    rseq = bp.Sequence(seq.dt, seq.rf, seq.grad, seq.adc_phase, list(seq.is_rf), list(seq.adc), list(seq.spoil),
+                       {}, seq.b0_offset, None, bound_only)
+    rph = bp.Phantom(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, b1=ph.b1, bound=ph.bound)
+    r = bp.simulate(rph, rseq, coils, m_init=m_init, scanner=scanner, engine="core")
+    plain = bp.simulate(bp.Phantom(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, b1=ph.b1), rseq, coils,
+                        m_init=None if m_init is None else m_init[:, :3], engine="core")
+    effect = float((r.signal - plain.signal).abs().max() / r.signal.abs().max())
+    fields = spin_fields(scanner, ph.pos)
+    out = dict(
+        pos=ph.pos.numpy(), pd=ph.pd.numpy(), t1=ph.t1.numpy(), t2=ph.t2.numpy(), db0=ph.db0.numpy(),
+        b1=(ph.b1.numpy() if ph.b1 is not None else np.zeros(0)),
+        coils_re=coils.real.numpy(), coils_im=coils.imag.numpy(),
+        dt=seq.dt.numpy(), rf=seq.rf.numpy(), grad=seq.grad.numpy(), adc_phase=seq.adc_phase.numpy(),
+        b0_offset=(seq.b0_offset.numpy() if seq.b0_offset is not None else np.zeros(0)),
+        is_rf=np.array(seq.is_rf, bool), adc=np.array(seq.adc, bool), spoil=np.array(seq.spoil, bool),
+        m_init=(m_init.numpy() if m_init is not None else np.zeros(0)),
+        bound_only=np.array(bound_only if bound_only is not None else [], bool),
+        sig_re=r.signal.real.numpy(), sig_im=r.signal.imag.numpy(), m=r.m.numpy(),
+        m_bound=(r.m_bound.numpy() if r.m_bound is not None else np.zeros(0)),
+        ref_enc=fields.pos.numpy(), ref_conc=(fields.conc.numpy() if fields.conc is not None else np.zeros(0)),
+        ref_mode=np.array(fields.mode), effect=np.array(effect),
+    )
+    if pool is not None:
+        out.update({f"pool_{k}": v.numpy() for k, v in pool.items()})
+        out["pool_shape"] = np.array(shape)
+        out["ref_rf_freq"] = rf_frequency(rseq).numpy()
+    if scanner_args is not None:
+        b0, conc, alpha, beta, r0 = scanner_args
+        out.update(sc_b0=np.array(np.nan if b0 is None else b0), sc_conc=np.array(conc or ""),
+                   sc_alpha=alpha.numpy() if alpha is not None else np.zeros(0),
+                   sc_beta=beta.numpy() if beta is not None else np.zeros(0), sc_r0=np.array(r0))
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, "effect of the physics on the signal", f"{effect:.2e}")
+
+
+def physics():
+    """The bound-pool and field-model fixtures, and the reference's super-Lorentzian table."""
+    from blochparty.exchange import _sl_table
+    from blochparty.fields import GradientNonlinearity, Scanner
+
+    lx, lf = _sl_table(F64, torch.device("cpu"))
+    np.savez_compressed(HERE / "sl_table.npz", lx=lx.numpy(), log_f=lf.numpy())
+    ph, seq, coils, pool = mt_case(11, "superlorentzian")
+    run_physics("mt_sl", ph, seq, coils, pool, "superlorentzian")
+    ph, seq, coils, pool = mt_case(12, "lorentzian")
+    g = torch.Generator().manual_seed(13)
+    m0 = torch.cat([(torch.rand(len(ph.pd), 2, generator=g, dtype=F64) - 0.5) * 0.4,
+                    0.3 + 0.5 * torch.rand(len(ph.pd), 1, generator=g, dtype=F64),
+                    0.05 * torch.rand(len(ph.pd), 1, generator=g, dtype=F64)], 1)
+    bo = [False] * len(seq)
+    for s in range(48, 96):  # the second saturation pulse: felt by the bound pool alone
+        bo[s] = bool(seq.is_rf[s])
+    run_physics("mt_lor", ph, seq, coils, pool, "lorentzian", bound_only=bo, m_init=m0)
+    alpha, beta, r0 = nonlinearity()
+    p = phantoms.ellipse_phantom_2d(16, 0.25, seed=2)
+    gseq = sequences.gre((16, 16), 0.25, flip_deg=30.0, tr=6e-3, te=3e-3, n_dummy=4, dwell=20e-6)
+    gcoils = phantoms.birdcage_sensitivities(p.pos, 4)
+    gph = bp.Phantom(p.pos, p.pd, p.t1, p.t2, p.db0, b1=p.b1)
+    for name, conc in (("field_nl", None), ("field_leading", "leading"), ("field_exact", "exact")):
+        nl = GradientNonlinearity(alpha, beta, r0)
+        sc = Scanner(field_strength=None if conc is None else 0.55, concomitant=conc, nonlinearity=nl)
+        run_physics(name, gph, gseq, gcoils, scanner=sc,
+                    scanner_args=(None if conc is None else 0.55, conc, alpha, beta, r0))
+    ph, seq, coils, pool = mt_case(14, "superlorentzian")
+    sc = Scanner(field_strength=0.55, concomitant="leading", nonlinearity=GradientNonlinearity(alpha, beta, r0))
+    run_physics("mt_field", ph, seq, coils, pool, "superlorentzian", scanner=sc,
+                scanner_args=(0.55, "leading", alpha, beta, r0))
+
+
 def main():
     torch.set_default_dtype(F64)
     if "adjoint128" in sys.argv[1:]:
         adjoint128()
+        return
+    if "physics" in sys.argv[1:]:
+        physics()
         return
     for seed in (0, 1):
         ph, seq, coils = rand_case(seed)

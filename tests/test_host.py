@@ -2,6 +2,7 @@
 window planner, the packing of segments and state, the capability refusals and argument errors of ``simulate``."""
 
 import re
+from dataclasses import replace
 from pathlib import Path
 
 import numpy as np
@@ -9,7 +10,7 @@ import pytest
 import torch
 
 import blochparty_b200 as bpb
-from blochparty_b200 import _lib, capabilities, engine, sequences
+from blochparty_b200 import _lib, capabilities, engine, physics, sequences
 
 ROOT = Path(__file__).resolve().parents[1]
 F64 = torch.float64
@@ -163,13 +164,20 @@ def test_refusals_use_the_reference_wording():
                                                   r"is not implemented; use blochparty.simulate \(the core\)"):
         bpb.simulate(ph, seq)
     ph.diffusion = None
-    with pytest.raises(NotImplementedError, match="scanner field model"):
-        bpb.simulate(ph, seq, scanner=object())
+    with pytest.raises(NotImplementedError, match="gradients through the scanner field model"):
+        bpb.simulate(replace(ph, t1=ph.t1.clone().requires_grad_()), seq, scanner=physics.Scanner(0.55))
+    with pytest.raises(NotImplementedError, match=r"simulating with field maps \(FieldMaps\)"):
+        bpb.simulate(ph, seq, maps=object())
+    gen = replace(ph, bound=physics.BoundPool(0.1, 30.0, 1.0, 12e-6, model="generalized"))
+    with pytest.raises(NotImplementedError, match="the generalized Bloch bound pool"):
+        bpb.simulate(gen, seq)
     seq.bound_only = [True] + [False] * (len(seq) - 1)
-    with pytest.raises(NotImplementedError, match="bound-pool-only"):
-        bpb.simulate(ph, seq)
+    with pytest.raises(NotImplementedError, match="gradients through .*bound-pool-only"):
+        bpb.simulate(replace(ph, t1=ph.t1.clone().requires_grad_()), seq)
     used = capabilities.features(ph, seq, torch.zeros(2, 3))
     assert "m_init" in used and "bound_only" in used
+    with pytest.raises(ValueError, match="m_init has a bound-pool column"):
+        bpb.simulate(ph, seq, m_init=torch.zeros(2, 4))
 
 
 def test_argument_errors():
@@ -242,7 +250,8 @@ def test_workspace_query_matches_the_host_allocations():
 
 
 def test_workspace_structs_match_the_header(tmp_path):
-    """The ctypes workspace structs have the C structs' sizes and field offsets (compiled with gcc)."""
+    """The ctypes workspace, NUFFT and physics structs have the C structs' sizes and field offsets (compiled with
+    gcc)."""
     import ctypes
     import shutil
     import subprocess
@@ -250,7 +259,7 @@ def test_workspace_structs_match_the_header(tmp_path):
     if shutil.which("gcc") is None:
         pytest.skip("no C compiler")
     inc = Path(__file__).resolve().parents[1] / "include"
-    for struct in (_lib.BpForwardWorkspace, _lib.BpAdjointWorkspace):
+    for struct in (_lib.BpForwardWorkspace, _lib.BpAdjointWorkspace, _lib.BpNufft, _lib.BpPhysics):
         name = struct.__name__
         fields = [f for f, _ in struct._fields_]
         src = tmp_path / f"{name}.c"

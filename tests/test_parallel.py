@@ -34,7 +34,7 @@ def test_shard_ranges_partition_the_spins():
 def _oracle_forward(inp):
     """One rank's part through the oracle: its demodulated float64 signal as (A, 2 C) sums (the demodulation is
     linear, so summing demodulated parts equals demodulating the summed raw sums)."""
-    case = bloch.Case(*[getattr(inp, f) for f in bloch.Case.__dataclass_fields__])
+    case = bloch.Case(**{f: getattr(inp, f) for f in bloch.Case.__dataclass_fields__ if hasattr(inp, f)})
     sig, m = bloch.simulate(case)
     raw = torch.view_as_real(sig.T.contiguous()).reshape(sig.shape[1], -1).contiguous()
     finish = lambda total: torch.view_as_complex(total.reshape(total.shape[0], -1, 2).contiguous()).T.contiguous()
@@ -44,7 +44,7 @@ def _oracle_forward(inp):
 def _oracle_grad_forward(inp):
     """One rank's differentiable part through the oracle (autograd through its float64 arithmetic): the demodulated
     signal as (A, 2 C) sums; ``finish`` turns the summed sums back into the (C, A) signal."""
-    case = bloch.Case(*[getattr(inp, f) for f in bloch.Case.__dataclass_fields__])
+    case = bloch.Case(**{f: getattr(inp, f) for f in bloch.Case.__dataclass_fields__ if hasattr(inp, f)})
     sig, m = bloch.simulate(case)
     raw = torch.view_as_real(sig.T.contiguous()).reshape(sig.shape[1], -1)
     finish = lambda total, adc_phase: torch.view_as_complex(total.reshape(total.shape[0], -1, 2).contiguous()).T

@@ -1,0 +1,77 @@
+"""The bound pool (magnetization transfer) and the scanner field model on the GPU (``bp_forward_physics``).
+
+Mirrors blochparty ``tests/engines/test_gpu.py:86-125`` (``test_scanner_field_model``, ``test_magnetization_transfer``):
+the engine against the reference's own float64 core on the fixtures ``tests/golden/mt_*.npz`` and ``field_*.npz``
+(bound pool with the super-Lorentzian and the Lorentzian lineshape, bound-only RF, a four-column m_init; gradient
+nonlinearity alone, leading-order and exact concomitant fields; bound pool and field model together). The
+reference's GPU engines are held to 1e-4 (signal, m and the bound pool's Mz, max-norm relative) with the bound pool
+and to 1e-4 / 1e-3 (signal / m) with the field model; the bars here are 1e-5 on all three. Also: the variant with
+no physics switched on is the plain kernel's result, and a 3D GRE with a sinc slab pulse against the oracle.
+"""
+
+from dataclasses import replace
+
+import pytest
+import torch
+
+import blochparty_b200 as bpb
+from blochparty_b200 import phantoms, physics, sequences
+from golden_cases import PHYSICS, load_physics
+from oracle import bloch
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    b = b.to(torch.float64)
+    return float((a.to(torch.float64) - b).abs().max() / b.abs().max())
+
+
+@pytest.mark.parametrize("name", PHYSICS)
+def test_against_the_reference_core(name):
+    (ph, seq, coils, m0, sc), (sig, m, mb), z = load_physics(name)
+    r = bpb.simulate(ph, seq, coils, m_init=m0, scanner=sc)
+    e = {"signal": rel(r.signal, sig), "m": rel(r.m, m)}
+    if mb is not None:
+        e["m_bound"] = float((r.m_bound.double() - mb).abs().max() / m.abs().max())
+    else:
+        assert r.m_bound is None
+    print(f"\n{name}: " + ", ".join(f"{k} {v:.2e}" for k, v in e.items()))
+    assert r.signal.dtype == torch.complex64 and r.m.dtype == torch.float32
+    assert max(e.values()) < 1e-5, e
+
+
+def test_without_physics_is_the_plain_kernel():
+    """A scanner with a zero nonlinearity and no concomitant fields runs the physics variant with nothing switched
+    on: the plain kernel's result to float32 rounding (the variant steps every RF segment alone)."""
+    p = phantoms.ellipse_phantom_2d(16, 0.25, seed=3)
+    seq = sequences.gre((16, 16), 0.25, flip_deg=30.0, tr=6e-3, te=3e-3, n_dummy=4, dwell=20e-6)
+    coils = phantoms.birdcage_sensitivities(p.pos, 4)
+    zero = physics.GradientNonlinearity(torch.zeros(3, 4, 4, dtype=torch.float64),
+                                        torch.zeros(3, 4, 4, dtype=torch.float64), 0.25)
+    a = bpb.simulate(p, seq, coils, scanner=physics.Scanner(nonlinearity=zero))
+    b = bpb.simulate(p, seq, coils)
+    assert rel(a.signal, b.signal) < 2e-6 and rel(a.m, b.m) < 2e-6
+
+
+def test_3d_slab_gre_with_pool_and_field_model_against_the_oracle():
+    """A 3D GRE (8 x 8 x 4, 2 spins per voxel, two echoes) with a 40-step sinc slab pulse, every spin with a
+    super-Lorentzian bound pool, at 0.55 T with leading-order concomitant fields, against the float64 oracle."""
+    p = phantoms.ellipsoid_phantom_3d(8, 0.25, spins_per_voxel=2, b0_max=50.0, sigma_vox=1.0)
+    n = len(p.pd)
+    g = torch.Generator().manual_seed(21)
+    rnd = lambda *s: torch.rand(*s, generator=g, dtype=torch.float64)
+    bound = physics.BoundPool(0.1 + 0.05 * rnd(n), 20 + 20 * rnd(n), torch.ones(n, dtype=torch.float64),
+                              (9 + 4 * rnd(n)) * 1e-6, (rnd(n) - 0.5) * 400)
+    ph = replace(p, bound=bound)
+    seq = sequences.gre((8, 8, 4), 0.25, flip_deg=20.0, tr=8e-3, te=3e-3, dwell=20e-6, rf="sinc", rf_duration=1.2e-3,
+                        rf_steps=40, slab_thickness=0.15, n_echoes=2, echo_spacing=0.5e-3, n_dummy=2)
+    coils = phantoms.birdcage_sensitivities(p.pos, 4)
+    sc = physics.Scanner(field_strength=0.55, concomitant="leading")
+    r = bpb.simulate(ph, seq, coils, scanner=sc)
+    sig, m, mb = bloch.simulate_with_pool(bloch.case_from(ph, seq, coils, scanner=sc))
+    e = {"signal": rel(r.signal, sig), "m": rel(r.m, m),
+         "m_bound": float((r.m_bound.double() - mb).abs().max() / m.abs().max())}
+    print(f"\n3D slab GRE, {n} spins x {len(seq)} segments, pool + field model: "
+          + ", ".join(f"{k} {v:.2e}" for k, v in e.items()))
+    assert max(e.values()) < 1e-5, e

@@ -116,11 +116,11 @@ def _tse_through_maps(n, first_order):
             skip = a + k
             continue
         if c.is_rf[a]:
-            mx, my, mz = bloch._rf_step(mx, my, mz, a, c, None)
+            mx, my, mz, _ = bloch._rf_step(mx, my, mz, a, c, None)
             if c.adc[a]:
                 cols.append(bloch._sample(mx, my, c.adc_phase[a], c)[:, None])
         else:
-            mx, my, mz, smp = bloch._free_run(mx, my, mz, a, b, c, None)
+            mx, my, mz, _, smp = bloch._free_run(mx, my, mz, a, b, c, None)
             cols += smp
         if c.spoil[b - 1]:
             mx, my = torch.zeros_like(mx), torch.zeros_like(my)
