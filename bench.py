@@ -298,7 +298,9 @@ def run_reference_gpu(args):
     ``simulate`` from CPU tensors (packing, copies and read-back inside the timing), one untimed warm-up each
     (NVRTC compile), then the fastest of ``--repeat`` runs, wall clock around a synchronising call. ``--grad``: forward
     + backward of sum |signal|^2 with respect to the flip angle, the T1 map and the coil maps (the reference's
-    ``run_grad_case``). One JSON line per case."""
+    ``run_grad_case``). A case name may add ``+mt`` (every spin with the reference's default bound pool: f 0.1,
+    k 30 /s, T1b 1 s, T2b 12 us, super-Lorentzian with its 1 kHz cutoff) and ``+field`` (``scanner``: 0.55 T,
+    leading-order concomitant fields), the reference's own objects given to both engines. One JSON line per case."""
     ref = ROOT / "baseline" / "_ref"
     if not (ref / "blochparty").is_dir():
         print(json.dumps({"impl": "reference_gpu", "unavailable": "the reference is not installed in baseline/_ref"}))
@@ -313,6 +315,21 @@ def run_reference_gpu(args):
     f32, F64 = torch.float32, torch.float64
 
     def case(name, grad):
+        import dataclasses
+
+        from blochparty.exchange import BoundPool
+        from blochparty.fields import Scanner
+
+        base, *extra = name.split("+")
+        ph, seq, coils, grad_of = plain_case(base, grad)
+        kw = {}
+        if "mt" in extra:
+            ph = dataclasses.replace(ph, bound=BoundPool(f=0.1, k=30.0, t1=1.0, t2=12e-6))
+        if "field" in extra:
+            kw["scanner"] = Scanner(field_strength=0.55, concomitant="leading")
+        return ph, seq, coils, grad_of, kw
+
+    def plain_case(name, grad):
         n = REF_CASES[name]
         if grad:
             maps = bp.shepp_logan_maps(n, ndim=3, dtype=f32)
@@ -333,10 +350,10 @@ def run_reference_gpu(args):
     def timed(simulate, name):
         best, out = float("inf"), None
         for i in range(1 + args.repeat):
-            ph, seq, coils, grad_of = case(name, args.grad)  # (built outside the timing, as the reference's bench)
+            ph, seq, coils, grad_of, kw = case(name, args.grad)  # (built outside the timing, as the reference's bench)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            sig = simulate(ph, seq, coils).signal
+            sig = simulate(ph, seq, coils, **kw).signal
             if grad_of:
                 (sig.abs() ** 2).sum().backward()
             torch.cuda.synchronize()
@@ -349,7 +366,8 @@ def run_reference_gpu(args):
     for name in args.cases.split(","):
         ctx = torch.enable_grad() if args.grad else torch.no_grad()
         with ctx:
-            t_ref, (s_ref, g_ref, n, S, n_adc) = timed(lambda p, s, c: bp.simulate(p, s, c, engine="cuda"), name)
+            t_ref, (s_ref, g_ref, n, S, n_adc) = timed(lambda p, s, c, **kw: bp.simulate(p, s, c, engine="cuda", **kw),
+                                                       name)
             t_b2, (s_b2, g_b2, _, _, _) = timed(bpb.simulate, name)
         rel = lambda a, b: float(torch.linalg.vector_norm((a - b).to(torch.complex128 if b.is_complex() else F64))
                                  / torch.linalg.vector_norm(b.to(torch.complex128 if b.is_complex() else F64)))

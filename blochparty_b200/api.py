@@ -21,9 +21,15 @@ from . import capabilities, engine
 from .types import SimResult
 
 ENGINES = ("b200", "gpu", "cuda")  # "gpu" and "cuda" name this engine too, so a caller's engine= still works
-OPTIONS = ("readout", "pulses", "surrogate", "surrogate_inference", "max_ctas")
-PULSES = ("step", "reuse", "surrogate")
+# blochparty's GPU-engine options (engines/gpu/cuda/__init__.py:93-110), accepted as they are: ``readouts``
+# "direct" / "nufft" is ``readout`` "fp32" / "nufft"; ``chunk`` and ``group`` (dispatch chunking and threadgroup
+# size), ``mma`` (the sensitivity layout; both of its kernels reduce the coils on the CUDA cores) and
+# ``nufft_width`` / ``nufft_terms`` (the NUFFT's kernel width and decay terms, defaults 6 and 3) tune the
+# reference's kernels and change nothing here: the persistent kernels have no dispatch chunks, and the NUFFT here
+# takes width 8 and its terms from a 5e-8 bound on the decay's interpolation (at least as accurate).
 REFERENCE_GPU_OPTIONS = ("chunk", "group", "mma", "readouts", "nufft_width", "nufft_terms")
+OPTIONS = ("readout", "pulses", "surrogate", "surrogate_inference", "max_ctas") + REFERENCE_GPU_OPTIONS
+PULSES = ("step", "reuse", "surrogate")
 READOUTS = ("fp32", "bf16x3", "nufft")
 
 
@@ -89,8 +95,9 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
     if engine not in ENGINES:
         raise ValueError(f"engine must be one of {ENGINES}, not {engine!r}")
     if unknown := sorted(set(options) - set(OPTIONS)):
-        hint = " (an option of blochparty's GPU engines)" if set(unknown) <= set(REFERENCE_GPU_OPTIONS) else ""
+        hint = " (an option of blochparty's chunked engine)" if unknown == ["spin_chunk"] else ""
         raise TypeError(f"simulate(engine={engine!r}) got unexpected keyword argument(s) {', '.join(unknown)}{hint}")
+    options = _reference_options(dict(options))
     if not merge_free_runs:
         raise ValueError(f"merge_free_runs=False is the core's segment-by-segment stepping, not engine={engine!r}'s")
     readout = options.get("readout", "fp32")
@@ -139,6 +146,24 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
     with torch.no_grad():
         sig, m = _forward(inp, dev, options)
     return SimResult(sig, m)
+
+
+def _reference_options(options: dict) -> dict:
+    """blochparty's GPU-engine options mapped onto this engine's (``REFERENCE_GPU_OPTIONS``)."""
+    if "readouts" in options:
+        ro = options.pop("readouts")
+        if ro not in ("direct", "nufft"):
+            raise ValueError(f"readouts must be 'direct' or 'nufft', not {ro!r}")
+        mapped = "fp32" if ro == "direct" else "nufft"
+        if options.get("readout", mapped) != mapped:
+            raise ValueError(f"readouts={ro!r} and readout={options['readout']!r} disagree")
+        options["readout"] = mapped
+    for k in ("chunk", "group", "nufft_width", "nufft_terms"):
+        v = options.pop(k, None)
+        if v is not None and (not isinstance(v, int) or v < 1):
+            raise ValueError(f"{k} must be a positive int, got {v!r}")
+    options.pop("mma", None)
+    return options
 
 
 def _forward(inp: Inputs, dev, options):

@@ -183,7 +183,15 @@ def test_refusals_use_the_reference_wording():
 def test_argument_errors():
     ph, seq = _tiny()
     with pytest.raises(TypeError, match="unexpected keyword argument"):
-        bpb.simulate(ph, seq, chunk=4)
+        bpb.simulate(ph, seq, spin_chunk=4)
+    with pytest.raises(ValueError, match="readouts must be"):
+        bpb.simulate(ph, seq, readouts="fast")
+    with pytest.raises(ValueError, match="disagree"):
+        bpb.simulate(ph, seq, readouts="nufft", readout="fp32")
+    from blochparty_b200.api import _reference_options
+    assert _reference_options({"readouts": "nufft", "chunk": 4096, "group": 128, "mma": True, "nufft_width": 6,
+                               "nufft_terms": 3}) == {"readout": "nufft"}
+    assert _reference_options({"readouts": "direct"}) == {"readout": "fp32"}
     with pytest.raises(ValueError, match="merge_free_runs=False"):
         bpb.simulate(ph, seq, merge_free_runs=False)
     with pytest.raises(ValueError, match="engine must be one of"):
