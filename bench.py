@@ -83,6 +83,12 @@ FLOP_RF_REV, FLOP_FREE_REV, FLOP_ADC_REV_PER_COIL, FLOP_ADC_REV = 130, 30, 8, 2
 # recompute; a free segment's reverse is lambda's alone, 9 flops, and a window of free segments with one factor set
 # recomputes nothing
 FLOP_RF_REV_NO_SPIN, FLOP_RF_BACK, FLOP_FREE_LAMBDA = 103, 138, 9
+# DRAM bytes per spin-segment of the forward kernel, measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of
+# one launch over its spins x segments): the float32 readout on the 4-echo head sequence at 96^3 x 4 TRs (14.16 GB for
+# 3,538,944 x 2,376) and the NUFFT readout at 64^3 x 4 TRs (3.015 GB for 1,048,576 x 1,864). The traffic is the
+# per-window state, spin parameters and coil sensitivities, so it scales with spins x windows.
+TRAFFIC_FP32_PER_SPIN_SEGMENT = 14.162e9 / (3538944 * 2376)
+TRAFFIC_NUFFT_PER_SPIN_SEGMENT = 3.0147e9 / (1048576 * 1864)
 
 
 def nufft_flops_per_spin(flags: np.ndarray, n_coils: int, plan) -> int:
@@ -664,6 +670,12 @@ def main():
     flops = n * (flops_per_spin(stepped, pk.n_coils) if nr is None else nufft_flops_per_spin(pk.flags, pk.n_coils,
                                                                                             nr.plan))
     achieved = flops / (kernel_ms * 1e-3) / 1e12
+    traffic = None  # DRAM bytes per launch, from one ncu capture of the same kernel scaled by spins x segments
+    if mma is None and replaced is None:
+        per = TRAFFIC_NUFFT_PER_SPIN_SEGMENT if nr is not None else TRAFFIC_FP32_PER_SPIN_SEGMENT
+        traffic = {"bytes": per * n * S, "bytes_per_spin_segment": per,
+                   "scaled_from": ("ncu capture of bp_forward_kernel with NUFFT runs, head 64^3 x 4 TRs"
+                                   if nr is not None else "ncu capture of bp_forward_kernel, head 96^3 x 4 TRs")}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -678,7 +690,8 @@ def main():
                    "l2": "inputs larger than L2 (state, spins, coils, segments: hundreds of MB per GPU) and a 256 MB L2 "
                          "flush between timed steps"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": None if traffic is None else traffic["bytes"],
+                     "traffic_source": traffic,
                      "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU; MEASURED_PEAKS.json has no FP32",
                      "kernel": ("bp_forward_mma_kernel" if mma is not None else
                                 "bp_forward_kernel (NUFFT runs) + bp_nufft_finish_kernel" if nr is not None

@@ -117,7 +117,7 @@ SIGNATURES = {
     "bp_forward_nufft": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P, _P]),
     "bp_forward_physics": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, c_int, _P, _P, _P]),
     "bp_nufft_finish": (c_int, [_P, _P, c_int, c_int, c_int, c_int, c_int, _P, _P, _P]),
-    "bp_adjoint_workspace_bytes": (c_int, [c_int, c_int64, c_int64, c_int, c_int, c_int, c_int, _P]),
+    "bp_adjoint_workspace_bytes": (c_int, [c_int, c_int64, c_int64, c_int, c_int, c_int, c_int, c_int, _P]),
 }
 
 _lib = None
@@ -170,9 +170,9 @@ def forward_workspace(n: int, n_adc: int, n_coils: int) -> BpForwardWorkspace:
 
 
 def adjoint_workspace(n: int, n_segments: int, n_adc: int, n_coils: int, every: int, max_interval_windows: int,
-                      grid: int) -> BpAdjointWorkspace:
+                      grid: int, outer_every: int = 0) -> BpAdjointWorkspace:
     """The checkpointed adjoint's buffer sizes (``bp_adjoint_workspace_bytes``; host arithmetic, no GPU)."""
     out = BpAdjointWorkspace()
     check(lib().bp_adjoint_workspace_bytes(n, n_segments, n_adc, n_coils, every, max_interval_windows, grid,
-                                           ctypes.byref(out)), "bp_adjoint_workspace_bytes")
+                                           outer_every, ctypes.byref(out)), "bp_adjoint_workspace_bytes")
     return out

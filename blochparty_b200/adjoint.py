@@ -47,6 +47,24 @@ def default_checkpoint_every(n_segments: int) -> int:
     return w * max(1, math.ceil(math.sqrt(w * max(n_segments, 1)) / w))
 
 
+def choose_checkpoints(n_segments: int, n_spins: int, budget_bytes: int | None = None) -> tuple[int, int]:
+    """(checkpoint_every, outer_every) for a sequence of ``n_segments`` on ``n_spins``: the two-level scheme of
+    ``default_checkpoint_every`` (outer_every 0) when its stored states (interval starts plus one interval's window
+    starts, 24 bytes per spin each) fit ``budget_bytes`` (default: half the device's free memory), else three
+    levels with the cube root of the window count for each (intervals of that many windows, blocks of that many
+    intervals): about 3 (S / 32)^(1/3) states instead of 2 (S / 32)^(1/2), for one more forward."""
+    w = _lib.BP_ADJ_WIN
+    every = default_checkpoint_every(n_segments)
+    per_state = 24 * max(n_spins, 1)
+    two = (math.ceil(max(n_segments, 1) / every) + every // w + 1) * per_state
+    if budget_bytes is None:
+        budget_bytes = torch.cuda.mem_get_info()[0] // 2 if torch.cuda.is_available() else 1 << 62
+    if two <= budget_bytes:
+        return every, 0
+    root = max(2, math.ceil((max(n_segments, 1) / w) ** (1.0 / 3.0)))
+    return w * root, root
+
+
 def run_breaks(flags: np.ndarray) -> np.ndarray:
     """Window breaks for the adjoint at the start of every run of like segments: where RF and free segments
     alternate, where an RF segment changes dt or offset, where a free segment changes its factors, and after every
@@ -102,29 +120,45 @@ class Plan:
 class Checkpointed:
     """The device side of a simulation with gradients on a packed case: the forward that stores the state at every
     interval start, and the backward (per interval in reverse: replay, reverse sweep, segment-gradient reduction).
-    Every buffer is sized by the C ABI's workspace query (``bp_forward_workspace_bytes``,
-    ``bp_adjoint_workspace_bytes``); the backward's buffers are allocated on its first call and reused."""
+    With ``outer`` > 1 intervals per block, the forward stores the state at every block start only, and the
+    backward first re-runs each block's forward (no readout) to store its intervals' starts. Every buffer is sized
+    by the C ABI's workspace query (``bp_forward_workspace_bytes``, ``bp_adjoint_workspace_bytes``); the backward's
+    buffers are allocated on its first call and reused."""
 
-    def __init__(self, pk: engine.Packed, every: int, device):
+    def __init__(self, pk: engine.Packed, every: int, device, outer: int = 0):
         self.pk, self.dev = pk, device
         self.plan = plan = Plan(pk, every, device)
+        k = len(plan.starts)
+        self.outer = outer if outer > 1 and k > outer else 0
         fws = _lib.forward_workspace(pk.n, pk.n_adc, pk.n_coils)
         self.grid = _lib.lib().bp_adjoint_grid(pk.n, pk.n_coils)
         if self.grid < 1:
             raise RuntimeError("bp_adjoint_grid failed")
-        self.ws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, every, plan.max_aw, self.grid)
-        self.ckpts = sized(self.ws.checkpoints, (len(plan.starts), 6, pk.n), F32, device)
+        self.ws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, every, plan.max_aw, self.grid,
+                                         self.outer)
+        # interval starts (two levels), or block starts followed by one block's interval starts (three)
+        n_states = k if not self.outer else (k + self.outer - 1) // self.outer + self.outer
+        self.ckpts = sized(self.ws.checkpoints, (n_states, 6, pk.n), F32, device)
         self.raw = sized(fws.raw, (max(pk.n_adc, 1), 2 * pk.n_coils), F64, device, zero=True)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self._bufs = None
 
+    def blocks(self):
+        """[(first interval, end interval)] of the outer blocks (one block of every interval on two levels)."""
+        k = len(self.plan.starts)
+        step = self.outer or k
+        return [(b, min(b + step, k)) for b in range(0, k, step)]
+
     def forward(self, state: torch.Tensor) -> None:
         """All intervals from ``state`` ([6][n], advanced in place), the raw coil sums into ``raw`` (zeroed first),
-        the state at every interval start into the checkpoints."""
+        the state at every interval start (at every block start with an outer level) into the checkpoints."""
         pk, plan = self.pk, self.plan
         self.raw.zero_()
         for k, (fa, fb) in enumerate(plan.franges):
-            self.ckpts[k].copy_(state)
+            if not self.outer:
+                self.ckpts[k].copy_(state)
+            elif k % self.outer == 0:
+                self.ckpts[k // self.outer].copy_(state)
             engine.run_forward(pk, state, plan.fwin_dev, fa, fb, self.raw if pk.n_adc else None, self.status)
 
     def buffers(self, need_seg: bool, want_gc: bool):
@@ -153,25 +187,41 @@ class Checkpointed:
         seg.zero_()
         if gc is not None:
             gc.zero_()
-        lib, stream, n, C, A = _lib.lib(), _lib.stream_ptr(), pk.n, pk.n_coils, pk.n_adc
-        for k in reversed(range(len(plan.starts))):
-            aa, ab = plan.aranges[k]
-            s0, s1 = plan.seg_ranges[k]
-            state.copy_(self.ckpts[k])
-            engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, self.status, wstates=wstates, wstate_stride=1)
-            wstates[ab - aa].copy_(state)  # the state after the interval's last window
-            code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
-                                  aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
-                                  seg_mask, self.grid, ptr(self.status), stream)
-            _lib.check(code, "bp_adjoint")
-            if need_seg:
-                _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
+        n_blocks = len(self.blocks())
+        for bi, (ka, kb) in reversed(list(enumerate(self.blocks()))):
+            if self.outer:  # this block's interval starts, from its start (no readout)
+                state.copy_(self.ckpts[bi])
+                for k in range(ka, kb):
+                    self.ckpts[n_blocks + k - ka].copy_(state)
+                    if k + 1 < kb:
+                        fa, fb = plan.franges[k]
+                        engine.run_forward(pk, state, plan.fwin_dev, fa, fb, None, self.status)
+            for k in reversed(range(ka, kb)):
+                self._interval(k, n_blocks + k - ka if self.outer else k, h, lam, gs, gc, gseg, seg, seg_mask,
+                               need_seg, wstates, state)
         return gs, gc, seg
+
+    def _interval(self, k, ck, h, lam, gs, gc, gseg, seg, seg_mask, need_seg, wstates, state):
+        """Interval k from checkpoint ``ck``: replay with window states, the reverse sweep, the segment reduction."""
+        pk, plan = self.pk, self.plan
+        lib, stream, n, C, A = _lib.lib(), _lib.stream_ptr(), pk.n, pk.n_coils, pk.n_adc
+        aa, ab = plan.aranges[k]
+        s0, s1 = plan.seg_ranges[k]
+        state.copy_(self.ckpts[ck])
+        engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, self.status, wstates=wstates, wstate_stride=1)
+        wstates[ab - aa].copy_(state)  # the state after the interval's last window
+        code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
+                              aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
+                              seg_mask, self.grid, ptr(self.status), stream)
+        _lib.check(code, "bp_adjoint")
+        if need_seg:
+            _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
 
     def launches(self, need_seg: bool) -> tuple[int, int]:
         """(forward, backward) kernel launches of one call each."""
         k = len(self.plan.starts)
-        return k, k * (3 if need_seg else 2)
+        rebuild = sum(kb - ka - 1 for ka, kb in self.blocks()) if self.outer else 0
+        return k, k * (3 if need_seg else 2) + rebuild
 
     def check(self, what: str = "bp_forward / bp_adjoint") -> None:
         torch.cuda.synchronize(self.dev)
@@ -211,7 +261,7 @@ class _Simulate(torch.autograd.Function):
         inp = Inputs(d(pos), d(pd), d(t1), d(t2), d(db0), d(b1), coils, d(dt), d(rf), d(grad), d(adc_phase),
                      d(b0_offset), *flags_in, d(m0))
         pk = engine.pack(inp, dev)
-        run = Checkpointed(pk, every, dev)
+        run = Checkpointed(pk, every, dev, opts.get("outer", 0))
         state = engine.initial_state(inp.pd, inp.m_init, dev)
         run.forward(state)
         sig = engine.finish_signal(pk, run.raw)
@@ -306,7 +356,7 @@ def _check_grad_options(options):
 
 def _apply(inp, dev, checkpoint_every, raw: bool):
     S = len(inp.dt)
-    every = checkpoint_every or default_checkpoint_every(S)
+    every, outer = (checkpoint_every, 0) if checkpoint_every else choose_checkpoints(S, inp.pd.shape[0])
     if every % _lib.BP_ADJ_WIN:
         raise ValueError(f"checkpoint_every must be a multiple of {_lib.BP_ADJ_WIN}, got {every}")
     n = inp.pd.shape[0]
@@ -315,7 +365,7 @@ def _apply(inp, dev, checkpoint_every, raw: bool):
         z = torch.zeros_like(inp.pd)
         m0 = torch.stack([z, z, inp.pd], -1)
     coils_ri = torch.view_as_real(inp.coils if inp.coils.is_complex() else inp.coils.to(torch.complex64))
-    opts = {"device": dev, "every": every, "flags": (inp.is_rf, inp.adc, inp.spoil), "raw": raw}
+    opts = {"device": dev, "every": every, "outer": outer, "flags": (inp.is_rf, inp.adc, inp.spoil), "raw": raw}
     return _Simulate.apply(opts, inp.pos, inp.pd, inp.t1, inp.t2, inp.db0, inp.b1, coils_ri, inp.dt, inp.rf, inp.grad,
                            inp.adc_phase, inp.b0_offset, m0)
 

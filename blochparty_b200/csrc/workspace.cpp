@@ -17,14 +17,20 @@ extern "C" int bp_forward_workspace_bytes(int n, int64_t n_adc, int n_coils, BpF
 }
 
 extern "C" int bp_adjoint_workspace_bytes(int n, int64_t n_segments, int64_t n_adc, int n_coils, int checkpoint_every,
-                                          int max_interval_windows, int grid, BpAdjointWorkspace* out) {
+                                          int max_interval_windows, int grid, int outer_every,
+                                          BpAdjointWorkspace* out) {
     if (!out || n < 1 || n_segments < 0 || n_adc < 0 || n_coils < 1 || n_coils > BP_MAX_COILS ||
-        checkpoint_every < BP_ADJ_WIN || checkpoint_every % BP_ADJ_WIN != 0 || max_interval_windows < 0 || grid < 1)
+        checkpoint_every < BP_ADJ_WIN || checkpoint_every % BP_ADJ_WIN != 0 || max_interval_windows < 0 || grid < 1 ||
+        outer_every < 0)
         return BP_E_ARG;
     const int64_t nn = n, every = checkpoint_every;
     const int64_t intervals = n_segments > 0 ? (n_segments + every - 1) / every : 0;
     const int64_t longest = n_segments < every ? n_segments : every;  // segments of the longest interval
-    out->checkpoints = intervals * 6 * nn * 4;
+    // with an outer level: the state at every block start, and one block's interval starts
+    const int64_t states = outer_every > 1 ? (intervals + outer_every - 1) / outer_every +
+                                                 (intervals < outer_every ? intervals : (int64_t)outer_every)
+                                           : intervals;
+    out->checkpoints = states * 6 * nn * 4;
     out->wstates = ((int64_t)max_interval_windows + 1) * 6 * nn * 4;
     out->replay_state = 6 * nn * 4;
     out->gseg = (int64_t)grid * longest * 8 * 4;

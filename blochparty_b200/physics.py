@@ -182,10 +182,15 @@ def rf_frequency(dt, rf, is_rf, rf_freq=None) -> np.ndarray:
     live = np.asarray(is_rf, dtype=bool) & ((rf[:, 0] ** 2 + rf[:, 1] ** 2) > 0)
     if dt.shape[0] < 2:
         return np.zeros_like(dt)
-    z = rf[:, 0] + 1j * rf[:, 1]
-    turn = z[1:] * np.conj(z[:-1])  # the phase step from segment s to s + 1
+    # the phase step from segment s to s + 1, angle(z_{s+1} conj(z_s)), its real and imaginary parts as two
+    # products each: a sign change of a real waveform (a sinc's lobes) is a step of +pi or -pi by the sign of the
+    # zero imaginary part, y1 x0 - x1 y0, which this order of operations keeps as blochparty's does
+    x, y = rf[:, 0], rf[:, 1]
+    re = x[1:] * x[:-1] + y[1:] * y[:-1]
+    im = y[1:] * x[:-1] - x[1:] * y[:-1]
     both = live[1:] & live[:-1]
-    step = np.where(both, -np.angle(np.where(both, turn, 1.0)) / (math.pi * (dt[1:] + dt[:-1])), 0.0)
+    step = np.where(both, -np.arctan2(np.where(both, im, 0.0), np.where(both, re, 1.0)) / (math.pi * (dt[1:] + dt[:-1])),
+                    0.0)
     total = np.concatenate([[0.0], step]) + np.concatenate([step, [0.0]])
     count = np.concatenate([[0.0], both]) + np.concatenate([both, [0.0]])
     return total / np.maximum(count, 1.0)

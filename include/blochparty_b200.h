@@ -46,7 +46,10 @@ int bp_plan_windows(const int32_t* flags, int64_t n_segments, int seg_max, int s
  * themselves. bp_forward_workspace_bytes: the forward's state, raw coil sums, receiver phases, demodulated signal
  * and status word for n spins, n_adc samples and n_coils coils (`raw` and `signal` keep one row when n_adc = 0).
  * bp_adjoint_workspace_bytes: what the checkpointed adjoint adds for a sequence of n_segments segments: the
- * checkpoints (one [6][n] state per interval of checkpoint_every segments, a multiple of BP_ADJ_WIN), the window
+ * checkpoints (one [6][n] state per interval of checkpoint_every segments, a multiple of BP_ADJ_WIN; with
+ * outer_every > 1 intervals per outer block, one state per block start plus one block's interval starts, which
+ * the backward rebuilds by one more forward of every block: for sequences whose interval starts alone would not
+ * fit the device, e.g. 11.8 M segments x 8.4 M spins), the window
  * states of one replayed interval (max_interval_windows + 1: the most adjoint windows in one interval, from the
  * caller's bp_plan_windows plan, and the state after them), the replayed state, the per-CTA segment gradients (`grid` = bp_adjoint_grid,
  * times the longest interval), the float64 segment gradients, lambda, the per-spin gradients, the coil gradients
@@ -59,7 +62,7 @@ typedef struct {
 } BpAdjointWorkspace;
 int bp_forward_workspace_bytes(int n, int64_t n_adc, int n_coils, BpForwardWorkspace* out);
 int bp_adjoint_workspace_bytes(int n, int64_t n_segments, int64_t n_adc, int n_coils, int checkpoint_every,
-                               int max_interval_windows, int grid, BpAdjointWorkspace* out);
+                               int max_interval_windows, int grid, int outer_every, BpAdjointWorkspace* out);
 
 /* ADC samples per window that bp_forward's float32 readout accumulates for `n_coils` coils (0 if unsupported). */
 int bp_forward_samp_max(int n_coils);

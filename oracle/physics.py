@@ -110,9 +110,10 @@ def rf_frequency(dt: torch.Tensor, rf: torch.Tensor, is_rf) -> torch.Tensor:
         for nb in (s - 1, s + 1):
             if 0 <= nb < S and live[s] and live[nb]:
                 a, b = (nb, s) if nb < s else (s, nb)
-                za = complex(float(rf[a, 0]), float(rf[a, 1]))
-                zb = complex(float(rf[b, 0]), float(rf[b, 1]))
-                ang = math.atan2((zb * za.conjugate()).imag, (zb * za.conjugate()).real)
+                xa, ya, xb, yb = float(rf[a, 0]), float(rf[a, 1]), float(rf[b, 0]), float(rf[b, 1])
+                # angle(z_b conj(z_a)); a real waveform's sign change is +pi or -pi by the sign of the zero
+                # imaginary part yb xa - xb ya, as blochparty forms it
+                ang = math.atan2(yb * xa - xb * ya, xb * xa + yb * ya)
                 acc += -ang / (2 * math.pi * 0.5 * float(dt[a] + dt[b]))
                 cnt += 1
         out[s] = acc / max(cnt, 1)

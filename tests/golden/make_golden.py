@@ -247,6 +247,14 @@ def run_physics(name, ph, seq, coils, pool=None, shape=None, bound_only=None, m_
     plain = bp.simulate(bp.Phantom(ph.pos, ph.pd, ph.t1, ph.t2, ph.db0, b1=ph.b1), rseq, coils,
                         m_init=None if m_init is None else m_init[:, :3], engine="core")
     effect = float((r.signal - plain.signal).abs().max() / r.signal.abs().max())
+    if scanner is not None and scanner.concomitant is not None:  # the concomitant field's own share
+        from blochparty.fields import Scanner
+
+        nl_only = bp.simulate(rph, rseq, coils, m_init=m_init, scanner=Scanner(nonlinearity=scanner.nonlinearity),
+                              engine="core")
+        conc_effect = float((r.signal - nl_only.signal).abs().max() / r.signal.abs().max())
+        print(name, "effect of the concomitant field", f"{conc_effect:.2e}")
+        assert conc_effect > 1e-3, conc_effect
     fields = spin_fields(scanner, ph.pos)
     out = dict(
         pos=ph.pos.numpy(), pd=ph.pd.numpy(), t1=ph.t1.numpy(), t2=ph.t2.numpy(), db0=ph.db0.numpy(),
@@ -294,8 +302,11 @@ def physics():
         bo[s] = bool(seq.is_rf[s])
     run_physics("mt_lor", ph, seq, coils, pool, "lorentzian", bound_only=bo, m_init=m0)
     alpha, beta, r0 = nonlinearity()
-    p = phantoms.ellipse_phantom_2d(16, 0.25, seed=2)
-    gseq = sequences.gre((16, 16), 0.25, flip_deg=30.0, tr=6e-3, te=3e-3, n_dummy=4, dwell=20e-6)
+    # a 3D slab GRE (8^3 ellipsoids, a 20-step sinc slab, two echoes): spins off the z = 0 plane and gradients on
+    # every axis, where the concomitant field matters
+    p = phantoms.ellipsoid_phantom_3d(8, 0.25, spins_per_voxel=1, b0_max=30.0, sigma_vox=1.0)
+    gseq = sequences.gre((8, 8, 8), 0.25, flip_deg=20.0, tr=8e-3, te=3e-3, dwell=20e-6, rf="sinc", rf_duration=1e-3,
+                         rf_steps=20, slab_thickness=0.2, n_echoes=2, echo_spacing=0.5e-3, n_dummy=2)
     gcoils = phantoms.birdcage_sensitivities(p.pos, 4)
     gph = bp.Phantom(p.pos, p.pd, p.t1, p.t2, p.db0, b1=p.b1)
     for name, conc in (("field_nl", None), ("field_leading", "leading"), ("field_exact", "exact")):
@@ -303,9 +314,15 @@ def physics():
         sc = Scanner(field_strength=None if conc is None else 0.55, concomitant=conc, nonlinearity=nl)
         run_physics(name, gph, gseq, gcoils, scanner=sc,
                     scanner_args=(None if conc is None else 0.55, conc, alpha, beta, r0))
-    ph, seq, coils, pool = mt_case(14, "superlorentzian")
+    # the same 3D slab GRE with a bound pool on every spin
+    g = torch.Generator().manual_seed(14)
+    n = len(p.pd)
+    rnd = lambda *sh: torch.rand(*sh, generator=g, dtype=F64)
+    pool = dict(f=0.08 + 0.12 * rnd(n), k=15 + 45 * rnd(n), t1=0.8 + 0.4 * rnd(n), t2=(8 + 6 * rnd(n)) * 1e-6,
+                dw=(rnd(n) - 0.5) * 600)
+    mph = bp.Phantom(p.pos, p.pd, p.t1, p.t2, p.db0, b1=p.b1, bound=BoundPool(**pool))
     sc = Scanner(field_strength=0.55, concomitant="leading", nonlinearity=GradientNonlinearity(alpha, beta, r0))
-    run_physics("mt_field", ph, seq, coils, pool, "superlorentzian", scanner=sc,
+    run_physics("mt_field", mph, gseq, gcoils, pool, "superlorentzian", scanner=sc,
                 scanner_args=(0.55, "leading", alpha, beta, r0))
 
 

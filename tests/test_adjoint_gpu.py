@@ -158,6 +158,23 @@ def test_gradients_do_not_depend_on_checkpoint_interval():
         assert torch.equal(b[k], c[k]), k
 
 
+def test_outer_checkpoint_level_keeps_the_gradients(monkeypatch):
+    """Three checkpoint levels (the forward stores every third interval start, the backward rebuilds the others
+    from it) give the two-level gradients bit for bit: the rebuilt interval starts are the forward's own states."""
+    from blochparty_b200 import adjoint
+
+    ph, seq, coils, flips, t1_target = _adjoint_case(16)
+    target = _target(ph, seq, coils, t1_target)
+    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum() + m.double().sum()
+    names = ("pd", "t1", "t2", "db0", "b1", "coils", "rf", "dt", "grad")
+    monkeypatch.setattr(adjoint, "choose_checkpoints", lambda S, n: (64, 0))
+    _, a = gpu_gradients(ph, seq, coils, None, loss, names)
+    monkeypatch.setattr(adjoint, "choose_checkpoints", lambda S, n: (64, 3))
+    _, b = gpu_gradients(ph, seq, coils, None, loss, names)
+    for k in names:
+        assert torch.equal(a[k], b[k]), k
+
+
 def test_sweep_without_offset_gradients_matches_the_full_sweep():
     """Asking for T1, T2, PD and the RF alone takes the sweep variant that skips the offsets' gradients (position,
     dB0, segment dt, moments, b0_offset): its gradients are the full sweep's, bit for bit."""

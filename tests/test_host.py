@@ -253,7 +253,11 @@ def test_workspace_query_matches_the_host_allocations():
     assert w.total == sum(getattr(w, k) for k in ("checkpoints", "wstates", "replay_state", "gseg", "seg", "lam",
                                                    "gs", "gc", "h"))
     lib = _lib.lib()
-    assert lib.bp_adjoint_workspace_bytes(n, S, A, C, every + 1, plan.max_aw, grid, None) == _lib.BP_E_ARG
+    assert lib.bp_adjoint_workspace_bytes(n, S, A, C, every + 1, plan.max_aw, grid, 0, None) == _lib.BP_E_ARG
+    # the outer level: the block starts plus one block's interval starts
+    k = len(plan.starts)
+    wo = _lib.adjoint_workspace(n, S, A, C, every, plan.max_aw, grid, 2)
+    assert wo.checkpoints == ((k + 1) // 2 + min(k, 2)) * 6 * n * 4
     assert lib.bp_forward_workspace_bytes(n, A, 33, None) == _lib.BP_E_ARG
 
 
@@ -278,3 +282,15 @@ def test_workspace_structs_match_the_header(tmp_path):
         subprocess.run(["gcc", f"-I{inc}", str(src), "-o", str(exe)], check=True)
         got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
         assert got == [getattr(struct, f).offset for f in fields] + [ctypes.sizeof(struct)]
+
+
+def test_checkpoint_choice():
+    """Two levels while their states fit the budget, three beyond it (about 3 (S/32)^(1/3) states)."""
+    from blochparty_b200 import adjoint
+
+    assert adjoint.choose_checkpoints(1_110_016, 1 << 20, budget_bytes=40 << 30)[1] == 0
+    every, outer = adjoint.choose_checkpoints(11_829_248, 8_388_608, budget_bytes=80 << 30)
+    assert outer > 1 and every % 32 == 0
+    k = -(-11_829_248 // every)
+    states = -(-k // outer) + outer + every // 32 + 1
+    assert states * 24 * 8_388_608 < 80 << 30
