@@ -62,6 +62,7 @@ struct AdjArgs {
     float* gseg;          // [gridDim.x][seg_len][N_SG] per-CTA segment gradients, or null
     int seg_mask;         // which of the N_SG segment gradients are reduced (bit k: component k)
     int* status;          // |= BP_ERR_BAD_WINDOW for a window outside the interval (skipped)
+    int grid_rows;        // rows of gseg (bp_adjoint's `grid`): a variant that launches fewer CTAs clears the rest
 };
 
 // Rodrigues factors of the rotation by |w| (p2 = |w|^2) with the third factor of its left Jacobian:
@@ -279,14 +280,22 @@ struct KindTag {
 // rows of gs and columns of gseg are left as they were); SG: whether any per-spin gradient is wanted (without them,
 // and without CG and OG, gs is left as it was and a window of free segments only carries lambda back, with no
 // recompute: only the RF segments' gradients and lambda are formed).
+//
+// Without per-spin gradients (SG false) the variant keeps no state slots: its windows of free segments carry lambda
+// alone and its windows of RF segments integrate their states backward, and the rare window that needs its states
+// recomputed (a spoil at its end, relaxation too strong to invert, RF and free segments mixed) recomputes each
+// segment's input from the window start in registers (n(n+1)/2 steps instead of n). Its shared memory holds the
+// window's cotangent rows instead, so a sample's coil sum reads shared memory, and five CTAs fit on an SM.
 template <int NCG, bool CG, bool OG, bool SG>
-__global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kernel(AdjArgs a) {
+__global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG == 1 ? 5 : 4))
+    bp_adjoint_kernel(AdjArgs a) {
     static_assert(SG || (!CG && !OG), "coil and offset gradients are per-spin gradients");
     extern __shared__ __align__(16) float sm[];
-    float* slots = sm;                                     // [ADJ_SLOTS][3][ADJ_THREADS]
-    float* segacc = slots + ADJ_SLOTS * 3 * ADJ_THREADS;  // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
+    float* slots = sm;                                              // SG: [ADJ_SLOTS][3][ADJ_THREADS]
+    float* segacc = sm + (SG ? ADJ_SLOTS * 3 * ADJ_THREADS : 0);   // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
     SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * N_SG);  // [BP_ADJ_WIN] the window's
     double4* wk64 = reinterpret_cast<double4*>(wrec + BP_ADJ_WIN);                     // records and moments
+    float2* hs = reinterpret_cast<float2*>(wk64 + BP_ADJ_WIN);  // !SG: [BP_ADJ_WIN][8 NCG] the window's rows of h
     __shared__ float wmax[1];  // the window's largest wx0^2 + wy0^2
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
@@ -294,8 +303,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
     const bool need_seg = a.gseg != nullptr;
     const bool rf_only = need_seg && (a.seg_mask & BP_SEG_ALL & ~((1 << S_WX) | (1 << S_WY))) == 0;
     for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) segacc[i] = 0.0f;
-    if (need_seg)
-        for (int i = tid; i < a.seg_len * N_SG; i += ADJ_THREADS) a.gseg[(size_t)blockIdx.x * a.seg_len * N_SG + i] = 0.0f;
+    if (need_seg)  // this CTA's rows of gseg, and those of CTAs this launch does not have
+        for (int r = blockIdx.x; r < a.grid_rows; r += gridDim.x)
+            for (int i = tid; i < a.seg_len * N_SG; i += ADJ_THREADS) a.gseg[(size_t)r * a.seg_len * N_SG + i] = 0.0f;
     __syncthreads();
 
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
@@ -327,7 +337,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
             // a window the sweep can run: at most BP_ADJ_WIN segments (the slots), inside the interval (the rows of
             // gseg), its samples inside h. Anything else is skipped (the same for the whole CTA) and reported.
             if (nseg < 0 || nseg > BP_ADJ_WIN || win.x < a.seg0 || win.y > a.seg0 + a.seg_len || win.z < 0 ||
-                win.w < 0 || (a.h != nullptr && win.z + win.w > a.n_adc)) {
+                win.w < 0 || win.w > nseg || (a.h != nullptr && win.z + win.w > a.n_adc)) {
                 if (tid == 0) atomicOr(a.status, BP_ERR_BAD_WINDOW);
                 continue;
             }
@@ -360,6 +370,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
             }
             for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
                 reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
+            if (!SG && a.h != nullptr) {  // the window's cotangent rows, zero-padded to 8 NCG coils (win.w <= nseg)
+                for (int i = tid; i < win.w * 8 * NCG; i += ADJ_THREADS) {
+                    const int r = i / (8 * NCG), c = i - r * (8 * NCG);
+                    hs[i] = c < a.n_coils ? reinterpret_cast<const float2*>(a.h + (size_t)(win.z + r) * nv)[c]
+                                          : make_float2(0.0f, 0.0f);
+                }
+            }
             // the window's kind (the same for the whole CTA): every segment RF with the dt and offset of the first,
             // no sample (the steps of an RF pulse); or every segment free with the factors of the first (a
             // readout's samples); in either, a spoil at most after the last segment. Their sweeps skip the
@@ -420,13 +437,35 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 // recompute the window in plain float32 from its (compensated) start state: slot k = state after
                 // segment k-1 (before its spoil), slot 0 = window start
                 float mx = m0x, my = m0y, mz = m0z;
-                if (!LAMBDA_ONLY) slots[tid] = mx, slots[ADJ_THREADS + tid] = my, slots[2 * ADJ_THREADS + tid] = mz;
+                if (SG && !LAMBDA_ONLY) slots[tid] = mx, slots[ADJ_THREADS + tid] = my, slots[2 * ADJ_THREADS + tid] = mz;
                 FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 RevRelax rr{0.f, 0.f, 1.f, 1.f, 1.f, 1.f, true};
                 float wz = 0.f;
                 if (URF) rr = rev_relax(wrec[0].dt, p), wz = rf_wz(wrec[0], p);
                 if (KIND == 2) ff = free_factors(wrec[0], wk64[0], p);
-                for (int s = 0; s < (LAMBDA_ONLY ? 0 : nseg); ++s) {
+                // !SG: the state after segments 0 .. upto-1 of the window (before the last one's spoil), recomputed
+                // from the window start with factors of its own (the sweep's are kept)
+                auto state_at = [&](int upto, float& x, float& y, float& z) {
+                    x = m0x, y = m0y, z = m0z;
+                    FreeFactors f2 = ff;
+                    RevRelax r2 = rr;
+                    float w2 = wz;
+                    for (int s = 0; s < upto; ++s) {
+                        const SegRec q = wrec[s];
+                        if (URF || (KIND == 0 && (q.flags & BP_RF))) {
+                            if (KIND == 0) {
+                                if (s == 0 || !(q.flags & BP_SAME_RFDT)) r2 = rev_relax(q.dt, p);
+                                if (s == 0 || !(q.flags & BP_SAME_OFF)) w2 = rf_wz(q, p);
+                            }
+                            rf_step_plain<KIND == 3>(q, p, r2, w2, x, y, z);
+                        } else {
+                            if (KIND == 0 && (s == 0 || !(q.flags & BP_SAME_FREE))) f2 = free_factors(q, wk64[s], p);
+                            free_step_plain(f2, p, x, y, z);
+                        }
+                        if (KIND == 0 && s + 1 < upto && (q.flags & BP_SPOIL)) x = y = 0.0f;
+                    }
+                };
+                for (int s = 0; s < ((LAMBDA_ONLY || !SG) ? 0 : nseg); ++s) {
                     const SegRec q = wrec[s];
                     if (URF || (KIND == 0 && (q.flags & BP_RF))) {
                         if (KIND == 0) {
@@ -450,7 +489,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 // base, checked by bp_adjoint). A readout window loads each sample's row one sample ahead, so the
                 // loads' latency overlaps the sweep of the sample before (rows [win.z, win.z + win.w) only)
                 float2 hnext[8 * NCG];
-                if (KIND == 2 && a.h != nullptr && win.w > 0) {
+                if (SG && KIND == 2 && a.h != nullptr && win.w > 0) {
                     const float2* hr = reinterpret_cast<const float2*>(a.h + (size_t)(row - 1) * nv);
 #pragma unroll
                     for (int c = 0; c < 8 * NCG; ++c) hnext[c] = c < a.n_coils ? hr[c] : make_float2(0.f, 0.f);
@@ -459,8 +498,12 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                 // previous iteration read as its input
                 float outx = 0.f, outy = 0.f, outz = 0.f;
                 if (!LAMBDA_ONLY) {
-                    outx = slots[nseg * 3 * ADJ_THREADS + tid], outy = slots[(nseg * 3 + 1) * ADJ_THREADS + tid];
-                    outz = slots[(nseg * 3 + 2) * ADJ_THREADS + tid];
+                    if (SG) {
+                        outx = slots[nseg * 3 * ADJ_THREADS + tid], outy = slots[(nseg * 3 + 1) * ADJ_THREADS + tid];
+                        outz = slots[(nseg * 3 + 2) * ADJ_THREADS + tid];
+                    } else {
+                        state_at(nseg, outx, outy, outz);
+                    }
                 }
                 for (int s = nseg - 1; s >= 0; --s) {
                     const SegRec q = wrec[s];
@@ -470,7 +513,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     if (!URF && (f & BP_ADC) && a.h != nullptr) {
                         --row;
                         float2 hrow[8 * NCG];
-                        if (KIND == 2) {
+                        if (!SG) {  // the staged row (zero-padded coils)
+                            const float2* hr = hs + (row - win.z) * 8 * NCG;
+#pragma unroll
+                            for (int c = 0; c < 8 * NCG; ++c) hrow[c] = hr[c];
+                        } else if (KIND == 2) {
 #pragma unroll
                             for (int c = 0; c < 8 * NCG; ++c) hrow[c] = hnext[c];
                             if (row > win.z) {
@@ -488,7 +535,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                         float dx = 0.0f, dy = 0.0f;
 #pragma unroll
                         for (int c = 0; c < 8 * NCG; ++c) {
-                            if (c < a.n_coils) {
+                            if (!SG || c < a.n_coils) {  // (!SG: padded coils are zero rows of hs and of sens)
                                 const float2 hc = hrow[c];
                                 const float h0 = hc.x, h1 = hc.y;
                                 dx = fmaf(h0, sr[c], fmaf(h1, si[c], dx));
@@ -504,8 +551,12 @@ __global__ void __launch_bounds__(ADJ_THREADS, NCG == 1 ? 4 : 3) bp_adjoint_kern
                     // the segment's input state: slot s, spoiled by segment s-1 if it spoils
                     float x0 = 0.f, y0 = 0.f, z0 = 0.f;
                     if (!LAMBDA_ONLY) {
-                        const float* in = slots + s * 3 * ADJ_THREADS;
-                        x0 = in[tid], y0 = in[ADJ_THREADS + tid], z0 = in[2 * ADJ_THREADS + tid];
+                        if (SG) {
+                            const float* in = slots + s * 3 * ADJ_THREADS;
+                            x0 = in[tid], y0 = in[ADJ_THREADS + tid], z0 = in[2 * ADJ_THREADS + tid];
+                        } else {
+                            state_at(s, x0, y0, z0);
+                        }
                     }
                     outx = x0, outy = y0, outz = z0;
                     if (KIND == 0 && (f & A_PREV_SPOIL)) x0 = y0 = 0.0f;
@@ -581,9 +632,10 @@ __global__ void bp_seg_reduce_kernel(const float* __restrict__ gseg, int n_cta, 
     seg[(size_t)seg0 * N_SG + i] += t;
 }
 
+template <int NCG, bool SG>
 static size_t adj_smem() {
-    return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) +
-           (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4));
+    return (SG ? (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) : (size_t)BP_ADJ_WIN * 8 * NCG * sizeof(float2)) +
+           (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) + (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4));
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.
@@ -594,7 +646,7 @@ static int adj_configure() {
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
         if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)adj_smem()) != cudaSuccess ||
+                                 (int)adj_smem<NCG, SG>()) != cudaSuccess ||
             cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return -1;
@@ -609,23 +661,29 @@ static int adj_per_sm() {
     int per_sm = 0;
     if (adj_configure<NCG, CG, OG, SG>() < 0 ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG, OG, SG>, ADJ_THREADS,
-                                                      adj_smem()) != cudaSuccess)
+                                                      adj_smem<NCG, SG>()) != cudaSuccess)
         return -1;
     return per_sm > 0 ? per_sm : 1;
 }
 
-// one grid for every variant: the smallest residency of them
-template <int NCG>
-static int adj_grid(int n) {
+static int adj_sms() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+// the rows of gseg: the largest residency of the variants (a variant with fewer resident CTAs launches fewer and
+// clears the other rows)
+template <int NCG>
+static int adj_grid(int n) {
+    const int sms = adj_sms();
     const int v[4] = {adj_per_sm<NCG, true, true, true>(), adj_per_sm<NCG, false, true, true>(),
                       adj_per_sm<NCG, false, false, true>(), adj_per_sm<NCG, false, false, false>()};
     int per_sm = v[0];
     for (int k = 0; k < 4; ++k) {
         if (v[k] < 0) return -1;
-        per_sm = v[k] < per_sm ? v[k] : per_sm;
+        per_sm = v[k] > per_sm ? v[k] : per_sm;
     }
     const int n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
     const int grid = sms * per_sm;
@@ -644,8 +702,10 @@ extern "C" int bp_adjoint_grid(int n, int n_coils) {
 
 template <int NCG, bool CG, bool OG, bool SG>
 static int launch_variant(const AdjArgs& a, int grid, cudaStream_t st) {
-    if (adj_configure<NCG, CG, OG, SG>() < 0) return BP_E_LAUNCH;
-    bp_adjoint_kernel<NCG, CG, OG, SG><<<grid, ADJ_THREADS, adj_smem(), st>>>(a);
+    const int per_sm = adj_per_sm<NCG, CG, OG, SG>();
+    if (per_sm < 0) return BP_E_LAUNCH;
+    const int own = adj_sms() * per_sm, ctas = grid < own ? grid : own;  // one wave of resident CTAs
+    bp_adjoint_kernel<NCG, CG, OG, SG><<<ctas, ADJ_THREADS, adj_smem<NCG, SG>(), st>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
@@ -675,7 +735,7 @@ extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_co
     if (wb == wa) return BP_OK;
     AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
               reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, n_adc, lam, gs,
-              gc, gseg, seg_mask, status};
+              gc, gseg, seg_mask, status, grid};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch ((n_coils + 7) / 8) {
         case 1: return launch_adj<1>(a, grid, st);

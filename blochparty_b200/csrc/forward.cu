@@ -255,6 +255,10 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                 __syncwarp();
             }
             FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            // the last readout run's merged factors and their repeat count (-1: none): the runs of one readout
+            // (cut at 32-segment blocks) mostly share both
+            FreeFactors fmc{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            int fmc_reps = -1;
             RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
             float wz = 0.0f;
             int slot = 0, row0 = 0;
@@ -355,6 +359,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                     }
                 } else {
                     if (s == 0 || !(f & BP_SAME_FREE)) {
+                        fmc_reps = -1;
                         if constexpr (PHYS)
                             ff = free_factors_phys(q, a.seg64[win.x + s], p, 1, a.ph.conc_mode, ck,
                                                    a.ph.segq + 6 * (size_t)(win.x + s));
@@ -403,8 +408,11 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                                 else
                                     free_step(fr, p, mx, my, mz, lx, ly, lz);
                             } else {
-                                const FreeFactors fr = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
-                                free_step(fr, p, mx, my, mz, lx, ly, lz);
+                                if (fmc_reps != e - s - 1) {
+                                    fmc = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
+                                    fmc_reps = e - s - 1;
+                                }
+                                free_step(fmc, p, mx, my, mz, lx, ly, lz);
                             }
                             if (q0[e - 1].flags & BP_SPOIL) mx = my = lx = ly = 0.0f;
                         }
