@@ -395,8 +395,8 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
     (the flip train), K timed steps with CUDA events around each half. Returns the ``fwd_adjoint`` object."""
     from blochparty_b200 import _lib, adjoint
 
-    every = adjoint.default_checkpoint_every(S)
-    run = adjoint.Checkpointed(pk, every, dev)
+    every, outer = adjoint.choose_checkpoints(S, pk.n)
+    run = adjoint.Checkpointed(pk, every, dev, outer)
     g = torch.Generator().manual_seed(7)
     w = torch.complex(torch.randn(pk.n_coils, pk.n_adc, generator=g, dtype=torch.float64),
                       torch.randn(pk.n_coils, pk.n_adc, generator=g, dtype=torch.float64))
@@ -441,6 +441,7 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
         "forward_ms": f_ms, "backward_ms": b_ms, "steps": args.steps, "warmup": args.warmup,
         "grad_wrt": "the RF waveform (flip train), seeded linear loss of the signal",
         "checkpoint_every": every, "intervals": len(run.plan.starts),
+        "outer_every": run.outer,  # intervals per outer block (0: two levels); its rebuild forward is not counted
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": None, "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU",
                      "kernel": "bp_forward_kernel (forward, replay) + bp_adjoint_kernel + bp_seg_reduce_kernel",

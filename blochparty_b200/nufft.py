@@ -120,10 +120,8 @@ class NufftPlan:
     order: np.ndarray  # spin order (sorted by x of the class)
 
 
-def plan(spins32: np.ndarray, segs: np.ndarray, seg64: np.ndarray, flags: np.ndarray, W: int = W_DEFAULT) -> NufftPlan:
-    """The NUFFT plan of a case: the runs of the class with the most samples, the spin order sorting them by x,
-    the grid and kernel parameters, the decay terms and the output weights. ``spins32`` [8][n] float32 (packed
-    order), ``segs`` (S, 8) float32 records, ``seg64`` (S, 4) float64, ``flags`` (S,) int32."""
+def run_class(segs: np.ndarray, seg64: np.ndarray, flags: np.ndarray) -> np.ndarray:
+    """(R, 2) the runs (first segment, length) of the class with the most samples: one segment's factors."""
     runs = find_runs(flags)
     if not runs:
         raise ValueError("readout='nufft': the sequence has no readout run of at least "
@@ -133,12 +131,24 @@ def plan(spins32: np.ndarray, segs: np.ndarray, seg64: np.ndarray, flags: np.nda
         key = (segs[a, :7].tobytes(), seg64[a].tobytes(), k)
         classes.setdefault(key, []).append((a, k))
     key = max(classes, key=lambda c: len(classes[c]) * c[2])
-    sel = np.asarray(classes[key], dtype=np.int64)
-    a0, L = int(sel[0, 0]), int(sel[0, 1])
+    return np.asarray(classes[key], dtype=np.int64)
+
+
+def plan(spins32: np.ndarray, segs: np.ndarray, seg64: np.ndarray, flags: np.ndarray, W: int = W_DEFAULT) -> NufftPlan:
+    """The NUFFT plan of a case: the runs of the class with the most samples, the spin order sorting them by x,
+    the grid and kernel parameters, the decay terms and the output weights. ``spins32`` [8][n] float32 (packed
+    order), ``segs`` (S, 8) float32 records, ``seg64`` (S, 4) float64, ``flags`` (S,) int32."""
+    sel = run_class(segs, seg64, flags)
+    a0 = int(sel[0, 0])
     x = run_phase(spins32, segs[a0], seg64[a0])
     order = np.argsort(x, kind="stable")
-    dt = float(segs[a0, 0])
     r2max = float(np.max(spins32[5].astype(np.float64))) if spins32.shape[1] else 0.0
+    return plan_of(sel, float(segs[a0, 0]), r2max, order, W)
+
+
+def plan_of(sel: np.ndarray, dt: float, r2max: float, order, W: int = W_DEFAULT) -> NufftPlan:
+    """The plan from the run class, its segment's dt, the largest 1/T2 and the spin order."""
+    L = int(sel[0, 1])
     M = terms_for(r2max, (L - 1) * dt)
     G = 1 << int(math.ceil(math.log2(2 * L)))
     beta = BETA_PER_W * W
@@ -204,22 +214,52 @@ def windows_for(p: NufftPlan, flags: np.ndarray, samp_max: int):
     return np.ascontiguousarray(win), run_of, rows
 
 
-class NufftRun:
-    """The device side of a forward with NUFFT readout runs on a packed case (spins already in ``plan.order``)."""
+def spin_tables_dev(p: NufftPlan, spins: torch.Tensor, rec: np.ndarray, k64: np.ndarray):
+    """``spin_tables`` on the device from the packed (sorted) float32 spins [8][n]: the same float64 arithmetic
+    in torch."""
+    F64_ = torch.float64
+    px, py, pz, db0 = (spins[i].to(F64_) for i in (0, 1, 2, 6))
+    cyc = k64[0] * px + k64[1] * py + k64[2] * pz + float(np.float32(rec[0])) * db0 + k64[3]
+    x = cyc - torch.floor(cyc)
+    u = x * p.G
+    fl = torch.floor(u)
+    base = (fl - p.W // 2 + 1).to(torch.int64)
+    frac = (u - fl).to(torch.float32)
+    h = p.L // 2
+    ang = -2.0 * math.pi * ((x * h) - torch.floor(x * h))
+    shift = torch.stack([torch.cos(ang), torch.sin(ang)], -1).to(torch.float32)
+    nodes = torch.as_tensor(p.nodes, dtype=F64_, device=spins.device)
+    decay = torch.exp(-nodes[:, None] * spins[5].to(F64_)[None, :]).to(torch.float32)
+    n = spins.shape[1]
+    n_tiles = (n + TILE - 1) // TILE
+    pad = n_tiles * TILE - n
+    bt = torch.cat([base, base[-1:].expand(pad)]).reshape(n_tiles, TILE)
+    tiles = torch.stack([bt.amin(1), bt.amax(1) + p.W], -1).to(torch.int32)
+    span = int((tiles[:, 1] - tiles[:, 0]).max()) if n_tiles else 0
+    if span * p.M > 64:
+        raise ValueError(f"readout='nufft': a tile of {TILE} sorted spins spans {span} of {p.G} grid cells (too "
+                         f"few spins for the grid: at most {64 // p.M}); use readout='fp32'")
+    return (base.to(torch.int32).contiguous(), frac.contiguous(), shift.contiguous(), decay.contiguous(),
+            tiles.contiguous())
 
-    def __init__(self, pk: engine.Packed, p: NufftPlan):
+
+class NufftRun:
+    """The device side of a forward with NUFFT readout runs on a packed case (spins already in ``plan.order``).
+    ``rec``, ``k64``: the class's segment record and float64 moments (host)."""
+
+    def __init__(self, pk: engine.Packed, p: NufftPlan, rec: np.ndarray | None = None, k64: np.ndarray | None = None):
         dev = pk.device
-        spins32 = pk.spins.cpu().numpy()
-        segs = pk.segs.cpu().numpy()
-        seg64 = pk.seg64.cpu().numpy()
-        base, frac, shift, decay, tiles = spin_tables(p, spins32, segs, seg64)
+        a0 = int(p.runs[0, 0])
+        if rec is None:
+            rec, k64 = pk.segs[a0].cpu().numpy(), pk.seg64[a0].cpu().numpy()
+        base, frac, shift, decay, tiles = spin_tables_dev(p, pk.spins, rec, k64)
         samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
         win, run_of, rows = windows_for(p, pk.flags, samp)
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
         self.plan, self.pk = p, pk
         self.windows, self.wdev = win, t(win)
-        self.run_of, self.base, self.frac = t(run_of), t(base), t(frac)
-        self.shift, self.decay, self.tiles = t(shift), t(decay), t(tiles)
+        self.run_of, self.base, self.frac = t(run_of), base, frac
+        self.shift, self.decay, self.tiles = shift, decay, tiles
         self.rows, self.weights = t(rows), t(p.weights.astype(np.float64))
         self.grid = torch.zeros(len(p.runs), p.G, p.M, 2 * pk.n_coils, dtype=F64, device=dev)
         self.desc = _lib.BpNufft(ptr(self.run_of), ptr(self.base), ptr(self.frac), ptr(self.shift), ptr(self.decay),
@@ -244,35 +284,46 @@ def sorted_inputs(inp, order: np.ndarray):
     """The inputs with every per-spin tensor in ``order``."""
     from dataclasses import replace
 
-    idx = torch.from_numpy(order)
+    idx = order if isinstance(order, torch.Tensor) else torch.from_numpy(order)
     take = lambda t: None if t is None else t[idx.to(t.device)]
     return replace(inp, pos=take(inp.pos), pd=take(inp.pd), t1=take(inp.t1), t2=take(inp.t2), db0=take(inp.db0),
                    b1=take(inp.b1), coils=take(inp.coils), m_init=take(inp.m_init))
 
 
 def prepare(inp, device):
-    """(packed case in the sorted order, NufftRun, order): the plan from a first packing (the spins' float32 values
-    fix x), then the case packed again in the order of x."""
+    """(packed case in the sorted order, NufftRun, order (a device tensor)): the case packed once onto the device,
+    x of the run class from its float32 spins (float64 arithmetic on the device), the spins and coil sensitivities
+    gathered into the order of x there, and the tables from them."""
     if inp.coils.shape[1] > 16:
         raise ValueError(f"readout='nufft' takes at most 16 coils, got {inp.coils.shape[1]}")
-    pk0 = engine.pack(inp, "cpu")
-    p = plan(pk0.spins.numpy(), pk0.segs.numpy(), pk0.seg64.numpy(), pk0.flags)
-    pk = engine.pack(sorted_inputs(inp, p.order), device)
-    return pk, NufftRun(pk, p), p.order
+    spins, sens = engine.pack_spins(inp.pos, inp.pd, inp.t1, inp.t2, inp.db0, inp.b1, inp.coils, device)
+    segs, seg64, psi, flags, n_adc = engine.pack_segments(inp.dt, inp.rf, inp.grad, inp.b0_offset, inp.adc_phase,
+                                                          inp.is_rf, inp.adc, inp.spoil, "cpu")
+    sel = run_class(segs.numpy(), seg64.numpy(), flags)
+    a0 = int(sel[0, 0])
+    rec, k64 = segs[a0].numpy(), seg64[a0].numpy()
+    px, py, pz, db0 = (spins[i].to(torch.float64) for i in (0, 1, 2, 6))
+    cyc = k64[0] * px + k64[1] * py + k64[2] * pz + float(np.float32(rec[0])) * db0 + k64[3]
+    order = torch.argsort(cyc - torch.floor(cyc), stable=True)
+    r2max = float(spins[5].max()) if spins.shape[1] else 0.0
+    p = plan_of(sel, float(rec[0]), r2max, order)
+    spins, sens = spins[:, order].contiguous(), sens[:, order].contiguous()
+    segs_d, seg64_d, psi = segs.to(device).contiguous(), seg64.to(device).contiguous(), psi.to(device)
+    engine.mark_small_rf(spins, segs_d, flags)
+    pk = engine.Packed(spins.shape[1], inp.coils.shape[1], n_adc, spins, sens, segs_d, seg64_d, psi, flags, device)
+    return pk, NufftRun(pk, p, rec, k64), order
 
 
 def forward_nufft(inp, device, max_ctas: int = 0):
     """Signal (C, A) complex64 and m (N, 3) float32 on the CPU, with the readout runs through the NUFFT."""
     pk, nr, order = prepare(inp, device)
-    idx = torch.from_numpy(order)
-    m_init = None if inp.m_init is None else inp.m_init[idx.to(inp.m_init.device)]
-    state = engine.initial_state(inp.pd[idx.to(inp.pd.device)], m_init, device)
+    state = engine.initial_state(inp.pd, inp.m_init, device)[:, order].contiguous()
     raw = torch.zeros(max(pk.n_adc, 1), 2 * pk.n_coils, dtype=F64, device=device)
     status = torch.zeros(1, dtype=torch.int32, device=device)
     nr.run(state, raw, status, max_ctas)
     sig = engine.finish_signal(pk, raw)
     torch.cuda.synchronize(device)
     _lib.check_status(status, "bp_forward_nufft")
-    inv = np.empty_like(order)
-    inv[order] = np.arange(order.shape[0])
-    return sig.cpu(), engine.final_m(state)[torch.from_numpy(inv)]
+    inv = torch.empty_like(order)
+    inv[order] = torch.arange(order.shape[0], device=order.device)
+    return sig.cpu(), engine.final_m(state[:, inv])

@@ -99,3 +99,22 @@ def test_refusals():
     with pytest.raises(ValueError, match="more than"):
         nufft.terms_for(1e4, 1.27e-3)
     assert nufft.terms_for(1.0 / 0.02, 1.26e-3) == 4 and nufft.terms_for(1.0 / 0.07, 1.26e-3) == 3
+
+
+def test_device_preparation_matches_the_host_tables():
+    """``nufft.prepare`` (one packing, the sort and the tables in torch on the target device; here the CPU) gives
+    the order and the tables of the host restatement (``plan``, ``spin_tables``): the same order, cells and decay
+    terms, and fractions and shifts within a float32 ulp."""
+    inp, _ = _case()
+    pk0 = engine.pack(inp, "cpu")
+    p = nufft.plan(pk0.spins.numpy(), pk0.segs.numpy(), pk0.seg64.numpy(), pk0.flags)
+    pk_h = engine.pack(nufft.sorted_inputs(inp, p.order), "cpu")
+    base, frac, shift, decay, tiles = nufft.spin_tables(p, pk_h.spins.numpy(), pk_h.segs.numpy(), pk_h.seg64.numpy())
+    pk, nr, order = nufft.prepare(inp, torch.device("cpu"))
+    assert np.array_equal(order.numpy(), p.order)
+    assert torch.equal(pk.spins, pk_h.spins) and torch.equal(pk.sens, pk_h.sens)
+    assert np.array_equal(nr.base.numpy(), base) and np.array_equal(nr.tiles.numpy(), tiles)
+    assert np.abs(nr.frac.numpy() - frac).max() <= 1e-6
+    assert np.abs(nr.shift.numpy() - shift).max() <= 2e-7
+    assert np.abs(nr.decay.numpy() - decay).max() <= 1e-7
+    assert (nr.plan.M, nr.plan.L, nr.plan.G) == (p.M, p.L, p.G) and np.array_equal(nr.plan.runs, p.runs)
