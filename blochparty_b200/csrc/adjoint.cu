@@ -275,6 +275,14 @@ struct KindTag {
     static constexpr int value = K;
 };
 
+// A window the sweep can run: at most BP_ADJ_WIN segments (the slots and staging buffers), inside the interval (the
+// rows of gseg), its samples (at most one per segment) inside h.
+__device__ __forceinline__ bool adj_window_ok(const int4& win, const AdjArgs& a) {
+    const int nseg = win.y - win.x;
+    return !(nseg < 0 || nseg > BP_ADJ_WIN || win.x < a.seg0 || win.y > a.seg0 + a.seg_len || win.z < 0 ||
+             win.w < 0 || win.w > nseg || (a.h != nullptr && win.z + win.w > a.n_adc));
+}
+
 // NCG: groups of 8 coils; CG: whether the coil gradients are wanted (a.gc not null); OG: whether the gradients
 // of the spins' offsets (position, dB0) or of the segments' dt, moments or b0_offset are wanted (otherwise their
 // rows of gs and columns of gseg are left as they were); SG: whether any per-spin gradient is wanted (without them,
@@ -295,7 +303,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     float* segacc = sm + (SG ? ADJ_SLOTS * 3 * ADJ_THREADS : 0);   // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
     SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * N_SG);  // [BP_ADJ_WIN] the window's
     double4* wk64 = reinterpret_cast<double4*>(wrec + BP_ADJ_WIN);                     // records and moments
-    float2* hs = reinterpret_cast<float2*>(wk64 + BP_ADJ_WIN);  // !SG: [BP_ADJ_WIN][8 NCG] the window's rows of h
+    // !SG: two staging buffers, each the raw records, the moments and the cotangent rows ([BP_ADJ_WIN][8 NCG]) of a
+    // window, filled by TMA bulk copies one window ahead; wk64 and hs point into the current one
+    SegRec* rawrec = reinterpret_cast<SegRec*>(wk64 + (SG ? BP_ADJ_WIN : 0));      // !SG: [2][BP_ADJ_WIN]
+    double4* wk64b = reinterpret_cast<double4*>(rawrec + 2 * BP_ADJ_WIN);          // !SG: [2][BP_ADJ_WIN]
+    float2* hsb = reinterpret_cast<float2*>(wk64b + 2 * BP_ADJ_WIN);               // !SG: [2][BP_ADJ_WIN][8 NCG]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(hsb + 2 * BP_ADJ_WIN * 8 * NCG);  // !SG: [2]
+    float2* hs = hsb;
     __shared__ float wmax[1];  // the window's largest wx0^2 + wy0^2
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
@@ -306,7 +320,33 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     if (need_seg)  // this CTA's rows of gseg, and those of CTAs this launch does not have
         for (int r = blockIdx.x; r < a.grid_rows; r += gridDim.x)
             for (int i = tid; i < a.seg_len * N_SG; i += ADJ_THREADS) a.gseg[(size_t)r * a.seg_len * N_SG + i] = 0.0f;
+    // !SG: the cotangent rows come by TMA when they are whole coil groups on a 16-byte aligned base (else the
+    // threads copy them, zero-padded); issue(w, b) stages window w into buffer b (thread 0): a window the sweep
+    // cannot run, or one without segments, completes the buffer's phase with no data
+    const bool h_tma = !SG && a.h != nullptr && 2 * a.n_coils == 16 * NCG && (reinterpret_cast<uintptr_t>(a.h) & 15) == 0;
+    auto issue = [&](int w, int b) {
+        const int4 win = a.windows[w];
+        const int ns = win.y - win.x;
+        if (!adj_window_ok(win, a) || ns == 0) {
+            mbar_arrive(&bars[b]);
+            return;
+        }
+        const bool th = h_tma && win.w > 0;
+        const uint32_t rec_bytes = (uint32_t)ns * sizeof(SegRec), hbytes = th ? (uint32_t)win.w * 64u * NCG : 0u;
+        fence_proxy_async_smem();
+        mbar_expect_tx(&bars[b], 2 * rec_bytes + hbytes);
+        tma_load_1d(rawrec + b * BP_ADJ_WIN, a.segs + win.x, rec_bytes, &bars[b]);
+        tma_load_1d(wk64b + b * BP_ADJ_WIN, a.seg64 + win.x, rec_bytes, &bars[b]);
+        if (th) tma_load_1d(hsb + b * BP_ADJ_WIN * 8 * NCG, a.h + (size_t)win.z * 16 * NCG, hbytes, &bars[b]);
+    };
+    int seq = 0;  // !SG: windows this CTA has staged so far (buffer seq & 1, its phase (seq >> 1) & 1)
+    if (!SG && tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
     __syncthreads();
+    if (!SG && tid == 0 && blockIdx.x < n_tiles && a.wb > a.wa) issue(a.wb - 1, 0);
 
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int j0 = tile * ADJ_THREADS + tid;
@@ -334,11 +374,33 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
         for (int w = a.wb - 1; w >= a.wa; --w) {
             const int4 win = a.windows[w];
             const int nseg = win.y - win.x;
-            // a window the sweep can run: at most BP_ADJ_WIN segments (the slots), inside the interval (the rows of
-            // gseg), its samples inside h. Anything else is skipped (the same for the whole CTA) and reported.
-            if (nseg < 0 || nseg > BP_ADJ_WIN || win.x < a.seg0 || win.y > a.seg0 + a.seg_len || win.z < 0 ||
-                win.w < 0 || win.w > nseg || (a.h != nullptr && win.z + win.w > a.n_adc)) {
+            const int buf = seq & 1;
+            if constexpr (!SG) {
+                // the next window (this tile's, or the next tile's first) into the other buffer: the barrier that
+                // ended the previous window ended every read of it
+                if (tid == 0) {
+                    if (w > a.wa)
+                        issue(w - 1, buf ^ 1);
+                    else if (tile + (int)gridDim.x < n_tiles)
+                        issue(a.wb - 1, buf ^ 1);
+                }
+                const bool ok = mbar_wait_bounded(&bars[buf], (seq >> 1) & 1);
+                ++seq;
+                if (__syncthreads_or(!ok)) {  // (a copy of a few KB never takes this long) give up and report
+                    if (tid == 0) {
+                        atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
+                        mbar_wait_bounded(&bars[buf ^ 1], (seq >> 1) & 1);  // the other buffer's copy, if any
+                    }
+                    return;
+                }
+                wk64 = wk64b + buf * BP_ADJ_WIN;
+                hs = hsb + buf * BP_ADJ_WIN * 8 * NCG;
+            }
+            // a window the sweep can run (adj_window_ok); anything else is skipped (the same for the whole CTA) and
+            // reported
+            if (!adj_window_ok(win, a)) {
                 if (tid == 0) atomicOr(a.status, BP_ERR_BAD_WINDOW);
+                if (!SG) __syncthreads();  // (the next window's staging waits for the end of this one)
                 continue;
             }
             // the window's records into shared memory (every warp of the CTA sweeps the same window); the barrier
@@ -356,7 +418,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                     mex = we[j] + we[3 * n + j], mey = we[n + j] + we[4 * n + j], mez = we[2 * n + j] + we[5 * n + j];
                 }
             }
-            const SegRec* gw = a.segs + win.x;
+            // the records: SG from global memory, !SG from the staging buffer (read only: every thread writes its
+            // own record of wrec)
+            const SegRec* gw = SG ? a.segs + win.x : rawrec + buf * BP_ADJ_WIN;
             for (int i = tid; i < nseg * 8; i += ADJ_THREADS)
                 if ((i & 7) != 7) reinterpret_cast<float*>(wrec)[i] = reinterpret_cast<const float*>(gw)[i];
             for (int i = tid; i < nseg; i += ADJ_THREADS) {
@@ -368,9 +432,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 if (!(f & BP_RF) && i + 1 < nseg && !(fn & BP_RF) && (fn & BP_SAME_FREE)) x |= A_KEEP_FREE;
                 wrec[i].flags = x;
             }
-            for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
-                reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
-            if (!SG && a.h != nullptr) {  // the window's cotangent rows, zero-padded to 8 NCG coils (win.w <= nseg)
+            if (SG)
+                for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
+                    reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
+            if (!SG && a.h != nullptr && !h_tma) {  // the cotangent rows, zero-padded to 8 NCG coils (win.w <= nseg)
                 for (int i = tid; i < win.w * 8 * NCG; i += ADJ_THREADS) {
                     const int r = i / (8 * NCG), c = i - r * (8 * NCG);
                     hs[i] = c < a.n_coils ? reinterpret_cast<const float2*>(a.h + (size_t)(win.z + r) * nv)[c]
@@ -634,8 +699,12 @@ __global__ void bp_seg_reduce_kernel(const float* __restrict__ gseg, int n_cta, 
 
 template <int NCG, bool SG>
 static size_t adj_smem() {
-    return (SG ? (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) : (size_t)BP_ADJ_WIN * 8 * NCG * sizeof(float2)) +
-           (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) + (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4));
+    const size_t common = (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) + (size_t)BP_ADJ_WIN * sizeof(SegRec);
+    if (SG)  // the slots, segacc, the records and the moments
+        return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + common + (size_t)BP_ADJ_WIN * sizeof(double4);
+    // segacc, the records, two staging buffers (raw records, moments, cotangent rows) and their two mbarriers
+    return common + 2 * (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4) + 8 * NCG * sizeof(float2)) +
+           2 * sizeof(uint64_t);
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.
@@ -732,6 +801,9 @@ extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_co
         return BP_E_ARG;
     if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs || !status) return BP_E_ARG;
     if ((reinterpret_cast<uintptr_t>(h) & 7) != 0) return BP_E_ALIGN;  // read as (re, im) pairs
+    // records and moments are staged by TMA bulk copies (16-byte aligned)
+    if ((reinterpret_cast<uintptr_t>(segs) & 15) != 0 || (reinterpret_cast<uintptr_t>(seg64) & 15) != 0)
+        return BP_E_ALIGN;
     if (wb == wa) return BP_OK;
     AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
               reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, n_adc, lam, gs,
