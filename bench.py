@@ -644,9 +644,10 @@ def main():
     grad_line = None
     if world == 1 and not args.no_grad and replaced is None and mma is None and nr is None:
         grad_line = measure_fwd_adjoint(args, dev, pk, state0, flush, n, S)
-        g_ms, g_d2h = e2e_fwd_adjoint(ph, seq, coils)
-        grad_line["e2e"] = {"value": n * S / (g_ms * 1e-3), "unit": UNIT, "ms_per_step": g_ms, "h2d_bytes_per_step": h2d,
-                            "d2h_bytes_per_step": d2h + g_d2h, "runs": 1}
+        if args.e2e_steps > 0:
+            g_ms, g_d2h = e2e_fwd_adjoint(ph, seq, coils)
+            grad_line["e2e"] = {"value": n * S / (g_ms * 1e-3), "unit": UNIT, "ms_per_step": g_ms,
+                                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h + g_d2h, "runs": 1}
 
     if rank != 0:
         dist.destroy_process_group() if world > 1 else None

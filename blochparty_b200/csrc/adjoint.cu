@@ -311,6 +311,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     uint64_t* bars = reinterpret_cast<uint64_t*>(hsb + 2 * BP_ADJ_WIN * 8 * NCG);  // !SG: [2]
     float2* hs = hsb;
     __shared__ float wmax[1];  // the window's largest wx0^2 + wy0^2
+    __shared__ unsigned wkind[ADJ_WARPS];  // per warp: a copy timed out (1), not all RF (2), not all free (4)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
     const int nv = 2 * a.n_coils;
@@ -373,8 +374,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
         }
         for (int w = a.wb - 1; w >= a.wa; --w) {
             const int4 win = a.windows[w];
-            const int nseg = win.y - win.x;
+            // a window the sweep can run (adj_window_ok); anything else is skipped (the same for the whole CTA) and
+            // reported, after the barrier below
+            const bool good = adj_window_ok(win, a);
             const int buf = seq & 1;
+            bool ok = true;
             if constexpr (!SG) {
                 // the next window (this tile's, or the next tile's first) into the other buffer: the barrier that
                 // ended the previous window ended every read of it
@@ -384,42 +388,30 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                     else if (tile + (int)gridDim.x < n_tiles)
                         issue(a.wb - 1, buf ^ 1);
                 }
-                const bool ok = mbar_wait_bounded(&bars[buf], (seq >> 1) & 1);
+                ok = mbar_wait_bounded(&bars[buf], (seq >> 1) & 1);  // (a copy of a few KB: never this long)
                 ++seq;
-                if (__syncthreads_or(!ok)) {  // (a copy of a few KB never takes this long) give up and report
-                    if (tid == 0) {
-                        atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
-                        mbar_wait_bounded(&bars[buf ^ 1], (seq >> 1) & 1);  // the other buffer's copy, if any
-                    }
-                    return;
-                }
                 wk64 = wk64b + buf * BP_ADJ_WIN;
                 hs = hsb + buf * BP_ADJ_WIN * 8 * NCG;
             }
-            // a window the sweep can run (adj_window_ok); anything else is skipped (the same for the whole CTA) and
-            // reported
-            if (!adj_window_ok(win, a)) {
-                if (tid == 0) atomicOr(a.status, BP_ERR_BAD_WINDOW);
-                if (!SG) __syncthreads();  // (the next window's staging waits for the end of this one)
-                continue;
-            }
-            // the window's records into shared memory (every warp of the CTA sweeps the same window); the barrier
-            // at the end of the previous window ended its reads. The flags word of record s is written by thread s
-            // alone, with the sweep's own bits added (from the global records, so no thread reads a word another
-            // writes)
-            // the window's start state (from the replay, in DRAM for long intervals): loaded first, so that its
-            // latency overlaps the staging below and its barrier
+            const int nseg = (good && ok) ? win.y - win.x : 0;  // (nothing is read of a window that is not run)
+            // the window's states from the replay (in DRAM for long intervals), loaded first so that their latency
+            // overlaps the staging below: SG its start (the recompute's); !SG the state after it (the next window's
+            // start, or the interval's end: RF windows integrate backward from it), its start only where a window
+            // recomputes (loaded there)
             float m0x = 0.f, m0y = 0.f, m0z = 0.f, mex = 0.f, mey = 0.f, mez = 0.f;
-            if (active) {
+            if (active && nseg > 0) {
                 const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
-                m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j], m0z = ws[2 * n + j] + ws[5 * n + j];
-                if (!SG) {  // the state after the window (the next one's start, or the interval's end)
+                if (SG) {
+                    m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j], m0z = ws[2 * n + j] + ws[5 * n + j];
+                } else {
                     const float* we = ws + 6 * (size_t)n;
                     mex = we[j] + we[3 * n + j], mey = we[n + j] + we[4 * n + j], mez = we[2 * n + j] + we[5 * n + j];
                 }
             }
-            // the records: SG from global memory, !SG from the staging buffer (read only: every thread writes its
-            // own record of wrec)
+            // the window's records into shared memory (every warp of the CTA sweeps the same window); the barrier
+            // at the end of the previous window ended its reads. The flags word of record s is written by thread s
+            // alone, with the sweep's own bits added: SG from the global records, !SG from the staging buffer (read
+            // only), so no thread reads a word another writes
             const SegRec* gw = SG ? a.segs + win.x : rawrec + buf * BP_ADJ_WIN;
             for (int i = tid; i < nseg * 8; i += ADJ_THREADS)
                 if ((i & 7) != 7) reinterpret_cast<float*>(wrec)[i] = reinterpret_cast<const float*>(gw)[i];
@@ -435,7 +427,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             if (SG)
                 for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
                     reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
-            if (!SG && a.h != nullptr && !h_tma) {  // the cotangent rows, zero-padded to 8 NCG coils (win.w <= nseg)
+            if (!SG && a.h != nullptr && !h_tma && nseg > 0) {  // cotangent rows, zero-padded to 8 NCG coils
                 for (int i = tid; i < win.w * 8 * NCG; i += ADJ_THREADS) {
                     const int r = i / (8 * NCG), c = i - r * (8 * NCG);
                     hs[i] = c < a.n_coils ? reinterpret_cast<const float2*>(a.h + (size_t)(win.z + r) * nv)[c]
@@ -458,7 +450,28 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(v));
                 if (lane == 0) *wmax = __uint_as_float(m);
             }
-            const bool all_rf = __syncthreads_and(rf_ok), all_free = __syncthreads_and(free_ok);
+            // one barrier for the staging, the copy's bounded wait (any thread gave up) and the window's kind (every
+            // thread agrees): each warp's OR of its threads' bits, then the warps' words
+            const unsigned bits = (ok ? 0u : 1u) | (rf_ok ? 0u : 2u) | (free_ok ? 0u : 4u);
+            const unsigned wbits = __reduce_or_sync(0xffffffffu, bits);
+            if (lane == 0) wkind[warp] = wbits;
+            __syncthreads();
+            unsigned kind_bits = 0;
+#pragma unroll
+            for (int k = 0; k < ADJ_WARPS; ++k) kind_bits |= wkind[k];
+            if (kind_bits & 1u) {  // a staging copy did not land within the bound: report and stop
+                if (tid == 0) {
+                    atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
+                    if (!SG) mbar_wait_bounded(&bars[buf ^ 1], (seq >> 1) & 1);  // the other buffer's copy, if any
+                }
+                return;
+            }
+            if (!good) {
+                if (tid == 0) atomicOr(a.status, BP_ERR_BAD_WINDOW);
+                __syncthreads();  // (every thread has read wkind before the next window writes it)
+                continue;
+            }
+            const bool all_rf = !(kind_bits & 2u), all_free = !(kind_bits & 4u);
             // the segment's partial gradients summed over the warp into its slice of segacc
             auto reduce_seg = [&](int s, const SegGrad& sg) {
                 if (rf_only) {  // only the RF's two components: a reduce-scatter of 2 values (lanes 0, 16 hold them)
@@ -501,6 +514,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 }
                 // recompute the window in plain float32 from its (compensated) start state: slot k = state after
                 // segment k-1 (before its spoil), slot 0 = window start
+                if constexpr (!SG) {  // (loaded only here: the windows that recompute)
+                    if (active) {
+                        const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
+                        m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j];
+                        m0z = ws[2 * n + j] + ws[5 * n + j];
+                    }
+                }
                 float mx = m0x, my = m0y, mz = m0z;
                 if (SG && !LAMBDA_ONLY) slots[tid] = mx, slots[ADJ_THREADS + tid] = my, slots[2 * ADJ_THREADS + tid] = mz;
                 FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
