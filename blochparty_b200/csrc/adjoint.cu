@@ -29,6 +29,9 @@
 #define ADJ_THREADS 128
 #define ADJ_WARPS (ADJ_THREADS / 32)
 #define ADJ_SLOTS (BP_ADJ_WIN + 1)
+// !SG: the RF gradient of an interval of at most this many segments is summed over the CTA's tiles in shared memory
+// ([ADJ_SACC_MAX][2] floats) and written to gseg once, instead of added to gseg after every window
+#define ADJ_SACC_MAX 2048
 // the sweep's own bits in a staged record's flags (above the record's): the segment before it (in the window)
 // spoils; the segment after it (in the window, swept just before) shares its RF relaxation, its RF off-resonance,
 // or its free factors, so the sweep keeps them
@@ -309,6 +312,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     double4* wk64b = reinterpret_cast<double4*>(rawrec + 2 * BP_ADJ_WIN);          // !SG: [2][BP_ADJ_WIN]
     float2* hsb = reinterpret_cast<float2*>(wk64b + 2 * BP_ADJ_WIN);               // !SG: [2][BP_ADJ_WIN][8 NCG]
     uint64_t* bars = reinterpret_cast<uint64_t*>(hsb + 2 * BP_ADJ_WIN * 8 * NCG);  // !SG: [2]
+    float2* iacc = reinterpret_cast<float2*>(bars + 2);  // !SG: [ADJ_SACC_MAX] the interval's RF gradient (x, y)
     float2* hs = hsb;
     __shared__ float wmax[1];  // the window's largest wx0^2 + wy0^2
     __shared__ unsigned wkind[ADJ_WARPS];  // per warp: a copy timed out (1), not all RF (2), not all free (4)
@@ -318,6 +322,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     const bool need_seg = a.gseg != nullptr;
     const bool rf_only = need_seg && (a.seg_mask & BP_SEG_ALL & ~((1 << S_WX) | (1 << S_WY))) == 0;
     for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) segacc[i] = 0.0f;
+    // !SG (only the RF's two components): the interval's sums in shared memory when they fit, in the order the
+    // global adds would take (tile by tile), so the bits are the same
+    const bool sacc = !SG && need_seg && a.seg_len <= ADJ_SACC_MAX;
+    if (sacc)
+        for (int i = tid; i < a.seg_len; i += ADJ_THREADS) iacc[i] = make_float2(0.0f, 0.0f);
     if (need_seg)  // this CTA's rows of gseg, and those of CTAs this launch does not have
         for (int r = blockIdx.x; r < a.grid_rows; r += gridDim.x)
             for (int i = tid; i < a.seg_len * N_SG; i += ADJ_THREADS) a.gseg[(size_t)r * a.seg_len * N_SG + i] = 0.0f;
@@ -677,7 +686,16 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 sweep(KindTag<0>{});
             }
             __syncthreads();  // segacc complete; every thread is done reading this window's slots
-            if (need_seg && !(rf_only && all_free)) {
+            if (sacc && !all_free) {  // (!SG: rf_only; a free window's RF partials are 0)
+                for (int i = tid; i < 2 * nseg; i += ADJ_THREADS) {
+                    const int sgi = i >> 1, comp = (i & 1) ? S_WY : S_WX;
+                    float t = 0.0f;
+#pragma unroll
+                    for (int ww = 0; ww < ADJ_WARPS; ++ww) t += segacc[(ww * BP_ADJ_WIN + sgi) * N_SG + comp];
+                    float* d = reinterpret_cast<float*>(iacc + (win.x - a.seg0 + sgi)) + (i & 1);
+                    *d += t;
+                }
+            } else if (need_seg && !(rf_only && all_free)) {
                 float* dst = a.gseg + ((size_t)blockIdx.x * a.seg_len + (win.x - a.seg0)) * N_SG;
                 for (int i = tid; i < nseg * N_SG; i += ADJ_THREADS) {
                     float t = 0.0f;
@@ -705,6 +723,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             }
         }
     }
+    if (sacc) {  // the interval's RF gradient of this CTA (its rows were cleared at the start; the last window's
+                 // barrier ended every add)
+        float* dst = a.gseg + (size_t)blockIdx.x * a.seg_len * N_SG;
+        for (int i = tid; i < a.seg_len; i += ADJ_THREADS) {
+            const float2 v = iacc[i];
+            dst[(size_t)i * N_SG + S_WX] = v.x;
+            dst[(size_t)i * N_SG + S_WY] = v.y;
+        }
+    }
 }
 
 // SEG[seg0 + s][k] += sum over CTAs (in order) of gseg[cta][s][k], in float64
@@ -722,9 +749,10 @@ static size_t adj_smem() {
     const size_t common = (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) + (size_t)BP_ADJ_WIN * sizeof(SegRec);
     if (SG)  // the slots, segacc, the records and the moments
         return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + common + (size_t)BP_ADJ_WIN * sizeof(double4);
-    // segacc, the records, two staging buffers (raw records, moments, cotangent rows) and their two mbarriers
+    // segacc, the records, two staging buffers (raw records, moments, cotangent rows), their two mbarriers and the
+    // interval's RF gradient
     return common + 2 * (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4) + 8 * NCG * sizeof(float2)) +
-           2 * sizeof(uint64_t);
+           2 * sizeof(uint64_t) + (size_t)ADJ_SACC_MAX * sizeof(float2);
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.
