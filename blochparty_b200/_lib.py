@@ -40,7 +40,8 @@ class BpPhysics(ctypes.Structure):
     """``BpPhysics`` of the C ABI: the bound pool and the field model of ``bp_forward_physics``."""
 
     _fields_ = [("mt", c_int), ("conc_mode", c_int), ("pool", c_void_p), ("bstate", c_void_p), ("rf_freq", c_void_p),
-                ("line", c_void_p), ("conc", c_void_p), ("segq", c_void_p)]
+                ("line", c_void_p), ("conc", c_void_p), ("segq", c_void_p), ("wstates", c_void_p),
+                ("wstate_stride", c_int)]
 
 
 class BpForwardWorkspace(ctypes.Structure):
@@ -95,6 +96,8 @@ SIGNATURES = {
     "bp_adjoint_grid": (c_int, [c_int, c_int]),
     "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, c_int, _P, _P, _P,
                            _P, c_int, c_int, _P, _P]),
+    "bp_adjoint_physics": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, c_int, _P,
+                                   _P, _P, _P, c_int, c_int, _P, _P, _P, _P]),
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),
     "bp_pulse_targets": (c_int, [_P, c_int, c_double, c_double, c_double, c_double, _P, c_int, _P, _P, _P]),
     "bp_mlp_grad_ctas": (c_int, [c_int]),

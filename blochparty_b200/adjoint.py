@@ -125,8 +125,9 @@ class Checkpointed:
     by the C ABI's workspace query (``bp_forward_workspace_bytes``, ``bp_adjoint_workspace_bytes``); the backward's
     buffers are allocated on its first call and reused."""
 
-    def __init__(self, pk: engine.Packed, every: int, device, outer: int = 0):
+    def __init__(self, pk: engine.Packed, every: int, device, outer: int = 0, phys=None):
         self.pk, self.dev = pk, device
+        self.phys = phys  # the field model (``PhysGrad``): the forward, replay and sweep take its variants
         self.plan = plan = Plan(pk, every, device)
         k = len(plan.starts)
         self.outer = outer if outer > 1 and k > outer else 0
@@ -159,7 +160,23 @@ class Checkpointed:
                 self.ckpts[k].copy_(state)
             elif k % self.outer == 0:
                 self.ckpts[k // self.outer].copy_(state)
-            engine.run_forward(pk, state, plan.fwin_dev, fa, fb, self.raw if pk.n_adc else None, self.status)
+            self._fwd(state, plan.fwin_dev, fa, fb, self.raw if pk.n_adc else None)
+
+    def _fwd(self, state, wdev, wa, wb, raw, wstates=None):
+        """The forward kernel over windows [wa, wb) (the physics variant with the field model)."""
+        pk = self.pk
+        if self.phys is None:
+            engine.run_forward(pk, state, wdev, wa, wb, raw, self.status, wstates=wstates, wstate_stride=1)
+            return
+        import ctypes
+
+        ph = self.phys.ph
+        ph.wstates, ph.wstate_stride = ptr(wstates), 1
+        code = _lib.lib().bp_forward_physics(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs),
+                                             ptr(pk.seg64), ptr(wdev), wa, wb, ptr(state), ptr(raw), 0,
+                                             ctypes.byref(ph), ptr(self.status), _lib.stream_ptr())
+        ph.wstates, ph.wstate_stride = None, 0
+        _lib.check(code, "bp_forward_physics")
 
     def buffers(self, need_seg: bool, want_gc: bool):
         pk, plan, ws, dev = self.pk, self.plan, self.ws, self.dev
@@ -187,6 +204,8 @@ class Checkpointed:
         seg.zero_()
         if gc is not None:
             gc.zero_()
+        if self.phys is not None and self.phys.gconc is not None:
+            self.phys.gconc.zero_()
         n_blocks = len(self.blocks())
         for bi, (ka, kb) in reversed(list(enumerate(self.blocks()))):
             if self.outer:  # this block's interval starts, from its start (no readout)
@@ -195,7 +214,7 @@ class Checkpointed:
                     self.ckpts[n_blocks + k - ka].copy_(state)
                     if k + 1 < kb:
                         fa, fb = plan.franges[k]
-                        engine.run_forward(pk, state, plan.fwin_dev, fa, fb, None, self.status)
+                        self._fwd(state, plan.fwin_dev, fa, fb, None)
             for k in reversed(range(ka, kb)):
                 self._interval(k, n_blocks + k - ka if self.outer else k, h, lam, gs, gc, gseg, seg, seg_mask,
                                need_seg, wstates, state)
@@ -208,11 +227,19 @@ class Checkpointed:
         aa, ab = plan.aranges[k]
         s0, s1 = plan.seg_ranges[k]
         state.copy_(self.ckpts[ck])
-        engine.run_forward(pk, state, plan.awin_dev, aa, ab, None, self.status, wstates=wstates, wstate_stride=1)
+        self._fwd(state, plan.awin_dev, aa, ab, None, wstates=wstates)
         wstates[ab - aa].copy_(state)  # the state after the interval's last window
-        code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
-                              aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
-                              seg_mask, self.grid, ptr(self.status), stream)
+        if self.phys is None:
+            code = lib.bp_adjoint(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64), ptr(plan.awin_dev),
+                                  aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam), ptr(gs), ptr(gc), ptr(gseg),
+                                  seg_mask, self.grid, ptr(self.status), stream)
+        else:
+            import ctypes
+
+            code = lib.bp_adjoint_physics(ptr(pk.spins), ptr(pk.sens), n, C, ptr(pk.segs), ptr(pk.seg64),
+                                          ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(wstates), ptr(h), A, ptr(lam),
+                                          ptr(gs), ptr(gc), ptr(gseg), seg_mask, self.grid,
+                                          ctypes.byref(self.phys.ph), ptr(self.phys.gconc), ptr(self.status), stream)
         _lib.check(code, "bp_adjoint")
         if need_seg:
             _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
@@ -238,21 +265,42 @@ class Checkpointed:
         return h
 
 
+class PhysGrad:
+    """The field model's device buffers for a gradient-carrying simulation: the concomitant coefficients ([7][n]
+    float32, rows of the mode's coefficients), the segments' dt-weighted gradient monomials ([S][6] float64, mode
+    1), the ``BpPhysics`` descriptor, and the coefficients' gradient ([7][n], when wanted)."""
+
+    def __init__(self, conc: torch.Tensor, mode: int, dt, grad, device, want_grad: bool):
+        from .physics import gradient_moments2
+
+        n = conc.shape[0]
+        cc = torch.zeros(7, n, dtype=F32)
+        cc[: conc.shape[1]] = conc.detach().to(F64).cpu().T.to(F32)
+        self.conc = cc.to(device).contiguous()
+        self.segq = (torch.from_numpy(np.ascontiguousarray(gradient_moments2(dt, grad))).to(device)
+                     if mode == 1 else None)
+        self.gconc = torch.zeros(7, n, dtype=F32, device=device) if want_grad else None
+        self.ph = _lib.BpPhysics()
+        self.ph.conc_mode, self.ph.conc, self.ph.segq = mode, ptr(self.conc), ptr(self.segq)
+        self.width = conc.shape[1]
+
+
 def seg_mask_for(need) -> int:
     """The segment gradients the chain rules use (``need``: ``_Simulate``'s needs_input_grad): dt needs all of
     them (the record's every field scales with dt), the RF its two components, the gradient the moments,
     b0_offset its phase; ``BP_SPIN_NO_OFFSETS`` unless the positions' or dB0's gradients are wanted, and
     ``BP_SPIN_NONE`` when no per-spin input (position, PD, T1, T2, dB0, B1, coils) needs one."""
-    spin_none = not any(need[i] for i in range(1, 8))
+    conc = len(need) > 14 and need[14]  # the concomitant coefficients (their gradient is an offsets' gradient)
+    spin_none = not any(need[i] for i in range(1, 8)) and not conc
     return (_lib.BP_SEG_ALL if need[8] else 0) | ((_lib.BP_SEG_WX | _lib.BP_SEG_WY) if need[9] else 0) | (
         (_lib.BP_SEG_KX | _lib.BP_SEG_KY | _lib.BP_SEG_KZ) if need[10] else 0) | (
-        _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5]) else _lib.BP_SPIN_NO_OFFSETS) | (
+        _lib.BP_SEG_BETA if need[12] else 0) | (0 if (need[1] or need[5] or conc) else _lib.BP_SPIN_NO_OFFSETS) | (
         _lib.BP_SPIN_NONE if spin_none else 0)
 
 
 class _Simulate(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0):
+    def forward(ctx, opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0, conc=None):
         from .api import Inputs
 
         dev, every, flags_in = opts["device"], opts["every"], opts["flags"]
@@ -261,14 +309,17 @@ class _Simulate(torch.autograd.Function):
         inp = Inputs(d(pos), d(pd), d(t1), d(t2), d(db0), d(b1), coils, d(dt), d(rf), d(grad), d(adc_phase),
                      d(b0_offset), *flags_in, d(m0))
         pk = engine.pack(inp, dev)
-        run = Checkpointed(pk, every, dev, opts.get("outer", 0))
+        phys = None
+        if conc is not None:  # the field model's concomitant coefficients (positions: the encoding ones)
+            phys = PhysGrad(conc, opts["conc_mode"], inp.dt, inp.grad, dev, ctx.needs_input_grad[14])
+        run = Checkpointed(pk, every, dev, opts.get("outer", 0), phys)
         state = engine.initial_state(inp.pd, inp.m_init, dev)
         run.forward(state)
         sig = engine.finish_signal(pk, run.raw)
         run.check("bp_forward")
         ctx.run, ctx.dev = run, dev
         ctx.like = [None if t is None else (t.dtype, t.device) for t in
-                    (pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0)]
+                    (pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0, conc)]
         ctx.raw_mode = bool(opts.get("raw"))
         ctx.set_materialize_grads(False)
         if ctx.raw_mode:  # the float64 raw coil sums on the device, not demodulated (the caller demodulates)
@@ -284,10 +335,10 @@ class _Simulate(torch.autograd.Function):
         t1, t2, dt, rf, grad, b0_offset, adc_phase, sig_ri = ctx.saved_tensors
         run, dev = ctx.run, ctx.dev
         pk = run.pk
-        # inputs: opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0
+        # inputs: opts, pos, pd, t1, t2, db0, b1, coils_ri, dt, rf, grad, adc_phase, b0_offset, m0, conc
         need = ctx.needs_input_grad
         if g_sig is None and g_m is None:
-            return (None,) * 14
+            return (None,) * 15
         n, C, A, S = pk.n, pk.n_coils, pk.n_adc, len(dt)
         if ctx.raw_mode:  # dL/d(raw coil sums) directly
             h = sized(run.ws.h, (A, 2 * C), F32, dev).copy_(g_sig) if (g_sig is not None and A) else None
@@ -300,7 +351,7 @@ class _Simulate(torch.autograd.Function):
         gs, gc, seg = run.backward(h, lam, seg_mask_for(need), need[7] and h is not None, need_seg)
         run.check("bp_forward (replay) / bp_adjoint")
         gs64, lam64 = gs.to(F64).cpu(), lam.to(F64).cpu()
-        out = [None] * 13
+        out = [None] * 14
         if need[1]:
             out[0] = gs64[0:3].T.contiguous()
         if need[2]:
@@ -339,6 +390,8 @@ class _Simulate(torch.autograd.Function):
             out[10] = gp
         if need[13]:
             out[12] = lam64.T.contiguous()
+        if need[14] and run.phys is not None and run.phys.gconc is not None:
+            out[13] = run.phys.gconc.to(F64).cpu()[: run.phys.width].T.contiguous()
         return (None, *[None if v is None or not need[i + 1] else v.to(dtype=ctx.like[i][0], device=ctx.like[i][1])
                         for i, v in enumerate(out)])
 
@@ -354,8 +407,16 @@ def _check_grad_options(options):
                                   "pulses='step' (or torch.no_grad())")
 
 
-def _apply(inp, dev, checkpoint_every, raw: bool):
+def _apply(inp, dev, checkpoint_every, raw: bool, scanner=None):
     S = len(inp.dt)
+    conc, mode = None, 0
+    if scanner is not None:  # encoding positions and concomitant coefficients, differentiable (physics)
+        from dataclasses import replace
+
+        from .physics import spin_fields_torch
+
+        enc, conc, mode = spin_fields_torch(scanner, inp.pos)
+        inp = replace(inp, pos=enc)
     every, outer = (checkpoint_every, 0) if checkpoint_every else choose_checkpoints(S, inp.pd.shape[0])
     if every % _lib.BP_ADJ_WIN:
         raise ValueError(f"checkpoint_every must be a multiple of {_lib.BP_ADJ_WIN}, got {every}")
@@ -365,15 +426,17 @@ def _apply(inp, dev, checkpoint_every, raw: bool):
         z = torch.zeros_like(inp.pd)
         m0 = torch.stack([z, z, inp.pd], -1)
     coils_ri = torch.view_as_real(inp.coils if inp.coils.is_complex() else inp.coils.to(torch.complex64))
-    opts = {"device": dev, "every": every, "outer": outer, "flags": (inp.is_rf, inp.adc, inp.spoil), "raw": raw}
+    opts = {"device": dev, "every": every, "outer": outer, "flags": (inp.is_rf, inp.adc, inp.spoil), "raw": raw,
+            "conc_mode": mode}
     return _Simulate.apply(opts, inp.pos, inp.pd, inp.t1, inp.t2, inp.db0, inp.b1, coils_ri, inp.dt, inp.rf, inp.grad,
-                           inp.adc_phase, inp.b0_offset, m0)
+                           inp.adc_phase, inp.b0_offset, m0, conc)
 
 
-def simulate_grad(inp, dev, checkpoint_every, options) -> SimResult:
-    """``simulate`` with gradients: the inputs as tensors of ``_Simulate``."""
+def simulate_grad(inp, dev, checkpoint_every, options, scanner=None) -> SimResult:
+    """``simulate`` with gradients: the inputs as tensors of ``_Simulate`` (with a scanner field model, the encoding
+    positions and concomitant coefficients from its differentiable host functions)."""
     _check_grad_options(options)
-    sig_ri, m = _apply(inp, dev, checkpoint_every, raw=False)
+    sig_ri, m = _apply(inp, dev, checkpoint_every, raw=False, scanner=scanner)
     return SimResult(torch.view_as_complex(sig_ri.contiguous()), m)
 
 

@@ -120,7 +120,7 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
         raise ValueError(f"m_init must be (N, 3) = ({n}, 3) (or (N, 4) with a bound pool), got {tuple(m_init.shape)}")
     if checkpoint_every is not None and checkpoint_every < 1:
         raise ValueError(f"checkpoint_every must be positive, got {checkpoint_every}")
-    grad = torch.is_grad_enabled() and requires_grad(phantom, seq, coils, m_init)
+    grad = torch.is_grad_enabled() and requires_grad(phantom, seq, coils, m_init, scanner)
     capabilities.check(capabilities.features(phantom, seq, m_init, scanner, maps), grad=grad)
     dev = _device()
     if coils is None:
@@ -131,7 +131,7 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
     if grad:
         from .adjoint import simulate_grad
 
-        return simulate_grad(inp, dev, checkpoint_every, options)
+        return simulate_grad(inp, dev, checkpoint_every, options, scanner)
     bound_only = getattr(seq, "bound_only", None)
     if bound is not None or scanner is not None or (bound_only is not None and any(bound_only)):
         if options.get("readout", "fp32") != "fp32" or options.get("pulses", "step") != "step":

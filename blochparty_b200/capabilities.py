@@ -2,8 +2,8 @@
 
 The feature names and the message follow blochparty ``engines/capabilities.py:12-91`` (``FEATURES``, ``features``,
 ``check``) so that a caller switching engines sees the same ``NotImplementedError`` text pattern. The b200 engine
-runs static spins with B1+ and an initial magnetization, forward and with gradients, and forward also with the
-rate-model bound pool (magnetization transfer, bound-only RF) and the scanner field model; every other feature of the
+runs static spins with B1+, an initial magnetization and the scanner field model, forward and with gradients, and
+forward also with the rate-model bound pool (magnetization transfer, bound-only RF); every other feature of the
 reference's engines is refused here.
 """
 
@@ -23,7 +23,7 @@ FEATURES = {
 }
 SUPPORTED = {
     "forward": frozenset({"b1", "m_init", "bound", "scanner", "bound_only"}),
-    "gradients": frozenset({"b1", "m_init"}),
+    "gradients": frozenset({"b1", "m_init", "scanner"}),
 }
 
 

@@ -24,6 +24,7 @@
 #include <mutex>
 
 #include "bloch_common.cuh"
+#include "physics.cuh"
 #include "../../include/blochparty_b200.h"
 
 #define ADJ_THREADS 128
@@ -66,6 +67,12 @@ struct AdjArgs {
     int seg_mask;         // which of the N_SG segment gradients are reduced (bit k: component k)
     int* status;          // |= BP_ERR_BAD_WINDOW for a window outside the interval (skipped)
     int grid_rows;        // rows of gseg (bp_adjoint's `grid`): a variant that launches fewer CTAs clears the rest
+    // the field model (bp_adjoint_physics, variant PH): concomitant mode, per-spin coefficients [7][n], the segments'
+    // dt-weighted gradient monomials [S][6] (mode 1), and the coefficients' gradient [7][n] (+=, or null)
+    int conc_mode;
+    const float* conc;
+    const double* segq;
+    float* gconc;
 };
 
 // Rodrigues factors of the rotation by |w| (p2 = |w|^2) with the third factor of its left Jacobian:
@@ -107,6 +114,66 @@ __device__ __forceinline__ void offset_grads(float gcyc, const SegRec& q, const 
     sg.v[S_KZ] += gcyc * p.pz;
     sg.v[S_BETA] += gcyc;
     sg.v[S_DT] += gcyc * p.db0;
+}
+
+// The field model in the sweep (variant PH): the spin's concomitant coefficients and the running totals of their
+// gradients.
+struct PhysSpin {
+    int mode;
+    Conc c;
+    float gk[7];
+};
+
+// dL/d(segment phase in cycles) `gcyc` with the field model: the concomitant field's share goes to the spin's
+// coefficients and to the segment's moments and dt, the rest (through the phase's dependence on the linear offset)
+// to offset_grads. Leading order: phase = lin + c . Q, Q = (kx^2, ky^2, kz^2, kx ky, kx kz, ky kz) / dt, so
+// dQ/dk and dQ/ddt (at fixed k) are the gradient monomials' derivatives; exact: phase = lin + E, E = sqrt(U^2 + T2)
+// - U with U = f0 dt + lin and T2 = (ax . k)^2 + (ay . k)^2, dE/dU = -E / S, dE/dT = T / S (S = sqrt(U^2 + T2)).
+// `sq`: the segment's dt-weighted monomials (mode 1).
+template <bool PH>
+__device__ __forceinline__ void phase_grads(float gcyc, const SegRec& q, const Spin& p, float* g, SegGrad& sg,
+                                            PhysSpin* ps, const double* __restrict__ sq) {
+    if constexpr (PH) {
+        const Conc& c = ps->c;
+        if (ps->mode == 1) {
+            float conc = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const float qi = (float)sq[i];
+                conc = fmaf(c.c[i], qi, conc);
+                ps->gk[i] = fmaf(gcyc, qi, ps->gk[i]);
+            }
+            const float idt = q.dt > 0.0f ? 1.0f / q.dt : 0.0f;
+            const float gx = q.kx * idt, gy = q.ky * idt, gz = q.kz * idt;
+            sg.v[S_KX] += gcyc * fmaf(2.0f * c.c[0], gx, fmaf(c.c[3], gy, c.c[4] * gz));
+            sg.v[S_KY] += gcyc * fmaf(2.0f * c.c[1], gy, fmaf(c.c[3], gx, c.c[5] * gz));
+            sg.v[S_KZ] += gcyc * fmaf(2.0f * c.c[2], gz, fmaf(c.c[4], gx, c.c[5] * gy));
+            sg.v[S_DT] -= gcyc * conc * idt;
+        } else if (ps->mode == 2) {
+            const float lin = fmaf(q.kx, p.px, fmaf(q.ky, p.py, fmaf(q.kz, p.pz, fmaf(q.dt, p.db0, q.beta))));
+            const float tx = fmaf(c.c[0], q.kx, fmaf(c.c[1], q.ky, c.c[2] * q.kz));
+            const float ty = fmaf(c.c[3], q.kx, fmaf(c.c[4], q.ky, c.c[5] * q.kz));
+            const float t2 = fmaf(tx, tx, ty * ty);
+            const float u = fmaf(c.c[6], q.dt, lin);
+            const float sr = sqrtf(fmaf(u, u, t2));
+            const float e = t2 > 0.0f ? t2 / (sr + u) : 0.0f;
+            const float isr = sr > 0.0f ? 1.0f / sr : 0.0f;
+            const float de_du = -e * isr, rx = tx * isr, ry = ty * isr;
+            ps->gk[0] = fmaf(gcyc * rx, q.kx, ps->gk[0]);
+            ps->gk[1] = fmaf(gcyc * rx, q.ky, ps->gk[1]);
+            ps->gk[2] = fmaf(gcyc * rx, q.kz, ps->gk[2]);
+            ps->gk[3] = fmaf(gcyc * ry, q.kx, ps->gk[3]);
+            ps->gk[4] = fmaf(gcyc * ry, q.ky, ps->gk[4]);
+            ps->gk[5] = fmaf(gcyc * ry, q.kz, ps->gk[5]);
+            ps->gk[6] = fmaf(gcyc * de_du, q.dt, ps->gk[6]);
+            sg.v[S_KX] += gcyc * fmaf(rx, c.c[0], ry * c.c[3]);
+            sg.v[S_KY] += gcyc * fmaf(rx, c.c[1], ry * c.c[4]);
+            sg.v[S_KZ] += gcyc * fmaf(rx, c.c[2], ry * c.c[5]);
+            sg.v[S_DT] += gcyc * de_du * c.c[6];
+            gcyc *= 1.0f + de_du;  // the linear offset's share
+        }
+    }
+    offset_grads(gcyc, q, p, g, sg);
 }
 
 // The half-step relaxation of an RF segment as the sweep uses it: e1h = expm1(-dt r1 / 2), a1 = 1 + e1h (and
@@ -160,10 +227,11 @@ __device__ __forceinline__ void free_step_plain(const FreeFactors& f, const Spin
 // gradients accumulated. The rotated state n = R m1 comes from the output, m2 = E n + c, by E's inverse (or, with
 // strong relaxation, from the input). dL/dw = J^T (n x a), a = dL/dn and J the rotation's left Jacobian
 // (R(w + d) = exp([J d]x) R(w)): J^T u = s1 u - s2 (w x u) + s3 (w . u) w.
-template <bool SMALL, bool OG, bool SG = true>
+template <bool SMALL, bool OG, bool SG = true, bool PH = false>
 __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const RevRelax& r, float wz, float x0,
                                            float y0, float z0, float ox, float oy, float oz, float& lx, float& ly,
-                                           float& lz, float* g, SegGrad& sg) {
+                                           float& lz, float* g, SegGrad& sg, PhysSpin* ps = nullptr,
+                                           const double* sq = nullptr) {
     const float h = 0.5f * q.dt;
     const float wx = q.wx0 * p.b1, wy = q.wy0 * p.b1;
     const float p2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
@@ -210,7 +278,7 @@ __device__ __forceinline__ void rf_reverse(const SegRec& q, const Spin& p, const
     sg.v[S_WY] += gwy * p.b1;
     if (OG) {  // the offset's and dt's gradients (position, dB0, segment dt, moments, b0_offset)
         sg.v[S_DT] -= 0.5f * (gd1 * p.r1 * a1 + gd2 * p.r2 * a2);
-        offset_grads(-BP_TWO_PI_F * gwz, q, p, g, sg);
+        phase_grads<PH>(-BP_TWO_PI_F * gwz, q, p, g, sg, ps, sq);
     }
 }
 
@@ -248,9 +316,10 @@ __device__ __forceinline__ void rf_back(const SegRec& q, const Spin& p, const Re
 
 // Reverse of a free segment (rotation about z by phi = -2 pi cyc, then exact relaxation). OG: the offset's and dt's
 // gradients are wanted.
-template <bool OG, bool SG = true>
+template <bool OG, bool SG = true, bool PH = false>
 __device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, const FreeFactors& f, float x0, float y0,
-                                             float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg) {
+                                             float z0, float& lx, float& ly, float& lz, float* g, SegGrad& sg,
+                                             PhysSpin* ps = nullptr, const double* sq = nullptr) {
     const float c = f.ch, s = f.sh, a2 = 1.0f + f.e2, a1 = 1.0f + f.e1;
     if (!SG && !OG) {  // lambda alone: no gradient of this segment is wanted (and the input state is not read)
         const float nlx = a2 * fmaf(c, lx, s * ly), nly = a2 * fmaf(-s, lx, c * ly);
@@ -269,7 +338,7 @@ __device__ __forceinline__ void free_reverse(const SegRec& q, const Spin& p, con
     g[G_R1] = fmaf(-gd1 * q.dt, a1, g[G_R1]);
     if (OG) {
         sg.v[S_DT] -= gd2 * p.r2 * a2 + gd1 * p.r1 * a1;
-        offset_grads(-BP_TWO_PI_F * gphi, q, p, g, sg);
+        phase_grads<PH>(-BP_TWO_PI_F * gphi, q, p, g, sg, ps, sq);
     }
 }
 
@@ -297,7 +366,7 @@ __device__ __forceinline__ bool adj_window_ok(const int4& win, const AdjArgs& a)
 // recomputed (a spoil at its end, relaxation too strong to invert, RF and free segments mixed) recomputes each
 // segment's input from the window start in registers (n(n+1)/2 steps instead of n). Its shared memory holds the
 // window's cotangent rows instead, so a sample's coil sum reads shared memory, and five CTAs fit on an SM.
-template <int NCG, bool CG, bool OG, bool SG>
+template <int NCG, bool CG, bool OG, bool SG, bool PH>
 __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG == 1 ? 5 : 4))
     bp_adjoint_kernel(AdjArgs a) {
     static_assert(SG || (!CG && !OG), "coil and offset gradients are per-spin gradients");
@@ -363,6 +432,24 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
         const bool active = j0 < n;
         const int j = active ? j0 : 0;
         const Spin p = load_spin(a.spins, n, j, active);
+        // PH: the spin's concomitant coefficients and their gradients' running totals (as g)
+        PhysSpin ps{};
+        if constexpr (PH) {
+            ps.mode = a.conc_mode;
+            ps.c = load_conc(a.conc, n, j, a.conc_mode);
+#pragma unroll
+            for (int k = 0; k < 7; ++k) ps.gk[k] = (SG && active && a.gconc) ? a.gconc[k * n + j] : 0.0f;
+        }
+        // the segment's rotation about z and free factors (PH: with the concomitant field), s its index in the
+        // sequence
+        auto wz_of = [&](const SegRec& q, int s) -> float {
+            if constexpr (PH) return phys_wz(q, p, ps.mode, ps.c, a.segq + 6 * (size_t)s);
+            return rf_wz(q, p);
+        };
+        auto ff_of = [&](const SegRec& q, const double4& k64, int s) -> FreeFactors {
+            if constexpr (PH) return free_factors_phys(q, k64, p, 1, ps.mode, ps.c, a.segq + 6 * (size_t)s);
+            return free_factors(q, k64, p);
+        };
         float lx = active ? a.lam[j] : 0.0f, ly = active ? a.lam[n + j] : 0.0f, lz = active ? a.lam[2 * n + j] : 0.0f;
         // per-spin gradients: running totals carried in registers through the interval (loaded here, stored after
         // its last window): every contribution is added to the total in segment order, so the results do not
@@ -508,7 +595,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 // after it, when that state is unspoiled and every lane's relaxation is invertible
                 if constexpr (URF && !SG && !OG) {
                     const RevRelax rb = rev_relax(wrec[0].dt, p);
-                    const float wzb = rf_wz(wrec[0], p);
+                    const float wzb = wz_of(wrec[0], win.x);
                     if (!(wrec[nseg - 1].flags & BP_SPOIL) && __all_sync(0xffffffffu, rb.invert)) {
                         float ox = mex, oy = mey, oz = mez;
                         for (int s = nseg - 1; s >= 0; --s) {
@@ -535,8 +622,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 RevRelax rr{0.f, 0.f, 1.f, 1.f, 1.f, 1.f, true};
                 float wz = 0.f;
-                if (URF) rr = rev_relax(wrec[0].dt, p), wz = rf_wz(wrec[0], p);
-                if (KIND == 2) ff = free_factors(wrec[0], wk64[0], p);
+                if (URF) rr = rev_relax(wrec[0].dt, p), wz = wz_of(wrec[0], win.x);
+                if (KIND == 2) ff = ff_of(wrec[0], wk64[0], win.x);
                 // !SG: the state after segments 0 .. upto-1 of the window (before the last one's spoil), recomputed
                 // from the window start with factors of its own (the sweep's are kept)
                 auto state_at = [&](int upto, float& x, float& y, float& z) {
@@ -549,11 +636,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                         if (URF || (KIND == 0 && (q.flags & BP_RF))) {
                             if (KIND == 0) {
                                 if (s == 0 || !(q.flags & BP_SAME_RFDT)) r2 = rev_relax(q.dt, p);
-                                if (s == 0 || !(q.flags & BP_SAME_OFF)) w2 = rf_wz(q, p);
+                                if (s == 0 || !(q.flags & BP_SAME_OFF)) w2 = wz_of(q, win.x + s);
                             }
                             rf_step_plain<KIND == 3>(q, p, r2, w2, x, y, z);
                         } else {
-                            if (KIND == 0 && (s == 0 || !(q.flags & BP_SAME_FREE))) f2 = free_factors(q, wk64[s], p);
+                            if (KIND == 0 && (s == 0 || !(q.flags & BP_SAME_FREE))) f2 = ff_of(q, wk64[s], win.x + s);
                             free_step_plain(f2, p, x, y, z);
                         }
                         if (KIND == 0 && s + 1 < upto && (q.flags & BP_SPOIL)) x = y = 0.0f;
@@ -564,11 +651,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                     if (URF || (KIND == 0 && (q.flags & BP_RF))) {
                         if (KIND == 0) {
                             if (s == 0 || !(q.flags & BP_SAME_RFDT)) rr = rev_relax(q.dt, p);
-                            if (s == 0 || !(q.flags & BP_SAME_OFF)) wz = rf_wz(q, p);
+                            if (s == 0 || !(q.flags & BP_SAME_OFF)) wz = wz_of(q, win.x + s);
                         }
                         rf_step_plain<KIND == 3>(q, p, rr, wz, mx, my, mz);
                     } else {
-                        if (KIND == 0 && (s == 0 || !(q.flags & BP_SAME_FREE))) ff = free_factors(q, wk64[s], p);
+                        if (KIND == 0 && (s == 0 || !(q.flags & BP_SAME_FREE))) ff = ff_of(q, wk64[s], win.x + s);
                         free_step_plain(ff, p, mx, my, mz);
                     }
                     float* sl = slots + (s + 1) * 3 * ADJ_THREADS;
@@ -661,12 +748,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                         // the factors of the segment after this one (swept just before) when they are the same
                         if (KIND == 0) {
                             if (!(f & A_KEEP_RELAX)) rr = rev_relax(q.dt, p);
-                            if (!(f & A_KEEP_WZ)) wz = rf_wz(q, p);
+                            if (!(f & A_KEEP_WZ)) wz = wz_of(q, win.x + s);
                         }
-                        rf_reverse<KIND == 3, OG, SG>(q, p, rr, wz, x0, y0, z0, ox, oy, oz, lx, ly, lz, g, sg);
+                        rf_reverse<KIND == 3, OG, SG, PH>(q, p, rr, wz, x0, y0, z0, ox, oy, oz, lx, ly, lz, g, sg, &ps,
+                                                          PH ? a.segq + 6 * (size_t)(win.x + s) : nullptr);
                     } else {
-                        if (KIND == 0 && !(f & A_KEEP_FREE)) ff = free_factors(q, wk64[s], p);
-                        free_reverse<OG, SG>(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg);
+                        if (KIND == 0 && !(f & A_KEEP_FREE)) ff = ff_of(q, wk64[s], win.x + s);
+                        free_reverse<OG, SG, PH>(q, p, ff, x0, y0, z0, lx, ly, lz, g, sg, &ps,
+                                                 PH ? a.segq + 6 * (size_t)(win.x + s) : nullptr);
                     }
                     if (!(rf_only && KIND == 2)) reduce_seg(s, sg);  // (a uniform free window's RF partials are 0)
                 }
@@ -674,7 +763,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             if (all_rf) {
                 // every rotation of the window below |w| = 1/4 for every spin of the warp: |w|^2 <= b1^2 max(wx0^2 +
                 // wy0^2) + wz^2 (one offset for the window)
-                const float wz0 = rf_wz(wrec[0], p);
+                const float wz0 = wz_of(wrec[0], win.x);
                 const bool small = fmaf(p.b1 * p.b1, *wmax, wz0 * wz0) < 0.0624f;
                 if (__all_sync(0xffffffffu, small))
                     sweep(KindTag<3>{});
@@ -711,6 +800,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             if (SG) {
 #pragma unroll
                 for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] = g[k];
+            }
+            if (PH && SG && a.gconc) {
+#pragma unroll
+                for (int k = 0; k < 7; ++k) a.gconc[k * n + j] = ps.gk[k];
             }
             if (CG) {
 #pragma unroll
@@ -756,15 +849,15 @@ static size_t adj_smem() {
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.
-template <int NCG, bool CG, bool OG, bool SG>
+template <int NCG, bool CG, bool OG, bool SG, bool PH = false>
 static int adj_configure() {
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)adj_smem<NCG, SG>()) != cudaSuccess ||
-            cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            cudaFuncSetAttribute(bp_adjoint_kernel<NCG, CG, OG, SG, PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared) != cudaSuccess)
             return -1;
         configured[dev] = true;
@@ -773,11 +866,11 @@ static int adj_configure() {
 }
 
 // CTAs per SM of one variant, or -1
-template <int NCG, bool CG, bool OG, bool SG>
+template <int NCG, bool CG, bool OG, bool SG, bool PH = false>
 static int adj_per_sm() {
     int per_sm = 0;
-    if (adj_configure<NCG, CG, OG, SG>() < 0 ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG, OG, SG>, ADJ_THREADS,
+    if (adj_configure<NCG, CG, OG, SG, PH>() < 0 ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_adjoint_kernel<NCG, CG, OG, SG, PH>, ADJ_THREADS,
                                                       adj_smem<NCG, SG>()) != cudaSuccess)
         return -1;
     return per_sm > 0 ? per_sm : 1;
@@ -817,16 +910,16 @@ extern "C" int bp_adjoint_grid(int n, int n_coils) {
     }
 }
 
-template <int NCG, bool CG, bool OG, bool SG>
+template <int NCG, bool CG, bool OG, bool SG, bool PH = false>
 static int launch_variant(const AdjArgs& a, int grid, cudaStream_t st) {
-    const int per_sm = adj_per_sm<NCG, CG, OG, SG>();
+    const int per_sm = adj_per_sm<NCG, CG, OG, SG, PH>();
     if (per_sm < 0) return BP_E_LAUNCH;
     const int own = adj_sms() * per_sm, ctas = grid < own ? grid : own;  // one wave of resident CTAs
-    bp_adjoint_kernel<NCG, CG, OG, SG><<<ctas, ADJ_THREADS, adj_smem<NCG, SG>(), st>>>(a);
+    bp_adjoint_kernel<NCG, CG, OG, SG, PH><<<ctas, ADJ_THREADS, adj_smem<NCG, SG>(), st>>>(a);
     return cudaGetLastError() == cudaSuccess ? BP_OK : BP_E_LAUNCH;
 }
 
-template <int NCG>
+template <int NCG, bool PH = false>
 static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
     // the offsets' gradients: wanted unless the caller marks the spins' ones unwanted and wants no segment
     // gradient that uses them (with coil gradients, always computed); the per-spin gradients: wanted unless marked
@@ -834,16 +927,17 @@ static int launch_adj(const AdjArgs& a, int grid, cudaStream_t st) {
     const bool seg_offsets = (a.seg_mask & (BP_SEG_ALL & ~(BP_SEG_WX | BP_SEG_WY))) != 0;
     const bool og = !(a.seg_mask & (BP_SPIN_NO_OFFSETS | BP_SPIN_NONE)) || seg_offsets;
     const bool sg = !(a.seg_mask & BP_SPIN_NONE) || og;
-    if (a.gc) return launch_variant<NCG, true, true, true>(a, grid, st);
-    if (og) return launch_variant<NCG, false, true, true>(a, grid, st);
-    if (sg) return launch_variant<NCG, false, false, true>(a, grid, st);
-    return launch_variant<NCG, false, false, false>(a, grid, st);
+    if (a.gc) return launch_variant<NCG, true, true, true, PH>(a, grid, st);
+    if (og || (PH && a.gconc)) return launch_variant<NCG, false, true, true, PH>(a, grid, st);
+    if (sg) return launch_variant<NCG, false, false, true, PH>(a, grid, st);
+    return launch_variant<NCG, false, false, false, PH>(a, grid, st);
 }
 
-extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs,
-                          const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
-                          const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc,
-                          float* gseg, int seg_mask, int grid, int32_t* status, void* stream) {
+static int adjoint_impl(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                        const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                        const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc,
+                        float* gseg, int seg_mask, int grid, int32_t* status, void* stream, const BpPhysics* ph,
+                        float* gconc) {
     if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg0 < 0 || seg_len < 0 || grid < 1 ||
         n_adc < 0)
         return BP_E_ARG;
@@ -852,17 +946,50 @@ extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_co
     // records and moments are staged by TMA bulk copies (16-byte aligned)
     if ((reinterpret_cast<uintptr_t>(segs) & 15) != 0 || (reinterpret_cast<uintptr_t>(seg64) & 15) != 0)
         return BP_E_ALIGN;
+    if (ph && (ph->mt || ph->conc_mode < 0 || ph->conc_mode > 2 || (ph->conc_mode && !ph->conc) ||
+               (ph->conc_mode == 1 && !ph->segq)))
+        return BP_E_ARG;
     if (wb == wa) return BP_OK;
     AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
               reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, n_adc, lam, gs,
               gc, gseg, seg_mask, status, grid};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (ph && ph->conc_mode) {
+        a.conc_mode = ph->conc_mode;
+        a.conc = ph->conc;
+        a.segq = ph->segq;
+        a.gconc = gconc;
+        switch ((n_coils + 7) / 8) {
+            case 1: return launch_adj<1, true>(a, grid, st);
+            case 2: return launch_adj<2, true>(a, grid, st);
+            case 3: return launch_adj<3, true>(a, grid, st);
+            default: return launch_adj<4, true>(a, grid, st);
+        }
+    }
     switch ((n_coils + 7) / 8) {
         case 1: return launch_adj<1>(a, grid, st);
         case 2: return launch_adj<2>(a, grid, st);
         case 3: return launch_adj<3>(a, grid, st);
         default: return launch_adj<4>(a, grid, st);
     }
+}
+
+extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                          const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                          const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc,
+                          float* gseg, int seg_mask, int grid, int32_t* status, void* stream) {
+    return adjoint_impl(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, n_adc, lam,
+                        gs, gc, gseg, seg_mask, grid, status, stream, nullptr, nullptr);
+}
+
+extern "C" int bp_adjoint_physics(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                                  const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                                  const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc,
+                                  float* gseg, int seg_mask, int grid, const BpPhysics* ph, float* gconc,
+                                  int32_t* status, void* stream) {
+    if (!ph) return BP_E_ARG;
+    return adjoint_impl(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, n_adc, lam,
+                        gs, gc, gseg, seg_mask, grid, status, stream, ph, gconc);
 }
 
 extern "C" int bp_seg_reduce(const float* gseg, int n_cta, int seg_len, int seg0, double* seg, void* stream) {

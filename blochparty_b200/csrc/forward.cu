@@ -624,10 +624,11 @@ extern "C" int bp_forward_physics(const float* spins, const float* sens, int n, 
                                   const double* seg64, const int* windows, int w_begin, int w_end, float* state,
                                   double* raw, int max_ctas, const BpPhysics* ph, int* status, void* stream) {
     FwdArgs a;
-    const int code = fill_args(a, spins, sens, n, n_coils, segs, seg64, windows, w_begin, w_end, state, raw, nullptr,
-                               1, status);
+    if (!ph) return BP_E_ARG;
+    const int code = fill_args(a, spins, sens, n, n_coils, segs, seg64, windows, w_begin, w_end, state, raw,
+                               ph->wstates, ph->wstate_stride, status);
     if (code != BP_OK) return code;
-    if (!ph || ph->conc_mode < 0 || ph->conc_mode > 2) return BP_E_ARG;
+    if (ph->conc_mode < 0 || ph->conc_mode > 2 || (ph->wstates && ph->mt)) return BP_E_ARG;
     if (ph->mt && (!ph->pool || !ph->bstate || !ph->rf_freq || !ph->line)) return BP_E_ARG;
     if (ph->conc_mode && !ph->conc) return BP_E_ARG;
     if (ph->conc_mode == 1 && !ph->segq) return BP_E_ARG;

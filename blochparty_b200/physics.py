@@ -199,66 +199,78 @@ def rf_frequency(dt, rf, is_rf, rf_freq=None) -> np.ndarray:
 # ---------------------------------------------------------------- the field model
 
 
-def solid_harmonics(pos: np.ndarray, n_max: int, r0: float) -> tuple[np.ndarray, np.ndarray]:
+def _t64(v, like: Tensor) -> Tensor:
+    """v as a float64 tensor on like's device, keeping its autograd graph."""
+    if isinstance(v, Tensor):
+        return v.to(dtype=torch.float64, device=like.device)
+    return torch.as_tensor(v, dtype=torch.float64, device=like.device)
+
+
+def solid_harmonics(pos: Tensor, n_max: int, r0: float) -> tuple[Tensor, Tensor]:
     """(N, n_max + 1, n_max + 1) cosine and sine solid harmonics R0 (r/R0)^n N_nm P_n^m(cos theta) (cos m phi,
     sin m phi) (zero for m > n), N_nm = sqrt((2n + 1) (n - m)! / (2 (n + m)!)) for m > 0 and 1 for m = 0, P_n^m
     without the Condon-Shortley phase, in Cartesian form: (x + i y)^m / R0^m, times r^n P_n^m / rho^m from its
     three-term recurrence in n (Q_m^m = (2m - 1)!!, Q_{m+1}^m = (2m + 1) z Q_m^m,
-    (n - m) Q_n^m = (2n - 1) z Q_{n-1}^m - (n + m - 1) r^2 Q_{n-2}^m, in units of R0)."""
-    p = np.asarray(pos, dtype=np.float64) / r0
+    (n - m) Q_n^m = (2n - 1) z Q_{n-1}^m - (n + m - 1) r^2 Q_{n-2}^m, in units of R0). float64 torch, differentiable
+    in the positions."""
+    p = pos / r0
     x, y, z = p[:, 0], p[:, 1], p[:, 2]
     r2 = x * x + y * y + z * z
     L = n_max + 1
-    n = p.shape[0]
-    cs, sn = np.zeros((n, L, L)), np.zeros((n, L, L))
-    cm, sm = np.ones(n), np.zeros(n)  # (x + i y)^m
+    zero = torch.zeros_like(x)
+    cs = [[zero] * L for _ in range(L)]
+    sn = [[zero] * L for _ in range(L)]
+    cm, sm = torch.ones_like(x), torch.zeros_like(x)  # (x + i y)^m
     dfact = 1.0  # (2m - 1)!!
     for m in range(L):
         if m > 0:
             cm, sm = x * cm - y * sm, x * sm + y * cm
             dfact *= 2 * m - 1
-        q_prev, q = None, np.full(n, dfact)
+        q_prev, q = None, torch.full_like(x, dfact)
         for deg in range(m, L):
             if deg == m + 1:
                 q_prev, q = q, (2 * m + 1) * z * q
             elif deg > m + 1:
                 q_prev, q = q, ((2 * deg - 1) * z * q - (deg + m - 1) * r2 * q_prev) / (deg - m)
             norm = 1.0 if m == 0 else math.sqrt((2 * deg + 1) * math.factorial(deg - m) / (2 * math.factorial(deg + m)))
-            cs[:, deg, m] = r0 * norm * q * cm
-            sn[:, deg, m] = r0 * norm * q * sm
-    return cs, sn
+            cs[deg][m] = r0 * norm * q * cm
+            sn[deg][m] = r0 * norm * q * sm
+    stack = lambda t: torch.stack([torch.stack(row, -1) for row in t], -2)
+    return stack(cs), stack(sn)
 
 
-def displacement(nl, pos: np.ndarray) -> np.ndarray:
-    """(N, 3) encoding position minus true position of ``nl`` (alpha, beta (3, L, L), r0)."""
-    alpha, beta = _f64(nl.alpha), _f64(nl.beta)
+def displacement(nl, pos: Tensor) -> Tensor:
+    """(N, 3) encoding position minus true position of ``nl`` (alpha, beta (3, L, L), r0), differentiable in the
+    positions and the coefficients."""
+    alpha, beta = _t64(nl.alpha, pos), _t64(nl.beta, pos)
     L = alpha.shape[-1]
-    keep = np.tril(np.ones((L, L)))
+    keep = torch.ones(L, L, dtype=torch.bool, device=pos.device).tril()
     cs, sn = solid_harmonics(pos, L - 1, float(nl.r0))
-    return np.einsum("pnm,anm->pa", cs, alpha * keep) + np.einsum("pnm,anm->pa", sn, beta * keep)
+    return torch.einsum("pnm,anm->pa", cs, alpha * keep) + torch.einsum("pnm,anm->pa", sn, beta * keep)
 
 
-def transverse_rows(pos: np.ndarray, a: float) -> np.ndarray:
+def transverse_rows(pos: Tensor, a) -> Tensor:
     """(N, 6) rows (ax, ay) of the transverse field (Bx, By) = (ax . g, ay . g) [Hz] of the cylindrical coil set
     (Bx = gx z - a gz x, By = gy z - (1 - a) gz y)."""
     x, y, z = pos[:, 0], pos[:, 1], pos[:, 2]
-    zero = np.zeros_like(x)
-    return np.stack([z, zero, -a * x, zero, z, -(1.0 - a) * y], axis=-1)
+    zero = torch.zeros_like(x)
+    return torch.stack([z, zero, -a * x, zero, z, -(1.0 - a) * y], dim=-1)
 
 
-def concomitant_coefficients(pos: np.ndarray, f0: float, a: float) -> np.ndarray:
+def concomitant_coefficients(pos: Tensor, f0, a) -> Tensor:
     """(N, 6) c with f_c = c . (gx^2, gy^2, gz^2, gx gy, gx gz, gy gz) = (Bx^2 + By^2) / (2 f0) [Hz]."""
     t = transverse_rows(pos, a)
     ax, ay = t[:, :3], t[:, 3:]
     sq = ax * ax + ay * ay
     cross = lambda i, j: 2.0 * (ax[:, i] * ax[:, j] + ay[:, i] * ay[:, j])
-    return np.stack([sq[:, 0], sq[:, 1], sq[:, 2], cross(0, 1), cross(0, 2), cross(1, 2)], axis=-1) / (2.0 * f0)
+    return torch.stack([sq[:, 0], sq[:, 1], sq[:, 2], cross(0, 1), cross(0, 2), cross(1, 2)], dim=-1) / (2.0 * f0)
 
 
-def spin_fields(scanner, pos) -> tuple[np.ndarray, np.ndarray | None, int]:
-    """(encoding positions (N, 3), coefficients (N, 6) or (N, 7) or None, mode 0 / 1 / 2) in float64 for
-    ``scanner`` (None: the ideal scanner) at the true positions ``pos``."""
-    p = _f64(pos)
+def spin_fields_torch(scanner, pos: Tensor) -> tuple[Tensor, Tensor | None, int]:
+    """(encoding positions (N, 3), coefficients (N, 6) or (N, 7) or None, mode 0 / 1 / 2) as float64 tensors on
+    pos's device for ``scanner`` (None: the ideal scanner) at the true positions ``pos``: differentiable in the
+    positions, the nonlinearity's coefficients, the field strength and the z coil's asymmetry."""
+    p = pos.to(torch.float64)
     if scanner is None:
         return p, None, 0
     nl = getattr(scanner, "nonlinearity", None)
@@ -267,11 +279,18 @@ def spin_fields(scanner, pos) -> tuple[np.ndarray, np.ndarray | None, int]:
     b0 = getattr(scanner, "field_strength", None)
     if mode is None or b0 is None:
         return enc, None, 0
-    f0 = GAMMA_BAR * float(_f64(b0))
-    a = float(_f64(getattr(scanner, "z_asymmetry", 0.5)))
+    f0 = GAMMA_BAR * _t64(b0, p)
+    a = _t64(getattr(scanner, "z_asymmetry", 0.5), p)
     if mode == "leading":
         return enc, concomitant_coefficients(p, f0, a), 1
-    return enc, np.concatenate([transverse_rows(p, a), np.full((p.shape[0], 1), f0)], axis=1), 2
+    return enc, torch.cat([transverse_rows(p, a), f0.expand(p.shape[0], 1)], dim=1), 2
+
+
+def spin_fields(scanner, pos) -> tuple[np.ndarray, np.ndarray | None, int]:
+    """``spin_fields_torch`` as float64 numpy arrays (no gradients)."""
+    with torch.no_grad():
+        enc, conc, mode = spin_fields_torch(scanner, torch.as_tensor(_f64(pos)))
+    return enc.numpy(), None if conc is None else conc.numpy(), mode
 
 
 def gradient_moments2(dt, grad) -> np.ndarray:

@@ -143,8 +143,9 @@ int bp_nufft_finish(const double* grid, const int32_t* run_rows, int n_runs, int
  *   conc       [7][n] float32: mode 1 the quadratic form's coefficients c (6; f_c = c . (gx^2, gy^2, gz^2, gx gy,
  *              gx gz, gy gz)); mode 2 the transverse field's rows ax (3), ay (3) and f0 [Hz]
  *   segq       [S][6] float64, mode 1: dt (gx^2, gy^2, gz^2, gx gy, gx gz, gy gz)
+ *   wstates, wstate_stride  as bp_forward's (the replay of the adjoint; without a bound pool), or NULL, 0
  * Positions in `spins` are the encoding positions (gradient nonlinearity applied on the host); the concomitant
- * coefficients come from the true ones. No NUFFT runs, no window states. */
+ * coefficients come from the true ones. No NUFFT runs. */
 #define BP_BOUND_ONLY 128
 typedef struct {
     int mt;
@@ -155,6 +156,8 @@ typedef struct {
     const float* line;
     const float* conc;
     const double* segq;
+    float* wstates;
+    int wstate_stride;
 } BpPhysics;
 int bp_forward_physics(const float* spins, const float* sens, int n, int n_coils, const void* segs,
                        const double* seg64, const int32_t* windows, int w_begin, int w_end, float* state, double* raw,
@@ -227,6 +230,17 @@ int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const 
                const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates, const float* h,
                int n_adc, float* lam, float* gs, float* gc, float* gseg, int seg_mask, int grid, int32_t* status,
                void* stream);
+
+/* bp_adjoint with the scanner field model (gradients through the concomitant field; replaces the V=1 adjoint of
+ * engines/gpu/cuda/adjoint.cu.in:5-121): `ph` as bp_forward_physics's (conc_mode 1 or 2, conc, segq; no bound pool:
+ * mt must be 0), positions the encoding positions. Besides bp_adjoint's outputs, gconc [7][n] (+=, or NULL) receives
+ * dL/d(the concomitant coefficients); the segment gradients include the concomitant field's dependence on the
+ * moments and dt. The spins' position gradient is with respect to the encoding positions (the host chains it
+ * through the nonlinearity). */
+int bp_adjoint_physics(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                       const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                       const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc, float* gseg,
+                       int seg_mask, int grid, const BpPhysics* ph, float* gconc, int32_t* status, void* stream);
 
 /* seg[seg0 + s][k] += sum over the `n_cta` CTAs, in CTA order, of gseg[cta][s][k], in float64 (replaces
  * seg_reduce, engines/gpu/cuda/seg_reduce.cu:3-11). `seg` is [S][8] float64. */

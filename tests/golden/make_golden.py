@@ -283,6 +283,42 @@ def run_physics(name, ph, seq, coils, pool=None, shape=None, bound_only=None, m_
     print(name, "effect of the physics on the signal", f"{effect:.2e}")
 
 
+def field_grad(name, concomitant):
+    """Gradients through the scanner field model: a seeded random case (RF waveforms, gradients x 30, a readout)
+    at 0.55 T with a nonlinearity, the reference's float64 autograd of a fixed linear loss of signal and m with
+    respect to the nonlinearity's alpha, the field strength, T1, the positions, dB0, the RF waveform and the
+    gradients."""
+    from blochparty.fields import GradientNonlinearity, Scanner
+
+    ph, seq, coils = rand_case(21, n=24, n_coils=2)
+    seq.grad = seq.grad * 30
+    alpha, beta, r0 = nonlinearity()
+    leaves = {"alpha": alpha.clone().requires_grad_(), "b0": torch.tensor(0.55, dtype=F64, requires_grad=True),
+              "t1": ph.t1.clone().requires_grad_(), "pos": ph.pos.clone().requires_grad_(),
+              "db0": ph.db0.clone().requires_grad_(), "rf": seq.rf.clone().requires_grad_(),
+              "grad": seq.grad.clone().requires_grad_()}
+    sc = Scanner(field_strength=leaves["b0"], concomitant=concomitant,
+                 nonlinearity=GradientNonlinearity(leaves["alpha"], beta, r0))
+    rph = bp.Phantom(leaves["pos"], ph.pd, leaves["t1"], ph.t2, leaves["db0"], b1=ph.b1)
+    rseq = bp.Sequence(seq.dt, leaves["rf"], leaves["grad"], seq.adc_phase, list(seq.is_rf), list(seq.adc),
+                       list(seq.spoil), {}, seq.b0_offset)
+    r = bp.simulate(rph, rseq, coils, scanner=sc, engine="core")
+    wr, wi, wm = weights_like(r.signal.detach(), r.m.detach())
+    loss = (r.signal.real * wr).sum() + (r.signal.imag * wi).sum() + (r.m * wm).sum()
+    g = dict(zip(leaves, torch.autograd.grad(loss, list(leaves.values()))))
+    out = dict(
+        pos=ph.pos.numpy(), pd=ph.pd.numpy(), t1=ph.t1.numpy(), t2=ph.t2.numpy(), db0=ph.db0.numpy(),
+        b1=ph.b1.numpy(), coils_re=coils.real.numpy(), coils_im=coils.imag.numpy(),
+        dt=seq.dt.numpy(), rf=seq.rf.numpy(), grad=seq.grad.numpy(), adc_phase=seq.adc_phase.numpy(),
+        b0_offset=seq.b0_offset.numpy(), is_rf=np.array(seq.is_rf, bool), adc=np.array(seq.adc, bool),
+        spoil=np.array(seq.spoil, bool), sc_alpha=alpha.numpy(), sc_beta=beta.numpy(), sc_r0=np.array(r0),
+        sc_b0=np.array(0.55), sc_conc=np.array(concomitant), w_re=wr.numpy(), w_im=wi.numpy(), w_m=wm.numpy(),
+        sig_re=r.signal.detach().real.numpy(), sig_im=r.signal.detach().imag.numpy(), m=r.m.detach().numpy(),
+        **{f"grad_{k}": v.numpy() for k, v in g.items()})
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, {k: float(v.abs().max()) for k, v in g.items()})
+
+
 def physics():
     """The bound-pool and field-model fixtures, and the reference's super-Lorentzian table."""
     from blochparty.exchange import _sl_table
@@ -324,6 +360,8 @@ def physics():
     sc = Scanner(field_strength=0.55, concomitant="leading", nonlinearity=GradientNonlinearity(alpha, beta, r0))
     run_physics("mt_field", mph, gseq, gcoils, pool, "superlorentzian", scanner=sc,
                 scanner_args=(0.55, "leading", alpha, beta, r0))
+    field_grad("grad_field_leading", "leading")
+    field_grad("grad_field_exact", "exact")
 
 
 def main():

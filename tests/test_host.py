@@ -164,8 +164,11 @@ def test_refusals_use_the_reference_wording():
                                                   r"is not implemented; use blochparty.simulate \(the core\)"):
         bpb.simulate(ph, seq)
     ph.diffusion = None
-    with pytest.raises(NotImplementedError, match="gradients through the scanner field model"):
-        bpb.simulate(replace(ph, t1=ph.t1.clone().requires_grad_()), seq, scanner=physics.Scanner(0.55))
+    pool = physics.BoundPool(0.1, 30.0, 1.0, 12e-6)
+    with pytest.raises(NotImplementedError, match=r"gradients through a bound pool \(Phantom.bound\)"):
+        bpb.simulate(replace(ph, t1=ph.t1.clone().requires_grad_(), bound=pool), seq)
+    b0 = torch.tensor(0.55, dtype=F64, requires_grad=True)  # a gradient through the scanner alone is one
+    assert bpb.api.requires_grad(ph, seq, None, None, physics.Scanner(b0))
     with pytest.raises(NotImplementedError, match=r"simulating with field maps \(FieldMaps\)"):
         bpb.simulate(ph, seq, maps=object())
     gen = replace(ph, bound=physics.BoundPool(0.1, 30.0, 1.0, 12e-6, model="generalized"))

@@ -104,3 +104,35 @@ def test_3d_slab_gre_with_pool_and_field_model_against_the_oracle():
           + ", ".join(f"{k} {v:.2e}" for k, v in e.items()))
     assert e["signal"] < 1e-4 and e["m"] < 1e-3 and e["m_bound"] < 1e-4, e
     assert e["signal_f32_inputs"] < 1e-5 and e["m_f32_inputs"] < 1e-5, e
+
+
+@pytest.mark.parametrize("name", ["grad_field_leading", "grad_field_exact"])
+def test_field_model_gradients_match_reference_autograd(name):
+    """Gradients through the scanner field model (mirrors blochparty ``tests/engines/test_gpu_grad.py:57-75``): a
+    random case with gradients x 30 at 0.55 T with a nonlinearity, the fixed linear loss of signal and m, against
+    the reference's float64 autograd with respect to the nonlinearity's alpha, the field strength, T1, the positions,
+    dB0, the RF waveform and the gradients. Bars: 2e-4 (largest error over the largest value), 1e-4 on B0 (the
+    reference's own for its GPU engines)."""
+    import numpy as np
+
+    from golden_cases import GOLDEN
+
+    z = np.load(GOLDEN / f"{name}.npz")
+    t = lambda k: torch.from_numpy(z[k]).to(F64)
+    leaves = {"alpha": t("sc_alpha").requires_grad_(), "b0": torch.tensor(float(z["sc_b0"]), dtype=F64,
+                                                                           requires_grad=True),
+              "t1": t("t1").requires_grad_(), "pos": t("pos").requires_grad_(), "db0": t("db0").requires_grad_(),
+              "rf": t("rf").requires_grad_(), "grad": t("grad").requires_grad_()}
+    sc = physics.Scanner(leaves["b0"], str(z["sc_conc"]),
+                         nonlinearity=physics.GradientNonlinearity(leaves["alpha"], t("sc_beta"), float(z["sc_r0"])))
+    ph = bpb.Phantom(leaves["pos"], t("pd"), leaves["t1"], t("t2"), leaves["db0"], b1=t("b1"))
+    seq = bpb.Sequence(t("dt"), leaves["rf"], leaves["grad"], t("adc_phase"), [bool(x) for x in z["is_rf"]],
+                       [bool(x) for x in z["adc"]], [bool(x) for x in z["spoil"]], b0_offset=t("b0_offset"))
+    coils = torch.complex(t("coils_re"), t("coils_im"))
+    r = bpb.simulate(ph, seq, coils, scanner=sc)
+    wr, wi, wm = t("w_re"), t("w_im"), t("w_m")
+    loss = (r.signal.real.double() * wr).sum() + (r.signal.imag.double() * wi).sum() + (r.m.double() * wm).sum()
+    grads = torch.autograd.grad(loss, list(leaves.values()))
+    e = {k: rel(g, t(f"grad_{k}")) for k, g in zip(leaves, grads)}
+    print(f"\n{name}: " + ", ".join(f"{k} {v:.1e}" for k, v in e.items()))
+    assert e["b0"] < 1e-4 and max(e.values()) < 2e-4, e

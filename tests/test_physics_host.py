@@ -76,7 +76,7 @@ def test_solid_harmonics_two_ways():
     """The product's Cartesian recurrences against the oracle's scipy Legendre functions, up to degree 7."""
     g = torch.Generator().manual_seed(5)
     pos = ((torch.rand(300, 3, generator=g, dtype=torch.float64) - 0.5) * 0.4).numpy()
-    a = physics.solid_harmonics(pos, 7, 0.25)
+    a = [t.numpy() for t in physics.solid_harmonics(torch.from_numpy(pos), 7, 0.25)]
     b = ophys._solid(pos, 7, 0.25)
     for x, y in zip(a, b):
         assert np.abs(x - y).max() < 1e-13 * max(1.0, np.abs(y).max())
@@ -92,3 +92,36 @@ def test_oracle_against_the_reference_core(name):
         assert rel(mb_o, mb) < 1e-11
     else:
         assert mb_o is None
+
+
+def test_field_model_host_functions_are_differentiable():
+    """The encoding positions and concomitant coefficients (``physics.spin_fields_torch``) carry gradients to the
+    nonlinearity's coefficients, the field strength and the positions: autograd against central differences."""
+    g = torch.Generator().manual_seed(7)
+    pos = ((torch.rand(40, 3, generator=g, dtype=torch.float64) - 0.5) * 0.3).requires_grad_()
+    alpha = (torch.randn(3, 4, 4, generator=g, dtype=torch.float64) * 0.3).requires_grad_()
+    beta = torch.randn(3, 4, 4, generator=g, dtype=torch.float64) * 0.3
+    b0 = torch.tensor(0.55, dtype=torch.float64, requires_grad=True)
+    wa, wb = torch.randn(40, 3, generator=g, dtype=torch.float64), torch.randn(40, 7, generator=g, dtype=torch.float64)
+
+    def f(pos, alpha, b0, mode):
+        sc = physics.Scanner(b0, mode, nonlinearity=physics.GradientNonlinearity(alpha, beta, 0.25))
+        enc, conc, _ = physics.spin_fields_torch(sc, pos)
+        # (each coefficient scaled to order one: the quadratic form's are ~1e-10, the transverse rows ~0.1 m, f0
+        # 2.3e7 Hz)
+        scale = 1e6 if mode == "leading" else torch.tensor([1.0] * 6 + [1e-7], dtype=torch.float64)
+        return (enc * wa).sum() + (conc * wb[:, : conc.shape[1]] * scale).sum()
+
+    for mode in ("leading", "exact"):
+        ga, gb, gp = torch.autograd.grad(f(pos, alpha, b0, mode), [alpha, b0, pos])
+        h = 1e-6
+        d = torch.zeros_like(alpha)
+        d[0, 3, 1] = 1.0
+        fd = (f(pos, alpha + h * d, b0, mode) - f(pos, alpha - h * d, b0, mode)) / (2 * h)
+        assert abs(float(ga[0, 3, 1]) - float(fd)) <= 1e-6 * max(1.0, abs(float(fd)))
+        fd = (f(pos, alpha, b0 + h, mode) - f(pos, alpha, b0 - h, mode)) / (2 * h)
+        assert abs(float(gb) - float(fd)) <= 1e-6 * max(1.0, abs(float(fd)))
+        dp = torch.zeros_like(pos)
+        dp[5, 2] = 1.0
+        fd = (f(pos + h * dp, alpha, b0, mode) - f(pos - h * dp, alpha, b0, mode)) / (2 * h)
+        assert abs(float(gp[5, 2]) - float(fd)) <= 1e-5 * max(1.0, abs(float(fd)))
