@@ -382,6 +382,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     float2* hsb = reinterpret_cast<float2*>(wk64b + 2 * BP_ADJ_WIN);               // !SG: [2][BP_ADJ_WIN][8 NCG]
     uint64_t* bars = reinterpret_cast<uint64_t*>(hsb + 2 * BP_ADJ_WIN * 8 * NCG);  // !SG: [2]
     float2* iacc = reinterpret_cast<float2*>(bars + 2);  // !SG: [ADJ_SACC_MAX] the interval's RF gradient (x, y)
+    float* mes = reinterpret_cast<float*>(iacc + ADJ_SACC_MAX);  // !SG: [2][6][ADJ_THREADS] the states after windows
     float2* hs = hsb;
     __shared__ float wmax[1];  // the window's largest wx0^2 + wy0^2
     __shared__ unsigned wkind[ADJ_WARPS];  // per warp: a copy timed out (1), not all RF (2), not all free (4)
@@ -403,7 +404,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     // threads copy them, zero-padded); issue(w, b) stages window w into buffer b (thread 0): a window the sweep
     // cannot run, or one without segments, completes the buffer's phase with no data
     const bool h_tma = !SG && a.h != nullptr && 2 * a.n_coils == 16 * NCG && (reinterpret_cast<uintptr_t>(a.h) & 15) == 0;
-    auto issue = [&](int w, int b) {
+    // the tile's state after the window (its six rows of the replay's window states: 128 spins each) comes by TMA
+    // too when every row starts on a 16-byte boundary (n a multiple of 4, the array 16-byte aligned)
+    const bool me_tma = !SG && (n & 3) == 0 && (reinterpret_cast<uintptr_t>(a.wstates) & 15) == 0;
+    auto issue = [&](int w, int b, int t) {
         const int4 win = a.windows[w];
         const int ns = win.y - win.x;
         if (!adj_window_ok(win, a) || ns == 0) {
@@ -412,11 +416,18 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
         }
         const bool th = h_tma && win.w > 0;
         const uint32_t rec_bytes = (uint32_t)ns * sizeof(SegRec), hbytes = th ? (uint32_t)win.w * 64u * NCG : 0u;
+        const int t0 = t * ADJ_THREADS, cnt = min(ADJ_THREADS, n - t0);
+        const uint32_t me_bytes = me_tma ? (uint32_t)cnt * 4u : 0u;  // (a multiple of 16: n and t0 are of 4)
         fence_proxy_async_smem();
-        mbar_expect_tx(&bars[b], 2 * rec_bytes + hbytes);
+        mbar_expect_tx(&bars[b], 2 * rec_bytes + hbytes + 6 * me_bytes);
         tma_load_1d(rawrec + b * BP_ADJ_WIN, a.segs + win.x, rec_bytes, &bars[b]);
         tma_load_1d(wk64b + b * BP_ADJ_WIN, a.seg64 + win.x, rec_bytes, &bars[b]);
         if (th) tma_load_1d(hsb + b * BP_ADJ_WIN * 8 * NCG, a.h + (size_t)win.z * 16 * NCG, hbytes, &bars[b]);
+        if (me_tma) {
+            const float* we = a.wstates + (size_t)(w - a.wa + 1) * 6 * n + t0;
+            for (int k = 0; k < 6; ++k)
+                tma_load_1d(mes + (b * 6 + k) * ADJ_THREADS, we + (size_t)k * n, me_bytes, &bars[b]);
+        }
     };
     int seq = 0;  // !SG: windows this CTA has staged so far (buffer seq & 1, its phase (seq >> 1) & 1)
     if (!SG && tid == 0) {
@@ -425,7 +436,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
         fence_mbar_init();
     }
     __syncthreads();
-    if (!SG && tid == 0 && blockIdx.x < n_tiles && a.wb > a.wa) issue(a.wb - 1, 0);
+    if (!SG && tid == 0 && blockIdx.x < n_tiles && a.wb > a.wa) issue(a.wb - 1, 0, blockIdx.x);
 
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int j0 = tile * ADJ_THREADS + tid;
@@ -480,9 +491,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 // ended the previous window ended every read of it
                 if (tid == 0) {
                     if (w > a.wa)
-                        issue(w - 1, buf ^ 1);
+                        issue(w - 1, buf ^ 1, tile);
                     else if (tile + (int)gridDim.x < n_tiles)
-                        issue(a.wb - 1, buf ^ 1);
+                        issue(a.wb - 1, buf ^ 1, tile + (int)gridDim.x);
                 }
                 ok = mbar_wait_bounded(&bars[buf], (seq >> 1) & 1);  // (a copy of a few KB: never this long)
                 ++seq;
@@ -499,6 +510,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
                 if (SG) {
                     m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j], m0z = ws[2 * n + j] + ws[5 * n + j];
+                } else if (me_tma) {  // staged with the window's records
+                    const float* me = mes + buf * 6 * ADJ_THREADS + tid;
+                    mex = me[0] + me[3 * ADJ_THREADS], mey = me[ADJ_THREADS] + me[4 * ADJ_THREADS];
+                    mez = me[2 * ADJ_THREADS] + me[5 * ADJ_THREADS];
                 } else {
                     const float* we = ws + 6 * (size_t)n;
                     mex = we[j] + we[3 * n + j], mey = we[n + j] + we[4 * n + j], mez = we[2 * n + j] + we[5 * n + j];
@@ -845,7 +860,7 @@ static size_t adj_smem() {
     // segacc, the records, two staging buffers (raw records, moments, cotangent rows), their two mbarriers and the
     // interval's RF gradient
     return common + 2 * (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4) + 8 * NCG * sizeof(float2)) +
-           2 * sizeof(uint64_t) + (size_t)ADJ_SACC_MAX * sizeof(float2);
+           2 * sizeof(uint64_t) + (size_t)ADJ_SACC_MAX * sizeof(float2) + 2 * 6 * ADJ_THREADS * sizeof(float);
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.
