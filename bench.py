@@ -120,9 +120,10 @@ def no_recompute_segments(flags: np.ndarray, windows: np.ndarray):
     return free, rf
 
 
-def grad_flops_per_spin(flags: np.ndarray, n_coils: int, no_spin=None) -> tuple[int, int]:
+def grad_flops_per_spin(flags: np.ndarray, n_coils: int, no_spin=None, replay: bool = True) -> tuple[int, int]:
     """(forward, backward) algorithmic flops per spin of a simulation with gradients (no coil gradients);
-    ``no_spin``: for the sweep without per-spin gradients, ``no_recompute_segments`` of its windows."""
+    ``no_spin``: for the sweep without per-spin gradients, ``no_recompute_segments`` of its windows; ``replay``:
+    whether the backward replays the intervals (not from saved states)."""
     rf = (flags & 1) != 0
     n_adc = int(((flags & 2) != 0).sum())
     fwd = flops_per_spin(flags, n_coils)
@@ -140,7 +141,7 @@ def grad_flops_per_spin(flags: np.ndarray, n_coils: int, no_spin=None) -> tuple[
     n_free_miss = int((~rf & ~lam & ((flags & 8) == 0)).sum())
     recomp = FLOP_RF_RECOMP * n_rf + FLOP_FREE_RECOMP * n_free + FLOP_FACTORS * n_free_miss
     rev = (FLOP_RF_BACK * n_rf_back + FLOP_RF_REV_NO_SPIN * n_rf + FLOP_FREE_LAMBDA * int((~rf).sum()) + adc)
-    return fwd, prop + recomp + rev
+    return fwd, (prop if replay else 0) + recomp + rev
 
 
 class Clocks:
@@ -390,13 +391,15 @@ def run_reference_gpu(args):
 
 
 def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
-    """Forward + adjoint on the resident inputs: the checkpointed forward and the backward (replay, reverse sweep,
-    segment-gradient reduction) of a seeded linear loss of the signal, gradient with respect to the RF waveform
-    (the flip train), K timed steps with CUDA events around each half. Returns the ``fwd_adjoint`` object."""
+    """Forward + adjoint on the resident inputs: the checkpointed forward and the backward (reverse sweep and
+    segment-gradient reduction per interval, from the states the forward saved after every RF run when they fit,
+    else with a replay of each interval first) of a seeded linear loss of the signal, gradient with respect to the
+    RF waveform (the flip train), K timed steps with CUDA events around each half. Returns the ``fwd_adjoint``
+    object."""
     from blochparty_b200 import _lib, adjoint
 
     every, outer = adjoint.choose_checkpoints(S, pk.n)
-    run = adjoint.Checkpointed(pk, every, dev, outer)
+    run = adjoint.Checkpointed(pk, every, dev, outer, saved=not args.replay)
     g = torch.Generator().manual_seed(7)
     w = torch.complex(torch.randn(pk.n_coils, pk.n_adc, generator=g, dtype=torch.float64),
                       torch.randn(pk.n_coils, pk.n_adc, generator=g, dtype=torch.float64))
@@ -432,7 +435,8 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
     f_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in times)
     b_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in times)
     ms = f_ms + b_ms
-    fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils, no_recompute_segments(pk.flags, run.plan.awin))
+    fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils, no_recompute_segments(pk.flags, run.plan.awin),
+                                   replay=run.saved is None)
     peak = ffma_peak_tflops(dev)
     achieved = n * (fwd + bwd) / (ms * 1e-3) / 1e12
     lf, lb = run.launches(True)
@@ -442,9 +446,12 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
         "grad_wrt": "the RF waveform (flip train), seeded linear loss of the signal",
         "checkpoint_every": every, "intervals": len(run.plan.starts),
         "outer_every": run.outer,  # intervals per outer block (0: two levels); its rebuild forward is not counted
+        "states": (f"saved by the forward after each of the {run.saved.n_slots} RF runs (no replay)"
+                   if run.saved is not None else "interval starts, each interval replayed"),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": None, "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU",
-                     "kernel": "bp_forward_kernel (forward, replay) + bp_adjoint_kernel + bp_seg_reduce_kernel",
+                     "kernel": ("bp_forward_kernel (forward" + (")" if run.saved is not None else ", replay)")
+                                + " + bp_adjoint_kernel + bp_seg_reduce_kernel"),
                      "flops_per_spin": {"forward": fwd, "backward": bwd}},
         "gpu_launches": args.steps * (lf + lb), "clocks": clocks.summary(),
     }
@@ -480,6 +487,8 @@ def main():
     ap.add_argument("--cases", default="3d-32,3d-48,3d-64,3d-96,gre3d-128", help="--impl reference_gpu: cases")
     ap.add_argument("--repeat", type=int, default=2, help="--impl reference_gpu: timed runs per case (fastest kept)")
     ap.add_argument("--grad", action="store_true", help="--impl reference_gpu: forward + backward")
+    ap.add_argument("--replay", action="store_true",
+                    help="forward + adjoint: replay every interval instead of the backward from saved states")
     ap.add_argument("--workload", default="gre3d_128_4echo", choices=("gre3d_128_4echo", "gre3d_64"))
     ap.add_argument("--trs", type=int, default=None,
                     help="time the workload's first TRs only (default: 64 for gre3d_128_4echo, all for gre3d_64)")

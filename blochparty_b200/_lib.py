@@ -76,7 +76,8 @@ BP_SPIN_NONE = 0x100  # with seg_mask: no row of the spin gradients is wanted
 ERRORS = {BP_E_ARG: "invalid argument", BP_E_ALIGN: "misaligned buffer", BP_E_LAUNCH: "CUDA launch failed",
           BP_E_SIZE: "size above the documented maximum"}
 STATUS_BITS = {1: "a TMA copy of a segment block did not complete (bounded wait gave up)",
-               2: "a window record was invalid (outside the sequence, the interval or the samples)"}
+               2: "a window record was invalid (outside the sequence, the interval or the samples)",
+               4: "the sweep from saved states met a window whose states were not saved"}
 
 _P = c_void_p
 # (restype, argtypes) of every exported entry point, as declared in include/blochparty_b200.h
@@ -96,6 +97,9 @@ SIGNATURES = {
     "bp_adjoint_grid": (c_int, [c_int, c_int]),
     "bp_adjoint": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, c_int, _P, _P, _P,
                            _P, c_int, c_int, _P, _P]),
+    "bp_adjoint_saved": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P, c_int, _P,
+                                 c_int, _P, _P, c_int, c_int, _P, _P]),
+    "bp_forward_saving": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, _P, _P, _P, _P, c_int, _P, _P]),
     "bp_adjoint_physics": (c_int, [_P, _P, c_int, c_int, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, c_int, _P,
                                    _P, _P, _P, c_int, c_int, _P, _P, _P, _P]),
     "bp_seg_reduce": (c_int, [_P, c_int, c_int, c_int, _P, _P]),

@@ -88,21 +88,87 @@ def run_breaks(flags: np.ndarray) -> np.ndarray:
     return out
 
 
-class Plan:
-    """Windows and intervals of one gradient-carrying simulation."""
+class SavedStates:
+    """Where the backward without a replay (``bp_adjoint_saved``) needs states: for adjoint windows ``awin`` whose
+    every window is either RF segments with one dt and offset, no sample and no spoil (``rf[w]``: integrated backward
+    from the state after it), or free segments with one set of factors spoiling at most in its last segment (lambda
+    alone), the state after each run of RF windows. ``slot`` [W + 1] int32: the slot of the state at window w's start
+    (-1: none); ``points``: the segments whose start states are saved, slots 0, 1, ... in order, and ``final``
+    whether the state after the last segment is saved too (the last slot). ``of(flags, awin)`` is None when some
+    window is of neither kind."""
 
-    def __init__(self, pk: engine.Packed, every: int, device):
+    def __init__(self, rf, slot, points, final):
+        self.rf, self.slot, self.points, self.final = rf, slot, points, final
+        self.n_slots = len(points) + int(final)
+
+    @classmethod
+    def of(cls, flags: np.ndarray, awin: np.ndarray):
+        W = awin.shape[0]
+        if W == 0:
+            return None
+        s0, s1 = awin[:, 0].astype(np.int64), awin[:, 1].astype(np.int64)
+        if (s1 <= s0).any():
+            return None
+        count = lambda b: np.add.reduceat(b.astype(np.int64), s0)  # per window
+        is_rf = (flags & engine.RF) != 0
+        spoil = (flags & engine.SPOIL) != 0
+        no_off = (flags & engine.SAME_OFF) == 0
+        no_free = (flags & engine.SAME_FREE) == 0
+        rf = ((count(~is_rf) == 0) & (count((flags & (engine.ADC | engine.SPOIL)) != 0) == 0)
+              & (count(no_off) - no_off[s0] == 0))
+        free = (count(is_rf) == 0) & (count(spoil) - spoil[s1 - 1] == 0) & (count(no_free) - no_free[s0] == 0)
+        if not (rf | free).all():
+            return None
+        nxt = np.append(rf[1:], False)
+        ends = np.flatnonzero(rf & ~nxt) + 1  # windows (or W: the end) whose start follows a run of RF windows
+        slot = np.full(W + 1, -1, dtype=np.int32)
+        slot[ends] = np.arange(len(ends), dtype=np.int32)
+        final = bool(len(ends) and ends[-1] == W)
+        points = awin[ends[:-1] if final else ends, 0].astype(np.int64)
+        return cls(rf, slot, points, final)
+
+
+def rf_relaxation_invertible(pk: engine.Packed) -> bool:
+    """Whether every spin's half-step relaxation over every RF segment keeps 1 + expm1(-dt r / 2) >= 1/2 (the
+    backward integration divides by it) with a margin: dt r <= 1.35 (2 ln 2 = 1.386) for the longest RF segment."""
+    rf = (pk.flags & engine.RF) != 0
+    if not rf.any():
+        return True
+    dt = float(pk.segs[torch.from_numpy(np.flatnonzero(rf)).to(pk.segs.device), 0].max())
+    r = float(torch.maximum(pk.spins[4], pk.spins[5]).max())
+    return dt * r <= 1.35
+
+
+class Plan:
+    """Windows and intervals of one gradient-carrying simulation. ``saved``: plan the states of the backward
+    without a replay (``self.saved``, a ``SavedStates``, or None where it does not apply); the forward's windows
+    then also start at every saved point."""
+
+    def __init__(self, pk: engine.Packed, every: int, device, saved: bool = False):
         S = pk.flags.shape[0]
         self.every = every
         self.starts = list(range(0, S, every))
         breaks = np.zeros(S, dtype=np.uint8)
         breaks[self.starts] = 1
         samp = _lib.lib().bp_forward_samp_max(pk.n_coils)
-        self.fwin = engine.plan_windows(pk.flags, samp, breaks=breaks)
         w = _lib.BP_ADJ_WIN
         self.awin = engine.plan_windows(pk.flags, w, seg_max=w, breaks=breaks | run_breaks(pk.flags))
+        self.saved = SavedStates.of(pk.flags, self.awin) if saved else None
+        fbreaks = breaks.copy()
+        if self.saved is not None:
+            # (a cut after an RF segment: no readout run of the forward is split, its states keep their bits)
+            fbreaks[self.saved.points] = 1
+        self.fwin = engine.plan_windows(pk.flags, samp, breaks=fbreaks)
         self.fwin_dev = torch.from_numpy(self.fwin).to(device)
         self.awin_dev = torch.from_numpy(self.awin).to(device)
+        if self.saved is not None:
+            fslot = np.full(self.fwin.shape[0], -1, dtype=np.int32)
+            at = np.searchsorted(self.fwin[:, 0], self.saved.points)
+            if not (self.fwin[at, 0] == self.saved.points).all():
+                raise RuntimeError("the forward's windows do not start at the saved points")
+            fslot[at] = np.arange(len(at), dtype=np.int32)
+            self.fslot_dev = torch.from_numpy(fslot).to(device)
+            self.aslot_dev = torch.from_numpy(self.saved.slot).to(device)
         # window ranges of every interval
         fstart, astart = self.fwin[:, 0], self.awin[:, 0]
         self.franges, self.aranges, self.seg_ranges = [], [], []
@@ -125,21 +191,35 @@ class Checkpointed:
     by the C ABI's workspace query (``bp_forward_workspace_bytes``, ``bp_adjoint_workspace_bytes``); the backward's
     buffers are allocated on its first call and reused."""
 
-    def __init__(self, pk: engine.Packed, every: int, device, outer: int = 0, phys=None):
+    def __init__(self, pk: engine.Packed, every: int, device, outer: int = 0, phys=None, saved: bool = False,
+                 budget_bytes: int | None = None):
         self.pk, self.dev = pk, device
         self.phys = phys  # the field model (``PhysGrad``): the forward, replay and sweep take its variants
-        self.plan = plan = Plan(pk, every, device)
+        # saved: the caller wants the RF waveform's gradient alone; then, where the sequence's windows allow it and
+        # the states fit half the free memory (or ``budget_bytes``), the forward saves the states after every run
+        # of RF windows and the backward needs no replay (bp_forward_saving, bp_adjoint_saved)
+        want = saved and phys is None and rf_relaxation_invertible(pk)
+        self.plan = plan = Plan(pk, every, device, saved=want)
+        if plan.saved is not None:
+            if budget_bytes is None:
+                budget_bytes = torch.cuda.mem_get_info(device)[0] // 2 if torch.cuda.is_available() else 1 << 62
+            if plan.saved.n_slots * 24 * pk.n > budget_bytes:
+                plan.saved = None
+        self.saved = plan.saved
         k = len(plan.starts)
-        self.outer = outer if outer > 1 and k > outer else 0
+        self.outer = outer if outer > 1 and k > outer and self.saved is None else 0
         fws = _lib.forward_workspace(pk.n, pk.n_adc, pk.n_coils)
         self.grid = _lib.lib().bp_adjoint_grid(pk.n, pk.n_coils)
         if self.grid < 1:
             raise RuntimeError("bp_adjoint_grid failed")
         self.ws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, every, plan.max_aw, self.grid,
                                          self.outer)
-        # interval starts (two levels), or block starts followed by one block's interval starts (three)
-        n_states = k if not self.outer else (k + self.outer - 1) // self.outer + self.outer
-        self.ckpts = sized(self.ws.checkpoints, (n_states, 6, pk.n), F32, device)
+        if self.saved is None:
+            # interval starts (two levels), or block starts followed by one block's interval starts (three)
+            n_states = k if not self.outer else (k + self.outer - 1) // self.outer + self.outer
+            self.ckpts = sized(self.ws.checkpoints, (n_states, 6, pk.n), F32, device)
+        else:  # the saved states, by slot (not in the workspace query: their count is the sequence's)
+            self.ckpts = torch.empty(self.saved.n_slots, 6, pk.n, dtype=F32, device=device)
         self.raw = sized(fws.raw, (max(pk.n_adc, 1), 2 * pk.n_coils), F64, device, zero=True)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self._bufs = None
@@ -155,6 +235,15 @@ class Checkpointed:
         the state at every interval start (at every block start with an outer level) into the checkpoints."""
         pk, plan = self.pk, self.plan
         self.raw.zero_()
+        if self.saved is not None:  # one launch, saving the states the backward needs
+            code = _lib.lib().bp_forward_saving(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs),
+                                                ptr(pk.seg64), ptr(plan.fwin_dev), 0, plan.fwin.shape[0], ptr(state),
+                                                ptr(self.raw if pk.n_adc else None), ptr(plan.fslot_dev),
+                                                ptr(self.ckpts), 0, ptr(self.status), _lib.stream_ptr())
+            _lib.check(code, "bp_forward_saving")
+            if self.saved.final:
+                self.ckpts[-1].copy_(state)
+            return
         for k, (fa, fb) in enumerate(plan.franges):
             if not self.outer:
                 self.ckpts[k].copy_(state)
@@ -181,9 +270,12 @@ class Checkpointed:
     def buffers(self, need_seg: bool, want_gc: bool):
         pk, plan, ws, dev = self.pk, self.plan, self.ws, self.dev
         if self._bufs is None:
-            self._bufs = {"gs": sized(ws.gs, (8, pk.n), F32, dev), "seg": sized(ws.seg, (pk.flags.shape[0], 8), F64, dev),
-                          "wstates": sized(ws.wstates, (plan.max_aw + 1, 6, pk.n), F32, dev),
-                          "state": sized(ws.replay_state, (6, pk.n), F32, dev)}
+            self._bufs = {"gs": sized(ws.gs, (8, pk.n), F32, dev), "seg": sized(ws.seg, (pk.flags.shape[0], 8), F64, dev)}
+            if self.saved is None:
+                self._bufs["wstates"] = sized(ws.wstates, (plan.max_aw + 1, 6, pk.n), F32, dev)
+                self._bufs["state"] = sized(ws.replay_state, (6, pk.n), F32, dev)
+            else:  # the chain's state between intervals
+                self._bufs["chain"] = torch.zeros(3, pk.n, dtype=F32, device=dev)
         b = self._bufs
         if need_seg and "gseg" not in b:
             b["gseg"] = sized(ws.gseg, (self.grid, plan.max_len, 8), F32, dev)
@@ -198,7 +290,7 @@ class Checkpointed:
         is checked by ``check``."""
         pk, plan = self.pk, self.plan
         b = self.buffers(need_seg, want_gc)
-        gs, seg, wstates, state = b["gs"], b["seg"], b["wstates"], b["state"]
+        gs, seg, wstates, state = b["gs"], b["seg"], b.get("wstates"), b.get("state")
         gc, gseg = (b["gc"] if want_gc else None), (b["gseg"] if need_seg else None)
         gs.zero_()
         seg.zero_()
@@ -206,6 +298,9 @@ class Checkpointed:
             gc.zero_()
         if self.phys is not None and self.phys.gconc is not None:
             self.phys.gconc.zero_()
+        if self.saved is not None:
+            self._saved_backward(h, lam, gseg if need_seg else None, seg, seg_mask, want_gc, b["chain"])
+            return gs, gc, seg
         n_blocks = len(self.blocks())
         for bi, (ka, kb) in reversed(list(enumerate(self.blocks()))):
             if self.outer:  # this block's interval starts, from its start (no readout)
@@ -244,9 +339,30 @@ class Checkpointed:
         if need_seg:
             _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
 
+    def _saved_backward(self, h, lam, gseg, seg, seg_mask, want_gc, chain):
+        """The backward without a replay: per interval in reverse, the sweep from the saved states, carrying the
+        chain of RF windows integrated backward across the intervals, and the segment reduction."""
+        pk, plan, sv = self.pk, self.plan, self.saved
+        lib, stream, W = _lib.lib(), _lib.stream_ptr(), plan.awin.shape[0]
+        if want_gc or not rf_only(seg_mask):
+            raise ValueError("the backward from saved states forms the RF waveform's gradient alone")
+        for k in reversed(range(len(plan.starts))):
+            aa, ab = plan.aranges[k]
+            s0, s1 = plan.seg_ranges[k]
+            chain_in = int(ab < W and bool(sv.rf[ab]))
+            code = lib.bp_adjoint_saved(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
+                                        ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(self.ckpts), ptr(plan.aslot_dev),
+                                        ptr(chain), chain_in, ptr(h), pk.n_adc, ptr(lam), ptr(gseg), seg_mask,
+                                        self.grid, ptr(self.status), stream)
+            _lib.check(code, "bp_adjoint_saved")
+            if gseg is not None:
+                _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
+
     def launches(self, need_seg: bool) -> tuple[int, int]:
         """(forward, backward) kernel launches of one call each."""
         k = len(self.plan.starts)
+        if self.saved is not None:
+            return 1, k * (2 if need_seg else 1)
         rebuild = sum(kb - ka - 1 for ka, kb in self.blocks()) if self.outer else 0
         return k, k * (3 if need_seg else 2) + rebuild
 
@@ -285,6 +401,12 @@ class PhysGrad:
         self.width = conc.shape[1]
 
 
+def rf_only(seg_mask: int) -> bool:
+    """Whether ``seg_mask`` asks for the RF waveform's gradient alone (no per-spin, coil or offset gradient): the
+    sweep that ``bp_adjoint_saved`` runs."""
+    return bool(seg_mask & _lib.BP_SPIN_NONE) and not seg_mask & _lib.BP_SEG_ALL & ~(_lib.BP_SEG_WX | _lib.BP_SEG_WY)
+
+
 def seg_mask_for(need) -> int:
     """The segment gradients the chain rules use (``need``: ``_Simulate``'s needs_input_grad): dt needs all of
     them (the record's every field scales with dt), the RF its two components, the gradient the moments,
@@ -312,7 +434,9 @@ class _Simulate(torch.autograd.Function):
         phys = None
         if conc is not None:  # the field model's concomitant coefficients (positions: the encoding ones)
             phys = PhysGrad(conc, opts["conc_mode"], inp.dt, inp.grad, dev, ctx.needs_input_grad[14])
-        run = Checkpointed(pk, every, dev, opts.get("outer", 0), phys)
+        # the RF waveform's gradient alone: the backward from saved states where the sequence allows it
+        run = Checkpointed(pk, every, dev, opts.get("outer", 0), phys,
+                           saved=opts.get("saved", True) and rf_only(seg_mask_for(ctx.needs_input_grad)))
         state = engine.initial_state(inp.pd, inp.m_init, dev)
         run.forward(state)
         sig = engine.finish_signal(pk, run.raw)

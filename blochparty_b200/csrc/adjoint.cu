@@ -73,6 +73,14 @@ struct AdjArgs {
     const float* conc;
     const double* segq;
     float* gconc;
+    // the sweep from saved states (bp_adjoint_saved; variant !SG): wstates holds states by slot and wslot[w] is the
+    // slot of the state at window w's start (-1: not saved). A window of RF segments takes the state after it from
+    // the window after it when that one was integrated backward too (its start state, carried in registers: the
+    // chain), else from the slot of the next window's start. chain [3][n] carries the chain between calls: read at
+    // the start when chain_in (window wb was integrated backward), written at the end (window wa's start state).
+    const int* wslot;
+    float* chain;
+    int chain_in;
 };
 
 // Rodrigues factors of the rotation by |w| (p2 = |w|^2) with the third factor of its left Jacobian:
@@ -407,6 +415,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     // the tile's state after the window (its six rows of the replay's window states: 128 spins each) comes by TMA
     // too when every row starts on a 16-byte boundary (n a multiple of 4, the array 16-byte aligned)
     const bool me_tma = !SG && (n & 3) == 0 && (reinterpret_cast<uintptr_t>(a.wstates) & 15) == 0;
+    // !SG: the rows of the state after window w (the next window's start), or null where it was not saved
+    auto after_state = [&](int w) -> const float* {
+        if (a.wslot) {
+            const int sl = a.wslot[w + 1];
+            return sl >= 0 ? a.wstates + (size_t)sl * 6 * n : nullptr;
+        }
+        return a.wstates + (size_t)(w - a.wa + 1) * 6 * n;
+    };
     auto issue = [&](int w, int b, int t) {
         const int4 win = a.windows[w];
         const int ns = win.y - win.x;
@@ -417,17 +433,16 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
         const bool th = h_tma && win.w > 0;
         const uint32_t rec_bytes = (uint32_t)ns * sizeof(SegRec), hbytes = th ? (uint32_t)win.w * 64u * NCG : 0u;
         const int t0 = t * ADJ_THREADS, cnt = min(ADJ_THREADS, n - t0);
-        const uint32_t me_bytes = me_tma ? (uint32_t)cnt * 4u : 0u;  // (a multiple of 16: n and t0 are of 4)
+        const float* we = after_state(w);
+        const uint32_t me_bytes = (me_tma && we) ? (uint32_t)cnt * 4u : 0u;  // (a multiple of 16: n, t0 are of 4)
         fence_proxy_async_smem();
         mbar_expect_tx(&bars[b], 2 * rec_bytes + hbytes + 6 * me_bytes);
         tma_load_1d(rawrec + b * BP_ADJ_WIN, a.segs + win.x, rec_bytes, &bars[b]);
         tma_load_1d(wk64b + b * BP_ADJ_WIN, a.seg64 + win.x, rec_bytes, &bars[b]);
         if (th) tma_load_1d(hsb + b * BP_ADJ_WIN * 8 * NCG, a.h + (size_t)win.z * 16 * NCG, hbytes, &bars[b]);
-        if (me_tma) {
-            const float* we = a.wstates + (size_t)(w - a.wa + 1) * 6 * n + t0;
+        if (me_bytes)
             for (int k = 0; k < 6; ++k)
-                tma_load_1d(mes + (b * 6 + k) * ADJ_THREADS, we + (size_t)k * n, me_bytes, &bars[b]);
-        }
+                tma_load_1d(mes + (b * 6 + k) * ADJ_THREADS, we + t0 + (size_t)k * n, me_bytes, &bars[b]);
     };
     int seq = 0;  // !SG: windows this CTA has staged so far (buffer seq & 1, its phase (seq >> 1) & 1)
     if (!SG && tid == 0) {
@@ -462,6 +477,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             return free_factors(q, k64, p);
         };
         float lx = active ? a.lam[j] : 0.0f, ly = active ? a.lam[n + j] : 0.0f, lz = active ? a.lam[2 * n + j] : 0.0f;
+        // from saved states: the chain (the start state of the window swept last, when it was integrated backward)
+        const bool saved = !SG && a.wslot != nullptr;
+        bool chain_ok = saved && a.chain_in != 0, no_state = false;
+        float cx = 0.f, cy = 0.f, cz = 0.f;
+        if (chain_ok && active) cx = a.chain[j], cy = a.chain[n + j], cz = a.chain[2 * n + j];
         // per-spin gradients: running totals carried in registers through the interval (loaded here, stored after
         // its last window): every contribution is added to the total in segment order, so the results do not
         // depend on where the checkpoint intervals fall
@@ -506,16 +526,18 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             // start, or the interval's end: RF windows integrate backward from it), its start only where a window
             // recomputes (loaded there)
             float m0x = 0.f, m0y = 0.f, m0z = 0.f, mex = 0.f, mey = 0.f, mez = 0.f;
+            const float* we = SG ? nullptr : after_state(w);
+            const bool chain_in_w = chain_ok;  // the window after this one was integrated backward (saved states)
+            chain_ok = false;
             if (active && nseg > 0) {
-                const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
                 if (SG) {
+                    const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
                     m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j], m0z = ws[2 * n + j] + ws[5 * n + j];
-                } else if (me_tma) {  // staged with the window's records
+                } else if (we && me_tma) {  // staged with the window's records
                     const float* me = mes + buf * 6 * ADJ_THREADS + tid;
                     mex = me[0] + me[3 * ADJ_THREADS], mey = me[ADJ_THREADS] + me[4 * ADJ_THREADS];
                     mez = me[2 * ADJ_THREADS] + me[5 * ADJ_THREADS];
-                } else {
-                    const float* we = ws + 6 * (size_t)n;
+                } else if (we) {
                     mex = we[j] + we[3 * n + j], mey = we[n + j] + we[4 * n + j], mez = we[2 * n + j] + we[5 * n + j];
                 }
             }
@@ -611,8 +633,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 if constexpr (URF && !SG && !OG) {
                     const RevRelax rb = rev_relax(wrec[0].dt, p);
                     const float wzb = wz_of(wrec[0], win.x);
-                    if (!(wrec[nseg - 1].flags & BP_SPOIL) && __all_sync(0xffffffffu, rb.invert)) {
-                        float ox = mex, oy = mey, oz = mez;
+                    const bool from_chain = saved && chain_in_w;
+                    if (!(wrec[nseg - 1].flags & BP_SPOIL) && __all_sync(0xffffffffu, rb.invert) &&
+                        (from_chain || we != nullptr)) {
+                        float ox = from_chain ? cx : mex, oy = from_chain ? cy : mey, oz = from_chain ? cz : mez;
                         for (int s = nseg - 1; s >= 0; --s) {
                             SegGrad sg;
 #pragma unroll
@@ -620,12 +644,17 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                             rf_back<KIND == 3>(wrec[s], p, rb, wzb, ox, oy, oz, lx, ly, lz, sg);
                             reduce_seg(s, sg);
                         }
+                        if (saved) cx = ox, cy = oy, cz = oz, chain_ok = true;  // the state after the window before
                         return;
                     }
                 }
                 // recompute the window in plain float32 from its (compensated) start state: slot k = state after
                 // segment k-1 (before its spoil), slot 0 = window start
-                if constexpr (!SG) {  // (loaded only here: the windows that recompute)
+                if constexpr (!SG && !LAMBDA_ONLY) {  // (loaded only here: the windows that recompute)
+                    if (saved) {  // no window start states were saved: this window cannot be swept (reported)
+                        no_state = true;
+                        return;
+                    }
                     if (active) {
                         const float* ws = a.wstates + (size_t)(w - a.wa) * 6 * n;
                         m0x = ws[j] + ws[3 * n + j], m0y = ws[n + j] + ws[4 * n + j];
@@ -810,8 +839,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             }
             __syncthreads();
         }
+        if (no_state && lane == 0) atomicOr(a.status, BP_ERR_NO_STATE);
         if (active) {
             a.lam[j] = lx, a.lam[n + j] = ly, a.lam[2 * n + j] = lz;
+            if (saved && a.chain) a.chain[j] = cx, a.chain[n + j] = cy, a.chain[2 * n + j] = cz;
             if (SG) {
 #pragma unroll
                 for (int k = 0; k < N_GS; ++k) a.gs[k * n + j] = g[k];
@@ -952,11 +983,16 @@ static int adjoint_impl(const float* spins, const float* sens, int n, int n_coil
                         const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
                         const float* wstates, const float* h, int n_adc, float* lam, float* gs, float* gc,
                         float* gseg, int seg_mask, int grid, int32_t* status, void* stream, const BpPhysics* ph,
-                        float* gconc) {
+                        float* gconc, const int32_t* wslot = nullptr, float* chain = nullptr, int chain_in = 0) {
     if (n < 1 || n_coils < 1 || n_coils > BP_MAX_COILS || wa < 0 || wb < wa || seg0 < 0 || seg_len < 0 || grid < 1 ||
         n_adc < 0)
         return BP_E_ARG;
-    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || !gs || !status) return BP_E_ARG;
+    if (!spins || !sens || !segs || !seg64 || !windows || !wstates || !lam || (!gs && !wslot) || !status)
+        return BP_E_ARG;
+    // from saved states: only the sweep without per-spin, coil and offset gradients (the RF's alone)
+    if (wslot && (!chain || ph || gc || !(seg_mask & BP_SPIN_NONE) ||
+                  (seg_mask & (BP_SEG_ALL & ~(BP_SEG_WX | BP_SEG_WY))) != 0))
+        return BP_E_ARG;
     if ((reinterpret_cast<uintptr_t>(h) & 7) != 0) return BP_E_ALIGN;  // read as (re, im) pairs
     // records and moments are staged by TMA bulk copies (16-byte aligned)
     if ((reinterpret_cast<uintptr_t>(segs) & 15) != 0 || (reinterpret_cast<uintptr_t>(seg64) & 15) != 0)
@@ -968,6 +1004,9 @@ static int adjoint_impl(const float* spins, const float* sens, int n, int n_coil
     AdjArgs a{spins, sens, static_cast<const SegRec*>(segs), reinterpret_cast<const double4*>(seg64),
               reinterpret_cast<const int4*>(windows), n, n_coils, wa, wb, seg0, seg_len, wstates, h, n_adc, lam, gs,
               gc, gseg, seg_mask, status, grid};
+    a.wslot = wslot;
+    a.chain = chain;
+    a.chain_in = chain_in;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (ph && ph->conc_mode) {
         a.conc_mode = ph->conc_mode;
@@ -995,6 +1034,17 @@ extern "C" int bp_adjoint(const float* spins, const float* sens, int n, int n_co
                           float* gseg, int seg_mask, int grid, int32_t* status, void* stream) {
     return adjoint_impl(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, n_adc, lam,
                         gs, gc, gseg, seg_mask, grid, status, stream, nullptr, nullptr);
+}
+
+extern "C" int bp_adjoint_saved(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                                const double* seg64, const int32_t* windows, int wa, int wb, int seg0, int seg_len,
+                                const float* wstates, const int32_t* wslot, float* chain, int chain_in,
+                                const float* h, int n_adc, float* lam, float* gseg, int seg_mask, int grid,
+                                int32_t* status, void* stream) {
+    if (!wslot) return BP_E_ARG;
+    return adjoint_impl(spins, sens, n, n_coils, segs, seg64, windows, wa, wb, seg0, seg_len, wstates, h, n_adc, lam,
+                        nullptr, nullptr, gseg, seg_mask, grid, status, stream, nullptr, nullptr, wslot, chain,
+                        chain_in);
 }
 
 extern "C" int bp_adjoint_physics(const float* spins, const float* sens, int n, int n_coils, const void* segs,

@@ -29,6 +29,7 @@
 // status bits written by the kernels (read by the host after the launch)
 #define BP_ERR_TMA_TIMEOUT 1
 #define BP_ERR_BAD_WINDOW 2
+#define BP_ERR_NO_STATE 4  // the sweep from saved states met a window whose states were not saved (results invalid)
 
 // One segment, 32 bytes: what every spin needs, derived on the host in float64.
 struct __align__(16) SegRec {

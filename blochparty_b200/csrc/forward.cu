@@ -65,6 +65,7 @@ struct FwdArgs {
     double* raw;          // [n_adc][2C] raw coil sums (float64 atomics), or null: no readout
     float* wstates;       // null, or [(w_end - w_begin) / stride rounded up][6][n]: state at window starts
     int wstate_stride;
+    const int* wslot;     // null, or [n_windows]: the slot of wstates that takes window w's start state (-1: none)
     int* status;
     NufArgs nu;           // NUFFT readout runs (bp_forward_nufft only)
     PhysArgs ph;          // the bound pool and the field model (bp_forward_physics only)
@@ -194,7 +195,12 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
         const int nseg = win.y - win.x;
         const int nrun = NUF ? a.nu.run_of[w] : -1;  // a NUFFT readout run (the same for the whole CTA)
         const bool readout = a.raw != nullptr && (win.w > 0 || nrun >= 0);
-        const bool save = a.wstates != nullptr && (i % a.wstate_stride) == 0;
+        // the wstates slot that takes this window's start state, or -1
+        const int wsl = a.wstates == nullptr                ? -1
+                        : a.wslot                           ? a.wslot[w]
+                        : (i % a.wstate_stride) == 0 ? i / a.wstate_stride
+                                                            : -1;
+        const bool save = wsl >= 0;
         // the CTA's tiles: one contiguous block (the NUFFT runs' spins are sorted, so the block covers few cells)
         const int tpc = (n_tiles + gridDim.x - 1) / gridDim.x;
         const int t_end = min(n_tiles, (blockIdx.x + 1) * tpc);
@@ -239,7 +245,7 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                 ly = a.state[4 * n + j];
                 lz = a.state[5 * n + j];
                 if (save) {
-                    float* ws = a.wstates + (size_t)(i / a.wstate_stride) * 6 * n;
+                    float* ws = a.wstates + (size_t)wsl * 6 * n;
                     ws[j] = mx, ws[n + j] = my, ws[2 * n + j] = mz;
                     ws[3 * n + j] = lx, ws[4 * n + j] = ly, ws[5 * n + j] = lz;
                 }
@@ -582,6 +588,25 @@ extern "C" int bp_forward(const float* spins, const float* sens, int n, int n_co
     const int code = fill_args(a, spins, sens, n, n_coils, segs, seg64, windows, w_begin, w_end, state, raw, wstates,
                                wstate_stride, status);
     if (code != BP_OK || w_end == w_begin) return code;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch ((n_coils + 7) / 8) {
+        case 1: return launch_forward<1, false>(a, max_ctas, st);
+        case 2: return launch_forward<2, false>(a, max_ctas, st);
+        case 3: return launch_forward<3, false>(a, max_ctas, st);
+        default: return launch_forward<4, false>(a, max_ctas, st);
+    }
+}
+
+extern "C" int bp_forward_saving(const float* spins, const float* sens, int n, int n_coils, const void* segs,
+                                 const double* seg64, const int* windows, int w_begin, int w_end, float* state,
+                                 double* raw, const int* wslot, float* wstates, int max_ctas, int* status,
+                                 void* stream) {
+    if (!wslot || !wstates) return BP_E_ARG;
+    FwdArgs a;
+    const int code = fill_args(a, spins, sens, n, n_coils, segs, seg64, windows, w_begin, w_end, state, raw, wstates,
+                               1, status);
+    if (code != BP_OK || w_end == w_begin) return code;
+    a.wslot = wslot;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch ((n_coils + 7) / 8) {
         case 1: return launch_forward<1, false>(a, max_ctas, st);

@@ -87,6 +87,14 @@ int bp_forward(const float* spins, const float* sens, int n, int n_coils, const 
                const int32_t* windows, int w_begin, int w_end, float* state, double* raw, float* wstates,
                int wstate_stride, int max_ctas, int32_t* status, void* stream);
 
+/* bp_forward that saves the state at chosen window starts (the checkpointed forward of a simulation whose backward
+ * needs no replay, see bp_adjoint_saved): wslot [n_windows] int32, wslot[w] >= 0 the slot of `wstates` ([slots][6][n]
+ * float32) that takes window w's start state, -1 none. Otherwise as bp_forward (no counterpart in the reference,
+ * whose checkpointed forward stores every interval start: engines/gpu/driver.py:658-662). */
+int bp_forward_saving(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
+                      const int32_t* windows, int w_begin, int w_end, float* state, double* raw, const int32_t* wslot,
+                      float* wstates, int max_ctas, int32_t* status, void* stream);
+
 /* Readout runs through a nonuniform FFT (simulate(..., readout="nufft"); replaces the NUFFT readouts of
  * engines/gpu/cuda/kernels.cu.in:91-140 with engines/gpu/driver.py:236-266). A run is L consecutive samples with
  * one free segment's factors (dt, moments, offset), so spin j's samples are z1 q^p, p < L, q = e^(-dt r2)
@@ -230,6 +238,27 @@ int bp_adjoint(const float* spins, const float* sens, int n, int n_coils, const 
                const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates, const float* h,
                int n_adc, float* lam, float* gs, float* gc, float* gseg, int seg_mask, int grid, int32_t* status,
                void* stream);
+
+/* The reverse sweep of bp_adjoint without a replay, for the gradient of the RF waveform alone (seg_mask: BP_SEG_WX,
+ * BP_SEG_WY and BP_SPIN_NONE; no coil, per-spin or offset gradient): its windows of free segments carry lambda alone,
+ * and its windows of RF segments integrate their states backward from the state after them, so the only states it
+ * needs are those after each run of such windows. Replaces the replay (bloch_replay,
+ * engines/gpu/cuda/replay.cu.in:3-33) for sequences whose every adjoint window is one of those two kinds (a
+ * window of RF segments with one dt and offset, no sample and no spoil, or of free segments with one set of factors
+ * spoiling at most in its last segment) and whose spins' relaxation over an RF segment is invertible (T1, T2 above
+ * 0.73 dt).
+ *   wstates [slots][6][n] the saved states (bp_forward_saving)
+ *   wslot   [n_windows + 1] int32: wslot[w] the slot of the state at window w's start (w = n_windows: after the
+ *           last window), -1 where none was saved; a window of RF segments whose next window is not one needs it
+ *   chain   [3][n] float32 in/out: the start state of the first window of [wa, wb) when it was integrated backward
+ *           (read by the next call, for the interval before, as its chain_in state)
+ *   chain_in  1 when window wb was integrated backward by the previous call (chain holds its start state)
+ * The other arguments are bp_adjoint's (gs and gc are not used). status |= 4 when a window needed a state that was
+ * not saved (its results are then invalid). */
+int bp_adjoint_saved(const float* spins, const float* sens, int n, int n_coils, const void* segs, const double* seg64,
+                     const int32_t* windows, int wa, int wb, int seg0, int seg_len, const float* wstates,
+                     const int32_t* wslot, float* chain, int chain_in, const float* h, int n_adc, float* lam,
+                     float* gseg, int seg_mask, int grid, int32_t* status, void* stream);
 
 /* bp_adjoint with the scanner field model (gradients through the concomitant field; replaces the V=1 adjoint of
  * engines/gpu/cuda/adjoint.cu.in:5-121): `ph` as bp_forward_physics's (conc_mode 1 or 2, conc, segq; no bound pool:

@@ -229,6 +229,46 @@ def test_sweep_without_spin_gradients_matches_the_full_sweep(case):
     assert err < 1e-5, err
 
 
+@pytest.mark.parametrize("case", ["adjoint", "head"])
+def test_backward_from_saved_states(case, monkeypatch):
+    """The RF waveform's gradient alone on a sequence whose adjoint windows are all runs of RF segments (one dt and
+    offset, no sample, no spoil) or of free segments takes the backward from saved states: the forward saves the
+    state after every RF run, the sweep integrates each run's windows backward from it (the chain carried across
+    the intervals) and replays nothing. Against the same sweep with a replay of every interval: RF gradient within
+    1e-5 (the chain's states are integrated over a whole pulse instead of one window), the forward's signal and m
+    the same bits (the forward's extra window starts fall after RF segments), and the same bits for any
+    checkpoint_every."""
+    from blochparty_b200 import adjoint
+
+    if case == "adjoint":
+        ph, seq, coils, flips, t1_target = _adjoint_case(16)
+        target = _target(ph, seq, coils, t1_target)
+    else:
+        ph, seq, coils = workloads.gre3d_128_4echo(16)
+        seq = workloads.first_n_trs(seq, 12)
+        target = torch.zeros(coils.shape[1], int(sum(seq.adc)), dtype=torch.complex128)
+    loss = lambda s, m: ((s.to(torch.complex128) - target).abs() ** 2).sum() + m.double().sum()
+    modes = []
+    init = adjoint.Checkpointed.__init__
+
+    def spy(self, *a, **k):
+        init(self, *a, **k)
+        modes.append(None if self.saved is None else self.saved.n_slots)
+
+    monkeypatch.setattr(adjoint.Checkpointed, "__init__", spy)
+    la, a = gpu_gradients(ph, seq, coils, None, loss, ("rf",), checkpoint_every=64)
+    lc, c = gpu_gradients(ph, seq, coils, None, loss, ("rf",), checkpoint_every=32 * 40)
+    monkeypatch.setattr(adjoint.SavedStates, "of", classmethod(lambda cls, flags, awin: None))
+    lb, b = gpu_gradients(ph, seq, coils, None, loss, ("rf",), checkpoint_every=64)
+    print(f"\n{case}: {modes[0]} saved states (one per TR)")
+    assert modes == [seq.meta["n_tr"], seq.meta["n_tr"], None], modes
+    assert la == lb == lc
+    assert torch.equal(a["rf"], c["rf"])
+    err = rel(a["rf"], b["rf"])
+    print(f"{case}: RF gradient from saved states against the replay's {err:.1e}")
+    assert err < 1e-5, err
+
+
 def test_checkpoint_every_must_be_window_multiple():
     ph, seq, coils, _, _ = _adjoint_case(8)
     with pytest.raises(ValueError, match="multiple of 32"):

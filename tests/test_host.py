@@ -1,6 +1,7 @@
 """Host-side checks that need no GPU: the C ABI library loads and exports what the header declares, the native
 window planner, the packing of segments and state, the capability refusals and argument errors of ``simulate``."""
 
+import ctypes
 import re
 from dataclasses import replace
 from pathlib import Path
@@ -297,3 +298,50 @@ def test_checkpoint_choice():
     k = -(-11_829_248 // every)
     states = -(-k // outer) + outer + every // 32 + 1
     assert states * 24 * 8_388_608 < 80 << 30
+
+
+def test_saved_states_plan():
+    """The backward from saved states: on the 4-echo head sequence every adjoint window is a run of RF or of free
+    segments, one state is saved per TR (after its slab pulse, at the first segment that is not RF), and the
+    forward's windows start there too; a window that mixes RF and free segments leaves it to the replay."""
+    from blochparty_b200 import adjoint, workloads
+
+    _, seq, _ = workloads.gre3d_128_4echo(16)
+    seq = workloads.first_n_trs(seq, 5)
+    flags = engine.pack_segments(seq.dt, seq.rf, seq.grad, None, seq.adc_phase, list(seq.is_rf), list(seq.adc),
+                                 list(seq.spoil), "cpu")[3]
+    S, w = len(flags), _lib.BP_ADJ_WIN
+    br = np.zeros(S, dtype=np.uint8)
+    br[::64] = 1
+    awin = engine.plan_windows(flags, w, seg_max=w, breaks=br | adjoint.run_breaks(flags))
+    sv = adjoint.SavedStates.of(flags, awin)
+    assert sv is not None and sv.n_slots == 5 and not sv.final
+    rf = (flags & engine.RF) != 0
+    pulse_ends = np.flatnonzero(rf[:-1] & ~rf[1:]) + 1
+    assert np.array_equal(sv.points, pulse_ends)
+    assert np.array_equal(np.flatnonzero(sv.slot >= 0), np.searchsorted(awin[:, 0], pulse_ends))
+    assert (sv.rf == (np.add.reduceat(rf.astype(int), awin[:, 0]) > 0)).all()
+    # a sample at the end of an RF segment: that window needs its states recomputed (no saved plan)
+    mixed = flags.copy()
+    mixed[int(np.flatnonzero(rf)[3])] |= engine.ADC
+    assert adjoint.SavedStates.of(mixed, awin) is None
+    # a sequence ending in an RF run saves the final state as its last slot
+    sub = flags[: pulse_ends[1] - 5]
+    sv2 = adjoint.SavedStates.of(sub, engine.plan_windows(sub, w, seg_max=w, breaks=adjoint.run_breaks(sub)))
+    assert sv2 is not None and sv2.final and sv2.n_slots == 2 and list(sv2.points) == [pulse_ends[0]]
+
+
+def test_saved_entry_points_check_their_arguments():
+    """bp_forward_saving and bp_adjoint_saved refuse a missing slot map, and the saved sweep refuses any gradient
+    but the RF waveform's (argument checks only: no GPU call)."""
+    lib = _lib.lib()
+    one = ctypes.c_void_p(16)
+    assert lib.bp_forward_saving(one, one, 4, 1, one, one, one, 0, 1, one, None, None, one, 0, one, None) \
+        == _lib.BP_E_ARG
+    args = lambda mask, wslot, chain: (one, one, 4, 1, one, one, one, 0, 1, 0, 32, one, wslot, chain, 0, None, 0,
+                                       one, None, mask, 1, one, None)
+    rf = _lib.BP_SEG_WX | _lib.BP_SEG_WY | _lib.BP_SPIN_NONE
+    assert lib.bp_adjoint_saved(*args(rf, None, one)) == _lib.BP_E_ARG
+    assert lib.bp_adjoint_saved(*args(rf, one, None)) == _lib.BP_E_ARG
+    assert lib.bp_adjoint_saved(*args(rf | _lib.BP_SEG_DT, one, one)) == _lib.BP_E_ARG
+    assert lib.bp_adjoint_saved(*args(_lib.BP_SEG_WX | _lib.BP_SEG_WY, one, one)) == _lib.BP_E_ARG
