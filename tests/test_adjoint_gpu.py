@@ -207,10 +207,12 @@ def test_sweep_without_offset_gradients_matches_the_full_sweep():
 def test_sweep_without_spin_gradients_matches_the_full_sweep(case):
     """Asking for the RF waveform alone takes the sweep variant without per-spin gradients: its windows of free
     segments carry lambda back without recomputing states, and its windows of RF segments integrate the states
-    backward from the state after the window instead of recomputing them forward. Its RF gradients are the full
-    sweep's within 1e-5 (largest error over the largest value: the two sweeps' float32 states differ by their
-    roundings), on the 2D flip-train case and on the 4-echo head workload at 16^3 with its readout runs; and the
-    variant's own gradients are the same bits for every checkpoint interval."""
+    backward from the state after them instead of recomputing them forward (on these sequences from the states the
+    forward saved after each RF run: the whole slab pulse, 200 steps, is integrated backward). Its RF gradients are
+    the full sweep's within 3e-5 (largest error over the largest value: the two sweeps' float32 states differ by
+    their roundings, which accumulate over a pulse integrated backward; 3.7e-6 with one 32-step window at a time),
+    on the 2D flip-train case and on the 4-echo head workload at 16^3 with its readout runs; and the variant's own
+    gradients are the same bits for every checkpoint interval."""
     if case == "adjoint":
         ph, seq, coils, flips, t1_target = _adjoint_case(16)
         target = _target(ph, seq, coils, t1_target)
@@ -226,7 +228,7 @@ def test_sweep_without_spin_gradients_matches_the_full_sweep(case):
     assert torch.equal(a["rf"], c["rf"])
     err = rel(a["rf"], b["rf"])
     print(f"\n{case}: RF gradient without per-spin gradients against the full sweep {err:.1e}")
-    assert err < 1e-5, err
+    assert err < 3e-5, err
 
 
 @pytest.mark.parametrize("case", ["adjoint", "head"])
@@ -235,8 +237,8 @@ def test_backward_from_saved_states(case, monkeypatch):
     offset, no sample, no spoil) or of free segments takes the backward from saved states: the forward saves the
     state after every RF run, the sweep integrates each run's windows backward from it (the chain carried across
     the intervals) and replays nothing. Against the same sweep with a replay of every interval: RF gradient within
-    1e-5 (the chain's states are integrated over a whole pulse instead of one window), the forward's signal and m
-    the same bits (the forward's extra window starts fall after RF segments), and the same bits for any
+    3e-5 (the chain's states are integrated over a whole pulse instead of one 32-step window), the forward's signal
+    and m the same bits (the forward's extra window starts fall after RF segments), and the same bits for any
     checkpoint_every."""
     from blochparty_b200 import adjoint
 
@@ -266,7 +268,7 @@ def test_backward_from_saved_states(case, monkeypatch):
     assert torch.equal(a["rf"], c["rf"])
     err = rel(a["rf"], b["rf"])
     print(f"{case}: RF gradient from saved states against the replay's {err:.1e}")
-    assert err < 1e-5, err
+    assert err < 3e-5, err
 
 
 def test_checkpoint_every_must_be_window_multiple():
