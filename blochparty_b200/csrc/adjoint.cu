@@ -380,9 +380,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     static_assert(SG || (!CG && !OG), "coil and offset gradients are per-spin gradients");
     extern __shared__ __align__(16) float sm[];
     float* slots = sm;                                              // SG: [ADJ_SLOTS][3][ADJ_THREADS]
-    float* segacc = sm + (SG ? ADJ_SLOTS * 3 * ADJ_THREADS : 0);   // [ADJ_WARPS][BP_ADJ_WIN][N_SG]
-    SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * N_SG);  // [BP_ADJ_WIN] the window's
-    double4* wk64 = reinterpret_cast<double4*>(wrec + BP_ADJ_WIN);                     // records and moments
+    // the warps' segment partials [ADJ_WARPS][BP_ADJ_WIN][N_SG] and the window's records [BP_ADJ_WIN]: one of
+    // each (SG), or two (!SG: window w uses buffer w's parity, so a window's staging never waits for the last
+    // reads of the window before it)
+    constexpr int NBUF = SG ? 1 : 2;
+    constexpr int PERBUF = ADJ_WARPS * BP_ADJ_WIN * N_SG + BP_ADJ_WIN * (int)(sizeof(SegRec) / sizeof(float));
+    float* wbuf0 = sm + (SG ? ADJ_SLOTS * 3 * ADJ_THREADS : 0);  // [NBUF]: segacc, then the records
+    double4* wk64 = reinterpret_cast<double4*>(wbuf0 + NBUF * PERBUF);  // SG: the window's moments
     // !SG: two staging buffers, each the raw records, the moments and the cotangent rows ([BP_ADJ_WIN][8 NCG]) of a
     // window, filled by TMA bulk copies one window ahead; wk64 and hs point into the current one
     SegRec* rawrec = reinterpret_cast<SegRec*>(wk64 + (SG ? BP_ADJ_WIN : 0));      // !SG: [2][BP_ADJ_WIN]
@@ -392,14 +396,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     float2* iacc = reinterpret_cast<float2*>(bars + 2);  // !SG: [ADJ_SACC_MAX] the interval's RF gradient (x, y)
     float* mes = reinterpret_cast<float*>(iacc + ADJ_SACC_MAX);  // !SG: [2][6][ADJ_THREADS] the states after windows
     float2* hs = hsb;
-    __shared__ float wmax[1];  // the window's largest wx0^2 + wy0^2
-    __shared__ unsigned wkind[ADJ_WARPS];  // per warp: a copy timed out (1), not all RF (2), not all free (4)
+    __shared__ float wmax[2];  // the window's largest wx0^2 + wy0^2 (by the window's parity, as wkind)
+    __shared__ unsigned wkind[2][ADJ_WARPS];  // per warp: a copy timed out (1), not all RF (2), not all free (4)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n, n_tiles = (n + ADJ_THREADS - 1) / ADJ_THREADS;
     const int nv = 2 * a.n_coils;
     const bool need_seg = a.gseg != nullptr;
     const bool rf_only = need_seg && (a.seg_mask & BP_SEG_ALL & ~((1 << S_WX) | (1 << S_WY))) == 0;
-    for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) segacc[i] = 0.0f;
+    for (int b = 0; b < NBUF; ++b)
+        for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) wbuf0[b * PERBUF + i] = 0.0f;
     // !SG (only the RF's two components): the interval's sums in shared memory when they fit, in the order the
     // global adds would take (tile by tile), so the bits are the same
     const bool sacc = !SG && need_seg && a.seg_len <= ADJ_SACC_MAX;
@@ -507,20 +512,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             const int buf = seq & 1;
             bool ok = true;
             if constexpr (!SG) {
-                // the next window (this tile's, or the next tile's first) into the other buffer: the barrier that
-                // ended the previous window ended every read of it
-                if (tid == 0) {
-                    if (w > a.wa)
-                        issue(w - 1, buf ^ 1, tile);
-                    else if (tile + (int)gridDim.x < n_tiles)
-                        issue(a.wb - 1, buf ^ 1, tile + (int)gridDim.x);
-                }
                 ok = mbar_wait_bounded(&bars[buf], (seq >> 1) & 1);  // (a copy of a few KB: never this long)
                 ++seq;
                 wk64 = wk64b + buf * BP_ADJ_WIN;
                 hs = hsb + buf * BP_ADJ_WIN * 8 * NCG;
             }
             const int nseg = (good && ok) ? win.y - win.x : 0;  // (nothing is read of a window that is not run)
+            float* segacc = wbuf0 + buf * PERBUF;  // (SG: buf is 0)
+            SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * N_SG);
             // the window's states from the replay (in DRAM for long intervals), loaded first so that their latency
             // overlaps the staging below: SG its start (the recompute's); !SG the state after it (the next window's
             // start, or the interval's end: RF windows integrate backward from it), its start only where a window
@@ -581,17 +580,25 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             if (warp == 0) {  // the window's largest wx0^2 + wy0^2 (non-negative floats order as their bits)
                 const float v = lane < nseg ? fmaf(gw[lane].wx0, gw[lane].wx0, gw[lane].wy0 * gw[lane].wy0) : 0.0f;
                 const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(v));
-                if (lane == 0) *wmax = __uint_as_float(m);
+                if (lane == 0) wmax[buf] = __uint_as_float(m);
             }
             // one barrier for the staging, the copy's bounded wait (any thread gave up) and the window's kind (every
             // thread agrees): each warp's OR of its threads' bits, then the warps' words
             const unsigned bits = (ok ? 0u : 1u) | (rf_ok ? 0u : 2u) | (free_ok ? 0u : 4u);
             const unsigned wbits = __reduce_or_sync(0xffffffffu, bits);
-            if (lane == 0) wkind[warp] = wbits;
+            if (lane == 0) wkind[buf][warp] = wbits;
             __syncthreads();
+            // !SG: the next window (this tile's, or the next tile's first) into the other buffer, now that every
+            // thread is past the barrier: its reads of that buffer (the window before this one's) have ended
+            if (!SG && tid == 0) {
+                if (w > a.wa)
+                    issue(w - 1, buf ^ 1, tile);
+                else if (tile + (int)gridDim.x < n_tiles)
+                    issue(a.wb - 1, buf ^ 1, tile + (int)gridDim.x);
+            }
             unsigned kind_bits = 0;
 #pragma unroll
-            for (int k = 0; k < ADJ_WARPS; ++k) kind_bits |= wkind[k];
+            for (int k = 0; k < ADJ_WARPS; ++k) kind_bits |= wkind[buf][k];
             if (kind_bits & 1u) {  // a staging copy did not land within the bound: report and stop
                 if (tid == 0) {
                     atomicOr(a.status, BP_ERR_TMA_TIMEOUT);
@@ -808,7 +815,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 // every rotation of the window below |w| = 1/4 for every spin of the warp: |w|^2 <= b1^2 max(wx0^2 +
                 // wy0^2) + wz^2 (one offset for the window)
                 const float wz0 = wz_of(wrec[0], win.x);
-                const bool small = fmaf(p.b1 * p.b1, *wmax, wz0 * wz0) < 0.0624f;
+                const bool small = fmaf(p.b1 * p.b1, wmax[buf], wz0 * wz0) < 0.0624f;
                 if (__all_sync(0xffffffffu, small))
                     sweep(KindTag<3>{});
                 else
@@ -818,7 +825,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             } else {
                 sweep(KindTag<0>{});
             }
-            __syncthreads();  // segacc complete; every thread is done reading this window's slots
+            // segacc complete (SG: and every thread is done reading this window's slots and records). Without
+            // per-spin gradients a window whose partials are not summed here (a free window's RF partials are 0)
+            // needs no barrier: its buffers alternate with the next window's
+            const bool summed = need_seg && !(rf_only && all_free);
+            if (SG || summed) __syncthreads();
             if (sacc && !all_free) {  // (!SG: rf_only; a free window's RF partials are 0)
                 for (int i = tid; i < 2 * nseg; i += ADJ_THREADS) {
                     const int sgi = i >> 1, comp = (i & 1) ? S_WY : S_WX;
@@ -837,7 +848,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                     dst[i] += t;
                 }
             }
-            __syncthreads();
+            if (SG) __syncthreads();
         }
         if (no_state && lane == 0) atomicOr(a.status, BP_ERR_NO_STATE);
         if (active) {
@@ -862,8 +873,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             }
         }
     }
-    if (sacc) {  // the interval's RF gradient of this CTA (its rows were cleared at the start; the last window's
-                 // barrier ended every add)
+    if (sacc) {  // the interval's RF gradient of this CTA (its rows were cleared at the start)
+        __syncthreads();  // every add has ended
         float* dst = a.gseg + (size_t)blockIdx.x * a.seg_len * N_SG;
         for (int i = tid; i < a.seg_len; i += ADJ_THREADS) {
             const float2 v = iacc[i];
@@ -888,9 +899,9 @@ static size_t adj_smem() {
     const size_t common = (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) + (size_t)BP_ADJ_WIN * sizeof(SegRec);
     if (SG)  // the slots, segacc, the records and the moments
         return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + common + (size_t)BP_ADJ_WIN * sizeof(double4);
-    // segacc, the records, two staging buffers (raw records, moments, cotangent rows), their two mbarriers and the
-    // interval's RF gradient
-    return common + 2 * (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4) + 8 * NCG * sizeof(float2)) +
+    // two of segacc and of the records, two staging buffers (raw records, moments, cotangent rows, the state
+    // after the window), their two mbarriers and the interval's RF gradient
+    return 2 * common + 2 * (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4) + 8 * NCG * sizeof(float2)) +
            2 * sizeof(uint64_t) + (size_t)ADJ_SACC_MAX * sizeof(float2) + 2 * 6 * ADJ_THREADS * sizeof(float);
 }
 
