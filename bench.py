@@ -390,6 +390,18 @@ def run_reference_gpu(args):
         print(json.dumps(line), flush=True)
 
 
+def saved_states_text(run) -> str:
+    """How the backward of ``run`` (an ``adjoint.Checkpointed``) gets its states."""
+    if run.saved is None:
+        return "interval starts, each interval replayed"
+    blocks = run.blocks()
+    if len(blocks) == 1:
+        return f"saved by the forward after each of the {run.saved.n_slots} RF runs (no replay)"
+    return (f"saved after each of the {run.saved.n_slots} RF runs, {run.layout[1]} at a time: the forward stores the "
+            f"starts of {len(blocks)} blocks of {run.layout[0]} intervals, the backward rebuilds each block's states "
+            "by one forward of the block (no readout) before its sweep")
+
+
 def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
     """Forward + adjoint on the resident inputs: the checkpointed forward and the backward (reverse sweep and
     segment-gradient reduction per interval, from the states the forward saved after every RF run when they fit,
@@ -435,8 +447,9 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
     f_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in times)
     b_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in times)
     ms = f_ms + b_ms
+    blocked = run.saved is not None and len(run.blocks()) > 1
     fwd, bwd = grad_flops_per_spin(pk.flags, pk.n_coils, no_recompute_segments(pk.flags, run.plan.awin),
-                                   replay=run.saved is None)
+                                   replay=run.saved is None or blocked)
     peak = ffma_peak_tflops(dev)
     achieved = n * (fwd + bwd) / (ms * 1e-3) / 1e12
     lf, lb = run.launches(True)
@@ -446,8 +459,7 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
         "grad_wrt": "the RF waveform (flip train), seeded linear loss of the signal",
         "checkpoint_every": every, "intervals": len(run.plan.starts),
         "outer_every": run.outer,  # intervals per outer block (0: two levels); its rebuild forward is not counted
-        "states": (f"saved by the forward after each of the {run.saved.n_slots} RF runs (no replay)"
-                   if run.saved is not None else "interval starts, each interval replayed"),
+        "states": saved_states_text(run),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": None, "peak_source": "live FFMA probe (bp_ffma_peak) on this GPU",
                      "kernel": ("bp_forward_kernel (forward" + (")" if run.saved is not None else ", replay)")

@@ -139,6 +139,31 @@ def rf_relaxation_invertible(pk: engine.Packed) -> bool:
     return dt * r <= 1.35
 
 
+def saved_layout(plan, state_bytes: int, budget_bytes: int):
+    """(intervals per block, slots) of the backward from saved states for ``plan`` (a ``Plan`` with its
+    ``saved``), or None when no layout fits ``budget_bytes`` (``state_bytes`` per stored state): every interval in
+    one block with one slot per saved state when they fit; else blocks of K intervals whose starts the forward
+    stores, the saved states of one block at a time in slots taken modulo the largest count one block's sweep
+    needs (its own runs' and the one after its end: consecutive runs never share a slot), K minimising the states
+    held."""
+    sv, k = plan.saved, len(plan.starts)
+    if sv.n_slots * state_bytes <= budget_bytes:
+        return k, sv.n_slots
+    ends = np.flatnonzero(sv.slot >= 0)  # the windows whose start state is saved, in slot order
+    lo = np.array([a for a, _ in plan.aranges])
+    hi = np.array([b for _, b in plan.aranges])
+    best = None
+    for K in np.unique(np.geomspace(1, k, 256).astype(int)):
+        first = np.arange(0, k, K)
+        last = np.minimum(first + K, k) - 1
+        need = np.searchsorted(ends, hi[last], "right") - np.searchsorted(ends, lo[first], "left")
+        cap = max(int(need.max()), 1)
+        held = len(first) + cap
+        if held * state_bytes <= budget_bytes and (best is None or held < best[0]):
+            best = (held, int(K), cap)
+    return None if best is None else best[1:]
+
+
 class Plan:
     """Windows and intervals of one gradient-carrying simulation. ``saved``: plan the states of the backward
     without a replay (``self.saved``, a ``SavedStates``, or None where it does not apply); the forward's windows
@@ -167,8 +192,7 @@ class Plan:
             if not (self.fwin[at, 0] == self.saved.points).all():
                 raise RuntimeError("the forward's windows do not start at the saved points")
             fslot[at] = np.arange(len(at), dtype=np.int32)
-            self.fslot_dev = torch.from_numpy(fslot).to(device)
-            self.aslot_dev = torch.from_numpy(self.saved.slot).to(device)
+            self.fslot = fslot  # the slot (run number) of each forward window's start state, -1: none
         # window ranges of every interval
         fstart, astart = self.fwin[:, 0], self.awin[:, 0]
         self.franges, self.aranges, self.seg_ranges = [], [], []
@@ -195,16 +219,22 @@ class Checkpointed:
                  budget_bytes: int | None = None):
         self.pk, self.dev = pk, device
         self.phys = phys  # the field model (``PhysGrad``): the forward, replay and sweep take its variants
-        # saved: the caller wants the RF waveform's gradient alone; then, where the sequence's windows allow it and
-        # the states fit half the free memory (or ``budget_bytes``), the forward saves the states after every run
-        # of RF windows and the backward needs no replay (bp_forward_saving, bp_adjoint_saved)
+        # saved: the caller wants the RF waveform's gradient alone; then, where the sequence's windows allow it, the
+        # forward saves the states after every run of RF windows and the backward needs no replay
+        # (bp_forward_saving, bp_adjoint_saved). When those states do not fit half the free memory (or
+        # ``budget_bytes``), the forward stores the state at every start of a block of intervals instead, and the
+        # backward rebuilds each block's saved states by one forward of the block (no readout) before its sweep.
+        # Its intervals are at most 2048 segments (the sweep sums an interval's RF gradient in shared memory).
         want = saved and phys is None and rf_relaxation_invertible(pk)
-        self.plan = plan = Plan(pk, every, device, saved=want)
-        if plan.saved is not None:
+        plan = Plan(pk, min(every, 2048), device, saved=True) if want else None
+        self.layout = None  # saved: (intervals per block, slots)
+        if plan is not None and plan.saved is not None:
             if budget_bytes is None:
                 budget_bytes = torch.cuda.mem_get_info(device)[0] // 2 if torch.cuda.is_available() else 1 << 62
-            if plan.saved.n_slots * 24 * pk.n > budget_bytes:
-                plan.saved = None
+            self.layout = saved_layout(plan, 24 * pk.n, budget_bytes)
+        if self.layout is None:
+            plan = Plan(pk, every, device)
+        self.plan = plan
         self.saved = plan.saved
         k = len(plan.starts)
         self.outer = outer if outer > 1 and k > outer and self.saved is None else 0
@@ -212,37 +242,56 @@ class Checkpointed:
         self.grid = _lib.lib().bp_adjoint_grid(pk.n, pk.n_coils)
         if self.grid < 1:
             raise RuntimeError("bp_adjoint_grid failed")
-        self.ws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, every, plan.max_aw, self.grid,
-                                         self.outer)
+        self.ws = _lib.adjoint_workspace(pk.n, pk.flags.shape[0], pk.n_adc, pk.n_coils, plan.every, plan.max_aw,
+                                         self.grid, self.outer)
         if self.saved is None:
             # interval starts (two levels), or block starts followed by one block's interval starts (three)
             n_states = k if not self.outer else (k + self.outer - 1) // self.outer + self.outer
             self.ckpts = sized(self.ws.checkpoints, (n_states, 6, pk.n), F32, device)
-        else:  # the saved states, by slot (not in the workspace query: their count is the sequence's)
-            self.ckpts = torch.empty(self.saved.n_slots, 6, pk.n, dtype=F32, device=device)
+        else:
+            # the block starts (none with one block), then the saved states by slot: the state after run r of RF
+            # windows in slot r mod `cap` (not in the workspace query: their count is the sequence's)
+            per_block, cap = self.layout
+            self.n_block_states = 0 if per_block >= k else -(-k // per_block)
+            self.ckpts = torch.empty(self.n_block_states + cap, 6, pk.n, dtype=F32, device=device)
+            self.slots = self.ckpts[self.n_block_states:]
+            mod = lambda m: torch.from_numpy(np.where(m >= 0, m % cap, -1).astype(np.int32)).to(device)
+            self.fslot_dev, self.aslot_dev = mod(plan.fslot), mod(plan.saved.slot)
+            self.final_slot = (self.saved.n_slots - 1) % cap
         self.raw = sized(fws.raw, (max(pk.n_adc, 1), 2 * pk.n_coils), F64, device, zero=True)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self._bufs = None
 
     def blocks(self):
-        """[(first interval, end interval)] of the outer blocks (one block of every interval on two levels)."""
+        """[(first interval, end interval)] of the outer blocks (one block of every interval on two levels), or of
+        the blocks of the backward from saved states."""
         k = len(self.plan.starts)
-        step = self.outer or k
+        step = self.layout[0] if self.saved is not None else (self.outer or k)
         return [(b, min(b + step, k)) for b in range(0, k, step)]
+
+    def _fwd_saving(self, state, ka, kb, raw):
+        """The forward over intervals [ka, kb), saving the states after the RF runs in them into their slots."""
+        pk, plan = self.pk, self.plan
+        fa, fb = plan.franges[ka][0], plan.franges[kb - 1][1]
+        code = _lib.lib().bp_forward_saving(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs),
+                                            ptr(pk.seg64), ptr(plan.fwin_dev), fa, fb, ptr(state), ptr(raw),
+                                            ptr(self.fslot_dev), ptr(self.slots), 0, ptr(self.status),
+                                            _lib.stream_ptr())
+        _lib.check(code, "bp_forward_saving")
 
     def forward(self, state: torch.Tensor) -> None:
         """All intervals from ``state`` ([6][n], advanced in place), the raw coil sums into ``raw`` (zeroed first),
         the state at every interval start (at every block start with an outer level) into the checkpoints."""
         pk, plan = self.pk, self.plan
         self.raw.zero_()
-        if self.saved is not None:  # one launch, saving the states the backward needs
-            code = _lib.lib().bp_forward_saving(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs),
-                                                ptr(pk.seg64), ptr(plan.fwin_dev), 0, plan.fwin.shape[0], ptr(state),
-                                                ptr(self.raw if pk.n_adc else None), ptr(plan.fslot_dev),
-                                                ptr(self.ckpts), 0, ptr(self.status), _lib.stream_ptr())
-            _lib.check(code, "bp_forward_saving")
+        if self.saved is not None:  # one launch per block, saving the states the backward needs (slots mod cap:
+            # the last block's are there at the end)
+            for bi, (ka, kb) in enumerate(self.blocks()):
+                if self.n_block_states:
+                    self.ckpts[bi].copy_(state)
+                self._fwd_saving(state, ka, kb, self.raw if pk.n_adc else None)
             if self.saved.final:
-                self.ckpts[-1].copy_(state)
+                self.slots[self.final_slot].copy_(state)
             return
         for k, (fa, fb) in enumerate(plan.franges):
             if not self.outer:
@@ -274,8 +323,10 @@ class Checkpointed:
             if self.saved is None:
                 self._bufs["wstates"] = sized(ws.wstates, (plan.max_aw + 1, 6, pk.n), F32, dev)
                 self._bufs["state"] = sized(ws.replay_state, (6, pk.n), F32, dev)
-            else:  # the chain's state between intervals
+            else:  # the chain's state between intervals, the rebuild's state
                 self._bufs["chain"] = torch.zeros(3, pk.n, dtype=F32, device=dev)
+                if self.n_block_states:
+                    self._bufs["state"] = sized(ws.replay_state, (6, pk.n), F32, dev)
         b = self._bufs
         if need_seg and "gseg" not in b:
             b["gseg"] = sized(ws.gseg, (self.grid, plan.max_len, 8), F32, dev)
@@ -299,7 +350,7 @@ class Checkpointed:
         if self.phys is not None and self.phys.gconc is not None:
             self.phys.gconc.zero_()
         if self.saved is not None:
-            self._saved_backward(h, lam, gseg if need_seg else None, seg, seg_mask, want_gc, b["chain"])
+            self._saved_backward(h, lam, gseg if need_seg else None, seg, seg_mask, want_gc, b["chain"], state)
             return gs, gc, seg
         n_blocks = len(self.blocks())
         for bi, (ka, kb) in reversed(list(enumerate(self.blocks()))):
@@ -339,30 +390,39 @@ class Checkpointed:
         if need_seg:
             _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
 
-    def _saved_backward(self, h, lam, gseg, seg, seg_mask, want_gc, chain):
-        """The backward without a replay: per interval in reverse, the sweep from the saved states, carrying the
-        chain of RF windows integrated backward across the intervals, and the segment reduction."""
+    def _saved_backward(self, h, lam, gseg, seg, seg_mask, want_gc, chain, state):
+        """The backward without a replay: per block in reverse, its saved states (rebuilt by one forward of the
+        block from its start, except the last block's, which the forward left), then per interval in reverse the
+        sweep from the saved states, carrying the chain of RF windows integrated backward across the intervals,
+        and the segment reduction."""
         pk, plan, sv = self.pk, self.plan, self.saved
         lib, stream, W = _lib.lib(), _lib.stream_ptr(), plan.awin.shape[0]
         if want_gc or not rf_only(seg_mask):
             raise ValueError("the backward from saved states forms the RF waveform's gradient alone")
-        for k in reversed(range(len(plan.starts))):
-            aa, ab = plan.aranges[k]
-            s0, s1 = plan.seg_ranges[k]
-            chain_in = int(ab < W and bool(sv.rf[ab]))
-            code = lib.bp_adjoint_saved(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs), ptr(pk.seg64),
-                                        ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(self.ckpts), ptr(plan.aslot_dev),
-                                        ptr(chain), chain_in, ptr(h), pk.n_adc, ptr(lam), ptr(gseg), seg_mask,
-                                        self.grid, ptr(self.status), stream)
-            _lib.check(code, "bp_adjoint_saved")
-            if gseg is not None:
-                _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream), "bp_seg_reduce")
+        blocks = self.blocks()
+        for bi, (ka, kb) in reversed(list(enumerate(blocks))):
+            if bi + 1 < len(blocks):
+                state.copy_(self.ckpts[bi])
+                self._fwd_saving(state, ka, kb, None)
+            for k in reversed(range(ka, kb)):
+                aa, ab = plan.aranges[k]
+                s0, s1 = plan.seg_ranges[k]
+                chain_in = int(ab < W and bool(sv.rf[ab]))
+                code = lib.bp_adjoint_saved(ptr(pk.spins), ptr(pk.sens), pk.n, pk.n_coils, ptr(pk.segs),
+                                            ptr(pk.seg64), ptr(plan.awin_dev), aa, ab, s0, s1 - s0, ptr(self.slots),
+                                            ptr(self.aslot_dev), ptr(chain), chain_in, ptr(h), pk.n_adc, ptr(lam),
+                                            ptr(gseg), seg_mask, self.grid, ptr(self.status), stream)
+                _lib.check(code, "bp_adjoint_saved")
+                if gseg is not None:
+                    _lib.check(lib.bp_seg_reduce(ptr(gseg), self.grid, s1 - s0, s0, ptr(seg), stream),
+                               "bp_seg_reduce")
 
     def launches(self, need_seg: bool) -> tuple[int, int]:
         """(forward, backward) kernel launches of one call each."""
         k = len(self.plan.starts)
         if self.saved is not None:
-            return 1, k * (2 if need_seg else 1)
+            nb = len(self.blocks())
+            return nb, nb - 1 + k * (2 if need_seg else 1)
         rebuild = sum(kb - ka - 1 for ka, kb in self.blocks()) if self.outer else 0
         return k, k * (3 if need_seg else 2) + rebuild
 

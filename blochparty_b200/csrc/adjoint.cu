@@ -380,11 +380,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     static_assert(SG || (!CG && !OG), "coil and offset gradients are per-spin gradients");
     extern __shared__ __align__(16) float sm[];
     float* slots = sm;                                              // SG: [ADJ_SLOTS][3][ADJ_THREADS]
-    // the warps' segment partials [ADJ_WARPS][BP_ADJ_WIN][N_SG] and the window's records [BP_ADJ_WIN]: one of
+    // the warps' segment partials [ADJ_WARPS][BP_ADJ_WIN][SGW] and the window's records [BP_ADJ_WIN]: one of
     // each (SG), or two (!SG: window w uses buffer w's parity, so a window's staging never waits for the last
-    // reads of the window before it)
-    constexpr int NBUF = SG ? 1 : 2;
-    constexpr int PERBUF = ADJ_WARPS * BP_ADJ_WIN * N_SG + BP_ADJ_WIN * (int)(sizeof(SegRec) / sizeof(float));
+    // reads of the window before it). !SG forms the RF's two components alone: SGW = 2 (S_WX, S_WY)
+    constexpr int NBUF = SG ? 1 : 2, SGW = SG ? N_SG : 2;
+    constexpr int PERBUF = ADJ_WARPS * BP_ADJ_WIN * SGW + BP_ADJ_WIN * (int)(sizeof(SegRec) / sizeof(float));
     float* wbuf0 = sm + (SG ? ADJ_SLOTS * 3 * ADJ_THREADS : 0);  // [NBUF]: segacc, then the records
     double4* wk64 = reinterpret_cast<double4*>(wbuf0 + NBUF * PERBUF);  // SG: the window's moments
     // !SG: two staging buffers, each the raw records, the moments and the cotangent rows ([BP_ADJ_WIN][8 NCG]) of a
@@ -395,7 +395,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     uint64_t* bars = reinterpret_cast<uint64_t*>(hsb + 2 * BP_ADJ_WIN * 8 * NCG);  // !SG: [2]
     float2* iacc = reinterpret_cast<float2*>(bars + 2);  // !SG: [ADJ_SACC_MAX] the interval's RF gradient (x, y)
     float* mes = reinterpret_cast<float*>(iacc + ADJ_SACC_MAX);  // !SG: [2][6][ADJ_THREADS] the states after windows
+    // !SG: the cotangent rows expanded for paired FMAs, (h_re, h_im, h_im, -h_re) per coil: [2][BP_ADJ_WIN][8 NCG]
+    float4* hs4b = reinterpret_cast<float4*>(mes + 2 * 6 * ADJ_THREADS);
     float2* hs = hsb;
+    float4* hs4 = hs4b;
     __shared__ float wmax[2];  // the window's largest wx0^2 + wy0^2 (by the window's parity, as wkind)
     __shared__ unsigned wkind[2][ADJ_WARPS];  // per warp: a copy timed out (1), not all RF (2), not all free (4)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -404,7 +407,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
     const bool need_seg = a.gseg != nullptr;
     const bool rf_only = need_seg && (a.seg_mask & BP_SEG_ALL & ~((1 << S_WX) | (1 << S_WY))) == 0;
     for (int b = 0; b < NBUF; ++b)
-        for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * N_SG; i += ADJ_THREADS) wbuf0[b * PERBUF + i] = 0.0f;
+        for (int i = tid; i < ADJ_WARPS * BP_ADJ_WIN * SGW; i += ADJ_THREADS) wbuf0[b * PERBUF + i] = 0.0f;
     // !SG (only the RF's two components): the interval's sums in shared memory when they fit, in the order the
     // global adds would take (tile by tile), so the bits are the same
     const bool sacc = !SG && need_seg && a.seg_len <= ADJ_SACC_MAX;
@@ -494,15 +497,20 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
 #pragma unroll
         for (int k = 0; k < N_GS; ++k) g[k] = (SG && active) ? a.gs[k * n + j] : 0.0f;
         const bool want_gc = CG && active;
-        float gcr[CG ? 8 * NCG : 1], gci[CG ? 8 * NCG : 1], sr[8 * NCG], si[8 * NCG];
+        // the spin's coil sensitivities: SG as two arrays, !SG as (re, im) pairs (the operands of paired FMAs)
+        float gcr[CG ? 8 * NCG : 1], gci[CG ? 8 * NCG : 1], sr[SG ? 8 * NCG : 1], si[SG ? 8 * NCG : 1];
+        float2 sp[SG ? 1 : 8 * NCG];
 #pragma unroll
         for (int c = 0; c < 8 * NCG; ++c) {
             if (CG) {
                 gcr[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c) * n + j] : 0.0f;
                 gci[c] = (want_gc && c < a.n_coils) ? a.gc[(2 * c + 1) * n + j] : 0.0f;
             }
-            sr[c] = active ? a.sens[(2 * c) * n + j] : 0.0f;
-            si[c] = active ? a.sens[(2 * c + 1) * n + j] : 0.0f;
+            const float re = active ? a.sens[(2 * c) * n + j] : 0.0f, im = active ? a.sens[(2 * c + 1) * n + j] : 0.0f;
+            if constexpr (SG)
+                sr[c] = re, si[c] = im;
+            else
+                sp[c] = make_float2(re, im);
         }
         for (int w = a.wb - 1; w >= a.wa; --w) {
             const int4 win = a.windows[w];
@@ -516,10 +524,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                 ++seq;
                 wk64 = wk64b + buf * BP_ADJ_WIN;
                 hs = hsb + buf * BP_ADJ_WIN * 8 * NCG;
+                hs4 = hs4b + buf * BP_ADJ_WIN * 8 * NCG;
             }
             const int nseg = (good && ok) ? win.y - win.x : 0;  // (nothing is read of a window that is not run)
             float* segacc = wbuf0 + buf * PERBUF;  // (SG: buf is 0)
-            SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * N_SG);
+            SegRec* wrec = reinterpret_cast<SegRec*>(segacc + ADJ_WARPS * BP_ADJ_WIN * SGW);
             // the window's states from the replay (in DRAM for long intervals), loaded first so that their latency
             // overlaps the staging below: SG its start (the recompute's); !SG the state after it (the next window's
             // start, or the interval's end: RF windows integrate backward from it), its start only where a window
@@ -559,11 +568,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
             if (SG)
                 for (int i = tid; i < nseg * 4; i += ADJ_THREADS)
                     reinterpret_cast<double*>(wk64)[i] = reinterpret_cast<const double*>(a.seg64 + win.x)[i];
-            if (!SG && a.h != nullptr && !h_tma && nseg > 0) {  // cotangent rows, zero-padded to 8 NCG coils
+            if (!SG && a.h != nullptr && nseg > 0) {  // cotangent rows, expanded, zero-padded to 8 NCG coils
                 for (int i = tid; i < win.w * 8 * NCG; i += ADJ_THREADS) {
                     const int r = i / (8 * NCG), c = i - r * (8 * NCG);
-                    hs[i] = c < a.n_coils ? reinterpret_cast<const float2*>(a.h + (size_t)(win.z + r) * nv)[c]
-                                          : make_float2(0.0f, 0.0f);
+                    const float2 v = h_tma ? hs[i]  // (staged by TMA)
+                                     : c < a.n_coils
+                                         ? reinterpret_cast<const float2*>(a.h + (size_t)(win.z + r) * nv)[c]
+                                         : make_float2(0.0f, 0.0f);
+                    hs4[i] = make_float4(v.x, v.y, v.y, -v.x);
                 }
             }
             // the window's kind (the same for the whole CTA): every segment RF with the dt and offset of the first,
@@ -620,13 +632,14 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                     float t = (up ? v1 : v0) + __shfl_xor_sync(0xffffffffu, up ? v0 : v1, 16);
 #pragma unroll
                     for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-                    if ((lane & 15) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + (up ? S_WY : S_WX)] = t;
-                } else if (need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
+                    const int col = SG ? (up ? S_WY : S_WX) : (up ? 1 : 0);
+                    if ((lane & 15) == 0) segacc[(warp * BP_ADJ_WIN + s) * SGW + col] = t;
+                } else if (SG && need_seg) {  // the warp's sums of the N_SG (= 8) values, one per group of four lanes
                     float v[N_SG];
 #pragma unroll
                     for (int k = 0; k < N_SG; ++k) v[k] = sg.v[k];
                     const float t = warp_reduce_scatter8(v, lane);
-                    if ((lane & 3) == 0) segacc[(warp * BP_ADJ_WIN + s) * N_SG + ((lane >> 2) & 7)] = t;
+                    if ((lane & 3) == 0) segacc[(warp * BP_ADJ_WIN + s) * SGW + ((lane >> 2) & 7)] = t;
                 }
             };
             auto sweep = [&](auto kind_tag) {
@@ -744,12 +757,21 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                     const float ox = outx, oy = outy, oz = outz;
                     if (!URF && (f & BP_ADC) && a.h != nullptr) {
                         --row;
-                        float2 hrow[8 * NCG];
-                        if (!SG) {  // the staged row (zero-padded coils)
-                            const float2* hr = hs + (row - win.z) * 8 * NCG;
+                        if constexpr (!SG) {
+                            // the staged row (zero-padded coils) by paired FMAs: u = sum (h_re, h_im) (s_re, s_im),
+                            // v = sum (h_im, -h_re) (s_re, s_im); dL/dm_x = u.x + u.y, dL/dm_y = v.x + v.y
+                            const float4* hr = hs4 + (row - win.z) * 8 * NCG;
+                            float2 u = make_float2(0.0f, 0.0f), v = make_float2(0.0f, 0.0f);
 #pragma unroll
-                            for (int c = 0; c < 8 * NCG; ++c) hrow[c] = hr[c];
-                        } else if (KIND == 2) {
+                            for (int c = 0; c < 8 * NCG; ++c) {
+                                const float4 h4 = hr[c];
+                                u = __ffma2_rn(make_float2(h4.x, h4.y), sp[c], u);
+                                v = __ffma2_rn(make_float2(h4.z, h4.w), sp[c], v);
+                            }
+                            lx += u.x + u.y, ly += v.x + v.y;
+                        } else {
+                        float2 hrow[8 * NCG];
+                        if (KIND == 2) {
 #pragma unroll
                             for (int c = 0; c < 8 * NCG; ++c) hrow[c] = hnext[c];
                             if (row > win.z) {
@@ -767,7 +789,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                         float dx = 0.0f, dy = 0.0f;
 #pragma unroll
                         for (int c = 0; c < 8 * NCG; ++c) {
-                            if (!SG || c < a.n_coils) {  // (!SG: padded coils are zero rows of hs and of sens)
+                            if (c < a.n_coils) {
                                 const float2 hc = hrow[c];
                                 const float h0 = hc.x, h1 = hc.y;
                                 dx = fmaf(h0, sr[c], fmaf(h1, si[c], dx));
@@ -779,6 +801,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                             }
                         }
                         lx += dx, ly += dy;
+                        }
                     }
                     // the segment's input state: slot s, spoiled by segment s-1 if it spoils
                     float x0 = 0.f, y0 = 0.f, z0 = 0.f;
@@ -835,17 +858,21 @@ __global__ void __launch_bounds__(ADJ_THREADS, SG ? (NCG == 1 ? 4 : 3) : (NCG ==
                     const int sgi = i >> 1, comp = (i & 1) ? S_WY : S_WX;
                     float t = 0.0f;
 #pragma unroll
-                    for (int ww = 0; ww < ADJ_WARPS; ++ww) t += segacc[(ww * BP_ADJ_WIN + sgi) * N_SG + comp];
+                    for (int ww = 0; ww < ADJ_WARPS; ++ww)
+                        t += segacc[(ww * BP_ADJ_WIN + sgi) * SGW + (SG ? comp : (i & 1))];
                     float* d = reinterpret_cast<float*>(iacc + (win.x - a.seg0 + sgi)) + (i & 1);
                     *d += t;
                 }
             } else if (need_seg && !(rf_only && all_free)) {
                 float* dst = a.gseg + ((size_t)blockIdx.x * a.seg_len + (win.x - a.seg0)) * N_SG;
-                for (int i = tid; i < nseg * N_SG; i += ADJ_THREADS) {
+                for (int i = tid; i < nseg * SGW; i += ADJ_THREADS) {
                     float t = 0.0f;
 #pragma unroll
-                    for (int ww = 0; ww < ADJ_WARPS; ++ww) t += segacc[ww * BP_ADJ_WIN * N_SG + i];
-                    dst[i] += t;
+                    for (int ww = 0; ww < ADJ_WARPS; ++ww) t += segacc[ww * BP_ADJ_WIN * SGW + i];
+                    if (SG)
+                        dst[i] += t;
+                    else  // (the RF's two components)
+                        dst[(i >> 1) * N_SG + ((i & 1) ? S_WY : S_WX)] += t;
                 }
             }
             if (SG) __syncthreads();
@@ -899,10 +926,13 @@ static size_t adj_smem() {
     const size_t common = (size_t)ADJ_WARPS * BP_ADJ_WIN * N_SG * sizeof(float) + (size_t)BP_ADJ_WIN * sizeof(SegRec);
     if (SG)  // the slots, segacc, the records and the moments
         return (size_t)ADJ_SLOTS * 3 * ADJ_THREADS * sizeof(float) + common + (size_t)BP_ADJ_WIN * sizeof(double4);
-    // two of segacc and of the records, two staging buffers (raw records, moments, cotangent rows, the state
-    // after the window), their two mbarriers and the interval's RF gradient
-    return 2 * common + 2 * (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4) + 8 * NCG * sizeof(float2)) +
-           2 * sizeof(uint64_t) + (size_t)ADJ_SACC_MAX * sizeof(float2) + 2 * 6 * ADJ_THREADS * sizeof(float);
+    // two of segacc (the RF's two components) and of the records, two staging buffers (raw records, moments,
+    // cotangent rows, the state after the window), their two mbarriers, the interval's RF gradient and two of the
+    // expanded cotangent rows
+    const size_t segacc2 = (size_t)ADJ_WARPS * BP_ADJ_WIN * 2 * sizeof(float) + (size_t)BP_ADJ_WIN * sizeof(SegRec);
+    return 2 * segacc2 + 2 * (size_t)BP_ADJ_WIN * (sizeof(SegRec) + sizeof(double4) + 8 * NCG * sizeof(float2)) +
+           2 * sizeof(uint64_t) + (size_t)ADJ_SACC_MAX * sizeof(float2) + 2 * 6 * ADJ_THREADS * sizeof(float) +
+           2 * (size_t)BP_ADJ_WIN * 8 * NCG * sizeof(float4);
 }
 
 // One variant's shared-memory size, set once per device: 0, or -1 on failure.

@@ -345,3 +345,39 @@ def test_saved_entry_points_check_their_arguments():
     assert lib.bp_adjoint_saved(*args(rf, one, None)) == _lib.BP_E_ARG
     assert lib.bp_adjoint_saved(*args(rf | _lib.BP_SEG_DT, one, one)) == _lib.BP_E_ARG
     assert lib.bp_adjoint_saved(*args(_lib.BP_SEG_WX | _lib.BP_SEG_WY, one, one)) == _lib.BP_E_ARG
+
+
+def test_saved_layout_in_blocks():
+    """When the states saved after the RF runs do not fit, blocks of intervals: every block's sweep finds the
+    states it needs (its own runs' and the one after its end) in distinct slots (run number mod the slot count),
+    and the block starts plus the slots fit the budget."""
+    from blochparty_b200 import adjoint, workloads
+
+    _, seq, _ = workloads.gre3d_128_4echo(16)
+    seq = workloads.first_n_trs(seq, 12)
+    flags = engine.pack_segments(seq.dt, seq.rf, seq.grad, None, seq.adc_phase, list(seq.is_rf), list(seq.adc),
+                                 list(seq.spoil), "cpu")[3]
+
+    class P:  # the parts of a Plan that saved_layout reads
+        pass
+
+    S, w, every = len(flags), _lib.BP_ADJ_WIN, 64
+    plan = P()
+    plan.starts = list(range(0, S, every))
+    br = np.zeros(S, dtype=np.uint8)
+    br[plan.starts] = 1
+    plan.awin = engine.plan_windows(flags, w, seg_max=w, breaks=br | adjoint.run_breaks(flags))
+    plan.saved = adjoint.SavedStates.of(flags, plan.awin)
+    a0 = np.searchsorted(plan.awin[:, 0], plan.starts)
+    plan.aranges = list(zip(a0.tolist(), list(a0[1:]) + [len(plan.awin)]))
+    k = len(plan.starts)
+    assert adjoint.saved_layout(plan, 1, 12) == (k, 12)  # all twelve fit
+    K, cap = adjoint.saved_layout(plan, 1, 9)
+    blocks = [(b, min(b + K, k)) for b in range(0, k, K)]
+    assert len(blocks) > 1 and len(blocks) + cap <= 9
+    run_of = np.cumsum(plan.saved.slot >= 0) - 1  # run number of each saved window start
+    for ka, kb in blocks:
+        lo, hi = plan.aranges[ka][0], plan.aranges[kb - 1][1]
+        live = [int(run_of[e]) for e in range(lo, hi + 1) if plan.saved.slot[e] >= 0]
+        assert len({r % cap for r in live}) == len(live), (ka, kb, live, cap)
+    assert adjoint.saved_layout(plan, 1, 2) is None

@@ -7,6 +7,7 @@ import os
 import socket
 from datetime import timedelta
 
+import numpy as np
 import pytest
 import torch
 import torch.distributed as dist
@@ -87,8 +88,24 @@ def _failing_forward(inp):
     return _oracle_forward(inp)
 
 
+def _by_value(x, back=False):
+    """Tensors as numpy arrays (and back): a queue then carries them by value, not as shared memory whose file
+    descriptor the receiver could only open while the sending process still runs."""
+    if isinstance(x, dict):
+        return {k: _by_value(v, back) for k, v in x.items()}
+    if isinstance(x, tuple):
+        return tuple(_by_value(v, back) for v in x)
+    if back and isinstance(x, np.ndarray):
+        return torch.from_numpy(x)
+    if not back and isinstance(x, torch.Tensor):
+        return x.detach().cpu().numpy().copy()
+    return x
+
+
 def _worker(rank, world, port, mode, out):
     os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    put = out.put
+    out = type("Out", (), {"put": staticmethod(lambda item: put(_by_value(item)))})
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     try:
         case, _, _, _ = golden_cases.load("busy")
@@ -135,7 +152,7 @@ def _run(mode, world=2):
     procs = [ctx.Process(target=_worker, args=(r, world, port, mode, out)) for r in range(world)]
     for p in procs:
         p.start()
-    res = [out.get(timeout=120) for _ in range(world)]
+    res = [_by_value(out.get(timeout=120), back=True) for _ in range(world)]
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
