@@ -457,7 +457,7 @@ def measure_fwd_adjoint(args, dev, pk, state0, flush, n, S):
         "metric": "isochromat-steps/s (fwd+adjoint)", "value": n * S / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
         "forward_ms": f_ms, "backward_ms": b_ms, "steps": args.steps, "warmup": args.warmup,
         "grad_wrt": "the RF waveform (flip train), seeded linear loss of the signal",
-        "checkpoint_every": every, "intervals": len(run.plan.starts),
+        "checkpoint_every": run.plan.every, "intervals": len(run.plan.starts),
         "outer_every": run.outer,  # intervals per outer block (0: two levels); its rebuild forward is not counted
         "states": saved_states_text(run),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,

@@ -581,12 +581,13 @@ class _Simulate(torch.autograd.Function):
 
 
 def _check_grad_options(options):
-    if options.get("readout", "fp32") != "fp32":
+    """With gradients, readout "nufft" and pulses "reuse" (forward-only accelerations) take the float32 readout and
+    stepped pulses, as blochparty's GPU engines do (engines/gpu/__init__.py:78-80 hand neither to their gradient
+    path); the split-BF16 readout and the learned surrogate are refused."""
+    if options.get("readout", "fp32") not in ("fp32", "nufft"):
         raise NotImplementedError(f"b200 engine: gradients through readout={options['readout']!r} are not "
                                   "implemented; use the default float32 readout (or torch.no_grad())")
-    if options.get("pulses", "step") == "reuse":
-        raise ValueError("pulses='reuse' is forward only")
-    if options.get("pulses", "step") != "step":
+    if options.get("pulses", "step") not in ("step", "reuse"):
         raise NotImplementedError("b200 engine: gradients through pulses='surrogate' are not implemented; use "
                                   "pulses='step' (or torch.no_grad())")
 

@@ -83,12 +83,13 @@ def simulate(phantom, seq, coils: Tensor | None = None, *, m_init: Tensor | None
 
     coils: (N, C) complex receive sensitivities (default: one uniform coil), C <= 32.
     m_init: (N, 3) starting magnetization (default: equilibrium, Mz = PD).
-    checkpoint_every: with gradients, the adjoint stores the state every this many segments (rounded to window
-        boundaries); default about sqrt(segments).
+    checkpoint_every: with gradients, the adjoint stores the state every this many segments (a multiple of 32);
+        default about sqrt(segments).
     options: ``readout`` "fp32" (default: float32 coil products reduced by warp shuffles), "bf16x3" (the coil
         contraction on the tensor cores in split bfloat16 with float32 accumulation) or "nufft" (readout runs
-        through a nonuniform FFT: forward only, at least a few thousand spins); ``pulses`` "step"
-        (default), "reuse" (every recurring pulse through its exact per-spin map, forward only) or "surrogate"
+        through a nonuniform FFT: at least a few thousand spins; with gradients the float32 readout is taken, as
+        blochparty's GPU engines do); ``pulses`` "step" (default), "reuse" (every recurring pulse through its exact
+        per-spin map; stepped with gradients) or "surrogate"
         (shaped pulses through a trained ``surrogate``), whose ``surrogate_inference`` is "mma" (default: the
         hidden 64 x 64 layers on the tensor cores) or "fp32"; ``max_ctas`` caps the grid.
     """

@@ -2,7 +2,9 @@
 every pulse (within 1e-5 relative L2: the maps are composed and applied in float64, while the stepped pulse
 rounds its per-step rotation factors to float32, so reuse is the closer of the two to float64) and within 1e-5 of
 the float64 oracle fed the engine's float32 spin inputs, on an RF-spoiled 3D GRE with sub-voxel spins, the
-3-slice TSE and the reference-core golden cases; a memory cap that leaves pulses stepped; forward only."""
+3-slice TSE and the reference-core golden cases; a memory cap that leaves pulses stepped; with gradients the pulses are stepped."""
+
+from dataclasses import replace
 
 import pytest
 import torch
@@ -67,9 +69,14 @@ def test_memory_cap_leaves_pulses_stepped():
         assert rel_l2(sig, step) < 1e-5
 
 
-def test_reuse_is_forward_only():
+def test_reuse_with_gradients_steps_the_pulses():
+    """Reuse is a forward-only acceleration: with gradients the pulses are stepped (as blochparty's GPU engines
+    do), so the gradient is the stepped run's bit for bit."""
     ph, seq, coils = workloads.gre3d_64(8)
-    t1 = ph.t1.clone().requires_grad_()
-    ph.t1 = t1
-    with pytest.raises(ValueError, match="forward only"):
-        bpb.simulate(ph, seq, coils, pulses="reuse")
+    grads = []
+    for pulses in ("reuse", "step"):
+        t1 = ph.t1.clone().requires_grad_()
+        r = bpb.simulate(replace(ph, t1=t1), seq, coils, pulses=pulses)
+        (g,) = torch.autograd.grad(r.signal.abs().pow(2).sum(), [t1])
+        grads.append(g)
+    assert torch.equal(grads[0], grads[1])
