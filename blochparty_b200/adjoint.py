@@ -8,6 +8,12 @@ recomputed into shared memory and swept backward) and ``bp_seg_reduce`` (segment
 fixed order, float64). Windows fall on multiples of 32 segments whatever the interval, so the gradients are the
 same bits for every ``checkpoint_every`` and every run.
 
+For the RF waveform's gradient alone, on sequences whose adjoint windows are all runs of RF segments or of free
+segments (every GRE here), the forward saves instead the state after each RF run (``bp_forward_saving``) and the
+backward sweeps every interval from those states with no replay (``bp_adjoint_saved``): its RF windows integrate
+their states backward from the state after the pulse, its free windows carry lambda alone (``SavedStates``,
+``saved_layout``; in blocks, each block's states rebuilt by one forward of the block, when they do not all fit).
+
 Chain rules on the host (float64), from the kernels' raw gradients: r1 = 1/T1 -> dL/dT1 = -dL/dr1 / T1^2; the
 segment record (dt, w_x = -2 pi dt rf_x, w_y, k = g dt, beta = b0_offset dt) -> dL/d(dt, rf, grad, b0_offset);
 the receiver phase: signal = raw exp(-i psi), so dL/dpsi = gr Im(signal) - gi Re(signal) (blochparty
@@ -209,7 +215,8 @@ class Plan:
 
 class Checkpointed:
     """The device side of a simulation with gradients on a packed case: the forward that stores the state at every
-    interval start, and the backward (per interval in reverse: replay, reverse sweep, segment-gradient reduction).
+    interval start, and the backward (per interval in reverse: replay, reverse sweep, segment-gradient reduction);
+    or, with ``saved``, the forward that saves the states after the RF runs and the backward without a replay.
     With ``outer`` > 1 intervals per block, the forward stores the state at every block start only, and the
     backward first re-runs each block's forward (no readout) to store its intervals' starts. Every buffer is sized
     by the C ABI's workspace query (``bp_forward_workspace_bytes``, ``bp_adjoint_workspace_bytes``); the backward's
