@@ -77,11 +77,13 @@ __host__ __device__ constexpr int samp_max() {
 }
 
 // The warp's staged samples (mb: [BP_STAGE][BP_MB_STRIDE] (mx, my) of its 32 spins) contracted with the coil
-// sensitivities of those spins (st: [32][16 NCG], coil c real at 2c, imaginary at 2c + 1) and added to the warp's
-// accumulator rows acc[row0 + s]. Lane l computes sample l & 7, coils 2 (l >> 3) and 2 (l >> 3) + 1 of every coil
-// group: a chain of FMAs over the 32 spins (the coil sum as a small matrix product, no shuffles). Reads are
-// conflict-free: the 8 samples' rows start 33 float2 apart, and every lane of a sample reads the same spin's
-// sensitivities (a broadcast of 4 float4s).
+// sensitivities of those spins (st: [32][16 NCG], coils 2q and 2q + 1 of a group at 4q as (re, re', im, im')) and
+// added to the warp's accumulator rows acc[row0 + s] (coil c real at 2c, imaginary at 2c + 1). Lane l computes
+// sample l & 7, coils 2 (l >> 3) and 2 (l >> 3) + 1 of every coil group, over the 32 spins on paired FMAs (two
+// float32 FMAs per instruction, each rounded as one FMA): a = sum mx (re, re'), b = sum my (im, im'),
+// c = sum mx (im, im'), d = sum my (re, re'), so that the real parts are a - b and the imaginary ones c + d (the
+// coil sum as a small matrix product, no shuffles). Reads are conflict-free: the 8 samples' rows start 33 float2
+// apart, and every lane of a sample reads the same spin's sensitivities (a broadcast of 4 float4s).
 template <int NCG>
 __device__ __forceinline__ void warp_contract(const float2* mb, const float* st, int nslot, float* acc, int row0,
                                               int lane) {
@@ -91,19 +93,21 @@ __device__ __forceinline__ void warp_contract(const float2* mb, const float* st,
     const float2* row = mb + smp * BP_MB_STRIDE;
 #pragma unroll
     for (int g = 0; g < NCG; ++g) {
-        float r0 = 0.f, i0 = 0.f, r1 = 0.f, i1 = 0.f;
+        float2 sa = make_float2(0.f, 0.f), sb = sa, sc = sa, sd = sa;
 #pragma unroll 8
         for (int j = 0; j < 32; ++j) {
             const float2 m = row[j];
-            const float4 a = *reinterpret_cast<const float4*>(st + j * VG + 16 * g + 4 * quarter);  // (r0 i0 r1 i1)
-            r0 = fmaf(m.x, a.x, fmaf(-m.y, a.y, r0));
-            i0 = fmaf(m.x, a.y, fmaf(m.y, a.x, i0));
-            r1 = fmaf(m.x, a.z, fmaf(-m.y, a.w, r1));
-            i1 = fmaf(m.x, a.w, fmaf(m.y, a.z, i1));
+            const float4 s4 = *reinterpret_cast<const float4*>(st + j * VG + 16 * g + 4 * quarter);
+            const float2 re = make_float2(s4.x, s4.y), im = make_float2(s4.z, s4.w);
+            const float2 xx = make_float2(m.x, m.x), yy = make_float2(m.y, m.y);
+            sa = __ffma2_rn(xx, re, sa);
+            sb = __ffma2_rn(yy, im, sb);
+            sc = __ffma2_rn(xx, im, sc);
+            sd = __ffma2_rn(yy, re, sd);
         }
         float4* dst = reinterpret_cast<float4*>(acc + (row0 + smp) * VG + 16 * g + 4 * quarter);
         float4 d = *dst;
-        d.x += r0, d.y += i0, d.z += r1, d.w += i1;
+        d.x += sa.x - sb.x, d.y += sc.x + sd.x, d.z += sa.y - sb.y, d.w += sc.y + sd.y;
         *dst = d;
     }
 }
@@ -202,12 +206,13 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                                                             : -1;
         const bool save = wsl >= 0;
         // the CTA's tiles: one contiguous block (the NUFFT runs' spins are sorted, so the block covers few cells)
-        const int tpc = (n_tiles + gridDim.x - 1) / gridDim.x;
-        const int t_end = min(n_tiles, (blockIdx.x + 1) * tpc);
+        // of floor(n_tiles / grid) or one more, spread evenly: every SM's CTAs hold the same work within a tile
+        const int t_begin = (int)((long long)blockIdx.x * n_tiles / gridDim.x);
+        const int t_end = (int)((long long)(blockIdx.x + 1) * n_tiles / gridDim.x);
         int cbase = 0, chi = 0;  // NUFFT: the cells the accumulator holds, [cbase, chi) so far
-        if (NUF && nrun >= 0 && blockIdx.x * tpc < t_end) cbase = chi = a.nu.tile_cells[blockIdx.x * tpc].x;
+        if (NUF && nrun >= 0 && t_begin < t_end) cbase = chi = a.nu.tile_cells[t_begin].x;
 
-        for (int tile = blockIdx.x * tpc; tile < t_end; ++tile) {
+        for (int tile = t_begin; tile < t_end; ++tile) {
             if (NUF && nrun >= 0) {
                 // the tile's cells must fit the accumulator's rows from cbase: if not, add what it holds to the
                 // grid and restart it at this tile (uniform: every warp of the CTA runs the same tiles)
@@ -250,21 +255,18 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                     ws[3 * n + j] = lx, ws[4 * n + j] = ly, ws[5 * n + j] = lz;
                 }
             }
-            if (readout) {  // this spin's coil sensitivities into the warp's tile (inactive lanes: zeros)
+            if (readout) {  // this spin's coil sensitivities into the warp's tile (inactive lanes: zeros), a pair of
+                            // coils as (re, re', im, im')
 #pragma unroll
                 for (int k = 0; k < VG; k += 4) {
                     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (active) v = make_float4(a.sens[k * n + j], a.sens[(k + 1) * n + j], a.sens[(k + 2) * n + j],
+                    if (active) v = make_float4(a.sens[k * n + j], a.sens[(k + 2) * n + j], a.sens[(k + 1) * n + j],
                                                 a.sens[(k + 3) * n + j]);
                     *reinterpret_cast<float4*>(st + lane * VG + k) = v;
                 }
                 __syncwarp();
             }
             FreeFactors ff{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            // the last readout run's merged factors and their repeat count (-1: none): the runs of one readout
-            // (cut at 32-segment blocks) mostly share both
-            FreeFactors fmc{1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            int fmc_reps = -1;
             RfRelax rr{1.f, 1.f, 0.f, 0.f, 0.f, 0.f};
             float wz = 0.0f;
             int slot = 0, row0 = 0;
@@ -365,7 +367,6 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                     }
                 } else {
                     if (s == 0 || !(f & BP_SAME_FREE)) {
-                        fmc_reps = -1;
                         if constexpr (PHYS)
                             ff = free_factors_phys(q, a.seg64[win.x + s], p, 1, a.ph.conc_mode, ck,
                                                    a.ph.segq + 6 * (size_t)(win.x + s));
@@ -414,11 +415,8 @@ __global__ void __launch_bounds__(BP_THREADS, NCG == 1 ? 5 : 4) bp_forward_kerne
                                 else
                                     free_step(fr, p, mx, my, mz, lx, ly, lz);
                             } else {
-                                if (fmc_reps != e - s - 1) {
-                                    fmc = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
-                                    fmc_reps = e - s - 1;
-                                }
-                                free_step(fmc, p, mx, my, mz, lx, ly, lz);
+                                const FreeFactors fr = free_factors_merged(q, a.seg64[win.x + s], p, e - s - 1);
+                                free_step(fr, p, mx, my, mz, lx, ly, lz);
                             }
                             if (q0[e - 1].flags & BP_SPOIL) mx = my = lx = ly = 0.0f;
                         }
