@@ -18,6 +18,13 @@
 // per-segment gradients are reduced over the warp by shuffles, over the CTA's warps in fixed order in shared
 // memory, and written as one float32 partial per CTA and segment; bp_seg_reduce adds the CTAs' partials in fixed
 // order in float64. No atomics: every run gives the same bits.
+//
+// Without per-spin gradients (the RF waveform's alone) the variant SG = false keeps no state slots: its windows of
+// free segments carry lambda alone, its windows of RF segments integrate their states backward from the state
+// after them (from the replay, or, in bp_adjoint_saved, from the state the forward saved after the pulse, carried
+// from window to window of the pulse in registers), a sample's coil sum runs on paired FMAs over cotangent rows
+// staged by TMA one window ahead, and its per-window shared buffers alternate by the window's parity, so a readout
+// window needs a single barrier.
 #include <cuda_runtime.h>
 
 #include <cstdint>

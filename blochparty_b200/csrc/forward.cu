@@ -7,11 +7,13 @@
 // Work decomposition (persistent, window-major):
 //  * The sequence is cut on the host into windows of consecutive segments (at most BP_SEG_MAX segments and
 //    samp_max(NCG) ADC samples each).
-//  * A CTA of 128 threads owns one contiguous block of spin tiles (128 spins each, one spin per thread). For every window it stages the window's segment records into shared memory with one
-//    TMA bulk copy (double-buffered: window w+1 is in flight while window w runs), then runs each of its tiles
-//    through the window: the tile's state is loaded from HBM, propagated in registers, and stored back.
-//  * ADC samples: each warp stages the (mx, my) of its 32 spins for 16 samples in shared memory, then contracts
-//    them with the spins' coil sensitivities (an FMA chain over the 32 spins per lane: a small matrix product)
+//  * A CTA of 128 threads owns every grid-th spin tile from its own index (128 spins each, one spin per thread;
+//    the NUFFT kernel a contiguous block of tiles). For every window it stages the window's segment records into
+//    shared memory with one TMA bulk copy (double-buffered: window w+1 is in flight while window w runs), then
+//    runs each of its tiles through the window: the tile's state is loaded from HBM, propagated in registers,
+//    and stored back.
+//  * ADC samples: each warp stages the (mx, my) of its 32 spins for 8 samples in shared memory, then contracts
+//    them with the spins' coil sensitivities (paired FMAs over the 32 spins per lane: a small matrix product)
 //    into its own slice of the window accumulator in shared memory, summed over all of the CTA's tiles. At the
 //    window's end the warps' slices are added in fixed order and the CTA's partial is added to the float64 signal
 //    with one float64 atomic per (sample, coil, re/im): the cross-block sum is float64 (float32 partials added in
