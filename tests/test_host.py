@@ -381,3 +381,57 @@ def test_saved_layout_in_blocks():
         live = [int(run_of[e]) for e in range(lo, hi + 1) if plan.saved.slot[e] >= 0]
         assert len({r % cap for r in live}) == len(live), (ka, kb, live, cap)
     assert adjoint.saved_layout(plan, 1, 2) is None
+
+
+@pytest.mark.parametrize("budget", [7, 9, 12, 40])
+def test_saved_slots_protocol_in_blocks(budget):
+    """The host's plan of the backward from saved states, replayed on the host with the slots as a dictionary: the
+    forward writes every run's state into slot run mod cap (the block starts aside), each block but the last is
+    rebuilt before its sweep, and every window of RF segments whose next window is not one reads the slot of the
+    next window's start: it must hold that run's state, for every layout the budget allows (4-echo head sequence,
+    12 TRs, intervals of 64 segments)."""
+    from blochparty_b200 import adjoint, workloads
+
+    _, seq, _ = workloads.gre3d_128_4echo(16)
+    seq = workloads.first_n_trs(seq, 12)
+    flags = engine.pack_segments(seq.dt, seq.rf, seq.grad, None, seq.adc_phase, list(seq.is_rf), list(seq.adc),
+                                 list(seq.spoil), "cpu")[3]
+    S, w, every = len(flags), _lib.BP_ADJ_WIN, 64
+    starts = list(range(0, S, every))
+    br = np.zeros(S, dtype=np.uint8)
+    br[starts] = 1
+    awin = engine.plan_windows(flags, w, seg_max=w, breaks=br | adjoint.run_breaks(flags))
+    sv = adjoint.SavedStates.of(flags, awin)
+
+    class P:
+        pass
+
+    plan = P()
+    plan.starts, plan.awin, plan.saved = starts, awin, sv
+    a0 = np.searchsorted(awin[:, 0], starts)
+    plan.aranges = list(zip(a0.tolist(), list(a0[1:]) + [len(awin)]))
+    K, cap = adjoint.saved_layout(plan, 1, budget)
+    k, W = len(starts), len(awin)
+    run_of = {int(e): r for r, e in enumerate(np.flatnonzero(sv.slot >= 0))}  # window start -> run number
+    slots = {}
+
+    def write_block(ka, kb):  # the forward over intervals [ka, kb) saves the runs whose window starts lie there
+        lo, hi = plan.aranges[ka][0], plan.aranges[kb - 1][1]
+        for e in range(lo, hi):
+            if e in run_of:
+                slots[run_of[e] % cap] = run_of[e]
+
+    blocks = [(b, min(b + K, k)) for b in range(0, k, K)]
+    for ka, kb in blocks:
+        write_block(ka, kb)
+    if sv.final:
+        slots[run_of[W] % cap] = run_of[W]
+    for bi, (ka, kb) in reversed(list(enumerate(blocks))):
+        if bi + 1 < len(blocks):
+            write_block(ka, kb)
+        for kk in reversed(range(ka, kb)):
+            aa, ab = plan.aranges[kk]
+            for win in range(ab - 1, aa - 1, -1):
+                e = win + 1
+                if sv.rf[win] and (e == W or not sv.rf[e]):  # the end of an RF run: its state is read
+                    assert slots.get(run_of[e] % cap) == run_of[e], (budget, K, cap, win)
